@@ -1,0 +1,134 @@
+/* kofm_oracle.h - CPU restatement (FP64) of the reference's D2Q9 + k-omega
+ * time step.  TEST INFRASTRUCTURE ONLY: the tests, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg use it as the checker.  The product path
+ * (komegafoulingmodel_b200) never links or calls it.
+ *
+ * Parity pinning: every LB and k-omega kernel restated here is compared
+ * against the reference's own kernel sources compiled for the CPU
+ * (oracle/_ref, built by oracle/Makefile) and against committed fixtures
+ * generated from them (tests/golden/).  The GMRES restatement follows the
+ * reference host loop GMRESSolver::solve (GMRESSolver.cpp:227-355) and the
+ * kernels of gmresKernels.cl; it is cross-checked against a direct sparse
+ * solve (scipy) because the reference ships no solver fixtures.
+ *
+ * Layout (the reference's): node (i, j) -> gi = i + nxf*j, nxf = XsizeFull;
+ * population q of node gi -> gi + q*nxf*ny (Array.h:2377-2383).
+ * Direction order C,E,W,N,S,NE,SW,SE,NW (Heading.cl:197-205).
+ */
+#ifndef KOFM_ORACLE_H
+#define KOFM_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_cfg {
+    int nx;               /* CHANNEL_LENGTH (nX) */
+    int nxf;              /* CHANNEL_LENGTH_FULL (XsizeFull) */
+    int ny;               /* CHANNEL_HEIGHT (nY) */
+    double tau0;          /* relaxation RATE 1/tau (the reference's "tau0") */
+    double fterm;         /* FTERM_VAL: velocity increment per step (EDM) */
+    double mu;            /* MU_NUMBER: laminar kinematic viscosity */
+    double max_turb_visc; /* MAX_TURB_VISC */
+} orc_cfg;
+
+/* nType bits (Heading.cl:223-251). */
+enum {
+    ORC_M_SOLID = 0x0001, ORC_M_FLUID = 0x0002, ORC_M0_SOLID = 0x0004,
+    ORC_M0_FLUID = 0x0008, ORC_SOLID_BOUNDARY = 0x0010,
+    ORC_SOLID_BOUNDARY0 = 0x0020, ORC_NESW_BOUNDARY0 = 0x0040,
+    ORC_BOUNDARY0 = 0x0080, ORC_E_BOUND = 0x0100, ORC_W_BOUND = 0x0200,
+    ORC_N_BOUND = 0x0400, ORC_S_BOUND = 0x0800, ORC_NE_BOUND = 0x1000,
+    ORC_SW_BOUND = 0x2000, ORC_SE_BOUND = 0x4000, ORC_NW_BOUND = 0x8000,
+    ORC_NESW_BOUNDARY = 0x0F00, ORC_BOUNDARY = 0xFF00
+};
+#define ORC_OPTION_SAVE_MACRO_FIELDS 0x2
+
+/* ---- LB ---------------------------------------------------------------- */
+void orc_feq(double rho, double ux, double uy, double* feq9);
+void orc_collide_push(const orc_cfg* c, const double* FA, double* FB,
+                      const int16_t* map, double* rho, double* ux, double* uy,
+                      double* K, double* O, const double* wallD, double* nut,
+                      double* Sxy, int options, int komega);
+void orc_ibb(const orc_cfg* c, const int32_t* ibb, const double* q, double* FB,
+             int n);
+void orc_macro(const orc_cfg* c, const double* F, const int16_t* map,
+               double* rho, double* ux, double* uy);
+
+/* ---- k-omega assembly --------------------------------------------------- */
+void orc_komega_diffusivities(const orc_cfg* c, const int16_t* map,
+                              const double* K, const double* O,
+                              const double* nut, const double* wallD,
+                              double* Dk, double* Do, double* F1,
+                              double* dkdxy, const double* rho,
+                              const double* dX);
+void orc_komega_coeffs(const orc_cfg* c, const int32_t* ind, const double* K,
+                       const double* O, const double* nut, const double* Dk,
+                       const double* Do, const double* F1, const double* dkdo,
+                       const double* Sxy, const double* rho, const double* ux,
+                       const double* uy, double* kA, double* oA, double* kb,
+                       double* ob, const double* dX, const double* wallD,
+                       const int16_t* map, double dt);
+
+/* ---- CSR pattern + GMRES ------------------------------------------------ */
+/* Returns nnz.  IA has nxf*ny+1 entries, ind has 5*nxf*ny (C,E,W,N,S planes);
+ * JA must hold nnz entries (call once with JA = NULL to size it). */
+int orc_csr_build(const orc_cfg* c, const int16_t* map, int32_t* IA,
+                  int32_t* JA, int32_t* ind);
+/* Fills the diagonal of solid-boundary rows with 1 (GMRESSolver.cpp:1421-1433). */
+void orc_csr_fill_solid_boundary(const orc_cfg* c, const int16_t* map,
+                                 const int32_t* ind, double* A);
+
+typedef struct orc_gmres_stats {
+    int iters;        /* accumulated iteration counter (iterCount) */
+    int restarts;     /* restart cycles entered */
+    int nan;          /* 1 when the residual became NaN (resetTimeFunc path) */
+    double rho0;      /* last residual norm */
+    double norm_rhs;  /* ||b - A x0|| */
+    double prev_err;  /* prevErr estimate */
+} orc_gmres_stats;
+
+/* GMRESSolver::solve.  b is overwritten with b - A x0 (updateRHS); x holds
+ * the initial guess on entry and the solution on exit. */
+void orc_gmres_solve(int n, const int32_t* IA, const int32_t* JA,
+                     const double* A, double* b, double* x, int krylov,
+                     int max_iters, double rel_tol, double abs_tol,
+                     orc_gmres_stats* st);
+
+/* ---- k-omega solve driver (kOmega::Solve) ------------------------------ */
+typedef struct orc_komega_state {
+    int steps_per_lb;          /* stepsPerLB */
+    int time_since_change;     /* timeSinceTimeStepChange */
+    double dt;                 /* timeStep */
+    int max_iters;
+    double rel_tol, abs_tol;
+    orc_gmres_stats last_k, last_o;
+} orc_komega_state;
+
+/* Runs kOmega::Solve on the given fields.  Work buffers: Dk, Do, F1 [n],
+ * dkdo [2n], kA, oA [nnz], kb, ob [n].  CSR arrays from orc_csr_build. */
+void orc_komega_solve(const orc_cfg* c, orc_komega_state* s,
+                      const int16_t* map, const int32_t* IA, const int32_t* JA,
+                      const int32_t* ind, double* K, double* O,
+                      const double* nut, const double* wallD, const double* rho,
+                      const double* ux, const double* uy, const double* Sxy,
+                      const double* dX, double* Dk, double* Do, double* F1,
+                      double* dkdo, double* kA, double* oA, double* kb,
+                      double* ob);
+
+/* ---- geometry ----------------------------------------------------------- */
+/* Straight channel: rows 0 and ny-1 solid, half-way walls at y = 0.5 and
+ * y = ny - 1.5.  Fills nType (with boundary bits), dX [4n] (E,W,N,S link
+ * fractions) and wall distance. */
+void orc_geom_straight(const orc_cfg* c, int16_t* map, double* dX,
+                       double* wallD);
+
+/* ---- reductions ---------------------------------------------------------- */
+double orc_sum(const double* a, int64_t n);
+double orc_min(const double* a, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,185 @@
+// CPU build of the reference's own LB and k-omega kernels (checker only).
+//
+// oracle/Makefile preprocesses source/Kernels/{Heading,lbKernels,kOmegaKernels}.cl
+// of the reference into oracle/_ref/gen/*.inc (vector literals such as
+// "(double2)(a, b)" become "make_double2(a, b)"), and this file includes them
+// inside `struct RefProgram`.  Each extern "C" entry point below runs one
+// reference kernel over the same NDRange the reference host code enqueues:
+//   collide kernels, Calc_Ro_J, the k-omega kernels: XsizeFull x nY work-items
+//     (clVariablesLB.cpp:141-144, kOmega.cpp:119-125);
+//   lbIBB: one work-item per IBB link (clVariablesLB.cpp:841-852).
+// The kernels contain no barriers and no local memory, so a serial/OpenMP loop
+// over (gx, gy) is an exact execution; the push-stream writes every output
+// slot from exactly one work-item, so row-parallel OpenMP is race-free.
+#include "cl_shim.hpp"
+#include <cstdio>
+
+thread_local size_t g_ref_gid[3];
+
+#define __kernel
+#define __global
+#define __local
+#define __constant
+#define constant
+#define new new_
+#undef RAND_MAX
+#undef MAX
+#undef MIN
+
+// Program-build-time defines of the reference, as run-time members.
+#define CHANNEL_LENGTH m_nx
+#define CHANNEL_LENGTH_FULL m_nxf
+#define CHANNEL_HEIGHT m_ny
+#define DIST_SIZE m_dist
+#define NTYPE_TYPE short
+#define tau0 m_tau0
+#define FTERM_VAL m_fterm
+#define MU_NUMBER m_mu
+#define MAX_TURB_VISC m_maxnut
+#define LSC_NN m_lscnn
+#define WALLD_SEARCH_RADIUS m_wallsr
+// Define set used by the reference's default build (ConstDef.h:25 DEBUG_TURBARR
+// -> DEBUG_ARRAYS via kOmega.cpp:662-664; USE_TURB_VEL_BC via
+// clVariablesLB.cpp:868-871 with the default turbVelBCFlag = true).
+#define DEBUG_ARRAYS
+#define OPENCL_VERSION_1_2
+#define USE_TURB_VEL_BC
+#define WORKGROUPSIZE_IBB 256
+// Particle-module defines referenced by helper functions in Heading.cl that
+// the LB/k-omega path never calls.
+#define TR_X_IND_START 0
+#define FULLSIZEX_TR_PADDED 1
+#define NUM_BL_BOT 0
+#define BL_BOT_START 0
+#define BL_TOP_START 0
+#define BL_TOP_STOP 0
+#define BL_BOT_STOP 0
+
+#pragma GCC diagnostic push
+#pragma GCC diagnostic ignored "-Wattributes"
+#pragma GCC diagnostic ignored "-Wunknown-pragmas"
+#pragma GCC diagnostic ignored "-Wunused-variable"
+#pragma GCC diagnostic ignored "-Wunused-but-set-variable"
+#pragma GCC diagnostic ignored "-Wsign-compare"
+
+struct RefProgram {
+    int m_nx, m_nxf, m_ny, m_dist;
+    double m_tau0, m_fterm, m_mu, m_maxnut;
+    int m_lscnn, m_wallsr;
+
+    RefProgram(int nx, int nxf, int ny, double tau, double fterm, double mu,
+               double maxnut, int lscnn, int wallsr)
+        : m_nx(nx), m_nxf(nxf), m_ny(ny), m_dist(nxf * ny), m_tau0(tau),
+          m_fterm(fterm), m_mu(mu), m_maxnut(maxnut), m_lscnn(lscnn),
+          m_wallsr(wallsr) {}
+
+#include "../_ref/gen/Heading.inc"
+#include "../_ref/gen/lbKernels.inc"
+#include "../_ref/gen/kOmegaKernels.inc"
+};
+
+#pragma GCC diagnostic pop
+#undef new
+
+struct RefCfg {
+    int nx, nxf, ny;
+    double tau0, fterm, mu, max_turb_visc;
+};
+
+static RefProgram make_prog(const RefCfg* c) {
+    return RefProgram(c->nx, c->nxf, c->ny, c->tau0, c->fterm, c->mu,
+                      c->max_turb_visc, 0, 50);
+}
+
+// 2-D NDRange XsizeFull x nY, rows in parallel.
+template <class F>
+static void ndrange2d(int gx_size, int gy_size, F&& body) {
+#pragma omp parallel for schedule(static)
+    for (int gy = 0; gy < gy_size; ++gy) {
+        for (int gx = 0; gx < gx_size; ++gx) {
+            g_ref_gid[0] = (size_t)gx;
+            g_ref_gid[1] = (size_t)gy;
+            g_ref_gid[2] = 0;
+            body();
+        }
+    }
+}
+
+extern "C" {
+
+// LB_collision_SRT_Fluid_w_kOmega (lbKernels.cl:345-633), USE_TURB_VEL_BC
+// signature (the two extra arguments are unused by the kernel body).
+int ref_collide_komega(const RefCfg* c, double* rho, double* ux, double* uy,
+                       double* FA, double* FB, short* map, double* wallD,
+                       double* nut, double* K, double* O, double* Sxy,
+                       int options) {
+    RefProgram p = make_prog(c);
+    ndrange2d(c->nxf, c->ny, [&] {
+        p.LB_collision_SRT_Fluid_w_kOmega(rho, ux, uy, FA, FB, map, wallD, nut,
+                                          K, O, Sxy, nullptr, nullptr, options);
+    });
+    return 0;
+}
+
+// LB_collision_SRT_Fluid (lbKernels.cl:175-335).
+int ref_collide_laminar(const RefCfg* c, double* rho, double* ux, double* uy,
+                        double* FA, double* FB, short* map, int options) {
+    RefProgram p = make_prog(c);
+    ndrange2d(c->nxf, c->ny, [&] {
+        p.LB_collision_SRT_Fluid(rho, ux, uy, FA, FB, map, options);
+    });
+    return 0;
+}
+
+// lbIBB (lbKernels.cl:640-668): one work-item per link, run in list order.
+int ref_ibb(const RefCfg* c, int* ibbArr, double* distArr, double* FB, int n) {
+    RefProgram p = make_prog(c);
+    for (int i = 0; i < n; ++i) {
+        g_ref_gid[0] = (size_t)i; g_ref_gid[1] = 0; g_ref_gid[2] = 0;
+        p.lbIBB(ibbArr, distArr, FB, n);
+    }
+    return 0;
+}
+
+// Calc_Ro_J (lbKernels.cl:137-164).  The kernel adds one to get_global_id(1);
+// rows 1..nY-1 are visited here (row nY-1 is solid and returns at once), which
+// keeps every access inside the nX_full x nY arrays.
+int ref_calc_ro_j(const RefCfg* c, double* rho, double* ux, double* uy,
+                  double* F, short* map) {
+    RefProgram p = make_prog(c);
+    ndrange2d(c->nxf, c->ny - 1, [&] { p.Calc_Ro_J(rho, ux, uy, F, map); });
+    return 0;
+}
+
+// Update_kOmega_Diffusivities (kOmegaKernels.cl:7-95).
+int ref_komega_diffusivities(const RefCfg* c, short* map, double* K, double* O,
+                             double* nut, double* wallD, double* Dk, double* Do,
+                             double* F1, double* dkdxy, double* rho,
+                             double* dX, double* dbg) {
+    RefProgram p = make_prog(c);
+    ndrange2d(c->nxf, c->ny, [&] {
+        p.Update_kOmega_Diffusivities(map, K, O, nut, wallD, Dk, Do, F1, dkdxy,
+                                      rho, dX, dbg);
+    });
+    return 0;
+}
+
+// Update_kOmega_Coeffs_Implicit (kOmegaKernels.cl:187-480).
+int ref_komega_coeffs(const RefCfg* c, int* ind, double* K, double* O,
+                      double* nut, double* Dk, double* Do, double* F1,
+                      double* dkdo, double* Sxy, double* rho, double* ux,
+                      double* uy, double* kA, double* oA, double* kb,
+                      double* ob, double* dX, double* wallD, short* map,
+                      double dt, double* dbg) {
+    RefProgram p = make_prog(c);
+    ndrange2d(c->nxf, c->ny, [&] {
+        p.Update_kOmega_Coeffs_Implicit(ind, K, O, nut, Dk, Do, F1, dkdo, Sxy,
+                                        rho, ux, uy, kA, oA, kb, ob, dX, wallD,
+                                        nullptr, nullptr, map, dt, dbg);
+    });
+    return 0;
+}
+
+int ref_abi_version(void) { return 1; }
+
+}  // extern "C"
