@@ -1,0 +1,389 @@
+"""Benchmark of the D2Q9 + k-omega time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--storage fp32|fp16|bf16]
+
+One "step" is one full time step of the reference's Solve_no_TR path over the
+whole lattice: collide-stream with the k-omega eddy viscosity, the fused k/omega
+assembly and the implicit GMRES solves of omega and k.  Default workload:
+komega_straight_16384x1024 (16.7M nodes, synthetic seeded channel).  The
+populations (1.2 GB) and solver vectors exceed the 126 MB L2, so no flush is
+needed between steps.
+
+With N > 1 (launched by torch.distributed.run) every rank advances its own
+replica of the channel; the path has no exchange step ("replicas only"), value
+is the lattice updates of all ranks over the slowest rank's time.
+
+--impl reference times the reference's own CPU code of the path on the host
+cores: its OpenCL kernel sources compiled as C++ (oracle/_ref) for the collide
+and k-omega assembly, with the oracle's C restatement of its GMRES solver, all
+OpenMP-parallel.  Only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D2Q9+k-omega MLUPS & % HBM roofline; FP16-storage vs FP32 at <=1e-3 rel-L2"
+UNIT = "MLUPS"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.lines = gpu, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [l.split(", ") for l in self.lines if l]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def solver_bytes_per_node(stats, K):
+    """Algorithmic bytes per lattice node of one solver launch (both systems):
+    every vector the restarted simpler-GMRES passes must read or write once
+    (FP64 vectors, four FP64 stencil coefficients; diagonal = 1 not stored)."""
+    total = 0
+    for cyc in (stats.omega_restarts, stats.k_restarts):
+        # residual passes: restart 0 reads b' and writes r; later ones apply A to x
+        res = 16 + 56 * cyc
+        per_cycle = 48 + sum(48 + 8 * (k - 1) for k in range(1, K)) \
+            + sum(24 + 8 * k for k in range(1, K))
+        upd = 8 + 8 * (K - 1) + 8  # upper bound: r, basis vectors, x write (x read after cycle 1)
+        total += res + cyc * per_cycle + cyc * upd + max(cyc - 1, 0) * 8 + 16
+    return total
+
+
+LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90}   # k-omega collide, per node
+ASM_BYTES = 122                                     # fused assembly, per node
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from komegafoulingmodel_b200 import _abi, build
+    from komegafoulingmodel_b200 import workloads as W
+    from komegafoulingmodel_b200.lattice import Lattice
+
+    build.build()
+    lib = _abi.load()
+    torch.cuda.set_device(local_rank)
+    storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV}[args.storage]
+    w = W.by_name(args.workload)
+    d = W.descriptor(w, storage=storage)
+    d.device = local_rank
+    L = Lattice(d)
+    W.apply(L, w)
+    stream = torch.cuda.ExternalStream(L.stream, device=local_rank)
+    nodes = w.nodes
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---- warm-up and timed region (inputs resident in HBM) --------------------
+    for _ in range(args.warmup):
+        L.step(1)
+    L.sync()
+    clocks = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        L.step(1)
+    e1.record(stream)
+    L.sync()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    st = L.stats()
+    value = nodes * args.steps * world / (ms * 1e-3) / 1e6
+    launches_per_step = 3 + 0  # collide, assembly, solver (per k-omega sub-step)
+
+    # ---- per-kernel breakdown (same stream, CUDA events) ------------------------
+    nb = max(3, min(args.steps, 10))
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(nb)]
+    passes, bytes_solver = [], []
+    for i in range(nb):
+        ev[i][0].record(stream)
+        L.lb_step(_abi.OPTION_SAVE_MACRO_FIELDS)
+        ev[i][1].record(stream)
+        L.komega_assemble(1.0)
+        ev[i][2].record(stream)
+        L.komega_solve(raise_on_error=False)
+        ev[i][3].record(stream)
+        s = L.stats()
+        passes.append(s.solver_passes)
+        bytes_solver.append(solver_bytes_per_node(s, d.krylov_dim))
+    torch.cuda.synchronize()
+    t_lb = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(nb)) / nb
+    t_as = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(nb)) / nb
+    t_sv = sum(ev[i][2].elapsed_time(ev[i][3]) for i in range(nb)) / nb
+    b_sv = sum(bytes_solver) / nb
+    peak, peak_kind = measured_peaks()
+    kern = {
+        "lb_step_kernel": {"ms": t_lb, "bytes_per_node": LB_BYTES[args.storage],
+                           "gbs": LB_BYTES[args.storage] * nodes / (t_lb * 1e-3) / 1e9},
+        "komega_assemble_kernel": {"ms": t_as, "bytes_per_node": ASM_BYTES,
+                                   "gbs": ASM_BYTES * nodes / (t_as * 1e-3) / 1e9},
+        "gmres_kernel": {"ms": t_sv, "bytes_per_node": b_sv,
+                         "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
+                         "passes": sum(passes) / nb},
+    }
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak,
+            "unit": "GB/s", "frac": kern[dom]["gbs"] / peak, "peak_kind": peak_kind,
+            "traffic": None, "bytes_per_node": kern[dom]["bytes_per_node"]}
+    step_bytes = LB_BYTES[args.storage] + ASM_BYTES + b_sv
+    step_ms = t_lb + t_as + t_sv
+
+    # ---- end to end through the public API with host buffers ---------------------
+    e2e = None
+    if not args.no_e2e:
+        n = w.channel.n
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        hf, hk, ho, hn, hs = pin(w.f), pin(w.k), pin(w.omega), pin(w.nut), pin(w.sxy)
+        hr, hu = torch.empty(n, dtype=torch.float64).pin_memory(), torch.empty(n, dtype=torch.float64).pin_memory()
+        dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))  # noqa: E731
+        out = C.c_double()
+        ctx = L._ctx
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _abi.check("set_state", lib.kofm_set_state(ctx, dp(hf), dp(hk), dp(ho), dp(hn), dp(hs)))
+        for _ in range(args.steps):
+            _abi.check("step", lib.kofm_step(ctx, 1, _abi.OPTION_SAVE_MACRO_FIELDS))
+            _abi.check("reduce", lib.kofm_reduce(ctx, _abi.FIELD_RHO, _abi.OP_SUM, C.byref(out)))
+            _abi.check("reduce", lib.kofm_reduce(ctx, _abi.FIELD_UX, _abi.OP_SUM, C.byref(out)))
+        _abi.check("get_macro", lib.kofm_get_macro(ctx, dp(hr), dp(hu), None))
+        t1 = time.perf_counter()
+        secs = t1 - t0
+        if world > 1:
+            t = torch.tensor([secs], device=f"cuda:{local_rank}")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            secs = float(t.item())
+        h2d = 8 * (9 * n + 3 * n + 3 * n)
+        d2h = 8 * 2 * args.steps + 8 * 2 * n
+        e2e = {"value": nodes * args.steps * world / secs / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "timing": "host wall clock around set_state (pinned host) + K x "
+                         "(kofm_step + 2 kofm_reduce D2H) + kofm_get_macro D2H"}
+    L.close()
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(w, steps=args.cpu_steps, warmup=0)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.storage == "fp32" else "f32", "data": "synthetic",
+            "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
+                       "nodes": nodes, "storage": f"{args.storage} f-w deviation",
+                       "krylov_dim": d.krylov_dim, "rel_tol": d.komega_rel_tol,
+                       "abs_tol": d.komega_abs_tol, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (1.2 GB populations), no flush"},
+            "roofline": roof,
+            "step_roofline": {"bytes_per_node": step_bytes,
+                              "achieved": step_bytes * nodes / (step_ms * 1e-3) / 1e9,
+                              "frac": step_bytes * nodes / (step_ms * 1e-3) / 1e9 / peak},
+            "kernels": kern,
+            "solver": {"omega_iters": st.omega_iters, "k_iters": st.k_iters,
+                       "omega_restarts": st.omega_restarts, "k_restarts": st.k_restarts,
+                       "passes": st.solver_passes},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(w, steps=2, warmup=0):
+    """The reference's CPU code of the path on this host's cores: the OpenCL
+    kernel sources compiled as C++ (oracle/_ref) for collide and assembly plus
+    the C restatement of GMRESSolver::solve; full-lattice steps."""
+    import ctypes as C
+
+    import numpy as np
+
+    from oracle.orc import LIB_REF, Oracle, OracleSim, RefKernels, make_cfg
+
+    orc = Oracle()
+    ch = w.channel
+    cfg = make_cfg(ch.nx, ch.ny, w.tau, w.fterm, w.mu, nxf=ch.nx_full)
+    sim = OracleSim(orc, cfg, ch.ntype, ch.dX, ch.wallD, w.f, w.k, w.omega, w.nut, w.sxy,
+                    komega=w.komega)
+    kind = "port"
+    ref = RefKernels() if os.path.exists(LIB_REF) else None
+    if ref is not None:
+        kind = "reference"
+    n = ch.n
+    dbg = np.zeros(40 * n) if (ref is not None and w.komega) else None
+
+    def one_step():
+        if ref is None:
+            sim.step(1)
+            return
+        cp = C.byref(cfg)
+        if w.komega:
+            ref.L.ref_collide_komega(cp, sim.rho, sim.ux, sim.uy, sim.FA, sim.FB, sim.m,
+                                     sim.wallD, sim.nut, sim.K, sim.O, sim.S, 2)
+        else:
+            ref.L.ref_collide_laminar(cp, sim.rho, sim.ux, sim.uy, sim.FA, sim.FB, sim.m, 2)
+        sim.FA, sim.FB = sim.FB, sim.FA
+        if w.komega:
+            ref.L.ref_komega_diffusivities(cp, sim.m, sim.K, sim.O, sim.nut, sim.wallD, sim.Dk,
+                                           sim.Do, sim.F1, sim.dkdo, sim.rho, sim.dX, dbg)
+            ref.L.ref_komega_coeffs(cp, sim.ind, sim.K, sim.O, sim.nut, sim.Dk, sim.Do, sim.F1,
+                                    sim.dkdo, sim.S, sim.rho, sim.ux, sim.uy, sim.kA, sim.oA,
+                                    sim.kb, sim.ob, sim.dX, sim.wallD, sim.m, 1.0, dbg)
+            from oracle.orc import GmresStats
+            for A, b, x in ((sim.oA, sim.ob, sim.O), (sim.kA, sim.kb, sim.K)):
+                st = GmresStats()
+                orc.L.orc_gmres_solve(n, sim.IA, sim.JA, A, b, x, 10, 1000, 1e-4, 1e-7, C.byref(st))
+
+    for _ in range(warmup):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_step()
+    secs = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0))
+    return {"value": w.nodes * steps / secs / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{steps} full steps of {w.name} ({w.nodes} nodes): reference kernels "
+                      "(oracle/_ref) for collide + k-omega assembly, C restatement of its "
+                      "GMRES(10); OpenMP over rows",
+            "seconds": secs}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from komegafoulingmodel_b200 import workloads as W
+    w = W.by_name(args.workload)
+    # warm-up steps and K timed steps, each a full-lattice step
+    res = cpu_reference_sample(w, steps=args.steps, warmup=args.warmup)
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["seconds"] * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
+                   "nodes": w.nodes, "parallelism": "host cores"},
+        "impl": "reference",
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="komega_straight_16384x1024")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if args.warmup > 1:
+            args.warmup = 1
+        args.steps = min(args.steps, 3)
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,212 @@
+/* kofm.h - C ABI of the B200 D2Q9 + k-omega time step.
+ *
+ * This is the drop-in boundary for the reference's LB/k-omega hot path.  The
+ * reference dispatches that path through positional OpenCL kernel objects
+ * (Kernel / DualKernel, source/Kernels.h:29-727) whose arguments are set in
+ * clVariablesLB::setKernelArgs (clVariablesLB.cpp:790-856),
+ * kOmega::setKernelArgs (kOmega.cpp:573-650) and GMRESSolver::createKernels
+ * (GMRESSolver.cpp:930-1210), and enqueues them from Solve_no_TR
+ * (LBLS.cpp:185-205), clVariablesLB::Solve (clVariablesLB.h:375-441) and
+ * kOmega::Solve (kOmega.cpp:31-73).  Each entry point below replaces one of
+ * those dispatch sites; the citation is beside it.
+ *
+ * Conventions
+ *  - Plain C types only.  Host arrays use the reference's padded FP64 layout
+ *    (Array.h:2377-2383): node (i, j) at i + nx_full*j, population q at
+ *    node + q*nx_full*ny, direction order C,E,W,N,S,NE,SW,SE,NW
+ *    (Kernels/Heading.cl:197-205).  Populations exchanged through
+ *    kofm_set_state / kofm_get_state are the reference's FA buffer
+ *    (pre-collision, post-stream; the content of its lbf.bin checkpoint).
+ *  - The context owns all device memory.  Host pointers are only read or
+ *    written during the call.  The device layout and storage precision are
+ *    private to the library.
+ *  - Every call returns an int status: 0 = ok, negative = error.  Codes
+ *    -100..-123 reuse the reference's error numbers (ConstDef.h:588-611)
+ *    where the meaning maps; -200 and below are new.  No call exits the
+ *    process.
+ *  - One context = one CUDA stream (the reference's LBQUEUE).  Calls on one
+ *    context are not thread-safe; several contexts may coexist.  Work is
+ *    asynchronous until kofm_sync, a kofm_get_* call or kofm_reduce.
+ */
+#ifndef KOFM_H
+#define KOFM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KOFM_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define KOFM_OK 0
+#define KOFM_ERR_BUFFER_ALLOCATION -101   /* ERROR_BUFFER_ALLOCATION */
+#define KOFM_ERR_MEMORY_COPY -103         /* ERROR_MEMORY_COPY */
+#define KOFM_ERR_CALLING_KERNEL -107      /* ERROR_CALLING_KERNEL */
+#define KOFM_ERR_LOADING_PARAMS -110      /* ERROR_LOADING_PARAMS: bad descriptor */
+#define KOFM_ERR_INITIALIZING_KOMEGA -111 /* ERROR_INITIALIZING_KOMEGA */
+#define KOFM_ERR_INITIALIZING_VLS -112    /* ERROR_INITIALIZING_VLS: bad geometry */
+#define KOFM_ERR_INITIALIZING_VLB -120    /* ERROR_INITIALIZING_VLB */
+#define KOFM_ERR_INVALID_ARG -200         /* NULL pointer / out-of-range value */
+#define KOFM_ERR_NO_DEVICE -201           /* no usable sm_100 device */
+#define KOFM_ERR_NOT_CONVERGED -202       /* k-omega solve hit its iteration cap */
+#define KOFM_ERR_NAN -203                 /* NaN residual; dt halving engaged */
+#define KOFM_ERR_TIMEOUT -204             /* a bounded device wait expired */
+#define KOFM_ERR_STATE -205               /* call order: geometry/state not set */
+
+/* ---- options (Kernels/Heading.cl:309-311) -------------------------------- */
+#define KOFM_OPTION_SAVE_MACRO_FIELDS 0x2 /* write rho, ux, uy this step */
+
+/* ---- storage forms of the populations ------------------------------------ */
+#define KOFM_STORE_FP32 0     /* f_i - w_i in FP32, FP64 collide arithmetic */
+#define KOFM_STORE_FP16_DEV 1 /* f_i - w_i in FP16, FP32 collide arithmetic */
+#define KOFM_STORE_BF16_DEV 2 /* f_i - w_i in BF16, FP32 collide arithmetic */
+
+/* ---- fields for kofm_reduce ---------------------------------------------- */
+#define KOFM_FIELD_RHO 0   /* Ro_array   (clVariablesLB.cpp:343-345 sumRo) */
+#define KOFM_FIELD_UX 1    /* Ux_array   (sumUx) */
+#define KOFM_FIELD_UY 2    /* Uy_array   (sumUy) */
+#define KOFM_FIELD_K 3     /* Kappa_array (kOmega.cpp:315-318 sumKappa/minKappa) */
+#define KOFM_FIELD_OMEGA 4 /* Omega_array (sumOmega/minOmega) */
+#define KOFM_FIELD_NUT 5   /* Nut_array */
+#define KOFM_FIELD_WALL_SHEAR 6 /* wall-shear integral (see kofm_reduce) */
+#define KOFM_OP_SUM 0
+#define KOFM_OP_MIN 1
+#define KOFM_OP_MAX 2
+
+typedef struct kofm_ctx kofm_ctx;
+
+/* Run parameters.  Replaces the program-build-time defines that
+ * clVariablesLB::setSourceDefines / kOmega::setSourceDefines /
+ * clProblem::setSourceDefines inject (clVariablesLB.cpp:860-877,
+ * kOmega.cpp:660-680) and the solver settings of
+ * GMRESSolver::CreateSolverWithVarTime (GMRESSolver.cpp:1304-1418). */
+typedef struct kofm_desc {
+    int32_t nx;          /* CHANNEL_LENGTH (nX) */
+    int32_t nx_full;     /* XsizeFull: row pitch of host arrays, >= nx */
+    int32_t ny;          /* CHANNEL_HEIGHT (nY); rows 0 and ny-1 must be solid */
+    int32_t use_komega;  /* kOmegaSolverFlag */
+    double tau;          /* relaxation RATE 1/tau (the reference's "Tau" / tau0) */
+    double fterm;        /* FTERM_VAL: EDM velocity increment per step */
+    double mu;           /* MU_NUMBER: laminar kinematic viscosity */
+    double max_turb_visc;/* MAX_TURB_VISC (ConstDef.h:195, 10.0) */
+    int32_t storage;     /* KOFM_STORE_* */
+    int32_t device;      /* CUDA device ordinal */
+    int32_t komega_max_iters; /* KOMEGA_MAX_ITERS (1000) */
+    int32_t krylov_dim;       /* GMRES_KRYLOV_DIM_SIZE (10); 1..12 */
+    double komega_rel_tol;    /* KOMEGA_MAX_REL_TOL (1e-4) */
+    double komega_abs_tol;    /* KOMEGA_MAX_ABS_TOL (1e-7) */
+    double komega_dt;         /* initial k-omega time step (p.dTlb = 1) */
+} kofm_desc;
+
+/* Per-context counters of the last k-omega update (kOmega::Solve). */
+typedef struct kofm_stats {
+    int32_t omega_iters, k_iters;       /* GMRESSolver::iterCount */
+    int32_t omega_restarts, k_restarts; /* restart cycles entered */
+    int32_t omega_nan, k_nan;           /* NaN residual seen */
+    int32_t steps_per_lb;               /* kOmega::stepsPerLB */
+    int32_t time_since_change;          /* kOmega::timeSinceTimeStepChange */
+    double dt;                          /* kOmega::timeStep */
+    double omega_rel_res, k_rel_res;    /* rho_0 / norm_rhs at exit */
+    int64_t steps;                      /* LB steps taken */
+    int32_t solver_passes;              /* grid sweeps of the last solve */
+    int32_t phase;                      /* 0: populations pre-collision, 1: post */
+} kofm_stats;
+
+int kofm_abi_version(void);
+const char* kofm_error_string(int status);
+
+/* Fills *d with the reference defaults (ConstDef.h: KOMEGA_* tolerances,
+ * GMRES_KRYLOV_DIM_SIZE, MAX_TURB_VISC, dTlb = 1, FP32 storage, device 0). */
+int kofm_desc_default(kofm_desc* d);
+
+/* Allocates device memory for the descriptor's lattice and its solver.
+ * Replaces clVariablesLB::allocateBuffers / kOmega::allocateBuffers /
+ * GMRESSolver::ini + CreateSolver (clVariablesLB.cpp:56-75,
+ * kOmega.cpp:99-108, GMRESSolver.cpp:1225-1259, 1314-1418). */
+int kofm_create(const kofm_desc* d, kofm_ctx** out);
+int kofm_destroy(kofm_ctx* ctx);
+
+/* Geometry: nType flags (Heading.cl:223-251 bits), wall distance WallD
+ * (kOmega.cpp:330-349), link fractions dXArr [4 planes E,W,N,S]
+ * (clVariablesLS.cpp:650-684) and the interpolated bounce-back link list
+ * ibbArr/ibbDistArr (population index + wall fraction q) consumed by lbIBB
+ * (lbKernels.cl:640-668; set at clVariablesLB.cpp:841-852).  wallD and dX4
+ * may be NULL when use_komega = 0; n_ibb may be 0.
+ * Rejects fluid nodes in rows 0 / ny-1 (clVariablesLS.cpp:935-937). */
+int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
+                      const double* dX4, const int32_t* ibb_idx,
+                      const double* ibb_q, int32_t n_ibb);
+
+/* State upload: f = FA (9 planes), k, omega, nut (1 plane each), sxy (3
+ * planes Sxx,Sxy,Syy).  The k-omega arrays may be NULL when use_komega = 0;
+ * nut may be NULL (it is recomputed by the next step).  Replaces the
+ * allocate_buffer_w_copy uploads of ini() and the lbf/lbkappa/lbomega bin
+ * loads (clVariablesLB.cpp:883-902, kOmega.cpp:685-710). */
+int kofm_set_state(kofm_ctx* ctx, const double* f, const double* k,
+                   const double* omega, const double* nut, const double* sxy);
+
+/* State download in the same layout (FA = what saveRestartFiles writes,
+ * clVariablesLB.cpp:752-765).  Any pointer may be NULL. */
+int kofm_get_state(kofm_ctx* ctx, double* f, double* k, double* omega,
+                   double* nut, double* sxy);
+
+/* Macroscopic fields written by the last step with
+ * KOFM_OPTION_SAVE_MACRO_FIELDS (Ro_array, Ux_array, Uy_array).  Any pointer
+ * may be NULL. */
+int kofm_get_macro(kofm_ctx* ctx, double* rho, double* ux, double* uy);
+
+/* One collide + stream + interpolated bounce-back pass:
+ * vlb.collisionKernel.call_kernel + vlb.ibbKernel.call_kernel
+ * (LBLS.cpp:188-190; LB_collision_SRT_Fluid[_w_kOmega], lbIBB). */
+int kofm_lb_step(kofm_ctx* ctx, int32_t options);
+
+/* Builds both implicit k/omega systems for time step dt:
+ * kOmegaUpdateDiffCoeffs + kOmegaUpdateCoeffs (kOmega.cpp:43-44;
+ * Update_kOmega_Diffusivities, Update_kOmega_Coeffs_Implicit). */
+int kofm_komega_assemble(kofm_ctx* ctx, double dt);
+
+/* Solves the assembled systems and updates omega and k:
+ * OmegaGMRES.solve(); KappaGMRES.solve() (kOmega.cpp:68-70;
+ * GMRESSolver::solve, GMRESSolver.cpp:227-355).  Both run in one
+ * device-resident launch.  iters/rel_res receive (omega, k) pairs; either
+ * may be NULL.  Returns KOFM_ERR_NAN if a residual was NaN (the caller's
+ * kOmega::Solve halves dt), KOFM_ERR_NOT_CONVERGED at the iteration cap. */
+int kofm_komega_solve(kofm_ctx* ctx, int32_t* iters, double* rel_res);
+
+/* kOmega::Solve (kOmega.cpp:31-73): adaptive sub-stepping (halve dt on a
+ * NaN residual, double it after 20 calm steps; kOmega.cpp:387-414) around
+ * assemble + solve. */
+int kofm_komega_update(kofm_ctx* ctx);
+
+/* nsteps x Solve_no_TR (LBLS.cpp:185-205): kofm_lb_step with
+ * options | KOFM_OPTION_SAVE_MACRO_FIELDS when k-omega is on, then
+ * kofm_komega_update. */
+int kofm_step(kofm_ctx* ctx, int32_t nsteps, int32_t options);
+
+/* Reducer<double>::reduceSingle (Reducer.h:240-278) over the full padded
+ * array of a field (FP64 accumulation, deterministic order).  For
+ * KOFM_FIELD_WALL_SHEAR and op SUM: sum over fluid nodes with an N or S wall
+ * link of rho*(mu + nu_t)*2*|S_xy| (a diagnostic of this library; the
+ * reference's per-link shear coefficients, trKernelsShear.cl, are not part
+ * of this path). */
+int kofm_reduce(kofm_ctx* ctx, int32_t field, int32_t op, double* out);
+
+int kofm_sync(kofm_ctx* ctx);
+int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);
+
+/* Diagnostic for the bounded device waits: runs the k-omega solver with a
+ * grid barrier that can never complete and the given spin bound (polls of
+ * about 100 ns).  Returns KOFM_ERR_TIMEOUT with the context still usable and
+ * the fields unchanged.  No counterpart in the reference. */
+int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
+
+/* The CUDA stream the context enqueues on (cudaStream_t as void*), for
+ * callers that order their own work against it. */
+void* kofm_stream(kofm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KOFM_H */

@@ -1,0 +1,113 @@
+"""ctypes declarations of the C ABI in include/kofm.h (libkofm.so).
+
+The library is built in-tree for sm_100a (komegafoulingmodel_b200/build.py).
+There is no CPU fallback: if the library or a B200 is missing, the calls
+raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkofm.so")
+
+KOFM_OK = 0
+ERRORS = {
+    -101: "BUFFER_ALLOCATION", -103: "MEMORY_COPY", -107: "CALLING_KERNEL",
+    -110: "LOADING_PARAMS", -111: "INITIALIZING_KOMEGA", -112: "INITIALIZING_VLS",
+    -120: "INITIALIZING_VLB", -200: "INVALID_ARG", -201: "NO_DEVICE",
+    -202: "NOT_CONVERGED", -203: "NAN", -204: "TIMEOUT", -205: "STATE",
+}
+ERR_NOT_CONVERGED = -202
+ERR_NAN = -203
+ERR_TIMEOUT = -204
+
+OPTION_SAVE_MACRO_FIELDS = 0x2
+STORE_FP32, STORE_FP16_DEV, STORE_BF16_DEV = 0, 1, 2
+FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_K, FIELD_OMEGA, FIELD_NUT, FIELD_WALL_SHEAR = range(7)
+OP_SUM, OP_MIN, OP_MAX = 0, 1, 2
+
+
+class KofmDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("nx_full", C.c_int32), ("ny", C.c_int32),
+        ("use_komega", C.c_int32),
+        ("tau", C.c_double), ("fterm", C.c_double), ("mu", C.c_double),
+        ("max_turb_visc", C.c_double),
+        ("storage", C.c_int32), ("device", C.c_int32),
+        ("komega_max_iters", C.c_int32), ("krylov_dim", C.c_int32),
+        ("komega_rel_tol", C.c_double), ("komega_abs_tol", C.c_double),
+        ("komega_dt", C.c_double),
+    ]
+
+
+class KofmStats(C.Structure):
+    _fields_ = [
+        ("omega_iters", C.c_int32), ("k_iters", C.c_int32),
+        ("omega_restarts", C.c_int32), ("k_restarts", C.c_int32),
+        ("omega_nan", C.c_int32), ("k_nan", C.c_int32),
+        ("steps_per_lb", C.c_int32), ("time_since_change", C.c_int32),
+        ("dt", C.c_double), ("omega_rel_res", C.c_double), ("k_rel_res", C.c_double),
+        ("steps", C.c_int64), ("solver_passes", C.c_int32), ("phase", C.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_i16p = C.POINTER(C.c_int16)
+_i32p = C.POINTER(C.c_int32)
+SIGNATURES = {
+    "kofm_abi_version": (C.c_int, []),
+    "kofm_error_string": (C.c_char_p, [C.c_int]),
+    "kofm_desc_default": (C.c_int, [C.POINTER(KofmDesc)]),
+    "kofm_create": (C.c_int, [C.POINTER(KofmDesc), C.POINTER(_vp)]),
+    "kofm_destroy": (C.c_int, [_vp]),
+    "kofm_set_geometry": (C.c_int, [_vp, _i16p, _dp, _dp, _i32p, _dp, C.c_int32]),
+    "kofm_set_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
+    "kofm_get_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
+    "kofm_get_macro": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "kofm_lb_step": (C.c_int, [_vp, C.c_int32]),
+    "kofm_komega_assemble": (C.c_int, [_vp, C.c_double]),
+    "kofm_komega_solve": (C.c_int, [_vp, _i32p, _dp]),
+    "kofm_komega_update": (C.c_int, [_vp]),
+    "kofm_step": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "kofm_reduce": (C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
+    "kofm_sync": (C.c_int, [_vp]),
+    "kofm_get_stats": (C.c_int, [_vp, C.POINTER(KofmStats)]),
+    "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
+    "kofm_stream": (_vp, [_vp]),
+}
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libkofm.so and declares every ABI symbol (raises if absent)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} not built: run `python -m komegafoulingmodel_b200.build` "
+            "(nvcc, sm_100a); there is no CPU fallback")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class KofmError(RuntimeError):
+    def __init__(self, fn: str, status: int):
+        self.status = status
+        super().__init__(f"{fn} -> {status} ({ERRORS.get(status, 'unknown')})")
+
+
+def check(fn: str, status: int) -> int:
+    if status != KOFM_OK:
+        raise KofmError(fn, status)
+    return status

@@ -1,0 +1,730 @@
+// kofm_api.cu - context, memory management and the C ABI (include/kofm.h).
+//
+// Everything the hot path needs lives in device memory owned by the context;
+// host arrays in the reference's padded FP64 layout cross the boundary only in
+// kofm_set_* / kofm_get_*.  All work is enqueued on the context's stream.
+#include "kofm.h"
+#include "kofm_common.cuh"
+#include "kofm_lb.cuh"
+#include "kofm_komega.cuh"
+#include "kofm_gmres.cuh"
+
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+using namespace kofm;
+
+namespace kofm {
+int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned int** bar,
+                    int* nblocks, int P, int ny, int K, int dev);
+void ko_system_free(KoSystem* s);
+}  // namespace kofm
+
+namespace {
+
+constexpr int RED_BLOCKS = 256;  // fixed => deterministic reduction order
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct kofm_ctx {
+    kofm_desc desc{};
+    int P = 0;            // device row pitch (nodes)
+    long long D = 0;      // plane stride (nodes)
+    int dev = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    size_t store_bytes = 4;
+
+    // lattice state
+    void* g[2] = {nullptr, nullptr};  // population buffers (9 planes each)
+    int cur = 0;                      // buffer holding the current state
+    int phase = 0;                    // 0: FA form, 1: post-collision (pull)
+    int16_t* ntype = nullptr;
+    int32_t* rec = nullptr;           // per-node IBB record index
+    IbbRecord* ibb = nullptr;
+    int n_ibb_rec = 0;
+    int32_t* dxrec_idx = nullptr;     // per-node dX record index
+    DxRecord* dxrec = nullptr;
+    float* wallD = nullptr;
+    float* K = nullptr;
+    float* O = nullptr;
+    float* S = nullptr;
+    float* nut = nullptr;
+    float* rho = nullptr;
+    float* ux = nullptr;
+    float* uy = nullptr;
+    double* lb_partials = nullptr;
+    long long n_lb_partials = 0;
+    double* red_partials = nullptr;   // RED_BLOCKS
+    double* red_out = nullptr;        // 1
+    double* h_red = nullptr;          // pinned, 64 doubles
+    double* staging = nullptr;        // FP64 host-layout staging
+    size_t staging_elems = 0;
+    bool have_geometry = false;
+    bool have_state = false;
+
+    // k-omega solver
+    KoSystem sys[2];                  // 0: omega, 1: k
+    GmresControl* ctl = nullptr;      // device control block
+    GmresControl* h_ctl = nullptr;    // pinned mirror
+    double* gpart = nullptr;          // solver partial sums
+    unsigned int* bar = nullptr;      // grid barrier words
+    int solver_blocks = 0;
+    int steps_per_lb = 1;
+    int time_since_change = 0;
+    double dt = 1.0;
+    kofm_stats stats{};
+};
+
+namespace {
+
+#define KOFM_CUDA_TRY(call, code)                                                 \
+    do {                                                                          \
+        cudaError_t _e = (call);                                                  \
+        if (_e != cudaSuccess) {                                                  \
+            fprintf(stderr, "kofm: %s failed: %s\n", #call, cudaGetErrorString(_e)); \
+            return (code);                                                        \
+        }                                                                         \
+    } while (0)
+
+int dalloc(void** p, size_t bytes) {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return KOFM_ERR_BUFFER_ALLOCATION;
+    if (cudaMemset(*p, 0, bytes) != cudaSuccess) return KOFM_ERR_BUFFER_ALLOCATION;
+    return KOFM_OK;
+}
+
+template <typename T>
+int dalloc_t(T** p, size_t n) {
+    return dalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+
+int ensure_staging(kofm_ctx* c, size_t elems) {
+    if (c->staging_elems >= elems) return KOFM_OK;
+    if (c->staging) cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_elems = 0;
+    int st = dalloc_t(&c->staging, elems);
+    if (st) return st;
+    c->staging_elems = elems;
+    return KOFM_OK;
+}
+
+// ---- conversion kernels ----------------------------------------------------
+// host-layout FP64 populations (FA) -> device deviations; solid/padding -> 0
+template <typename ST>
+__global__ void k_fa_in(const double* __restrict__ f, ST* __restrict__ g,
+                        const int16_t* __restrict__ nt, int nx, int nxf, int ny,
+                        int P, long long D) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= P) return;
+    const long long node = (long long)y * P + x;
+    const bool fluid = x < nx && !((uint16_t)nt[node] & M_SOLID);
+    const long long Dh = (long long)nxf * ny;
+    for (int q = 0; q < 9; ++q) {
+        double v = 0.0;
+        if (fluid) v = f[q * Dh + (long long)y * nxf + x] - weight_of(q);
+        g[q * D + node] = Store<ST>::from_f64(v);
+    }
+}
+
+// device state -> host-layout FP64 FA.  phase 0: own deviations; phase 1:
+// gather + bounce-back + interpolated bounce-back (the next step's pull).
+template <typename ST>
+__global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ nt,
+                         const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
+                         int has_ibb, double* __restrict__ f, int nx, int nxf, int ny,
+                         int P, long long D, int phase) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= nxf) return;
+    const long long Dh = (long long)nxf * ny;
+    const long long hnode = (long long)y * nxf + x;
+    const long long node = (long long)y * P + x;
+    const int type = x < nx ? (uint16_t)nt[node] : M_SOLID;
+    if (type & M_SOLID) {
+        for (int q = 0; q < 9; ++q) f[q * Dh + hnode] = 0.0;
+        return;
+    }
+    double d[9];
+    for (int q = 0; q < 9; ++q) {
+        if (phase == 0) {
+            d[q] = Store<ST>::to_f64(g[q * D + node]);
+        } else {
+            int xs = x - cx_of(q);
+            xs = xs < 0 ? xs + nx : (xs >= nx ? xs - nx : xs);
+            int ys = y - cy_of(q);
+            ys = ys < 0 ? 0 : (ys >= ny ? ny - 1 : ys);
+            d[q] = Store<ST>::to_f64(g[q * D + (long long)ys * P + xs]);
+        }
+    }
+    if (phase == 1 && (type & BOUNDARY)) {
+        double pre[9];
+        pre[0] = d[0];
+        for (int q = 1; q < 9; ++q) {
+            if (type & bound_of(rev_of(q))) d[q] = Store<ST>::to_f64(g[rev_of(q) * D + node]);
+            pre[q] = d[q];
+        }
+        if (has_ibb && rec[node] >= 0) {
+            const IbbRecord r = ibb[rec[node]];
+            for (int dd = 1; dd < 9; ++dd) {
+                const double qf = r.q[dd - 1];
+                if (qf < 0.0) continue;
+                const int rd = rev_of(dd);
+                const double q2 = 2.0 * qf;
+                if (q2 <= 1.0) d[rd] = q2 * pre[rd] + (1.0 - q2) * pre[dd];
+                else d[rd] = (1.0 / q2) * (pre[rd] + (q2 - 1.0) * Store<ST>::to_f64(g[rd * D + node]));
+            }
+        }
+    }
+    for (int q = 0; q < 9; ++q) f[q * Dh + hnode] = d[q] + weight_of(q);
+}
+
+// FP64 host-layout scalar field <-> FP32 device field
+__global__ void k_field_in(const double* __restrict__ h, float* __restrict__ dv, int nxf,
+                           int ny, int P) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= P) return;
+    dv[(long long)y * P + x] = x < nxf ? (float)h[(long long)y * nxf + x] : 0.f;
+}
+__global__ void k_field_out(const float* __restrict__ dv, double* __restrict__ h, int nxf,
+                            int ny, int P) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= nxf) return;
+    h[(long long)y * nxf + x] = (double)dv[(long long)y * P + x];
+}
+
+// ---- deterministic reductions -------------------------------------------------
+// Block b sums the fixed contiguous range [b*n/B, (b+1)*n/B) of the padded
+// field (rows of P nodes; columns >= nxf excluded), then one block combines the
+// B partials in order.
+template <int OP>
+__device__ __forceinline__ double red_op(double a, double b) {
+    return OP == KOFM_OP_SUM ? a + b : (OP == KOFM_OP_MIN ? fmin(a, b) : fmax(a, b));
+}
+template <int OP>
+__device__ __forceinline__ double red_init() {
+    return OP == KOFM_OP_SUM ? 0.0 : (OP == KOFM_OP_MIN ? 1.0e308 : -1.0e308);
+}
+
+template <int OP>
+__global__ void k_reduce_field(const float* __restrict__ v, long long nnodes, int P, int nxf,
+                               double* __restrict__ part) {
+    __shared__ double sh[32];
+    const long long s = (long long)((double)blockIdx.x * nnodes / gridDim.x);
+    const long long e = (long long)((double)(blockIdx.x + 1) * nnodes / gridDim.x);
+    double acc = red_init<OP>();
+    for (long long i = s + threadIdx.x; i < e; i += blockDim.x) {
+        if ((int)(i % P) < nxf) acc = red_op<OP>(acc, (double)v[i]);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc = red_op<OP>(acc, __shfl_down_sync(0xffffffffu, acc, off));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : red_init<OP>();
+        for (int off = 16; off > 0; off >>= 1) acc = red_op<OP>(acc, __shfl_down_sync(0xffffffffu, acc, off));
+        if (threadIdx.x == 0) part[blockIdx.x] = acc;
+    }
+}
+
+template <int OP>
+__global__ void k_reduce_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double acc = red_init<OP>();
+        for (int i = 0; i < n; ++i) acc = red_op<OP>(acc, part[i]);
+        out[0] = acc;
+    }
+}
+
+// wall-shear integrand: rho (mu + nu_t) 2 |Sxy| on fluid nodes with an N or S
+// wall link, summed per block.
+__global__ void k_wall_shear(const int16_t* __restrict__ nt, const float* __restrict__ rho,
+                             const float* __restrict__ nut, const float* __restrict__ S,
+                             long long nnodes, long long D, int P, int nx, double mu,
+                             double* __restrict__ part) {
+    __shared__ double sh[32];
+    const long long s = (long long)((double)blockIdx.x * nnodes / gridDim.x);
+    const long long e = (long long)((double)(blockIdx.x + 1) * nnodes / gridDim.x);
+    double acc = 0.0;
+    for (long long i = s + threadIdx.x; i < e; i += blockDim.x) {
+        const int t = (uint16_t)nt[i];
+        if ((int)(i % P) < nx && !(t & M_SOLID) && (t & (N_BOUND | S_BOUND)))
+            acc += (double)rho[i] * (mu + (double)nut[i]) * 2.0 * fabs((double)S[D + i]);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (threadIdx.x == 0) part[blockIdx.x] = acc;
+    }
+}
+
+// ---- LB step dispatch ------------------------------------------------------------
+template <typename ST, typename AT>
+cudaError_t launch_lb(kofm_ctx* c, const LbParams& p, bool komega, bool phase0) {
+    dim3 block(32, 4);
+    dim3 grid(c->P / 128, (c->desc.ny + 3) / 4);
+    if (komega) {
+        if (phase0) lb_step_kernel<ST, AT, true, true><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, true, false><<<grid, block, 0, c->stream>>>(p);
+    } else {
+        if (phase0) lb_step_kernel<ST, AT, false, true><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, false, false><<<grid, block, 0, c->stream>>>(p);
+    }
+    return cudaGetLastError();
+}
+
+int validate_desc(const kofm_desc* d) {
+    if (!d) return KOFM_ERR_INVALID_ARG;
+    if (d->nx < 4 || d->ny < 3 || d->nx_full < d->nx) return KOFM_ERR_LOADING_PARAMS;
+    if ((long long)d->nx_full * d->ny > (1LL << 31) - 1) return KOFM_ERR_LOADING_PARAMS;
+    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_BF16_DEV) return KOFM_ERR_LOADING_PARAMS;
+    if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
+    if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
+    if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
+    return KOFM_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int kofm_abi_version(void) { return KOFM_ABI_VERSION; }
+
+const char* kofm_error_string(int s) {
+    switch (s) {
+        case KOFM_OK: return "ok";
+        case KOFM_ERR_BUFFER_ALLOCATION: return "device buffer allocation failed";
+        case KOFM_ERR_MEMORY_COPY: return "host/device copy failed";
+        case KOFM_ERR_CALLING_KERNEL: return "kernel launch or execution failed";
+        case KOFM_ERR_LOADING_PARAMS: return "invalid run parameters";
+        case KOFM_ERR_INITIALIZING_KOMEGA: return "k-omega initialisation failed";
+        case KOFM_ERR_INITIALIZING_VLS: return "invalid geometry";
+        case KOFM_ERR_INITIALIZING_VLB: return "LB initialisation failed";
+        case KOFM_ERR_INVALID_ARG: return "invalid argument";
+        case KOFM_ERR_NO_DEVICE: return "no usable CUDA device";
+        case KOFM_ERR_NOT_CONVERGED: return "k-omega solve reached its iteration cap";
+        case KOFM_ERR_NAN: return "NaN residual in the k-omega solve (dt halved)";
+        case KOFM_ERR_TIMEOUT: return "bounded device wait expired";
+        case KOFM_ERR_STATE: return "geometry or state not set";
+        default: return "unknown status";
+    }
+}
+
+int kofm_desc_default(kofm_desc* d) {
+    if (!d) return KOFM_ERR_INVALID_ARG;
+    memset(d, 0, sizeof(*d));
+    d->nx = 256; d->nx_full = 256; d->ny = 64;
+    d->use_komega = 0;
+    d->tau = 1.25;                // rate; LB_TAU_NUMBER is 1.99
+    d->fterm = 0.0;
+    d->mu = (1.0 / 1.25 - 0.5) / 3.0;
+    d->max_turb_visc = 10.0;      // MAX_TURB_VISC
+    d->storage = KOFM_STORE_FP32;
+    d->device = 0;
+    d->komega_max_iters = 1000;   // KOMEGA_MAX_ITERS
+    d->krylov_dim = 10;           // GMRES_KRYLOV_DIM_SIZE
+    d->komega_rel_tol = 1.0e-4;   // KOMEGA_MAX_REL_TOL
+    d->komega_abs_tol = 1.0e-7;   // KOMEGA_MAX_ABS_TOL
+    d->komega_dt = 1.0;           // p.dTlb
+    return KOFM_OK;
+}
+
+int kofm_destroy(kofm_ctx* c) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* bufs[] = {c->g[0], c->g[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
+                    c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
+                    c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
+                    c->gpart, c->bar};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
+    if (c->h_red) cudaFreeHost(c->h_red);
+    if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return KOFM_OK;
+}
+
+int kofm_create(const kofm_desc* d, kofm_ctx** out) {
+    if (!out) return KOFM_ERR_INVALID_ARG;
+    *out = nullptr;
+    int st = validate_desc(d);
+    if (st) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= d->device || d->device < 0)
+        return KOFM_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, d->device) != cudaSuccess) return KOFM_ERR_NO_DEVICE;
+    if (prop.major < 10) return KOFM_ERR_NO_DEVICE;  // built for sm_100a only
+    kofm_ctx* c = new (std::nothrow) kofm_ctx();
+    if (!c) return KOFM_ERR_BUFFER_ALLOCATION;
+    c->desc = *d;
+    c->dev = d->device;
+    c->num_sms = prop.multiProcessorCount;
+    c->P = ((d->nx_full + 127) / 128) * 128;
+    c->D = (long long)c->P * d->ny;
+    c->store_bytes = d->storage == KOFM_STORE_FP32 ? 4 : 2;
+    c->dt = d->komega_dt;
+    c->steps_per_lb = (int)(1.0 / d->komega_dt);
+    if (c->steps_per_lb < 1) c->steps_per_lb = 1;
+    if (cudaSetDevice(c->dev) != cudaSuccess) { delete c; return KOFM_ERR_NO_DEVICE; }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return KOFM_ERR_NO_DEVICE;
+    }
+    const long long D = c->D;
+#define ALLOC(ptr, n)                                       \
+    do {                                                    \
+        int _s = dalloc_t(&(ptr), (size_t)(n));             \
+        if (_s) { kofm_destroy(c); return _s; }             \
+    } while (0)
+    for (int b = 0; b < 2; ++b) {
+        int _s = dalloc(&c->g[b], (size_t)(9 * D) * c->store_bytes);
+        if (_s) { kofm_destroy(c); return _s; }
+    }
+    ALLOC(c->ntype, D);
+    ALLOC(c->rec, D);
+    ALLOC(c->dxrec_idx, D);
+    ALLOC(c->rho, D);
+    ALLOC(c->ux, D);
+    ALLOC(c->uy, D);
+    c->n_lb_partials = (long long)(c->P / 128) * ((d->ny + 3) / 4) * 4 * 3;
+    ALLOC(c->lb_partials, c->n_lb_partials);
+    ALLOC(c->red_partials, RED_BLOCKS);
+    ALLOC(c->red_out, 8);
+    if (d->use_komega) {
+        ALLOC(c->wallD, D);
+        ALLOC(c->K, D);
+        ALLOC(c->O, D);
+        ALLOC(c->S, 3 * D);
+        ALLOC(c->nut, D);
+        int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks,
+                                 c->P, d->ny, d->krylov_dim, c->dev);
+        if (s2) { kofm_destroy(c); return s2; }
+        if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {
+            kofm_destroy(c);
+            return KOFM_ERR_BUFFER_ALLOCATION;
+        }
+    }
+#undef ALLOC
+    if (cudaMallocHost(&c->h_red, 64 * sizeof(double)) != cudaSuccess) {
+        kofm_destroy(c);
+        return KOFM_ERR_BUFFER_ALLOCATION;
+    }
+    // rec / dxrec_idx default to -1 (no record)
+    cudaMemset(c->rec, 0xff, D * sizeof(int32_t));
+    cudaMemset(c->dxrec_idx, 0xff, D * sizeof(int32_t));
+    c->stats.steps_per_lb = c->steps_per_lb;
+    c->stats.dt = c->dt;
+    *out = c;
+    return KOFM_OK;
+}
+
+void* kofm_stream(kofm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
+                      const double* dX4, const int32_t* ibb_idx, const double* ibb_q,
+                      int32_t n_ibb) {
+    if (!c || !ntype) return KOFM_ERR_INVALID_ARG;
+    const kofm_desc& d = c->desc;
+    if (d.use_komega && (!wallD || !dX4)) return KOFM_ERR_INVALID_ARG;
+    if (n_ibb < 0 || (n_ibb > 0 && (!ibb_idx || !ibb_q))) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    const int nx = d.nx, nxf = d.nx_full, ny = d.ny, P = c->P;
+    const long long Dh = (long long)nxf * ny;
+    // rows 0 and ny-1 may hold no fluid node (clVariablesLS.cpp:935-937)
+    for (int x = 0; x < nx; ++x) {
+        if (!((uint16_t)ntype[x] & M_SOLID) || !((uint16_t)ntype[(long long)(ny - 1) * nxf + x] & M_SOLID))
+            return KOFM_ERR_INITIALIZING_VLS;
+    }
+    std::vector<int16_t> nt((size_t)c->D, (int16_t)M_SOLID);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) nt[(size_t)y * P + x] = ntype[(long long)y * nxf + x];
+    // interpolated bounce-back records, one per node that owns a link
+    std::vector<int32_t> rec((size_t)c->D, -1);
+    std::vector<IbbRecord> recs;
+    for (int i = 0; i < n_ibb; ++i) {
+        const long long loc = ibb_idx[i];
+        const int dir = (int)(loc / Dh);
+        const long long hnode = loc - (long long)dir * Dh;
+        if (dir < 1 || dir > 8 || hnode < 0 || hnode >= Dh) return KOFM_ERR_INITIALIZING_VLS;
+        const int x = (int)(hnode % nxf), y = (int)(hnode / nxf);
+        if (x >= nx) return KOFM_ERR_INITIALIZING_VLS;
+        const size_t node = (size_t)y * P + x;
+        if (rec[node] < 0) {
+            IbbRecord r;
+            for (int k = 0; k < 8; ++k) r.q[k] = -1.0;
+            rec[node] = (int32_t)recs.size();
+            recs.push_back(r);
+        }
+        recs[rec[node]].q[dir - 1] = ibb_q[i];
+    }
+    // FD link-fraction records for nodes whose dX differs from 1
+    std::vector<int32_t> dxi((size_t)c->D, -1);
+    std::vector<DxRecord> dxr;
+    std::vector<float> wd;
+    if (d.use_komega) {
+        wd.assign((size_t)c->D, 0.f);
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const long long h = (long long)y * nxf + x;
+                const size_t node = (size_t)y * P + x;
+                wd[node] = (float)wallD[h];
+                if ((uint16_t)ntype[h] & M_SOLID) continue;
+                DxRecord r;
+                bool unit = true;
+                for (int k = 0; k < 4; ++k) {
+                    r.dx[k] = dX4[k * Dh + h];
+                    if (r.dx[k] != 1.0) unit = false;
+                }
+                if (!unit) {
+                    dxi[node] = (int32_t)dxr.size();
+                    dxr.push_back(r);
+                }
+            }
+    }
+    if (c->ibb) { cudaFree(c->ibb); c->ibb = nullptr; }
+    if (c->dxrec) { cudaFree(c->dxrec); c->dxrec = nullptr; }
+    c->n_ibb_rec = (int)recs.size();
+    if (!recs.empty()) {
+        if (dalloc_t(&c->ibb, recs.size())) return KOFM_ERR_BUFFER_ALLOCATION;
+        KOFM_CUDA_TRY(cudaMemcpy(c->ibb, recs.data(), recs.size() * sizeof(IbbRecord), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    }
+    if (!dxr.empty()) {
+        if (dalloc_t(&c->dxrec, dxr.size())) return KOFM_ERR_BUFFER_ALLOCATION;
+        KOFM_CUDA_TRY(cudaMemcpy(c->dxrec, dxr.data(), dxr.size() * sizeof(DxRecord), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    }
+    KOFM_CUDA_TRY(cudaMemcpy(c->ntype, nt.data(), nt.size() * sizeof(int16_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaMemcpy(c->rec, rec.data(), rec.size() * sizeof(int32_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaMemcpy(c->dxrec_idx, dxi.data(), dxi.size() * sizeof(int32_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    if (d.use_komega)
+        KOFM_CUDA_TRY(cudaMemcpy(c->wallD, wd.data(), wd.size() * sizeof(float), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    c->have_geometry = true;
+    return KOFM_OK;
+}
+
+static int upload_field(kofm_ctx* c, const double* h, float* dv) {
+    const kofm_desc& d = c->desc;
+    const size_t n = (size_t)d.nx_full * d.ny;
+    KOFM_CUDA_TRY(cudaMemcpyAsync(c->staging, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream), KOFM_ERR_MEMORY_COPY);
+    dim3 grid((c->P + 255) / 256, d.ny);
+    k_field_in<<<grid, 256, 0, c->stream>>>(c->staging, dv, d.nx_full, d.ny, c->P);
+    KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    return KOFM_OK;
+}
+
+static int download_field(kofm_ctx* c, const float* dv, double* h) {
+    const kofm_desc& d = c->desc;
+    const size_t n = (size_t)d.nx_full * d.ny;
+    dim3 grid((d.nx_full + 255) / 256, d.ny);
+    k_field_out<<<grid, 256, 0, c->stream>>>(dv, c->staging, d.nx_full, d.ny, c->P);
+    KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    KOFM_CUDA_TRY(cudaMemcpyAsync(h, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_MEMORY_COPY);
+    return KOFM_OK;
+}
+
+int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* omega,
+                   const double* nut, const double* sxy) {
+    if (!c || !f) return KOFM_ERR_INVALID_ARG;
+    if (!c->have_geometry) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    if (d.use_komega && (!k || !omega || !sxy)) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    const size_t Dh = (size_t)d.nx_full * d.ny;
+    int st = ensure_staging(c, 9 * Dh);
+    if (st) return st;
+    KOFM_CUDA_TRY(cudaMemcpyAsync(c->staging, f, 9 * Dh * sizeof(double), cudaMemcpyHostToDevice, c->stream), KOFM_ERR_MEMORY_COPY);
+    dim3 grid((c->P + 127) / 128, d.ny);
+    c->cur = 0;
+    switch (d.storage) {
+        case KOFM_STORE_FP32:
+            k_fa_in<float><<<grid, 128, 0, c->stream>>>(c->staging, (float*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+            break;
+        case KOFM_STORE_FP16_DEV:
+            k_fa_in<__half><<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+            break;
+        default:
+            k_fa_in<__nv_bfloat16><<<grid, 128, 0, c->stream>>>(c->staging, (__nv_bfloat16*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+    }
+    KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    if (d.use_komega) {
+        if ((st = upload_field(c, k, c->K))) return st;
+        if ((st = upload_field(c, omega, c->O))) return st;
+        if (nut) {
+            if ((st = upload_field(c, nut, c->nut))) return st;
+        }
+        for (int s = 0; s < 3; ++s)
+            if ((st = upload_field(c, sxy + s * Dh, c->S + s * c->D))) return st;
+    }
+    KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_MEMORY_COPY);
+    c->phase = 0;
+    c->have_state = true;
+    c->stats.phase = 0;
+    return KOFM_OK;
+}
+
+int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut, double* sxy) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    if (!c->have_state) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    cudaSetDevice(c->dev);
+    const size_t Dh = (size_t)d.nx_full * d.ny;
+    int st = ensure_staging(c, 9 * Dh);
+    if (st) return st;
+    if (f) {
+        dim3 grid((d.nx_full + 127) / 128, d.ny);
+        const int has_ibb = c->n_ibb_rec > 0;
+        switch (d.storage) {
+            case KOFM_STORE_FP32:
+                k_fa_out<float><<<grid, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+                break;
+            case KOFM_STORE_FP16_DEV:
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+                break;
+            default:
+                k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+        }
+        KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+        KOFM_CUDA_TRY(cudaMemcpyAsync(f, c->staging, 9 * Dh * sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
+        KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_MEMORY_COPY);
+    }
+    if (d.use_komega) {
+        if (k && (st = download_field(c, c->K, k))) return st;
+        if (omega && (st = download_field(c, c->O, omega))) return st;
+        if (nut && (st = download_field(c, c->nut, nut))) return st;
+        if (sxy)
+            for (int s = 0; s < 3; ++s)
+                if ((st = download_field(c, c->S + s * c->D, sxy + s * Dh))) return st;
+    }
+    return KOFM_OK;
+}
+
+int kofm_get_macro(kofm_ctx* c, double* rho, double* ux, double* uy) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    const kofm_desc& d = c->desc;
+    int st = ensure_staging(c, (size_t)d.nx_full * d.ny);
+    if (st) return st;
+    if (rho && (st = download_field(c, c->rho, rho))) return st;
+    if (ux && (st = download_field(c, c->ux, ux))) return st;
+    if (uy && (st = download_field(c, c->uy, uy))) return st;
+    return KOFM_OK;
+}
+
+int kofm_lb_step(kofm_ctx* c, int32_t options) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    if (!c->have_state) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    LbParams p;
+    p.gin = c->g[c->cur];
+    p.gout = c->g[c->cur ^ 1];
+    p.ntype = c->ntype;
+    p.rec = c->rec;
+    p.ibb = c->ibb;
+    p.wallD = c->wallD;
+    p.K = c->K; p.O = c->O; p.S = c->S; p.nut = c->nut;
+    p.rho = c->rho; p.ux = c->ux; p.uy = c->uy;
+    p.partials = c->lb_partials;
+    p.nx = d.nx; p.ny = d.ny; p.P = c->P; p.D = c->D;
+    p.tau = d.tau; p.fterm = d.fterm; p.mu = d.mu; p.maxnut = d.max_turb_visc;
+    p.options = options;
+    p.has_ibb = c->n_ibb_rec > 0;
+    const bool ko = d.use_komega != 0, ph0 = c->phase == 0;
+    cudaError_t e;
+    switch (d.storage) {
+        case KOFM_STORE_FP32: e = launch_lb<float, double>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP16_DEV: e = launch_lb<__half, float>(c, p, ko, ph0); break;
+        default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
+    }
+    if (e != cudaSuccess) {
+        fprintf(stderr, "kofm: lb step launch failed: %s\n", cudaGetErrorString(e));
+        return KOFM_ERR_CALLING_KERNEL;
+    }
+    c->cur ^= 1;
+    c->phase = 1;
+    c->stats.phase = 1;
+    c->stats.steps += 1;
+    return KOFM_OK;
+}
+
+int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
+    if (!c || !out) return KOFM_ERR_INVALID_ARG;
+    const kofm_desc& d = c->desc;
+    const float* v = nullptr;
+    switch (field) {
+        case KOFM_FIELD_RHO: v = c->rho; break;
+        case KOFM_FIELD_UX: v = c->ux; break;
+        case KOFM_FIELD_UY: v = c->uy; break;
+        case KOFM_FIELD_K: v = c->K; break;
+        case KOFM_FIELD_OMEGA: v = c->O; break;
+        case KOFM_FIELD_NUT: v = c->nut; break;
+        case KOFM_FIELD_WALL_SHEAR: break;
+        default: return KOFM_ERR_INVALID_ARG;
+    }
+    if (field != KOFM_FIELD_WALL_SHEAR && !v) return KOFM_ERR_STATE;
+    if (op < KOFM_OP_SUM || op > KOFM_OP_MAX) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    const long long n = c->D;
+    if (field == KOFM_FIELD_WALL_SHEAR) {
+        if (!d.use_komega || op != KOFM_OP_SUM) return KOFM_ERR_INVALID_ARG;
+        k_wall_shear<<<RED_BLOCKS, 256, 0, c->stream>>>(c->ntype, c->rho, c->nut, c->S, n, c->D, c->P, d.nx, d.mu, c->red_partials);
+        k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    } else if (op == KOFM_OP_SUM) {
+        k_reduce_field<KOFM_OP_SUM><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    } else if (op == KOFM_OP_MIN) {
+        k_reduce_field<KOFM_OP_MIN><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_final<KOFM_OP_MIN><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    } else {
+        k_reduce_field<KOFM_OP_MAX><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_final<KOFM_OP_MAX><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    }
+    KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    KOFM_CUDA_TRY(cudaMemcpyAsync(c->h_red, c->red_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_CALLING_KERNEL);
+    *out = c->h_red[0];
+    return KOFM_OK;
+}
+
+int kofm_sync(kofm_ctx* c) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "kofm: stream error: %s\n", cudaGetErrorString(e));
+        return KOFM_ERR_CALLING_KERNEL;
+    }
+    return KOFM_OK;
+}
+
+int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
+    if (!c || !out) return KOFM_ERR_INVALID_ARG;
+    c->stats.steps_per_lb = c->steps_per_lb;
+    c->stats.time_since_change = c->time_since_change;
+    c->stats.dt = c->dt;
+    *out = c->stats;
+    return KOFM_OK;
+}
+
+}  // extern "C"
+
+// k-omega entry points live in kofm_komega_api.inc (same translation unit).
+#include "kofm_komega_api.inc"

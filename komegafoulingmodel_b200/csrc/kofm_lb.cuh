@@ -1,0 +1,307 @@
+// kofm_lb.cuh - D2Q9 pull-scheme collide-stream kernel (the reference's
+// LB_collision_SRT_Fluid / LB_collision_SRT_Fluid_w_kOmega + lbIBB,
+// Kernels/lbKernels.cl:175-335, 345-633, 640-668), re-designed for sm_100a.
+//
+// One thread owns 4 consecutive nodes of one row (x0..x0+3); a warp covers a
+// 128-node row segment, a 32x4 block covers 4 rows.  Per population plane the
+// warp issues one 16-byte (FP32) or 8-byte (FP16/BF16) load per thread of
+// the upstream row; the +-1 x-shift of the pull is done with warp shuffles,
+// lanes 0 / 31 fetch the single element across the segment edge (with the
+// periodic wrap over nx).  Every plane row is read once and written once per
+// step, so HBM traffic is the compulsory bytes.
+//
+// Pull vs the reference's push: the buffers hold post-collision populations
+// G of the previous step; node x gathers G(x - c_q, q).  A link whose
+// upstream node is solid (the node carries the bound flag of direction
+// rev(q)) takes the node's own G(x, rev q): the reference's same-step
+// half-way bounce-back (postCollisionBC, lbKernels.cl:166-171).  lbIBB's
+// Bouzidi correction, which the reference applies to the post-stream buffer
+// after the push, is applied here to the gathered values before collision:
+//   2q <= 1: P(x, rev d) = 2q G(x, d) + (1 - 2q) P(x, d)
+//   2q  > 1: P(x, rev d) = (G(x, d) + (2q - 1) G(x, rev d)) / (2q)
+// where d is the link direction pointing into the wall.  All links of one node
+// use the pre-correction values (the reference's list order only matters for
+// a node with walls on two opposite sides).
+//
+// Collision in deviation form (d_q = f_q - w_q), exact-difference forcing
+// with the product-form equilibrium (clVariablesLB.cpp:77-117):
+//   rho = 1 + sum d,  u = j / rho,
+//   feq_q - w_q = drho phx phy + dphx phy0 + phx0 dphy + dphx dphy,
+//   d'_q = d_q - w (d_q - (feq_q - w_q)) + rho phy [phx(ux + F) - phx(ux)],
+// with phi0(0) = 2/3, phi0(+-1) = 1/6, dphi(0, u) = -u^2,
+// dphi(+-1, u) = (+-u + u^2)/2.  No term subtracts two O(1) numbers, so the
+// FP32-stored deviations keep their relative precision.
+#pragma once
+#include "kofm_common.cuh"
+
+namespace kofm {
+
+struct LbParams {
+    const void* gin;        // populations read (9 planes)
+    void* gout;             // populations written (9 planes)
+    const int16_t* ntype;
+    const int32_t* rec;     // per-node IBB record index (-1: none)
+    const IbbRecord* ibb;   // IBB records
+    const float* wallD;
+    float* K;
+    float* O;
+    float* S;               // 3 planes Sxx, Sxy, Syy
+    float* nut;
+    float* rho;
+    float* ux;
+    float* uy;
+    double* partials;       // per block: sum rho, sum ux, sum uy (FP64)
+    int nx, ny, P;
+    long long D;
+    double tau, fterm, mu, maxnut;
+    int options;
+    int has_ibb;
+};
+
+template <typename AT>
+__device__ __forceinline__ AT phi0(int c) { return c == 0 ? AT(2.0 / 3.0) : AT(1.0 / 6.0); }
+template <typename AT>
+__device__ __forceinline__ AT dphi(int c, AT u) {
+    return c == 0 ? -u * u : AT(0.5) * (AT(c) * u + u * u);
+}
+// phi(c, u + g) - phi(c, u)
+template <typename AT>
+__device__ __forceinline__ AT dphiF(int c, AT u, AT g) {
+    return c == 0 ? -g * (AT(2) * u + g) : AT(0.5) * g * (AT(c) + AT(2) * u + g);
+}
+template <typename AT>
+__device__ __forceinline__ AT amax(AT a, AT b) { return a < b ? b : a; }
+template <typename AT>
+__device__ __forceinline__ AT amin(AT a, AT b) { return b < a ? b : a; }
+
+template <typename ST>
+__device__ __forceinline__ float ld1(const ST* base, long long idx) {
+    return Store<ST>::to_f32(base[idx]);
+}
+
+// ---------------------------------------------------------------------------
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0>
+__global__ void __launch_bounds__(128)
+lb_step_kernel(const LbParams p) {
+    const int lane = threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    // Each warp owns one partial-sum slot; warps that leave early clear it.
+    double* slot = nullptr;
+    if (p.partials && (p.options & OPTION_SAVE_MACRO_FIELDS))
+        slot = p.partials + (((long long)blockIdx.y * gridDim.x + blockIdx.x) * 4 + threadIdx.y) * 3;
+    if (y >= p.ny) {  // warp-uniform
+        if (slot && lane == 0) { slot[0] = 0.0; slot[1] = 0.0; slot[2] = 0.0; }
+        return;
+    }
+    const int x0 = (blockIdx.x * 32 + lane) * 4;
+    const ST* gin = static_cast<const ST*>(p.gin);
+    ST* gout = static_cast<ST*>(p.gout);
+    const long long rowoff = (long long)y * p.P;
+    const long long D = p.D;
+
+    int type[4];
+    bool fl[4];
+    {
+        const short4 t4 = *reinterpret_cast<const short4*>(p.ntype + rowoff + x0);
+        type[0] = (uint16_t)t4.x; type[1] = (uint16_t)t4.y;
+        type[2] = (uint16_t)t4.z; type[3] = (uint16_t)t4.w;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) fl[j] = (x0 + j < p.nx) && !(type[j] & M_SOLID);
+    }
+    const bool any_fluid = fl[0] | fl[1] | fl[2] | fl[3];
+    if (!__any_sync(0xffffffffu, any_fluid)) {  // whole warp solid
+        if (slot && lane == 0) { slot[0] = 0.0; slot[1] = 0.0; slot[2] = 0.0; }
+        return;
+    }
+
+    AT d[9][4];
+    // ---- gather (pull) -----------------------------------------------------
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int cx = cx_of(q), cy = cy_of(q);
+        float v[4];
+        if (PHASE0) {
+            Store<ST>::load4(gin + q * D + rowoff + x0, v);
+        } else {
+            int ys = y - cy;
+            ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);  // only solid rows clamp
+            const ST* src = gin + q * D + (long long)ys * p.P;
+            float c[4];
+            Store<ST>::load4(src + x0, c);
+            if (cx == 0) {
+                v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = c[3];
+            } else if (cx == 1) {
+                float left = __shfl_up_sync(0xffffffffu, c[3], 1);
+                if (lane == 0) {
+                    const int xs = x0 > 0 ? x0 - 1 : p.nx - 1;
+                    left = ld1(src, xs);
+                }
+                v[0] = left; v[1] = c[0]; v[2] = c[1]; v[3] = c[2];
+            } else {
+                float right = __shfl_down_sync(0xffffffffu, c[0], 1);
+                if (lane == 31) {
+                    const int xs = (x0 + 4 < p.nx) ? x0 + 4 : 0;
+                    right = ld1(src, xs);
+                }
+                v[0] = c[1]; v[1] = c[2]; v[2] = c[3]; v[3] = right;
+                const int jw = p.nx - 1 - x0;  // node nx-1 wraps to x = 0
+                if (jw >= 0 && jw < 4) v[jw] = ld1(src, 0);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[q][j] = AT(v[j]);
+    }
+
+    // ---- half-way bounce-back and interpolated bounce-back -----------------
+    if (!PHASE0) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!fl[j] || !(type[j] & BOUNDARY)) continue;
+            const long long node = rowoff + x0 + j;
+            AT pre[9];
+#pragma unroll
+            for (int q = 1; q < 9; ++q) {
+                if (type[j] & bound_of(rev_of(q))) d[q][j] = AT(ld1(gin, rev_of(q) * D + node));
+                pre[q] = d[q][j];
+            }
+            if (p.has_ibb) {
+                const int r = p.rec[node];
+                if (r >= 0) {
+                    const IbbRecord rec = p.ibb[r];
+#pragma unroll
+                    for (int dd = 1; dd < 9; ++dd) {
+                        const double qf = rec.q[dd - 1];
+                        if (qf < 0.0) continue;
+                        const int rd = rev_of(dd);
+                        const AT q2 = AT(2.0 * qf);
+                        if (q2 <= AT(1)) {
+                            d[rd][j] = q2 * pre[rd] + (AT(1) - q2) * pre[dd];
+                        } else {
+                            const AT own = AT(ld1(gin, rd * D + node));
+                            d[rd][j] = (AT(1) / q2) * (pre[rd] + (q2 - AT(1)) * own);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // ---- collision ----------------------------------------------------------
+    const AT tau0 = AT(p.tau), fterm = AT(p.fterm), mu = AT(p.mu);
+    float o_rho[4], o_ux[4], o_uy[4], o_nut[4], o_s[3][4];
+    float kin[4], oin[4], win[4], sin3[3][4];
+    if (KOMEGA) {
+        const float4 k4 = *reinterpret_cast<const float4*>(p.K + rowoff + x0);
+        const float4 o4 = *reinterpret_cast<const float4*>(p.O + rowoff + x0);
+        const float4 w4 = __ldg(reinterpret_cast<const float4*>(p.wallD + rowoff + x0));
+        kin[0] = k4.x; kin[1] = k4.y; kin[2] = k4.z; kin[3] = k4.w;
+        oin[0] = o4.x; oin[1] = o4.y; oin[2] = o4.z; oin[3] = o4.w;
+        win[0] = w4.x; win[1] = w4.y; win[2] = w4.z; win[3] = w4.w;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float4 s4 = *reinterpret_cast<const float4*>(p.S + c * D + rowoff + x0);
+            sin3[c][0] = s4.x; sin3[c][1] = s4.y; sin3[c][2] = s4.z; sin3[c][3] = s4.w;
+        }
+    }
+    double bsum_rho = 0.0, bsum_ux = 0.0, bsum_uy = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (!fl[j]) {
+            o_rho[j] = 0.f; o_ux[j] = 0.f; o_uy[j] = 0.f; o_nut[j] = 0.f;
+            o_s[0][j] = 0.f; o_s[1][j] = 0.f; o_s[2][j] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) d[q][j] = AT(0);
+            continue;
+        }
+        AT drho = AT(0);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) drho += d[q][j];
+        const AT rho = AT(1) + drho;
+        const AT jx = d[1][j] - d[2][j] + d[5][j] - d[6][j] + d[7][j] - d[8][j];
+        const AT jy = d[3][j] - d[4][j] + d[5][j] - d[6][j] - d[7][j] + d[8][j];
+        const AT inv = AT(1) / rho;
+        const AT ux = inv * jx, uy = inv * jy;
+
+        AT w = tau0;
+        if (KOMEGA) {
+            AT om = AT(oin[j]), kv = AT(kin[j]);
+            const AT yv = AT(win[j]);
+            const long long node = rowoff + x0 + j;
+            if (om < AT(0)) { om = fabs(om); p.O[node] = (float)om; }
+            if (kv < AT(0)) { kv = AT(1e-16); p.K[node] = 1e-16f; }
+            const AT a = AT(2) * sqrt(kv) / (AT(KO_BETA_STAR) * om * yv);
+            const AT b = AT(500) * mu / (yv * yv * om);
+            const AT arg = amax(a, b);
+            AT F2 = tanh(arg * arg);
+            const AT sxx = AT(sin3[0][j]), sxy = AT(sin3[1][j]), syy = AT(sin3[2][j]);
+            F2 *= sqrt(AT(2) * (sxx * sxx + AT(2) * sxy * sxy + syy * syy));
+            const AT nut = amax(amin(AT(p.maxnut), AT(KO_A1) * kv / amax(AT(KO_A1) * om, F2)),
+                                AT(1e-16));
+            o_nut[j] = (float)nut;
+            w = AT(1) / (AT(3) * (nut + mu) + AT(0.5));
+        }
+        AT sxx_n = AT(0), sxy_n = AT(0), syy_n = AT(0);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const int cx = cx_of(q), cy = cy_of(q);
+            const AT px0 = phi0<AT>(cx), py0 = phi0<AT>(cy);
+            const AT dpx = dphi<AT>(cx, ux), dpy = dphi<AT>(cy, uy);
+            const AT phy = py0 + dpy;
+            const AT feqdev = drho * (px0 + dpx) * phy + (dpx * py0 + px0 * dpy + dpx * dpy);
+            const AT neq = d[q][j] - feqdev;
+            if (KOMEGA) {
+                if (cx != 0) sxx_n += neq;
+                if (cy != 0) syy_n += neq;
+                if (cx * cy == 1) sxy_n += neq;
+                if (cx * cy == -1) sxy_n -= neq;
+            }
+            d[q][j] = d[q][j] - w * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
+        }
+        if (KOMEGA) {
+            const AT s = AT(-1.5) * tau0 / rho;
+            o_s[0][j] = (float)(s * sxx_n);
+            o_s[1][j] = (float)(s * sxy_n);
+            o_s[2][j] = (float)(s * syy_n);
+        }
+        o_rho[j] = (float)rho;
+        o_ux[j] = (float)(ux + fterm / AT(2));
+        o_uy[j] = (float)uy;
+        bsum_rho += (double)rho;
+        bsum_ux += (double)(ux + fterm / AT(2));
+        bsum_uy += (double)uy;
+    }
+
+    // ---- stores -----------------------------------------------------------------
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = (float)d[q][j];
+        Store<ST>::store4(gout + q * D + rowoff + x0, v);
+    }
+    if (p.options & OPTION_SAVE_MACRO_FIELDS) {
+        *reinterpret_cast<float4*>(p.rho + rowoff + x0) = make_float4(o_rho[0], o_rho[1], o_rho[2], o_rho[3]);
+        *reinterpret_cast<float4*>(p.ux + rowoff + x0) = make_float4(o_ux[0], o_ux[1], o_ux[2], o_ux[3]);
+        *reinterpret_cast<float4*>(p.uy + rowoff + x0) = make_float4(o_uy[0], o_uy[1], o_uy[2], o_uy[3]);
+    }
+    if (KOMEGA) {
+        *reinterpret_cast<float4*>(p.nut + rowoff + x0) = make_float4(o_nut[0], o_nut[1], o_nut[2], o_nut[3]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            *reinterpret_cast<float4*>(p.S + c * D + rowoff + x0) =
+                make_float4(o_s[c][0], o_s[c][1], o_s[c][2], o_s[c][3]);
+    }
+
+    // ---- per-block FP64 partial sums of rho, ux, uy ----------------------------
+    if (slot) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            bsum_rho += __shfl_down_sync(0xffffffffu, bsum_rho, off);
+            bsum_ux += __shfl_down_sync(0xffffffffu, bsum_ux, off);
+            bsum_uy += __shfl_down_sync(0xffffffffu, bsum_uy, off);
+        }
+        if (lane == 0) { slot[0] = bsum_rho; slot[1] = bsum_ux; slot[2] = bsum_uy; }
+    }
+}
+
+}  // namespace kofm

@@ -1,0 +1,131 @@
+"""Python handle on one kofm context (one lattice on one GPU).
+
+A thin wrapper over the C ABI (include/kofm.h): numpy arrays in the
+reference's padded FP64 layout go in and out; the state lives on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import KofmDesc, KofmStats, check
+
+_dp = C.POINTER(C.c_double)
+
+
+def _ptr(a, ctype=C.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def desc_default() -> KofmDesc:
+    lib = _abi.load()
+    d = KofmDesc()
+    check("kofm_desc_default", lib.kofm_desc_default(C.byref(d)))
+    return d
+
+
+class Lattice:
+    """Device-resident D2Q9 (+ k-omega) lattice driven through the C ABI."""
+
+    def __init__(self, desc: KofmDesc):
+        self.lib = _abi.load()
+        self.desc = desc
+        self._ctx = C.c_void_p()
+        check("kofm_create", self.lib.kofm_create(C.byref(desc), C.byref(self._ctx)))
+        self.nxf, self.ny = desc.nx_full, desc.ny
+        self.n = self.nxf * self.ny
+
+    # -- lifecycle ------------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self.lib.kofm_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- geometry / state ---------------------------------------------------------
+    def set_geometry(self, ntype, wallD=None, dX=None, ibb_idx=None, ibb_q=None):
+        ntype = np.ascontiguousarray(ntype, np.int16)
+        wallD = None if wallD is None else np.ascontiguousarray(wallD, np.float64)
+        dX = None if dX is None else np.ascontiguousarray(dX, np.float64)
+        n_ibb = 0 if ibb_idx is None else len(ibb_idx)
+        ii = None if ibb_idx is None else np.ascontiguousarray(ibb_idx, np.int32)
+        qq = None if ibb_q is None else np.ascontiguousarray(ibb_q, np.float64)
+        check("kofm_set_geometry", self.lib.kofm_set_geometry(
+            self._ctx, _ptr(ntype, C.c_int16), _ptr(wallD), _ptr(dX),
+            _ptr(ii, C.c_int32), _ptr(qq), n_ibb))
+
+    def set_state(self, f, k=None, omega=None, nut=None, sxy=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64)
+                for a in (f, k, omega, nut, sxy)]
+        check("kofm_set_state", self.lib.kofm_set_state(self._ctx, *[_ptr(a) for a in arrs]))
+
+    def get_state(self):
+        f = np.empty(9 * self.n)
+        if self.desc.use_komega:
+            k, o, nut, s = np.empty(self.n), np.empty(self.n), np.empty(self.n), np.empty(3 * self.n)
+        else:
+            k = o = nut = s = None
+        check("kofm_get_state", self.lib.kofm_get_state(
+            self._ctx, _ptr(f), _ptr(k), _ptr(o), _ptr(nut), _ptr(s)))
+        return f, k, o, nut, s
+
+    def get_macro(self):
+        rho, ux, uy = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        check("kofm_get_macro", self.lib.kofm_get_macro(self._ctx, _ptr(rho), _ptr(ux), _ptr(uy)))
+        return rho, ux, uy
+
+    # -- stepping -------------------------------------------------------------------
+    def lb_step(self, options=_abi.OPTION_SAVE_MACRO_FIELDS):
+        check("kofm_lb_step", self.lib.kofm_lb_step(self._ctx, options))
+
+    def komega_assemble(self, dt=1.0):
+        check("kofm_komega_assemble", self.lib.kofm_komega_assemble(self._ctx, dt))
+
+    def komega_solve(self, raise_on_error=True):
+        it = (C.c_int32 * 2)()
+        rr = (C.c_double * 2)()
+        st = self.lib.kofm_komega_solve(self._ctx, it, rr)
+        if raise_on_error:
+            check("kofm_komega_solve", st)
+        return st, (it[0], it[1]), (rr[0], rr[1])
+
+    def komega_update(self):
+        check("kofm_komega_update", self.lib.kofm_komega_update(self._ctx))
+
+    def step(self, nsteps=1, options=_abi.OPTION_SAVE_MACRO_FIELDS):
+        check("kofm_step", self.lib.kofm_step(self._ctx, nsteps, options))
+
+    def sync(self):
+        check("kofm_sync", self.lib.kofm_sync(self._ctx))
+
+    def reduce(self, field, op=_abi.OP_SUM) -> float:
+        out = C.c_double()
+        check("kofm_reduce", self.lib.kofm_reduce(self._ctx, field, op, C.byref(out)))
+        return out.value
+
+    def stats(self) -> KofmStats:
+        s = KofmStats()
+        check("kofm_get_stats", self.lib.kofm_get_stats(self._ctx, C.byref(s)))
+        return s
+
+    def debug_barrier_timeout(self, spin_limit: int) -> int:
+        return self.lib.kofm_debug_barrier_timeout(self._ctx, spin_limit)
+
+    @property
+    def stream(self) -> int:
+        return self.lib.kofm_stream(self._ctx) or 0

@@ -583,6 +583,9 @@ void orc_komega_solve(const orc_cfg* c, orc_komega_state* s,
         orc_gmres_solve(n, IA, JA, kA, kb, K, 10, s->max_iters, s->rel_tol,
                         s->abs_tol, &s->last_k);
         if (s->last_k.nan) orc_halve(s, &cur);
+        /* A NaN that persists halves dt without end in the reference (the
+         * state is not restored); stop at 2^20 sub-steps, as the product does. */
+        if (s->steps_per_lb > (1 << 20)) break;
         cur++;
     }
 }

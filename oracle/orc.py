@@ -32,13 +32,9 @@ SOLID_BOUNDARY = 0x0010
 NESW_BOUNDARY = 0x0F00
 
 
-def build(force: bool = False) -> None:
-    """Build liboracle.so and (when the reference tree is mounted) _ref."""
-    if force or not os.path.exists(LIB_ORACLE) or (
-        os.path.exists(os.path.join(HERE, "..", "..", "reference"))
-    ):
-        pass
-    subprocess.run(["make", "-s", "-C", HERE, "CXX=g++", "CC=gcc"], check=True)
+def build() -> None:
+    """Builds liboracle.so and, when the reference tree is mounted, _ref."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
 class _Cfg(C.Structure):
@@ -148,3 +144,63 @@ class RefKernels:
     @staticmethod
     def available(path: str = LIB_REF) -> bool:
         return os.path.exists(path)
+
+
+class OracleSim:
+    """FP64 CPU run of the reference step loop (Solve_no_TR, LBLS.cpp:185-205):
+    collide + push (LB_collision_SRT_Fluid[_w_kOmega]), lbIBB, then
+    kOmega::Solve (diffusivities, coefficients, GMRES for omega then k).
+
+    State arrays use the reference layout; ``f`` is the FA buffer."""
+
+    def __init__(self, orc: Oracle, cfg, ntype, dX, wallD, f, k=None, omega=None,
+                 nut=None, sxy=None, komega=False, ibb_idx=None, ibb_q=None,
+                 max_iters=1000, rel_tol=1e-4, abs_tol=1e-7, dt=1.0):
+        self.o, self.cfg, self.komega = orc, cfg, komega
+        n = cfg.nxf * cfg.ny
+        self.n = n
+        self.m = np.ascontiguousarray(ntype, np.int16)
+        self.dX = np.ascontiguousarray(dX, np.float64)
+        self.wallD = np.ascontiguousarray(wallD, np.float64)
+        self.FA = np.ascontiguousarray(f, np.float64).copy()
+        self.FB = np.zeros_like(self.FA)
+        self.rho, self.ux, self.uy = np.zeros(n), np.zeros(n), np.zeros(n)
+        z = np.zeros(n)
+        self.K = z.copy() if k is None else np.array(k, np.float64)
+        self.O = z.copy() if omega is None else np.array(omega, np.float64)
+        self.nut = z.copy() if nut is None else np.array(nut, np.float64)
+        self.S = np.zeros(3 * n) if sxy is None else np.array(sxy, np.float64)
+        self.ibb_idx = np.zeros(0, np.int32) if ibb_idx is None else np.ascontiguousarray(ibb_idx, np.int32)
+        self.ibb_q = np.zeros(0) if ibb_q is None else np.ascontiguousarray(ibb_q, np.float64)
+        if komega:
+            self.IA, self.JA, self.ind = orc.csr(cfg, self.m)
+            nnz = len(self.JA)
+            self.kA, self.oA = np.zeros(nnz), np.zeros(nnz)
+            orc.L.orc_csr_fill_solid_boundary(C.byref(cfg), self.m, self.ind, self.kA)
+            orc.L.orc_csr_fill_solid_boundary(C.byref(cfg), self.m, self.ind, self.oA)
+            self.kb, self.ob = np.zeros(n), np.zeros(n)
+            self.Dk = np.where((self.m & M_FLUID) != 0, cfg.mu, 0.0)
+            self.Do = self.Dk.copy()
+            self.F1 = np.zeros(n)
+            self.dkdo = np.zeros(2 * n)
+            self.kst = KOmegaState(1, 0, dt, max_iters, rel_tol, abs_tol)
+
+    def step(self, nsteps=1, options=OPTION_SAVE_MACRO_FIELDS):
+        L, cp = self.o.L, C.byref(self.cfg)
+        opt = options | (OPTION_SAVE_MACRO_FIELDS if self.komega else 0)
+        for _ in range(nsteps):
+            L.orc_collide_push(cp, self.FA, self.FB, self.m, self.rho, self.ux, self.uy,
+                               self.K, self.O, self.wallD, self.nut, self.S, opt,
+                               1 if self.komega else 0)
+            if len(self.ibb_idx):
+                L.orc_ibb(cp, self.ibb_idx, self.ibb_q, self.FB, len(self.ibb_idx))
+            self.FA, self.FB = self.FB, self.FA
+            if self.komega:
+                self.komega_solve()
+
+    def komega_solve(self):
+        L, cp = self.o.L, C.byref(self.cfg)
+        L.orc_komega_solve(cp, C.byref(self.kst), self.m, self.IA, self.JA, self.ind,
+                           self.K, self.O, self.nut, self.wallD, self.rho, self.ux,
+                           self.uy, self.S, self.dX, self.Dk, self.Do, self.F1,
+                           self.dkdo, self.kA, self.oA, self.kb, self.ob)

@@ -1,0 +1,41 @@
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) and libkofm.so")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    """The FP64 CPU restatement (built on demand; test infrastructure only)."""
+    from oracle.orc import LIB_ORACLE, Oracle
+    if not os.path.exists(LIB_ORACLE):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True)
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def refk():
+    """The reference's own kernels compiled for the CPU (oracle/_ref)."""
+    from oracle.orc import LIB_REF, RefKernels
+    if not os.path.exists(LIB_REF):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False)
+    if not os.path.exists(LIB_REF):
+        pytest.skip("oracle/_ref not built (reference tree absent); golden fixtures cover the pin")
+    return RefKernels()
+
+
+@pytest.fixture(scope="session")
+def kofm_lib():
+    from komegafoulingmodel_b200 import build
+    build.build()
+    from komegafoulingmodel_b200 import _abi
+    return _abi.load()

@@ -1,0 +1,110 @@
+"""GPU parity of the k-omega path (collide with nu_t, fused assembly, the
+device-resident GMRES for omega and k) against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+from komegafoulingmodel_b200 import geometry as G
+from oracle.orc import OracleSim, make_cfg
+from tests.cases import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def channel_case(nx=256, ny=66, u_max=0.05, nu=5e-4):
+    """Straight k-omega channel: parabolic start, body force from Re on the
+    half-height (clVariablesLB.cpp:584-600), k and omega from the inlet
+    turbulence intensity of 5% and a length scale 0.07 H."""
+    ch = G.straight_channel(nx, ny)
+    R = ch.pipe_radius
+    y = np.arange(ny)[:, None] - 0.5
+    ux = np.clip(u_max * (1 - ((y - R) / R) ** 2), 0, None) * np.ones((1, nx))
+    f = G.equilibrium_state(ch, ux=ux)
+    re = (2.0 / 3.0) * u_max * R / nu
+    g = G.force_from_re(re, nu, R)
+    k0 = 1.5 * (0.05 * u_max) ** 2
+    o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * 2 * R)
+    k, o, nut = G.komega_fields(ch, k0, o0)
+    rate = 1.0 / (3 * nu + 0.5)
+    return ch, f, k, o, nut, rate, g, nu
+
+
+def make_lattice(ch, rate, g, nu, krylov=10):
+    d = desc_default()
+    d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
+    d.tau, d.fterm, d.mu = rate, g, nu
+    d.use_komega = 1
+    d.krylov_dim = krylov
+    L = Lattice(d)
+    L.set_geometry(ch.ntype, ch.wallD, ch.dX)
+    return L
+
+
+def test_one_update_matches_oracle(kofm_lib, oracle):
+    ch, f, k, o, nut, rate, g, nu = channel_case(nx=128, ny=34)
+    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
+    sim.step(2)
+    with make_lattice(ch, rate, g, nu) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        L.step(2)
+        st = L.stats()
+        _, k2, o2, nut2, s2 = L.get_state()
+    fl = ch.fluid_mask().ravel()
+    assert (st.omega_iters, st.k_iters) == (sim.kst.last_o.iters, sim.kst.last_k.iters)
+    assert rel_l2(k2, sim.K, fl) < 1e-6
+    assert rel_l2(o2, sim.O, fl) < 1e-6
+    assert rel_l2(nut2, sim.nut, fl) < 1e-6
+
+
+def test_channel_1000_steps_parity(kofm_lib, oracle):
+    """rho, u, k, omega within rel-L2 1e-5 of the FP64 oracle after 1000 steps."""
+    ch, f, k, o, nut, rate, g, nu = channel_case()
+    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
+    sim.step(1000)
+    with make_lattice(ch, rate, g, nu) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        L.step(1000)
+        rho, ux, uy = L.get_macro()
+        _, k2, o2, _, _ = L.get_state()
+    fl = ch.fluid_mask().ravel()
+    errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl),
+                uy=rel_l2(uy, sim.uy, fl), k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
+    print(errs)
+    for key in ("rho", "ux", "k", "omega"):
+        assert errs[key] < 1e-5, errs
+
+
+def test_barrier_timeout_is_reported_and_context_survives(kofm_lib):
+    """A grid barrier that can never complete ends by its spin bound with
+    KOFM_ERR_TIMEOUT; the fields are unchanged and the context still works."""
+    ch, f, k, o, nut, rate, g, nu = channel_case(nx=128, ny=34)
+    with make_lattice(ch, rate, g, nu) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        L.lb_step()
+        L.komega_assemble(1.0)
+        _, k_before, o_before, _, _ = L.get_state()
+        assert L.debug_barrier_timeout(2000) == _abi.ERR_TIMEOUT
+        _, k_after, o_after, _, _ = L.get_state()
+        assert np.array_equal(k_before, k_after) and np.array_equal(o_before, o_after)
+        st, iters, rel = L.komega_solve(raise_on_error=False)
+        assert st == 0 and iters[0] > 0 and iters[1] > 0
+
+
+def test_wall_shear_and_turbulence_reductions(kofm_lib):
+    ch, f, k, o, nut, rate, g, nu = channel_case(nx=128, ny=34)
+    with make_lattice(ch, rate, g, nu) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        L.step(5)
+        _, k2, o2, nut2, s2 = L.get_state()
+        rho, _, _ = L.get_macro()
+        ks = L.reduce(_abi.FIELD_K)
+        omin = L.reduce(_abi.FIELD_OMEGA, _abi.OP_MIN)
+        tw = L.reduce(_abi.FIELD_WALL_SHEAR)
+    assert abs(ks - np.sum(np.float32(k2))) <= 1e-6 * abs(ks)
+    assert omin == pytest.approx(np.min(np.float32(o2)), rel=1e-7)
+    t = (ch.ntype.astype(np.int32) & 0xFFFF)
+    wall = ((t & 0x0C00) != 0) & ((t & 1) == 0)
+    ref = np.sum(rho[wall] * (nu + nut2[wall]) * 2 * np.abs(s2[ch.n:2 * ch.n][wall]))
+    assert tw == pytest.approx(ref, rel=1e-6)
