@@ -73,6 +73,29 @@ __device__ __forceinline__ void fd_weights(double dpos, double dneg, Fd3& d1, Fd
     d2.c = -2. / (a * b);
 }
 
+// Weights for unit link fractions (every node without an E/W/N/S wall link):
+// d1 = (1/2, -1/2, 0), d2 = (1, 1, -2), exactly what fd_weights(1, 1) gives.
+__device__ __forceinline__ void fd_unit(Fd3& d1, Fd3& d2) {
+    d1.e = 0.5; d1.w = -0.5; d1.c = 0.0;
+    d2.e = 1.0; d2.w = 1.0; d2.c = -2.0;
+}
+
+// Weights of one node: constants unless it has a dX record.
+__device__ __forceinline__ void node_weights(const AsmParams& p, int t, long long g, Fd3& X,
+                                             Fd3& X2, Fd3& Y, Fd3& Y2) {
+    if (t & NESW_BOUNDARY) {
+        const int r = p.dxidx[g];
+        if (r >= 0) {
+            const DxRecord rec = p.dxrec[r];
+            fd_weights(rec.dx[0], rec.dx[1], X, X2);
+            fd_weights(rec.dx[2], rec.dx[3], Y, Y2);
+            return;
+        }
+    }
+    fd_unit(X, X2);
+    fd_unit(Y, Y2);
+}
+
 __device__ __forceinline__ double dmaxr(double a, double b) { return a < b ? b : a; }
 __device__ __forceinline__ double dminr(double a, double b) { return b < a ? b : a; }
 
@@ -120,17 +143,8 @@ komega_assemble_kernel(const AsmParams p) {
             const long long g = (long long)gy * P + gx;
             const int t = (uint16_t)p.ntype[g];
             if (!(t & M_SOLID)) {
-                double dxe = 1.0, dxw = 1.0, dyn = 1.0, dys = 1.0;
-                if (t & NESW_BOUNDARY) {
-                    const int r = p.dxidx[g];
-                    if (r >= 0) {
-                        const DxRecord rec = p.dxrec[r];
-                        dxe = rec.dx[0]; dxw = rec.dx[1]; dyn = rec.dx[2]; dys = rec.dx[3];
-                    }
-                }
                 Fd3 X, Y, X2, Y2;
-                fd_weights(dxe, dxw, X, X2);
-                fd_weights(dyn, dys, Y, Y2);
+                node_weights(p, t, g, X, X2, Y, Y2);
                 const int sy = ry + 1, sx = rx + 1;  // position in the 2-ring tile
                 const double om = sO[sy][sx], kv = sK[sy][sx];
                 const double yv = p.wallD[g];
@@ -171,17 +185,8 @@ komega_assemble_kernel(const AsmParams p) {
         p.rhs_k[g] = 0.0;
         return;
     }
-    double dxe = 1.0, dxw = 1.0, dyn = 1.0, dys = 1.0;
-    if (t & NESW_BOUNDARY) {
-        const int r = p.dxidx[g];
-        if (r >= 0) {
-            const DxRecord rec = p.dxrec[r];
-            dxe = rec.dx[0]; dxw = rec.dx[1]; dyn = rec.dx[2]; dys = rec.dx[3];
-        }
-    }
     Fd3 X, Y, X2, Y2;
-    fd_weights(dxe, dxw, X, X2);
-    fd_weights(dyn, dys, Y, Y2);
+    node_weights(p, t, g, X, X2, Y, Y2);
     const int ry = ty + 1, rx = tx + 1;
     const double dk = sDk[ry][rx], dom = sDo[ry][rx];
     const double dk_dx = X.e * sDk[ry][rx + 1] + X.w * sDk[ry][rx - 1] + X.c * dk;
