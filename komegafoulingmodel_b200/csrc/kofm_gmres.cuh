@@ -283,7 +283,7 @@ __device__ __forceinline__ bool is_fluid(const int16_t* nt, long long g) {
 // ---- shared tile of one Krylov pass -------------------------------------------
 struct KTile {
     double U1[R2H][R2W];        // stencil input u_{k-1} (or r) on the 2-ring
-    float C[4][R1H][R1W];       // coefficients E, W, N, S on the 1-ring
+    double C[4][R1H][R1W];      // coefficients E, W, N, S on the 1-ring
     double UK[R1H][R1W];        // u_k on the 1-ring
     unsigned char F[R2H][R2W];  // fluid flags on the 2-ring
     double g[KOFM_MAX_KRYLOV];  // h_j s_j
@@ -336,7 +336,7 @@ __device__ __forceinline__ void krylov_tile(const GmresArgs& a, const KoSystem& 
         const int ry = p / R1W, rx = p % R1W;
         const int gy = y0 - 1 + ry;
         const int gx = wrap_mod(x0 - 1 + rx, nx);
-        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
         if (T.F[ry + 1][rx + 1]) {
             const long long g = (long long)gy * P + gx;
             c0 = __ldg(S.coef + g);

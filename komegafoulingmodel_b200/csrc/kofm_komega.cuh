@@ -22,11 +22,14 @@ namespace kofm {
 
 constexpr int KO_TX = 32, KO_TY = 8;
 
-// One implicit system (index 0: omega, 1: k) as the solver sees it.  Vectors
-// that every Krylov pass streams are stored in FP32 (all arithmetic is FP64);
-// the accumulated correction x stays FP64.
+// One implicit system (index 0: omega, 1: k) as the solver sees it.  The
+// matrix stays FP64: an FP32-rounded operator would perturb every implicit
+// update by ~1e-8 relative, and that bias accumulates over the time steps.
+// Krylov basis, residual and right-hand side only carry the per-step
+// increment, so they are FP32 (all arithmetic is FP64); the accumulated
+// correction x stays FP64.
 struct KoSystem {
-    float* coef = nullptr;   // [4][D] normalised off-diagonals E, W, N, S
+    double* coef = nullptr;  // [4][D] normalised off-diagonals E, W, N, S
     float* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
     float* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
@@ -45,9 +48,9 @@ struct AsmParams {
     const float* ux;
     const float* uy;
     const float* S;
-    float* coef_o;
+    double* coef_o;
     float* rhs_o;
-    float* coef_k;
+    double* coef_k;
     float* rhs_k;
     int nx, ny, P;
     long long D;
@@ -182,7 +185,7 @@ komega_assemble_kernel(const AsmParams p) {
     const long long D = p.D;
     const int t = (uint16_t)p.ntype[g];
     if (t & M_SOLID) {
-        for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.f; p.coef_k[c * D + g] = 0.f; }
+        for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
         p.rhs_o[g] = 0.f;
         p.rhs_k[g] = 0.f;
         return;
@@ -242,10 +245,8 @@ komega_assemble_kernel(const AsmParams p) {
     const double oS = sO[sy - 1][sx], oW = sO[sy][sx - 1], oE = sO[sy][sx + 1], oN = sO[sy + 1][sx];
     const double Axk = Ks * kS + Kw * kW + Kraw + Ke * kE + Kn * kN;
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
-    p.coef_o[g] = (float)We; p.coef_o[D + g] = (float)Ww;
-    p.coef_o[2 * D + g] = (float)Wn; p.coef_o[3 * D + g] = (float)Ws;
-    p.coef_k[g] = (float)Ke; p.coef_k[D + g] = (float)Kw;
-    p.coef_k[2 * D + g] = (float)Kn; p.coef_k[3 * D + g] = (float)Ks;
+    p.coef_o[g] = We; p.coef_o[D + g] = Ww; p.coef_o[2 * D + g] = Wn; p.coef_o[3 * D + g] = Ws;
+    p.coef_k[g] = Ke; p.coef_k[D + g] = Kw; p.coef_k[2 * D + g] = Kn; p.coef_k[3 * D + g] = Ks;
     p.rhs_o[g] = (float)(Wsrc - Axo);
     p.rhs_k[g] = (float)(Ksrc - Axk);
 }

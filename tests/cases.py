@@ -36,3 +36,16 @@ def rel_l2(a, b, mask=None):
         a, b = a[mask], b[mask]
     den = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def fp32_state(f, *fields):
+    """The state as the FP32 device form holds it: populations rounded as
+    deviations f - w, scalar fields rounded to FP32 (so the oracle starts
+    from exactly the GPU's stored state)."""
+    from komegafoulingmodel_b200 import geometry as G
+    n = len(f) // 9
+    w = np.repeat(G.W, n)
+    out = [(f - w).astype(np.float32).astype(np.float64) + w]
+    for a in fields:
+        out.append(None if a is None else np.asarray(a).astype(np.float32).astype(np.float64))
+    return out

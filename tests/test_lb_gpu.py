@@ -10,7 +10,7 @@ import pytest
 from komegafoulingmodel_b200 import Lattice, _abi, desc_default
 from komegafoulingmodel_b200 import geometry as G
 from oracle.orc import OracleSim, make_cfg
-from tests.cases import komega_state, perturbed_state, rel_l2
+from tests.cases import fp32_state, komega_state, perturbed_state, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -57,7 +57,7 @@ def test_state_round_trip_phase0(kofm_lib):
 def test_laminar_steps_match_oracle(kofm_lib, oracle, nsteps):
     nx, ny = 128, 20
     ch = G.straight_channel(nx, ny)
-    f = perturbed_state(ch, seed=2)
+    (f,) = fp32_state(perturbed_state(ch, seed=2))
     cfg = make_cfg(nx, ny, 1.25, 1e-5, 0.1)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f)
     sim.step(nsteps)
@@ -85,6 +85,7 @@ def test_komega_collide_matches_oracle(kofm_lib, oracle):
     idx = np.nonzero(fl)[0]
     k[idx[:4]] *= -1.0
     o[idx[10:13]] *= -1.0
+    f, k, o, nut, s = fp32_state(f, k, o, nut, s)
     cfg = make_cfg(nx, ny, 1.9, 1e-6, 0.01)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, s, komega=True)
     import ctypes as C
