@@ -54,6 +54,7 @@ extern "C" {
 #define KOFM_ERR_NAN -203                 /* NaN residual; dt halving engaged */
 #define KOFM_ERR_TIMEOUT -204             /* a bounded device wait expired */
 #define KOFM_ERR_STATE -205               /* call order: geometry/state not set */
+#define KOFM_ERR_TOO_LARGE -206           /* input beyond a fixed scratch limit */
 
 /* ---- options (Kernels/Heading.cl:309-311) -------------------------------- */
 #define KOFM_OPTION_SAVE_MACRO_FIELDS 0x2 /* write rho, ux, uy this step */
@@ -202,6 +203,28 @@ int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);
  * about 100 ns).  Returns KOFM_ERR_TIMEOUT with the context still usable and
  * the fields unchanged.  No counterpart in the reference. */
 int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
+
+/* ---- reduction without device allocation ---------------------------------
+ * No counterpart in the reference.  For callers that must not let the library
+ * allocate device memory (an application that owns a fixed device-memory
+ * budget and serves every buffer from its own pool, or a latency-critical
+ * caller that cannot accept an allocation's implicit device synchronisation).
+ * Reduces (KOFM_OP_SUM / MIN / MAX, FP64 accumulation, deterministic order) a
+ * device FP32 field of ny rows of `pitch` floats, counting the first `ncols`
+ * columns of each row, into *out (one double in device memory), on `stream`.
+ * Both buffers belong to the caller.  The only scratch is a fixed array of
+ * KOFM_NOALLOC_MAX_PARTIALS doubles (32 KiB) inside the library, kept by every
+ * device that loads it until the process exits: one partial per
+ * KOFM_NOALLOC_CHUNK nodes, so pitch*ny may not exceed KOFM_NOALLOC_MAX_NODES
+ * (KOFM_ERR_TOO_LARGE otherwise).  All calls share that array: calls that
+ * overlap on the GPU race.  Each call overwrites the partials it uses.  The
+ * first call on a device resolves the array's address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture. */
+#define KOFM_NOALLOC_MAX_PARTIALS 4096
+#define KOFM_NOALLOC_CHUNK 65536
+#define KOFM_NOALLOC_MAX_NODES (4096LL * 65536LL)
+int kofm_reduce_field_noalloc(const float* field, int32_t ncols, int32_t pitch, int32_t ny,
+                              int32_t op, double* out, void* stream);
 
 /* The CUDA stream the context enqueues on (cudaStream_t as void*), for
  * callers that order their own work against it. */

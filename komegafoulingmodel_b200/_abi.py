@@ -18,7 +18,10 @@ ERRORS = {
     -110: "LOADING_PARAMS", -111: "INITIALIZING_KOMEGA", -112: "INITIALIZING_VLS",
     -120: "INITIALIZING_VLB", -200: "INVALID_ARG", -201: "NO_DEVICE",
     -202: "NOT_CONVERGED", -203: "NAN", -204: "TIMEOUT", -205: "STATE",
+    -206: "TOO_LARGE",
 }
+ERR_TOO_LARGE = -206
+NOALLOC_MAX_NODES = 4096 * 65536
 ERR_NOT_CONVERGED = -202
 ERR_NAN = -203
 ERR_TIMEOUT = -204
@@ -79,6 +82,8 @@ SIGNATURES = {
     "kofm_get_stats": (C.c_int, [_vp, C.POINTER(KofmStats)]),
     "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
     "kofm_stream": (_vp, [_vp]),
+    "kofm_reduce_field_noalloc": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                            _vp, _vp]),
 }
 
 _LIB = None

@@ -321,6 +321,7 @@ const char* kofm_error_string(int s) {
         case KOFM_ERR_NAN: return "NaN residual in the k-omega solve (dt halved)";
         case KOFM_ERR_TIMEOUT: return "bounded device wait expired";
         case KOFM_ERR_STATE: return "geometry or state not set";
+        case KOFM_ERR_TOO_LARGE: return "input larger than the fixed scratch allows";
         default: return "unknown status";
     }
 }
