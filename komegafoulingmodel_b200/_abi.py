@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libkofm.so")
+# KOFM_LIBRARY selects another build of the same ABI (e.g. a differently
+# configured libkofm.so); the default is the in-tree build.
+LIB_PATH = os.environ.get("KOFM_LIBRARY") or os.path.join(HERE, "libkofm.so")
 
 KOFM_OK = 0
 ERRORS = {

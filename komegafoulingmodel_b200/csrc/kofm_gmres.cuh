@@ -13,18 +13,17 @@
 //    k are independent in the reference, kOmega.cpp:68-70) with no host
 //    round-trip; the reference needs >= 4 blocking host synchronisations and
 //    ~40 kernel launches per restart.
-//  * One fused sweep per Krylov vector.  For vector k a block stages, for a
-//    64x8 tile, u_{k-1} on a 2-node ring and the stencil coefficients on a
-//    1-node ring in shared memory, recomputes z_k = A u_{k-1} on the 1-ring,
-//    orthogonalises u_k = s_{k-1} z_k - sum_j h_j s_j u_j there (classical
-//    Gram-Schmidt, the reference's order), writes u_k, and applies the
-//    stencil once more to get w = A u_k for the NEXT vector's Gram-Schmidt
-//    dot products -- so each vector costs one sweep and one grid barrier
-//    instead of the reference's product / two Gram-Schmidt stages / normalise.
+//  * One fused sweep per Krylov vector.  A block marches down a strip of
+//    columns keeping rolling rows of u_{k-1} and u_k in shared memory; per
+//    row it recomputes z_k = A u_{k-1}, orthogonalises
+//    u_k = s_{k-1} z_k - sum_j h_j s_j u_j (classical Gram-Schmidt, the
+//    reference's order), writes u_k, and one row behind applies the stencil
+//    to u_k to get w = A u_k for the NEXT vector's Gram-Schmidt dot
+//    products -- so each vector costs one sweep and one grid barrier instead
+//    of the reference's product / two Gram-Schmidt stages / normalise.
 //    Krylov vectors are kept un-normalised; the scales 1/||u_j|| are applied
-//    lazily in FP64.
-//  * Streamed vectors (basis, residual, coefficients, right-hand side) are
-//    FP32 in HBM; every product and dot product is FP64.
+//    lazily.  Vectors and matrix are FP64 (an FP32 basis stalls the first
+//    cycle near 1e-5 relative residual on the omega wall rows).
 //  * Dot products are reduced per block and combined, in a fixed order, by
 //    the last block to reach the grid barrier, which also runs the scalar
 //    logic (the reference's host code) before releasing the grid.  The
@@ -40,12 +39,12 @@
 
 namespace kofm {
 
-constexpr int GM_THREADS = 256;
+constexpr int GM_THREADS = 128;
+#ifndef KOFM_GM_MINBLOCKS
+#define KOFM_GM_MINBLOCKS 6  // resident blocks per SM the register budget targets
+#endif
 constexpr int GM_SLOTS = 32;                    // partial-sum slots per block
 constexpr int GM_SYS_SLOTS = 16;                // per system
-constexpr int TW = 64, TH = 8;                  // tile
-constexpr int R1W = TW + 2, R1H = TH + 2;       // tile + 1-node ring
-constexpr int R2W = TW + 4, R2H = TH + 4;       // tile + 2-node ring
 
 struct GmresSys {
     int active;     // still iterating this restart
@@ -90,7 +89,7 @@ struct GmresArgs {
     int max_restarts;
     double rel_tol, abs_tol;
     long long spin_limit;     // barrier spin bound (polls of >= 100 ns)
-    int tiles_x, tiles_y;
+    int strips, chunks, chunk_rows;  // row-streaming work units
 };
 
 // ---- coherent access to data written inside the launch (bypass L1) --------
@@ -108,6 +107,22 @@ __device__ void sys_store(GmresSys* dst, const GmresSys& src) {
     unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
     for (int i = 0; i < (int)(sizeof(GmresSys) / 8); ++i) __stcg(d + i, s[i]);
 }
+
+// pair loads / stores of solver vectors (FP32 or FP64 storage, FP64 values)
+__device__ __forceinline__ double2 ldvec2(const float* p) {
+    const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+    return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ double2 ldvec2(const double* p) {
+    return __ldcg(reinterpret_cast<const double2*>(p));
+}
+__device__ __forceinline__ void stvec2(float* p, double a, double b) {
+    __stcg(reinterpret_cast<float2*>(p), make_float2((float)a, (float)b));
+}
+__device__ __forceinline__ void stvec2(double* p, double a, double b) {
+    __stcg(reinterpret_cast<double2*>(p), make_double2(a, b));
+}
+__device__ __forceinline__ double rnd(double v) { return (double)(vec_t)v; }
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     unsigned int v;
@@ -271,142 +286,146 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
     return ldc(&a.ctl->error) == 0;
 }
 
+// ---- row-streaming Krylov pass ----------------------------------------------
+// A work unit is a strip of RS_W columns times a chunk of rows.  One thread
+// owns one column of the strip (the edge threads also the column just outside
+// it) and the block marches down the rows keeping a rolling window of the
+// last four rows of u_{k-1} (or r) and of u_k in shared memory:
+//   row y:   load u_{k-1}(y+1); u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j
+//            on the strip plus one column each side; store u_k(y);
+//   row y-1: w = A u_k on the strip -> dot products <w, u_j>.
+// Every array is read once from HBM per pass; the only repeated reads are the
+// two rows above and below each chunk and the columns beside each strip.
+constexpr int RS_W = GM_THREADS;
+
+struct RowWin {
+    double U1[4][RS_W + 4];         // rows of u_{k-1} (or r); column c <-> x0 - 2 + c
+    double UK[4][RS_W + 2];         // rows of u_k;             column c <-> x0 - 1 + c
+    unsigned char F[4][RS_W + 4];   // fluid flags of the U1 rows
+    double g[KOFM_MAX_KRYLOV];      // h_j s_j
+    double sk1;                     // s_{k-1}
+};
+
 __device__ __forceinline__ int wrap_mod(int x, int n) {
     int r = x % n;
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ bool is_fluid(const int16_t* nt, long long g) {
-    return !((uint16_t)nt[g] & M_SOLID);
+__device__ __forceinline__ void load_coef(const KoSystem& S, long long D, long long g, double c[4]) {
+    c[0] = __ldg(S.coef + g);
+    c[1] = __ldg(S.coef + D + g);
+    c[2] = __ldg(S.coef + 2 * D + g);
+    c[3] = __ldg(S.coef + 3 * D + g);
 }
 
-// ---- shared tile of one Krylov pass -------------------------------------------
-struct KTile {
-    double U1[R2H][R2W];        // stencil input u_{k-1} (or r) on the 2-ring
-    double C[4][R1H][R1W];      // coefficients E, W, N, S on the 1-ring
-    double UK[R1H][R1W];        // u_k on the 1-ring
-    unsigned char F[R2H][R2W];  // fluid flags on the 2-ring
-    double g[KOFM_MAX_KRYLOV];  // h_j s_j
-    double sk1;                 // s_{k-1}
-};
-
-// 5-point stencil in the CSR order of an interior row (S, W, C, E, N) on a
-// value grid V centred at (cy, cx), coefficients of the 1-ring at (ry, rx).
-template <typename VG>
-__device__ __forceinline__ double tile_stencil(const VG& V, int cy, int cx, const KTile& T,
-                                               int ry, int rx) {
-    return (double)T.C[3][ry][rx] * V[cy - 1][cx] + (double)T.C[1][ry][rx] * V[cy][cx - 1] +
-           V[cy][cx] + (double)T.C[0][ry][rx] * V[cy][cx + 1] +
-           (double)T.C[2][ry][rx] * V[cy + 1][cx];
-}
-
-// One fused Krylov pass for vector k of system S over one tile.  The tile is
-// a window onto the periodic lattice: column positions map to x mod nx, so
-// positions at or beyond nx alias columns 0, 1, ... (computed, never stored).
-//   k == 0: u_0 = A r                  (r = residual, un-normalised)
-//   k >= 1: u_k = s_{k-1} A u_{k-1} - sum_j g_j u_j
-// then, if k < K-1, w = A u_k on the tile.  Accumulates ||u_k||^2, <r, u_k>
-// and <w, u_j> (j <= k) into acc.
-__device__ __forceinline__ void krylov_tile(const GmresArgs& a, const KoSystem& S,
-                                            const float* rsrc, int k, int tile, KTile& T,
-                                            double (&acc)[2 + KOFM_MAX_KRYLOV]) {
-    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    const int x0 = tx * TW, y0 = ty * TH;
-    const int nx = a.nx, ny = a.ny, P = a.P;
-    const long long D = a.D;
-    const float* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
-    // 1) u_{k-1} (or r) and fluid flags on the 2-ring
-    for (int p = threadIdx.x; p < R2H * R2W; p += GM_THREADS) {
-        const int ry = p / R2W, rx = p % R2W;
-        const int gy = y0 - 2 + ry;
-        const int gx = wrap_mod(x0 - 2 + rx, nx);
+// U1 row y (and its fluid flags) for the columns this thread owns.
+__device__ __forceinline__ void load_u1(const GmresArgs& a, const vec_t* src, RowWin& W, int y, int x0) {
+    const int slot = y & 3;
+    const int t = threadIdx.x;
+    auto one = [&](int c) {
         double v = 0.0;
         unsigned char f = 0;
-        if (gy >= 0 && gy < ny) {
-            const long long g = (long long)gy * P + gx;
-            f = is_fluid(a.ntype, g);
+        if (y >= 0 && y < a.ny) {
+            const long long g = (long long)y * a.P + wrap_mod(x0 - 2 + c, a.nx);
+            f = !((uint16_t)a.ntype[g] & M_SOLID);
             if (f) v = (double)__ldcg(src + g);
         }
-        T.U1[ry][rx] = v;
-        T.F[ry][rx] = f;
-    }
-    __syncthreads();
-    // 2) coefficients on the 1-ring
-    for (int p = threadIdx.x; p < R1H * R1W; p += GM_THREADS) {
-        const int ry = p / R1W, rx = p % R1W;
-        const int gy = y0 - 1 + ry;
-        const int gx = wrap_mod(x0 - 1 + rx, nx);
-        double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
-        if (T.F[ry + 1][rx + 1]) {
-            const long long g = (long long)gy * P + gx;
-            c0 = __ldg(S.coef + g);
-            c1 = __ldg(S.coef + D + g);
-            c2 = __ldg(S.coef + 2 * D + g);
-            c3 = __ldg(S.coef + 3 * D + g);
-        }
-        T.C[0][ry][rx] = c0; T.C[1][ry][rx] = c1; T.C[2][ry][rx] = c2; T.C[3][ry][rx] = c3;
-    }
-    __syncthreads();
-    // 3) z = A u_{k-1} on the 1-ring, scaled; Gram-Schmidt with u_{k-1} last
-    for (int p = threadIdx.x; p < R1H * R1W; p += GM_THREADS) {
-        const int ry = p / R1W, rx = p % R1W;
-        double u = 0.0;
-        if (T.F[ry + 1][rx + 1]) {
-            const double z = tile_stencil(T.U1, ry + 1, rx + 1, T, ry, rx);
-            if (k == 0) {
-                u = z;
-            } else {
-                u = T.sk1 * z;
-                const int gy = y0 - 1 + ry;
-                const int gx = wrap_mod(x0 - 1 + rx, nx);
-                const long long g = (long long)gy * P + gx;
-                for (int j = 0; j < k - 1; ++j)
-                    u -= T.g[j] * (double)__ldcg(S.V + (long long)j * D + g);
-                u -= T.g[k - 1] * T.U1[ry + 1][rx + 1];
-            }
-            u = (double)(float)u;  // the stored (FP32) value defines u_k
-        }
-        T.UK[ry][rx] = u;
-    }
-    __syncthreads();
-    // 4) interior: store u_k, dot products, w = A u_k
+        W.U1[slot][c] = v;
+        W.F[slot][c] = f;
+    };
+    one(t + 2);
+    if (t == 0) { one(0); one(1); }
+    if (t == RS_W - 1) { one(RS_W + 2); one(RS_W + 3); }
+}
+
+// u_k at UK column cu of row y (cf = the node's coefficients).
+__device__ __forceinline__ double uk_at(const GmresArgs& a, const KoSystem& S, const RowWin& W,
+                                        int k, int y, int cu, int x0, const double cf[4]) {
+    const int c = cu + 1;  // same column in U1
+    const int s0 = y & 3, sm = (y - 1) & 3, sp = (y + 1) & 3;
+    if (!W.F[s0][c]) return 0.0;
+    // CSR order of an interior row: S, W, C, E, N
+    const double z = cf[3] * W.U1[sm][c] + cf[1] * W.U1[s0][c - 1] + W.U1[s0][c] +
+                     cf[0] * W.U1[s0][c + 1] + cf[2] * W.U1[sp][c];
+    if (k == 0) return rnd(z);
+    double u = W.sk1 * z;
+    const long long g = (long long)y * a.P + wrap_mod(x0 - 1 + cu, a.nx);
+    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * (double)__ldcg(S.V + (long long)j * a.D + g);
+    u -= W.g[k - 1] * W.U1[s0][c];
+    return rnd(u);  // the stored value defines u_k
+}
+
+__device__ void krylov_unit(const GmresArgs& a, const KoSystem& S, const vec_t* rsrc, int k,
+                            int unit, RowWin& W, double (&acc)[2 + KOFM_MAX_KRYLOV]) {
+    const int strip = unit % a.strips, chunk = unit / a.strips;
+    const int x0 = strip * RS_W;
+    const int ya = chunk * a.chunk_rows;
+    const int yb = min(ya + a.chunk_rows, a.ny);
+    const int t = threadIdx.x;
+    const bool real = x0 + t < a.nx;             // not a padding / alias column
+    const int gx = wrap_mod(x0 + t, a.nx);
+    const long long D = a.D;
+    const vec_t* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
     const bool need_w = k < a.K - 1;
-    for (int p = threadIdx.x; p < TW * TH; p += GM_THREADS) {
-        const int iy = p / TW, ix = p % TW;
-        const int gy = y0 + iy, gxr = x0 + ix;
-        if (gy >= ny || gxr >= nx) continue;  // padding / alias columns
-        const long long g = (long long)gy * P + gxr;
-        const double u = T.UK[iy + 1][ix + 1];
-        __stcg(S.V + (long long)k * D + g, (float)u);
-        if (!T.F[iy + 2][ix + 2]) continue;
-        const double r = (double)__ldcg(rsrc + g);
-        acc[0] += u * u;
-        acc[1] += r * u;
-        if (need_w) {
-            const double w = tile_stencil(T.UK, iy + 1, ix + 1, T, iy + 1, ix + 1);
-            const double um1 = T.U1[iy + 2][ix + 2];
+    double cf[4] = {0.0, 0.0, 0.0, 0.0}, cfp[4] = {0.0, 0.0, 0.0, 0.0}, cfh[4];
+    __syncthreads();  // the window may still be read by the previous unit
+    load_u1(a, src, W, ya - 2, x0);
+    load_u1(a, src, W, ya - 1, x0);
+    for (int y = ya - 1; y <= yb; ++y) {
+        load_u1(a, src, W, y + 1, x0);
+        const bool rowok = y >= 0 && y < a.ny;
+        const long long g = (long long)y * a.P + gx;
+        if (rowok && !((uint16_t)a.ntype[g] & M_SOLID)) load_coef(S, D, g, cf);
+        else cf[0] = cf[1] = cf[2] = cf[3] = 0.0;
+        int ch = -1;  // halo column of an edge thread (UK index)
+        if (t == 0) ch = 0;
+        if (t == RS_W - 1) ch = RS_W + 1;
+        cfh[0] = cfh[1] = cfh[2] = cfh[3] = 0.0;
+        if (ch >= 0 && rowok) {
+            const long long gh = (long long)y * a.P + wrap_mod(x0 - 1 + ch, a.nx);
+            if (!((uint16_t)a.ntype[gh] & M_SOLID)) load_coef(S, D, gh, cfh);
+        }
+        __syncthreads();
+        const double u = uk_at(a, S, W, k, y, t + 1, x0, cf);
+        W.UK[y & 3][t + 1] = u;
+        if (ch >= 0) W.UK[y & 3][ch] = uk_at(a, S, W, k, y, ch, x0, cfh);
+        if (y >= ya && y < yb && real) {
+            __stcg(S.V + (long long)k * D + g, (vec_t)u);
+            if (W.F[y & 3][t + 2]) {
+                const double r = (double)__ldcg(rsrc + g);
+                acc[0] += u * u;
+                acc[1] += r * u;
+            }
+        }
+        __syncthreads();
+        const int ym = y - 1;
+        if (need_w && ym >= ya && ym < yb && real && W.F[ym & 3][t + 2]) {
+            const int sm = ym & 3, smm = (ym - 1) & 3, sp = y & 3;
+            const double w = cfp[3] * W.UK[smm][t + 1] + cfp[1] * W.UK[sm][t] + W.UK[sm][t + 1] +
+                             cfp[0] * W.UK[sm][t + 2] + cfp[2] * W.UK[sp][t + 1];
+            const long long gm = (long long)ym * a.P + gx;
 #pragma unroll
             for (int j = 0; j < KOFM_MAX_KRYLOV; ++j) {
-                if (j < k - 1) acc[2 + j] += w * (double)__ldcg(S.V + (long long)j * D + g);
-                else if (j == k - 1) acc[2 + j] += w * um1;
-                else if (j == k) acc[2 + j] += w * u;
+                if (j < k - 1) acc[2 + j] += w * (double)__ldcg(S.V + (long long)j * D + gm);
+                else if (j == k - 1) acc[2 + j] += w * W.U1[sm][t + 2];
+                else if (j == k) acc[2 + j] += w * W.UK[sm][t + 1];
             }
         }
+        cfp[0] = cf[0]; cfp[1] = cf[1]; cfp[2] = cf[2]; cfp[3] = cf[3];
     }
-    __syncthreads();
 }
 
 // ---- the solver kernel ---------------------------------------------------------
-__global__ void __launch_bounds__(GM_THREADS)
+__global__ void __launch_bounds__(GM_THREADS, KOFM_GM_MINBLOCKS)
 gmres_kernel(const GmresArgs a) {
     GmresControl* ctl = a.ctl;
-    __shared__ KTile T;
+    __shared__ RowWin T;
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
     const long long npairs = a.D / 2;
     const long long stride = (long long)gridDim.x * GM_THREADS;
     const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
-    const int ntiles = a.tiles_x * a.tiles_y;
+    const int nunits = a.strips * a.chunks;
     const int K = a.K;
 
     for (int restart = 0; restart < a.max_restarts; ++restart) {
@@ -425,12 +444,12 @@ gmres_kernel(const GmresArgs a) {
                     const bool f0 = !((t2 & 0xffff) & M_SOLID);
                     const bool f1 = (x + 1 < a.nx) && !((t2 >> 16) & M_SOLID);
                     if (!f0 && !f1) {
-                        if (restart > 0) __stcg(reinterpret_cast<float2*>(S.r + g), make_float2(0.f, 0.f));
+                        if (restart > 0) stvec2(S.r + g, 0.0, 0.0);
                         continue;
                     }
                     if (restart == 0) {
-                        const float2 b = __ldcg(reinterpret_cast<const float2*>(S.rhs + g));
-                        const double b0 = f0 ? (double)b.x : 0.0, b1 = f1 ? (double)b.y : 0.0;
+                        const double2 b = ldvec2(S.rhs + g);
+                        const double b0 = f0 ? b.x : 0.0, b1 = f1 ? b.y : 0.0;
                         acc[0] += b0 * b0 + b1 * b1;
                     } else {
                         double rr[2];
@@ -449,9 +468,9 @@ gmres_kernel(const GmresArgs a) {
                                 __ldcg(S.x + gj) +
                                 (double)__ldg(S.coef + gj) * __ldcg(S.x + row + xe) +
                                 (double)__ldg(S.coef + 2 * a.D + gj) * __ldcg(S.x + gj + a.P);
-                            rr[j] = (double)(float)((double)__ldcg(S.rhs + gj) - Ax);
+                            rr[j] = rnd((double)__ldcg(S.rhs + gj) - Ax);
                         }
-                        __stcg(reinterpret_cast<float2*>(S.r + g), make_float2((float)rr[0], (float)rr[1]));
+                        stvec2(S.r + g, rr[0], rr[1]);
                         acc[0] += rr[0] * rr[0] + rr[1] * rr[1];
                     }
                 }
@@ -476,9 +495,9 @@ gmres_kernel(const GmresArgs a) {
                     if (threadIdx.x < k) T.g[threadIdx.x] = ldc(&C->h[threadIdx.x]) * ldc(&C->s[threadIdx.x]);
                     if (threadIdx.x == 0 && k > 0) T.sk1 = ldc(&C->s[k - 1]);
                     __syncthreads();
-                    const float* rsrc = restart == 0 ? S.rhs : S.r;
-                    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-                        krylov_tile(a, S, rsrc, k, tile, T, acc);
+                    const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
+                    for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x)
+                        krylov_unit(a, S, rsrc, k, unit, T, acc);
                 }
                 block_reduce_slots<2 + KOFM_MAX_KRYLOV>(acc, sh_act[s] ? nslots : 0, a.part,
                                                         GM_SYS_SLOTS * s);
@@ -501,19 +520,19 @@ gmres_kernel(const GmresArgs a) {
         for (int s = 0; s < 2; ++s) {
             if (!sh_act[s]) continue;
             const KoSystem& S = a.sys[s];
-            const float* rsrc = restart == 0 ? S.rhs : S.r;
+            const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
             for (long long pr = t0; pr < npairs; pr += stride) {
                 const long long g = pr * 2;
                 double2 xv = make_double2(0.0, 0.0);
                 if (restart > 0) xv = __ldcg(reinterpret_cast<const double2*>(S.x + g));
-                const float2 r = __ldcg(reinterpret_cast<const float2*>(rsrc + g));
-                double v0 = xv.x + sh_c[s][0] * (double)r.x, v1 = xv.y + sh_c[s][0] * (double)r.y;
+                const double2 r = ldvec2(rsrc + g);
+                double v0 = xv.x + sh_c[s][0] * r.x, v1 = xv.y + sh_c[s][0] * r.y;
                 for (int j = 1; j < K; ++j) {
                     const double cj = sh_c[s][j];
                     if (cj == 0.0) continue;
-                    const float2 u = __ldcg(reinterpret_cast<const float2*>(S.V + (long long)(j - 1) * a.D + g));
-                    v0 += cj * (double)u.x;
-                    v1 += cj * (double)u.y;
+                    const double2 u = ldvec2(S.V + (long long)(j - 1) * a.D + g);
+                    v0 += cj * u.x;
+                    v1 += cj * u.y;
                 }
                 __stcg(reinterpret_cast<double2*>(S.x + g), make_double2(v0, v1));
             }

@@ -28,12 +28,17 @@ constexpr int KO_TX = 32, KO_TY = 8;
 // Krylov basis, residual and right-hand side only carry the per-step
 // increment, so they are FP32 (all arithmetic is FP64); the accumulated
 // correction x stays FP64.
+#ifndef KOFM_SOLVER_VEC
+#define KOFM_SOLVER_VEC double
+#endif
+using vec_t = KOFM_SOLVER_VEC;  // storage type of the streamed solver vectors
+
 struct KoSystem {
     double* coef = nullptr;  // [4][D] normalised off-diagonals E, W, N, S
-    float* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
-    float* r = nullptr;      // [D] residual of restarts >= 1
+    vec_t* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
+    vec_t* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
-    float* V = nullptr;      // [K][D] Krylov basis (orthogonalised, unscaled)
+    vec_t* V = nullptr;      // [K][D] Krylov basis (orthogonalised, unscaled)
 };
 
 struct AsmParams {
@@ -49,9 +54,9 @@ struct AsmParams {
     const float* uy;
     const float* S;
     double* coef_o;
-    float* rhs_o;
+    vec_t* rhs_o;
     double* coef_k;
-    float* rhs_k;
+    vec_t* rhs_k;
     int nx, ny, P;
     long long D;
     double mu, dt;
@@ -186,8 +191,8 @@ komega_assemble_kernel(const AsmParams p) {
     const int t = (uint16_t)p.ntype[g];
     if (t & M_SOLID) {
         for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
-        p.rhs_o[g] = 0.f;
-        p.rhs_k[g] = 0.f;
+        p.rhs_o[g] = vec_t(0);
+        p.rhs_k[g] = vec_t(0);
         return;
     }
     Fd3 X, Y, X2, Y2;
@@ -247,8 +252,8 @@ komega_assemble_kernel(const AsmParams p) {
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
     p.coef_o[g] = We; p.coef_o[D + g] = Ww; p.coef_o[2 * D + g] = Wn; p.coef_o[3 * D + g] = Ws;
     p.coef_k[g] = Ke; p.coef_k[D + g] = Kw; p.coef_k[2 * D + g] = Kn; p.coef_k[3 * D + g] = Ks;
-    p.rhs_o[g] = (float)(Wsrc - Axo);
-    p.rhs_k[g] = (float)(Ksrc - Axk);
+    p.rhs_o[g] = (vec_t)(Wsrc - Axo);
+    p.rhs_k[g] = (vec_t)(Ksrc - Axk);
 }
 
 }  // namespace kofm
