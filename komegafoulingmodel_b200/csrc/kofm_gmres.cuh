@@ -301,6 +301,8 @@ constexpr int RS_W = GM_THREADS;
 struct RowWin {
     double U1[4][RS_W + 4];         // rows of u_{k-1} (or r); column c <-> x0 - 2 + c
     double UK[4][RS_W + 2];         // rows of u_k;             column c <-> x0 - 1 + c
+    double VJ[2][KOFM_MAX_KRYLOV][RS_W];  // u_j (j < k-1) of the own column, rows y and y-1
+    double VH[2][KOFM_MAX_KRYLOV];  // u_j of the two halo columns (edge threads), row y
     unsigned char F[4][RS_W + 4];   // fluid flags of the U1 rows
     double g[KOFM_MAX_KRYLOV];      // h_j s_j
     double sk1;                     // s_{k-1}
@@ -338,9 +340,21 @@ __device__ __forceinline__ void load_u1(const GmresArgs& a, const vec_t* src, Ro
     if (t == RS_W - 1) { one(RS_W + 2); one(RS_W + 3); }
 }
 
-// u_k at UK column cu of row y (cf = the node's coefficients).
-__device__ __forceinline__ double uk_at(const GmresArgs& a, const KoSystem& S, const RowWin& W,
-                                        int k, int y, int cu, int x0, const double cf[4]) {
+// u_j (j < k-1) of node g, all loads issued together
+__device__ __forceinline__ void load_basis(const KoSystem& S, long long D, long long g, int k,
+                                           double* dst, int stride) {
+    double v[KOFM_MAX_KRYLOV];
+#pragma unroll
+    for (int j = 0; j < KOFM_MAX_KRYLOV; ++j)
+        v[j] = (j < k - 1) ? (double)__ldcg(S.V + (long long)j * D + g) : 0.0;
+#pragma unroll
+    for (int j = 0; j < KOFM_MAX_KRYLOV; ++j)
+        if (j < k - 1) dst[j * stride] = v[j];
+}
+
+// u_k at UK column cu of row y (cf = the node's coefficients, vj = its u_j).
+__device__ __forceinline__ double uk_at(const RowWin& W, int k, int y, int cu, const double cf[4],
+                                        const double* vj, int stride) {
     const int c = cu + 1;  // same column in U1
     const int s0 = y & 3, sm = (y - 1) & 3, sp = (y + 1) & 3;
     if (!W.F[s0][c]) return 0.0;
@@ -349,8 +363,7 @@ __device__ __forceinline__ double uk_at(const GmresArgs& a, const KoSystem& S, c
                      cf[0] * W.U1[s0][c + 1] + cf[2] * W.U1[sp][c];
     if (k == 0) return rnd(z);
     double u = W.sk1 * z;
-    const long long g = (long long)y * a.P + wrap_mod(x0 - 1 + cu, a.nx);
-    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * (double)__ldcg(S.V + (long long)j * a.D + g);
+    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * vj[j * stride];
     u -= W.g[k - 1] * W.U1[s0][c];
     return rnd(u);  // the stored value defines u_k
 }
@@ -367,46 +380,59 @@ __device__ void krylov_unit(const GmresArgs& a, const KoSystem& S, const vec_t* 
     const long long D = a.D;
     const vec_t* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
     const bool need_w = k < a.K - 1;
+    int ch = -1;  // halo column of an edge thread (UK index)
+    if (t == 0) ch = 0;
+    if (t == RS_W - 1) ch = RS_W + 1;
+    const int hslot = t == 0 ? 0 : 1;
     double cf[4] = {0.0, 0.0, 0.0, 0.0}, cfp[4] = {0.0, 0.0, 0.0, 0.0}, cfh[4];
     __syncthreads();  // the window may still be read by the previous unit
     load_u1(a, src, W, ya - 2, x0);
     load_u1(a, src, W, ya - 1, x0);
     for (int y = ya - 1; y <= yb; ++y) {
+        // ---- loads of row y (and u_{k-1} row y+1), issued together ----------
         load_u1(a, src, W, y + 1, x0);
         const bool rowok = y >= 0 && y < a.ny;
         const long long g = (long long)y * a.P + gx;
-        if (rowok && !((uint16_t)a.ntype[g] & M_SOLID)) load_coef(S, D, g, cf);
-        else cf[0] = cf[1] = cf[2] = cf[3] = 0.0;
-        int ch = -1;  // halo column of an edge thread (UK index)
-        if (t == 0) ch = 0;
-        if (t == RS_W - 1) ch = RS_W + 1;
+        const bool fl = rowok && !((uint16_t)a.ntype[g] & M_SOLID);
+        if (fl) {
+            load_coef(S, D, g, cf);
+            if (k > 1) load_basis(S, D, g, k, &W.VJ[y & 1][0][t], RS_W);
+        } else {
+            cf[0] = cf[1] = cf[2] = cf[3] = 0.0;
+        }
+        double r = 0.0;
+        if (fl && real && y >= ya && y < yb) r = (double)__ldcg(rsrc + g);
         cfh[0] = cfh[1] = cfh[2] = cfh[3] = 0.0;
         if (ch >= 0 && rowok) {
             const long long gh = (long long)y * a.P + wrap_mod(x0 - 1 + ch, a.nx);
-            if (!((uint16_t)a.ntype[gh] & M_SOLID)) load_coef(S, D, gh, cfh);
+            if (!((uint16_t)a.ntype[gh] & M_SOLID)) {
+                load_coef(S, D, gh, cfh);
+                if (k > 1) load_basis(S, D, gh, k, &W.VH[hslot][0], 1);
+            }
         }
         __syncthreads();
-        const double u = uk_at(a, S, W, k, y, t + 1, x0, cf);
+        // ---- u_k(y) on the strip and its two halo columns ---------------------------
+        const double u = uk_at(W, k, y, t + 1, cf, &W.VJ[y & 1][0][t], RS_W);
         W.UK[y & 3][t + 1] = u;
-        if (ch >= 0) W.UK[y & 3][ch] = uk_at(a, S, W, k, y, ch, x0, cfh);
+        if (ch >= 0) W.UK[y & 3][ch] = uk_at(W, k, y, ch, cfh, &W.VH[hslot][0], 1);
         if (y >= ya && y < yb && real) {
             __stcg(S.V + (long long)k * D + g, (vec_t)u);
-            if (W.F[y & 3][t + 2]) {
-                const double r = (double)__ldcg(rsrc + g);
+            if (fl) {
                 acc[0] += u * u;
                 acc[1] += r * u;
             }
         }
         __syncthreads();
+        // ---- w = A u_k at row y-1, dot products with u_j(y-1) -----------------------
         const int ym = y - 1;
         if (need_w && ym >= ya && ym < yb && real && W.F[ym & 3][t + 2]) {
             const int sm = ym & 3, smm = (ym - 1) & 3, sp = y & 3;
             const double w = cfp[3] * W.UK[smm][t + 1] + cfp[1] * W.UK[sm][t] + W.UK[sm][t + 1] +
                              cfp[0] * W.UK[sm][t + 2] + cfp[2] * W.UK[sp][t + 1];
-            const long long gm = (long long)ym * a.P + gx;
+            const double* vj = &W.VJ[ym & 1][0][t];
 #pragma unroll
             for (int j = 0; j < KOFM_MAX_KRYLOV; ++j) {
-                if (j < k - 1) acc[2 + j] += w * (double)__ldcg(S.V + (long long)j * D + gm);
+                if (j < k - 1) acc[2 + j] += w * vj[j * RS_W];
                 else if (j == k - 1) acc[2 + j] += w * W.U1[sm][t + 2];
                 else if (j == k) acc[2 + j] += w * W.UK[sm][t + 1];
             }
