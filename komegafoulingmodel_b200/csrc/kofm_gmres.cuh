@@ -96,18 +96,6 @@ struct GmresArgs {
 template <typename T>
 __device__ __forceinline__ T ldc(const T* p) { return __ldcg(p); }
 
-__device__ void sys_load(GmresSys& dst, const GmresSys* src) {
-    static_assert(sizeof(GmresSys) % 8 == 0, "GmresSys must be 8-byte granular");
-    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
-    unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
-    for (int i = 0; i < (int)(sizeof(GmresSys) / 8); ++i) d[i] = __ldcg(s + i);
-}
-__device__ void sys_store(GmresSys* dst, const GmresSys& src) {
-    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(&src);
-    unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
-    for (int i = 0; i < (int)(sizeof(GmresSys) / 8); ++i) __stcg(d + i, s[i]);
-}
-
 // pair loads / stores of solver vectors (FP32 or FP64 storage, FP64 values)
 __device__ __forceinline__ double2 ldvec2(const float* p) {
     const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
@@ -193,59 +181,76 @@ __device__ void cycle_logic(GmresSys& S, int K, double rel_tol) {
     S.prev_err = fabs(S.rho * S.rho0 / S.norm_rhs);
 }
 
-// Serial section: executed by all threads of the last-arriving block.
+// Serial section: executed by all threads of the last-arriving block.  The
+// block sums the partials and stages each system's scalars in shared memory;
+// thread 0 runs the scalar logic.
 __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int restart, int nblocks) {
     GmresControl* ctl = a.ctl;
     __shared__ double tot[GM_SLOTS];
-    __shared__ GmresSys sS;  // working copy of one system's scalars (thread 0)
+    __shared__ GmresSys sS;
+    __shared__ int s_any;
     const int warp = threadIdx.x >> 5, nwarps = GM_THREADS / 32;
     for (int slot = warp; slot < GM_SLOTS; slot += nwarps) {
         const double v = sum_slot_warp(a.part, nblocks, slot);
         if ((threadIdx.x & 31) == 0) tot[slot] = v;
     }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    int any = 0;
+    if (threadIdx.x == 0) s_any = 0;
+    constexpr int NW = (int)(sizeof(GmresSys) / 8);
     for (int s = 0; s < 2; ++s) {
-        GmresSys& S = sS;
-        sys_load(S, &ctl->sys[s]);
-        if (!S.active) continue;
-        const double* t = tot + GM_SYS_SLOTS * s;
-        if (kind == SER_RESIDUAL) {
-            S.rho0 = sqrt(t[0]);
-            if (restart == 0) S.norm_rhs = S.rho0;
-            S.rinv = 1.0 / S.rho0;
-            S.rho = 1.0;
-            S.restarts += 1;
-            const double resid = S.rho0 / S.norm_rhs;
-            if (isnan(resid)) { S.nan = 1; S.active = 0; }
-            else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
-            else { S.cycles += 1; }
-        } else if (kind == SER_KRYLOV) {
-            // t[0] = ||u_k||^2, t[1] = <r_raw, u_k>, t[2 + j] = <A u_k, u_j> (j <= k)
-            const int k = kcur, K = a.K;
-            const double nk = sqrt(t[0]);
-            S.s[k] = 1.0 / nk;
-            if (k == 0) {
-                for (int i = 0; i < K * K; ++i) S.R[i] = 0.0;
-                S.R[0] = S.rinv * nk;  // ||A r|| with r = r_raw / rho0
-            } else {
-                for (int j = 0; j < k; ++j) S.R[j + k * K] = S.h[j];
-                S.R[k + k * K] = nk;
-            }
-            S.xi[k] = S.rinv * t[1] * S.s[k];  // <r, v_k>
-            if (k < K - 1) {
-                // h_j = <A v_k, v_j> with v = s u
-                for (int j = 0; j <= k; ++j) S.h[j] = S.s[k] * S.s[j] * t[2 + j];
-            } else {
-                cycle_logic(S, K, a.rel_tol);
-            }
+        __syncthreads();
+        {
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&ctl->sys[s]);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sS);
+            for (int i = threadIdx.x; i < NW; i += GM_THREADS) dst[i] = __ldcg(src + i);
         }
-        any |= S.active;
-        sys_store(&ctl->sys[s], S);
+        __syncthreads();
+        if (threadIdx.x == 0 && sS.active) {
+            GmresSys& S = sS;
+            const double* t = tot + GM_SYS_SLOTS * s;
+            if (kind == SER_RESIDUAL) {
+                S.rho0 = sqrt(t[0]);
+                if (restart == 0) S.norm_rhs = S.rho0;
+                S.rinv = 1.0 / S.rho0;
+                S.rho = 1.0;
+                S.restarts += 1;
+                const double resid = S.rho0 / S.norm_rhs;
+                if (isnan(resid)) { S.nan = 1; S.active = 0; }
+                else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+                else { S.cycles += 1; }
+            } else if (kind == SER_KRYLOV) {
+                // t[0] = ||u_k||^2, t[1] = <r_raw, u_k>, t[2 + j] = <A u_k, u_j> (j <= k)
+                const int k = kcur, K = a.K;
+                const double nk = sqrt(t[0]);
+                S.s[k] = 1.0 / nk;
+                if (k == 0) {
+                    for (int i = 0; i < K * K; ++i) S.R[i] = 0.0;
+                    S.R[0] = S.rinv * nk;  // ||A r|| with r = r_raw / rho0
+                } else {
+                    for (int j = 0; j < k; ++j) S.R[j + k * K] = S.h[j];
+                    S.R[k + k * K] = nk;
+                }
+                S.xi[k] = S.rinv * t[1] * S.s[k];  // <r, v_k>
+                if (k < K - 1) {
+                    // h_j = <A v_k, v_j> with v = s u
+                    for (int j = 0; j <= k; ++j) S.h[j] = S.s[k] * S.s[j] * t[2 + j];
+                } else {
+                    cycle_logic(S, K, a.rel_tol);
+                }
+            }
+            s_any |= S.active;
+        }
+        __syncthreads();
+        {
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&sS);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&ctl->sys[s]);
+            for (int i = threadIdx.x; i < NW; i += GM_THREADS) __stcg(dst + i, src[i]);
+        }
     }
-    __stcg(&ctl->any_active, any);
-    __stcg(&ctl->passes, ldc(&ctl->passes) + 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __stcg(&ctl->any_active, s_any);
+        __stcg(&ctl->passes, ldc(&ctl->passes) + 1);
+    }
 }
 
 // Bounded grid barrier with a serial section run by the last block to arrive.
@@ -266,6 +271,7 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
     if (s_last) {
         __threadfence();
         if (kind != SER_NONE) serial_section(a, kind, kcur, restart, nblocks);
+        __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
             atomicExch(&a.bar->count, 0u);

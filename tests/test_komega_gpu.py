@@ -57,8 +57,10 @@ def test_one_update_matches_oracle(kofm_lib, oracle):
     # extra directions carry components below rho.  Restart counts and the
     # fields must agree.
     assert (st.omega_restarts, st.k_restarts) == (sim.kst.last_o.restarts, sim.kst.last_k.restarts)
-    assert rel_l2(k2, sim.K, fl) < 1e-6
-    assert rel_l2(o2, sim.O, fl) < 1e-6
+    # the cut also moves the converged correction by up to the residual
+    # estimate at the cut (~1e-5 of the increment here)
+    assert rel_l2(k2, sim.K, fl) < 1e-5
+    assert rel_l2(o2, sim.O, fl) < 1e-5
     # nu_t follows the strain rate S, a non-equilibrium moment of the
     # FP32-stored populations (difference of nearly equal terms)
     assert rel_l2(nut2, sim.nut, fl) < 1e-4
