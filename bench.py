@@ -101,18 +101,17 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def solver_bytes_per_node(stats, K):
     """Algorithmic bytes per lattice node of one solver launch (both systems):
-    every array the restarted simpler-GMRES sweeps must read or write once.
-    Basis, residual, right-hand side and the four stencil coefficients are
-    FP32, the correction x is FP64.  Per Krylov vector k: u_{k-1} (or r), the
-    older basis vectors u_j (j < k-1), the coefficients, r, and the store of
-    u_k; halo re-reads served by L2 are not counted."""
+    every array the restarted simpler-GMRES sweeps must read or write once,
+    all FP64.  Krylov vector k: u_{k-1} (or r), the older basis vectors u_j
+    (j < k-1), the four stencil coefficients, r, and the store of u_k.  Halo
+    rows / columns re-read from L2 are not counted."""
     total = 0
     for restarts, cycles, iters in ((stats.omega_restarts, stats.omega_cycles, stats.omega_iters),
                                     (stats.k_restarts, stats.k_cycles, stats.k_iters)):
-        res = 4 + 32 * max(restarts - 1, 0)          # restart 0 reads b'; later r = b' - A x
-        per_cycle = 24 + sum(4 * k + 24 for k in range(1, K))
+        res = 8 + 56 * max(restarts - 1, 0)          # restart 0 reads b'; later r = b' - A x
+        per_cycle = 48 + sum(8 * k + 48 for k in range(1, K))
         kk = max(1, iters // max(cycles, 1))
-        upd = cycles * (8 + 4 + 4 * (kk - 1)) + 8 * max(cycles - 1, 0)
+        upd = cycles * (16 + 8 * (kk - 1)) + 8 * max(cycles - 1, 0)
         total += res + cycles * per_cycle + upd + 16   # + write-back x, field
     return total
 

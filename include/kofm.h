@@ -95,7 +95,7 @@ typedef struct kofm_desc {
     int32_t storage;     /* KOFM_STORE_* */
     int32_t device;      /* CUDA device ordinal */
     int32_t komega_max_iters; /* KOMEGA_MAX_ITERS (1000) */
-    int32_t krylov_dim;       /* GMRES_KRYLOV_DIM_SIZE (10); 1..12 */
+    int32_t krylov_dim;       /* GMRES_KRYLOV_DIM_SIZE (10); 1..10 */
     double komega_rel_tol;    /* KOMEGA_MAX_REL_TOL (1e-4) */
     double komega_abs_tol;    /* KOMEGA_MAX_ABS_TOL (1e-7) */
     double komega_dt;         /* initial k-omega time step (p.dTlb = 1) */

@@ -34,14 +34,14 @@
 #include "kofm_komega.cuh"
 
 #ifndef KOFM_MAX_KRYLOV
-#define KOFM_MAX_KRYLOV 12
+#define KOFM_MAX_KRYLOV 10
 #endif
 
 namespace kofm {
 
 constexpr int GM_THREADS = 128;
 #ifndef KOFM_GM_MINBLOCKS
-#define KOFM_GM_MINBLOCKS 6  // resident blocks per SM the register budget targets
+#define KOFM_GM_MINBLOCKS 2  // resident blocks per SM the register budget targets
 #endif
 constexpr int GM_SLOTS = 32;                    // partial-sum slots per block
 constexpr int GM_SYS_SLOTS = 16;                // per system
@@ -293,25 +293,30 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
 }
 
 // ---- row-streaming Krylov pass ----------------------------------------------
-// A work unit is a strip of RS_W columns times a chunk of rows.  One thread
-// owns one column of the strip (the edge threads also the column just outside
-// it) and the block marches down the rows keeping a rolling window of the
-// last four rows of u_{k-1} (or r) and of u_k in shared memory:
-//   row y:   load u_{k-1}(y+1); u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j
-//            on the strip plus one column each side; store u_k(y);
-//   row y-1: w = A u_k on the strip -> dot products <w, u_j>.
-// Every array is read once from HBM per pass; the only repeated reads are the
-// two rows above and below each chunk and the columns beside each strip.
-constexpr int RS_W = GM_THREADS;
+// A work unit is a strip of RS_W = 256 columns times a chunk of rows.  Each of
+// the 128 threads owns two adjacent columns (16-byte copies); the edge threads
+// also carry the column just outside the strip.  The block marches down the
+// rows keeping rolling rows of u_{k-1} (or r) and of u_k in shared memory:
+//   row y:   u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j on the strip plus one
+//            column each side; store u_k(y);  dots ||u_k||^2, <r, u_k>;
+//   row y-1: w = A u_k on the strip -> dots <w, u_j> for the next vector.
+// The inputs of row y+1 (u_{k-1} of row y+2, the coefficients, the older
+// basis vectors and r of row y+1) are copied into shared memory with
+// cp.async.cg while row y computes.  Vectors and coefficients are zero on
+// every non-fluid node, so no fluid test is needed in the sweep.
+constexpr int RS_W = 2 * GM_THREADS;
+constexpr int RS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
 
 struct RowWin {
-    double U1[4][RS_W + 4];         // rows of u_{k-1} (or r); column c <-> x0 - 2 + c
-    double UK[4][RS_W + 2];         // rows of u_k;             column c <-> x0 - 1 + c
-    double VJ[2][KOFM_MAX_KRYLOV][RS_W];  // u_j (j < k-1) of the own column, rows y and y-1
-    double VH[2][KOFM_MAX_KRYLOV];  // u_j of the two halo columns (edge threads), row y
-    unsigned char F[4][RS_W + 4];   // fluid flags of the U1 rows
-    double g[KOFM_MAX_KRYLOV];      // h_j s_j
-    double sk1;                     // s_{k-1}
+    double U1[4][RS_W + 4];            // u_{k-1} (or r) rows; column i <-> x0 - 2 + i
+    double UK[4][RS_W + 2];            // u_k rows;             column i <-> x0 - 1 + i
+    double VJ[3][RS_KV][RS_W];         // u_j (j < k-1), own columns
+    double VJH[3][2][RS_KV][2];        // u_j of the halo pairs (left, right)
+    double CF[3][4][RS_W];             // coefficients E, W, N, S, own columns
+    double CFH[3][2][4][2];            // coefficients of the halo pairs
+    double RR[3][RS_W];                // r, own columns
+    double g[KOFM_MAX_KRYLOV];         // h_j s_j
+    double sk1;                        // s_{k-1}
 };
 
 __device__ __forceinline__ int wrap_mod(int x, int n) {
@@ -319,57 +324,77 @@ __device__ __forceinline__ int wrap_mod(int x, int n) {
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ void load_coef(const KoSystem& S, long long D, long long g, double c[4]) {
-    c[0] = __ldg(S.coef + g);
-    c[1] = __ldg(S.coef + D + g);
-    c[2] = __ldg(S.coef + 2 * D + g);
-    c[3] = __ldg(S.coef + 3 * D + g);
+__device__ __forceinline__ void cp16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Copy the pair of doubles at (y, columns x, x+1 mod nx) into dst[0..1]:
+// one 16-byte async copy when the pair is contiguous, two 8-byte plain loads
+// at the periodic seam of an odd nx; zeros outside the rows.
+__device__ __forceinline__ void pair_copy(const GmresArgs& a, const double* base, int y, int x,
+                                          double* dst) {
+    if (y < 0 || y >= a.ny) { dst[0] = 0.0; dst[1] = 0.0; return; }
+    const int xa = wrap_mod(x, a.nx), xb = wrap_mod(x + 1, a.nx);
+    const long long row = (long long)y * a.P;
+    if (xb == xa + 1 && (xa & 1) == 0) {
+        cp16(dst, base + row + xa);
+    } else {
+        dst[0] = __ldcg(base + row + xa);
+        dst[1] = __ldcg(base + row + xb);
+    }
 }
 
-// U1 row y (and its fluid flags) for the columns this thread owns.
-__device__ __forceinline__ void load_u1(const GmresArgs& a, const vec_t* src, RowWin& W, int y, int x0) {
-    const int slot = y & 3;
-    const int t = threadIdx.x;
-    auto one = [&](int c) {
-        double v = 0.0;
-        unsigned char f = 0;
-        if (y >= 0 && y < a.ny) {
-            const long long g = (long long)y * a.P + wrap_mod(x0 - 2 + c, a.nx);
-            f = !((uint16_t)a.ntype[g] & M_SOLID);
-            if (f) v = (double)__ldcg(src + g);
+// Async copies of everything row y needs, except u_{k-1}(y+1) (own row slot
+// y % 3) plus u_{k-1} row y + 1 (slot (y+1) & 3).
+__device__ __forceinline__ void issue_row(const GmresArgs& a, const KoSystem& S, const vec_t* src,
+                                          const vec_t* rsrc, int k, int y, int x0, RowWin& W) {
+    const int t = threadIdx.x, c = 2 * t;
+    const long long D = a.D;
+    // u_{k-1} of row y+1 (and the halo pairs)
+    {
+        const int yu = y + 1, su = yu & 3;
+        pair_copy(a, src, yu, x0 + c, &W.U1[su][c + 2]);
+        if (t == 0) pair_copy(a, src, yu, x0 - 2, &W.U1[su][0]);
+        if (t == GM_THREADS - 1) pair_copy(a, src, yu, x0 + RS_W, &W.U1[su][RS_W + 2]);
+    }
+    const int sr = y % 3;
+    if (y < 0 || y >= a.ny) {
+        for (int q = 0; q < 4; ++q) { W.CF[sr][q][c] = 0.0; W.CF[sr][q][c + 1] = 0.0; }
+        for (int j = 0; j < RS_KV; ++j) { W.VJ[sr][j][c] = 0.0; W.VJ[sr][j][c + 1] = 0.0; }
+        W.RR[sr][c] = 0.0; W.RR[sr][c + 1] = 0.0;
+        if (t == 0 || t == GM_THREADS - 1) {
+            const int h = t == 0 ? 0 : 1;
+            for (int q = 0; q < 4; ++q) { W.CFH[sr][h][q][0] = 0.0; W.CFH[sr][h][q][1] = 0.0; }
+            for (int j = 0; j < RS_KV; ++j) { W.VJH[sr][h][j][0] = 0.0; W.VJH[sr][h][j][1] = 0.0; }
         }
-        W.U1[slot][c] = v;
-        W.F[slot][c] = f;
-    };
-    one(t + 2);
-    if (t == 0) { one(0); one(1); }
-    if (t == RS_W - 1) { one(RS_W + 2); one(RS_W + 3); }
+        return;
+    }
+    for (int q = 0; q < 4; ++q) pair_copy(a, S.coef + q * D, y, x0 + c, &W.CF[sr][q][c]);
+    for (int j = 0; j < k - 1; ++j) pair_copy(a, S.V + (long long)j * D, y, x0 + c, &W.VJ[sr][j][c]);
+    pair_copy(a, rsrc, y, x0 + c, &W.RR[sr][c]);
+    if (t == 0 || t == GM_THREADS - 1) {
+        const int h = t == 0 ? 0 : 1;
+        const int xh = t == 0 ? x0 - 2 : x0 + RS_W;  // pair holding the halo column
+        for (int q = 0; q < 4; ++q) pair_copy(a, S.coef + q * D, y, xh, &W.CFH[sr][h][q][0]);
+        for (int j = 0; j < k - 1; ++j) pair_copy(a, S.V + (long long)j * D, y, xh, &W.VJH[sr][h][j][0]);
+    }
 }
 
-// u_j (j < k-1) of node g, all loads issued together
-__device__ __forceinline__ void load_basis(const KoSystem& S, long long D, long long g, int k,
-                                           double* dst, int stride) {
-    double v[KOFM_MAX_KRYLOV];
-#pragma unroll
-    for (int j = 0; j < KOFM_MAX_KRYLOV; ++j)
-        v[j] = (j < k - 1) ? (double)__ldcg(S.V + (long long)j * D + g) : 0.0;
-#pragma unroll
-    for (int j = 0; j < KOFM_MAX_KRYLOV; ++j)
-        if (j < k - 1) dst[j * stride] = v[j];
-}
-
-// u_k at UK column cu of row y (cf = the node's coefficients, vj = its u_j).
-__device__ __forceinline__ double uk_at(const RowWin& W, int k, int y, int cu, const double cf[4],
-                                        const double* vj, int stride) {
-    const int c = cu + 1;  // same column in U1
+// u_k at UK column i of row y; cf(q) and vj(j) give the node's coefficients
+// and older basis vectors.
+template <typename CF, typename VJ>
+__device__ __forceinline__ double uk_at(const RowWin& W, int k, int y, int i, CF cf, VJ vj) {
+    const int c = i + 1;  // same column in U1
     const int s0 = y & 3, sm = (y - 1) & 3, sp = (y + 1) & 3;
-    if (!W.F[s0][c]) return 0.0;
     // CSR order of an interior row: S, W, C, E, N
-    const double z = cf[3] * W.U1[sm][c] + cf[1] * W.U1[s0][c - 1] + W.U1[s0][c] +
-                     cf[0] * W.U1[s0][c + 1] + cf[2] * W.U1[sp][c];
+    const double z = cf(3) * W.U1[sm][c] + cf(1) * W.U1[s0][c - 1] + W.U1[s0][c] +
+                     cf(0) * W.U1[s0][c + 1] + cf(2) * W.U1[sp][c];
     if (k == 0) return rnd(z);
     double u = W.sk1 * z;
-    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * vj[j * stride];
+    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * vj(j);
     u -= W.g[k - 1] * W.U1[s0][c];
     return rnd(u);  // the stored value defines u_k
 }
@@ -380,78 +405,78 @@ __device__ void krylov_unit(const GmresArgs& a, const KoSystem& S, const vec_t* 
     const int x0 = strip * RS_W;
     const int ya = chunk * a.chunk_rows;
     const int yb = min(ya + a.chunk_rows, a.ny);
-    const int t = threadIdx.x;
-    const bool real = x0 + t < a.nx;             // not a padding / alias column
-    const int gx = wrap_mod(x0 + t, a.nx);
+    const int t = threadIdx.x, c = 2 * t;
     const long long D = a.D;
     const vec_t* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
     const bool need_w = k < a.K - 1;
-    int ch = -1;  // halo column of an edge thread (UK index)
-    if (t == 0) ch = 0;
-    if (t == RS_W - 1) ch = RS_W + 1;
-    const int hslot = t == 0 ? 0 : 1;
-    double cf[4] = {0.0, 0.0, 0.0, 0.0}, cfp[4] = {0.0, 0.0, 0.0, 0.0}, cfh[4];
+    const bool real0 = x0 + c < a.nx, real1 = x0 + c + 1 < a.nx;  // not padding / alias
     __syncthreads();  // the window may still be read by the previous unit
-    load_u1(a, src, W, ya - 2, x0);
-    load_u1(a, src, W, ya - 1, x0);
-    for (int y = ya - 1; y <= yb; ++y) {
-        // ---- loads of row y (and u_{k-1} row y+1), issued together ----------
-        load_u1(a, src, W, y + 1, x0);
-        const bool rowok = y >= 0 && y < a.ny;
-        const long long g = (long long)y * a.P + gx;
-        const bool fl = rowok && !((uint16_t)a.ntype[g] & M_SOLID);
-        if (fl) {
-            load_coef(S, D, g, cf);
-            if (k > 1) load_basis(S, D, g, k, &W.VJ[y & 1][0][t], RS_W);
-        } else {
-            cf[0] = cf[1] = cf[2] = cf[3] = 0.0;
+    // prologue: u_{k-1} rows ya-2 and ya-1, then row ya-1's inputs (+ u_{k-1}(ya))
+    {
+        for (int yy = ya - 2; yy <= ya - 1; ++yy) {
+            const int su = yy & 3;
+            pair_copy(a, src, yy, x0 + c, &W.U1[su][c + 2]);
+            if (t == 0) pair_copy(a, src, yy, x0 - 2, &W.U1[su][0]);
+            if (t == GM_THREADS - 1) pair_copy(a, src, yy, x0 + RS_W, &W.U1[su][RS_W + 2]);
         }
-        double r = 0.0;
-        if (fl && real && y >= ya && y < yb) r = (double)__ldcg(rsrc + g);
-        cfh[0] = cfh[1] = cfh[2] = cfh[3] = 0.0;
-        if (ch >= 0 && rowok) {
-            const long long gh = (long long)y * a.P + wrap_mod(x0 - 1 + ch, a.nx);
-            if (!((uint16_t)a.ntype[gh] & M_SOLID)) {
-                load_coef(S, D, gh, cfh);
-                if (k > 1) load_basis(S, D, gh, k, &W.VH[hslot][0], 1);
-            }
-        }
-        __syncthreads();
-        // ---- u_k(y) on the strip and its two halo columns ---------------------------
-        const double u = uk_at(W, k, y, t + 1, cf, &W.VJ[y & 1][0][t], RS_W);
-        W.UK[y & 3][t + 1] = u;
-        if (ch >= 0) W.UK[y & 3][ch] = uk_at(W, k, y, ch, cfh, &W.VH[hslot][0], 1);
-        if (y >= ya && y < yb && real) {
-            __stcg(S.V + (long long)k * D + g, (vec_t)u);
-            if (fl) {
-                acc[0] += u * u;
-                acc[1] += r * u;
-            }
-        }
-        __syncthreads();
-        // ---- w = A u_k at row y-1, dot products with u_j(y-1) -----------------------
-        const int ym = y - 1;
-        if (need_w && ym >= ya && ym < yb && real && W.F[ym & 3][t + 2]) {
-            const int sm = ym & 3, smm = (ym - 1) & 3, sp = y & 3;
-            const double w = cfp[3] * W.UK[smm][t + 1] + cfp[1] * W.UK[sm][t] + W.UK[sm][t + 1] +
-                             cfp[0] * W.UK[sm][t + 2] + cfp[2] * W.UK[sp][t + 1];
-            const double* vj = &W.VJ[ym & 1][0][t];
-#pragma unroll
-            for (int j = 0; j < KOFM_MAX_KRYLOV; ++j) {
-                if (j < k - 1) acc[2 + j] += w * vj[j * RS_W];
-                else if (j == k - 1) acc[2 + j] += w * W.U1[sm][t + 2];
-                else if (j == k) acc[2 + j] += w * W.UK[sm][t + 1];
-            }
-        }
-        cfp[0] = cf[0]; cfp[1] = cf[1]; cfp[2] = cf[2]; cfp[3] = cf[3];
+        issue_row(a, S, src, rsrc, k, ya - 1, x0, W);
+        cp_commit();
     }
+    for (int y = ya - 1; y <= yb; ++y) {
+        cp_wait_all();
+        __syncthreads();  // row y's inputs visible; row y-2's w phase finished
+        if (y + 1 <= yb) { issue_row(a, S, src, rsrc, k, y + 1, x0, W); }
+        cp_commit();
+        // ---- u_k(y) on the two own columns and the halo columns -------------------
+        const int sr = y % 3, s0 = y & 3;
+        const bool rowin = y >= ya && y < yb;
+        for (int e = 0; e < 2; ++e) {
+            const int cc = c + e;
+            const double u = uk_at(W, k, y, cc + 1, [&](int q) { return W.CF[sr][q][cc]; },
+                                   [&](int j) { return W.VJ[sr][j][cc]; });
+            W.UK[s0][cc + 1] = u;
+            if (rowin && (e == 0 ? real0 : real1)) {
+                __stcg(S.V + (long long)k * D + (long long)y * a.P + x0 + cc, (vec_t)u);
+                acc[0] += u * u;
+                acc[1] += W.RR[sr][cc] * u;
+            }
+        }
+        if (t == 0)
+            W.UK[s0][0] = uk_at(W, k, y, 0, [&](int q) { return W.CFH[sr][0][q][1]; },
+                                [&](int j) { return W.VJH[sr][0][j][1]; });
+        if (t == GM_THREADS - 1)
+            W.UK[s0][RS_W + 1] = uk_at(W, k, y, RS_W + 1, [&](int q) { return W.CFH[sr][1][q][0]; },
+                                       [&](int j) { return W.VJH[sr][1][j][0]; });
+        __syncthreads();
+        // ---- w = A u_k at row y-1, dots with u_j(y-1) ----------------------------
+        const int ym = y - 1;
+        if (need_w && ym >= ya && ym < yb) {
+            const int sm = ym & 3, smm = (ym - 1) & 3, sp = y & 3, srm = ym % 3;
+            for (int e = 0; e < 2; ++e) {
+                const int cc = c + e;
+                if (!(e == 0 ? real0 : real1)) continue;
+                const int i = cc + 1;  // UK column
+                const double w = W.CF[srm][3][cc] * W.UK[smm][i] + W.CF[srm][1][cc] * W.UK[sm][i - 1] +
+                                 W.UK[sm][i] + W.CF[srm][0][cc] * W.UK[sm][i + 1] +
+                                 W.CF[srm][2][cc] * W.UK[sp][i];
+#pragma unroll
+                for (int j = 0; j < KOFM_MAX_KRYLOV; ++j) {
+                    if (j < k - 1) acc[2 + j] += w * W.VJ[srm][j][cc];
+                    else if (j == k - 1) acc[2 + j] += w * W.U1[sm][cc + 2];
+                    else if (j == k) acc[2 + j] += w * W.UK[sm][i];
+                }
+            }
+        }
+    }
+    cp_wait_all();
 }
 
 // ---- the solver kernel ---------------------------------------------------------
 __global__ void __launch_bounds__(GM_THREADS, KOFM_GM_MINBLOCKS)
 gmres_kernel(const GmresArgs a) {
     GmresControl* ctl = a.ctl;
-    __shared__ RowWin T;
+    extern __shared__ __align__(16) unsigned char gm_smem[];
+    RowWin& T = *reinterpret_cast<RowWin*>(gm_smem);  // dynamic: larger than 48 KiB
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
     const long long npairs = a.D / 2;
