@@ -99,6 +99,10 @@ typedef struct kofm_desc {
     double komega_rel_tol;    /* KOMEGA_MAX_REL_TOL (1e-4) */
     double komega_abs_tol;    /* KOMEGA_MAX_ABS_TOL (1e-7) */
     double komega_dt;         /* initial k-omega time step (p.dTlb = 1) */
+    int32_t komega_full_cycle;/* 1: always build all krylov_dim vectors of a
+                                 restart cycle, as GMRESSolver::solve does;
+                                 0 (default): end the cycle as soon as its
+                                 truncation tests fire (see kofm_komega_solve) */
 } kofm_desc;
 
 /* Per-context counters of the last k-omega update (kOmega::Solve). */
@@ -172,7 +176,13 @@ int kofm_komega_assemble(kofm_ctx* ctx, double dt);
 /* Solves the assembled systems and updates omega and k:
  * OmegaGMRES.solve(); KappaGMRES.solve() (kOmega.cpp:68-70;
  * GMRESSolver::solve, GMRESSolver.cpp:227-355).  Both run in one
- * device-resident launch.  iters/rel_res receive (omega, k) pairs; either
+ * device-resident launch.  The reference builds all krylov_dim vectors of a
+ * cycle and only then applies its truncation tests (diag(R) against
+ * relTol * R(0,0), then |xi_i| >= rho); the default here applies the same
+ * tests as each vector is made and stops at the first that fires, which gives
+ * the reference's update unless a diag(R) cut would fall after the xi cut
+ * (the reference then indexes its back-substitution with that later cut).
+ * komega_full_cycle = 1 keeps the reference's full cycle.  iters/rel_res receive (omega, k) pairs; either
  * may be NULL.  Returns KOFM_ERR_NAN if a residual was NaN (the caller's
  * kOmega::Solve halves dt), KOFM_ERR_NOT_CONVERGED at the iteration cap. */
 int kofm_komega_solve(kofm_ctx* ctx, int32_t* iters, double* rel_res);

@@ -44,6 +44,7 @@ class KofmDesc(C.Structure):
         ("komega_max_iters", C.c_int32), ("krylov_dim", C.c_int32),
         ("komega_rel_tol", C.c_double), ("komega_abs_tol", C.c_double),
         ("komega_dt", C.c_double),
+        ("komega_full_cycle", C.c_int32),
     ]
 
 

@@ -342,6 +342,7 @@ int kofm_desc_default(kofm_desc* d) {
     d->komega_rel_tol = 1.0e-4;   // KOMEGA_MAX_REL_TOL
     d->komega_abs_tol = 1.0e-7;   // KOMEGA_MAX_ABS_TOL
     d->komega_dt = 1.0;           // p.dTlb
+    d->komega_full_cycle = 0;     // end each cycle at its first truncation
     return KOFM_OK;
 }
 

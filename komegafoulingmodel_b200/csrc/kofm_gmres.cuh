@@ -54,7 +54,7 @@ struct GmresSys {
     int cycles;     // Krylov cycles run (restarts that did not converge)
     int iters;      // iterCount
     int kk;         // number of update coefficients used
-    int pad;
+    int done;       // current cycle finished (no more Krylov vectors needed)
     double rho0, norm_rhs, rinv, rho, prev_err;
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||
     double h[KOFM_MAX_KRYLOV];   // Gram-Schmidt coefficients for the next vector
@@ -89,6 +89,7 @@ struct GmresArgs {
     int max_restarts;
     double rel_tol, abs_tol;
     long long spin_limit;     // barrier spin bound (polls of >= 100 ns)
+    int full_cycle;           // 1: build all K vectors before the truncation tests
     int strips, chunks, chunk_rows;  // row-streaming work units
 };
 
@@ -160,6 +161,31 @@ enum SerialKind : int {
     SER_KRYLOV,     // after the pass that made u_k (kcur = k)
 };
 
+// Back-substitution and update coefficients for a cycle cut at k with R
+// indexed by stride `full` (GMRESSolver.cpp:330-343).
+__device__ void cycle_finish(GmresSys& S, int K, int k, int full) {
+    for (int i2 = k - 1; i2 > -1; --i2) {
+        for (int j = i2 + 1; j < k; ++j) S.xi[i2] -= S.R[i2 + j * full] * S.xi[j];
+        S.xi[i2] /= S.R[i2 + i2 * full];
+    }
+    for (int i = 0; i < k; ++i) S.xi[i] *= S.rho0;
+    for (int i = 0; i < K; ++i) S.c[i] = S.xi[i];
+    S.kk = k;
+    S.prev_err = fabs(S.rho * S.rho0 / S.norm_rhs);
+    S.done = 1;
+}
+
+// The reference's tests applied as vector k becomes available: the diag(R)
+// cut at k (then full = k), else one xi-test iteration (iterCount += 1;
+// |xi_k| >= rho cuts at k with full = K), else the estimator update.
+__device__ void cycle_step(GmresSys& S, int K, int k, double rel_tol) {
+    if (fabs(S.R[k + k * K]) < rel_tol * S.R[0]) { cycle_finish(S, K, k, k); return; }
+    S.iters += 1;
+    if (S.xi[k] >= S.rho || S.xi[k] <= -S.rho) { cycle_finish(S, K, k, K); return; }
+    S.rho *= sin(acos(S.xi[k] / S.rho));
+    if (k == K - 1) cycle_finish(S, K, K, K);
+}
+
 // End of one restart cycle for one system (GMRESSolver.cpp:300-350).
 __device__ void cycle_logic(GmresSys& S, int K, double rel_tol) {
     int k = K;
@@ -179,6 +205,7 @@ __device__ void cycle_logic(GmresSys& S, int K, double rel_tol) {
     for (int i = 0; i < K; ++i) S.c[i] = S.xi[i];
     S.kk = k;
     S.prev_err = fabs(S.rho * S.rho0 / S.norm_rhs);
+    S.done = 1;
 }
 
 // Serial section: executed by all threads of the last-arriving block.  The
@@ -204,7 +231,7 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
             for (int i = threadIdx.x; i < NW; i += GM_THREADS) dst[i] = __ldcg(src + i);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && sS.active) {
+        if (threadIdx.x == 0 && sS.active && !(kind == SER_KRYLOV && sS.done)) {
             GmresSys& S = sS;
             const double* t = tot + GM_SYS_SLOTS * s;
             if (kind == SER_RESIDUAL) {
@@ -216,7 +243,7 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
                 const double resid = S.rho0 / S.norm_rhs;
                 if (isnan(resid)) { S.nan = 1; S.active = 0; }
                 else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
-                else { S.cycles += 1; }
+                else { S.cycles += 1; S.done = 0; }
             } else if (kind == SER_KRYLOV) {
                 // t[0] = ||u_k||^2, t[1] = <r_raw, u_k>, t[2 + j] = <A u_k, u_j> (j <= k)
                 const int k = kcur, K = a.K;
@@ -230,14 +257,17 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
                     S.R[k + k * K] = nk;
                 }
                 S.xi[k] = S.rinv * t[1] * S.s[k];  // <r, v_k>
-                if (k < K - 1) {
+                if (a.full_cycle) {
+                    if (k == K - 1) cycle_logic(S, K, a.rel_tol);
+                } else {
+                    cycle_step(S, K, k, a.rel_tol);
+                }
+                if (!S.done && k < K - 1) {
                     // h_j = <A v_k, v_j> with v = s u
                     for (int j = 0; j <= k; ++j) S.h[j] = S.s[k] * S.s[j] * t[2 + j];
-                } else {
-                    cycle_logic(S, K, a.rel_tol);
                 }
             }
-            s_any |= S.active;
+            s_any |= kind == SER_KRYLOV ? (S.active && !S.done) : S.active;
         }
         __syncthreads();
         {
@@ -539,8 +569,10 @@ gmres_kernel(const GmresArgs a) {
 
         // ---- K fused Krylov passes ---------------------------------------------
         for (int k = 0; k < K; ++k) {
-            if (threadIdx.x < 2) sh_act[threadIdx.x] = ldc(&ctl->sys[threadIdx.x].active);
+            if (threadIdx.x < 2)
+                sh_act[threadIdx.x] = ldc(&ctl->sys[threadIdx.x].active) && !ldc(&ctl->sys[threadIdx.x].done);
             __syncthreads();
+            if (!sh_act[0] && !sh_act[1]) break;  // block-uniform, same in every block
             for (int s = 0; s < 2; ++s) {
                 double acc[2 + KOFM_MAX_KRYLOV];
 #pragma unroll

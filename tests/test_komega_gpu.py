@@ -29,23 +29,25 @@ def channel_case(nx=256, ny=66, u_max=0.05, nu=5e-4):
     return ch, f, k, o, nut, rate, g, nu
 
 
-def make_lattice(ch, rate, g, nu, krylov=10):
+def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0):
     d = desc_default()
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = rate, g, nu
     d.use_komega = 1
     d.krylov_dim = krylov
+    d.komega_full_cycle = full_cycle
     L = Lattice(d)
     L.set_geometry(ch.ntype, ch.wallD, ch.dX)
     return L
 
 
-def test_one_update_matches_oracle(kofm_lib, oracle):
+@pytest.mark.parametrize("full_cycle", [0, 1])
+def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle):
     ch, f, k, o, nut, rate, g, nu = channel_case(nx=128, ny=34)
     cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
     sim.step(2)
-    with make_lattice(ch, rate, g, nu) as L:
+    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle) as L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
         L.step(2)
         st = L.stats()
@@ -66,13 +68,27 @@ def test_one_update_matches_oracle(kofm_lib, oracle):
     assert rel_l2(nut2, sim.nut, fl) < 1e-4
 
 
-def test_channel_1000_steps_parity(kofm_lib, oracle):
-    """rho, u, k, omega within rel-L2 1e-5 of the FP64 oracle after 1000 steps."""
+_ORACLE_1000 = {}
+
+
+def _oracle_channel_1000(oracle):
+    if "sim" not in _ORACLE_1000:
+        ch, f, k, o, nut, rate, g, nu = channel_case()
+        cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+        sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
+        sim.step(1000)
+        _ORACLE_1000["sim"] = sim
+    return _ORACLE_1000["sim"]
+
+
+@pytest.mark.parametrize("full_cycle", [0, 1])
+def test_channel_1000_steps_parity(kofm_lib, oracle, full_cycle):
+    """rho, u, k, omega within rel-L2 1e-5 of the FP64 oracle after 1000
+    steps, with cycles ended at their first truncation (default) and with the
+    reference's full cycles."""
     ch, f, k, o, nut, rate, g, nu = channel_case()
-    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
-    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
-    sim.step(1000)
-    with make_lattice(ch, rate, g, nu) as L:
+    sim = _oracle_channel_1000(oracle)
+    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle) as L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
         L.step(1000)
         rho, ux, uy = L.get_macro()
