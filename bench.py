@@ -100,19 +100,29 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------
 def solver_bytes_per_node(stats, K):
-    """Algorithmic bytes per lattice node of one solver launch (both systems):
-    every array the restarted simpler-GMRES sweeps must read or write once,
-    all FP64.  Krylov vector k: u_{k-1} (or r), the older basis vectors u_j
-    (j < k-1), the four stencil coefficients, r, and the store of u_k.  Halo
-    rows / columns re-read from L2 are not counted."""
+    """Algorithmic bytes per lattice node of one solver launch (both systems),
+    from the launch's own counts of the passes it made; every array is FP64.
+
+    * residual pass: restart 0 reads b' (8); a later restart forms
+      r = b' - A x from b', x, the four coefficients and stores r (56);
+    * Krylov vector k of a cycle: u_{k-1} (or r) and the older basis vectors
+      u_j (j < k-1), the four coefficients, r for <r, u_k>, and the store of
+      u_k: 48 + 8 k;
+    * cycle update: r, the kk - 1 basis vectors with a non-zero coefficient,
+      x (after the first cycle) and the store of x;
+    * write-back: x, the field (FP32 read + write) and the node flag.
+    Halo rows and columns re-read from L2 or shared memory are not counted."""
     total = 0
-    for restarts, cycles, iters in ((stats.omega_restarts, stats.omega_cycles, stats.omega_iters),
-                                    (stats.k_restarts, stats.k_cycles, stats.k_iters)):
-        res = 8 + 56 * max(restarts - 1, 0)          # restart 0 reads b'; later r = b' - A x
-        per_cycle = 48 + sum(8 * k + 48 for k in range(1, K))
-        kk = max(1, iters // max(cycles, 1))
-        upd = cycles * (16 + 8 * (kk - 1)) + 8 * max(cycles - 1, 0)
-        total += res + cycles * per_cycle + upd + 16   # + write-back x, field
+    for sysname in ("omega", "k"):
+        restarts = getattr(stats, sysname + "_restarts")
+        cycles = getattr(stats, sysname + "_cycles")
+        vecs = getattr(stats, sysname + "_vectors")
+        vsum = getattr(stats, sysname + "_vec_index_sum")
+        terms = getattr(stats, sysname + "_update_terms")
+        res = 8 + 56 * max(restarts - 1, 0)
+        kry = 48 * vecs + 8 * vsum
+        upd = 16 * cycles + 8 * max(terms - cycles, 0) + 8 * max(cycles - 1, 0)
+        total += res + kry + upd + 18
     return total
 
 
@@ -265,6 +275,7 @@ def run_ours(args, rank, world, local_rank):
             "kernels": kern,
             "solver": {"omega_iters": st.omega_iters, "k_iters": st.k_iters,
                        "omega_restarts": st.omega_restarts, "k_restarts": st.k_restarts,
+                       "omega_vectors": st.omega_vectors, "k_vectors": st.k_vectors,
                        "passes": st.solver_passes},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,

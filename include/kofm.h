@@ -110,6 +110,9 @@ typedef struct kofm_stats {
     int32_t omega_iters, k_iters;       /* GMRESSolver::iterCount */
     int32_t omega_restarts, k_restarts; /* restart-loop iterations entered */
     int32_t omega_cycles, k_cycles;     /* Krylov cycles run */
+    int32_t omega_vectors, k_vectors;   /* Krylov vectors built (device passes) */
+    int32_t omega_vec_index_sum, k_vec_index_sum; /* sum of in-cycle indices */
+    int32_t omega_update_terms, k_update_terms;   /* sum of update lengths kk */
     int32_t omega_nan, k_nan;           /* NaN residual seen */
     int32_t steps_per_lb;               /* kOmega::stepsPerLB */
     int32_t time_since_change;          /* kOmega::timeSinceTimeStepChange */

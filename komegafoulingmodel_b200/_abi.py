@@ -53,6 +53,9 @@ class KofmStats(C.Structure):
         ("omega_iters", C.c_int32), ("k_iters", C.c_int32),
         ("omega_restarts", C.c_int32), ("k_restarts", C.c_int32),
         ("omega_cycles", C.c_int32), ("k_cycles", C.c_int32),
+        ("omega_vectors", C.c_int32), ("k_vectors", C.c_int32),
+        ("omega_vec_index_sum", C.c_int32), ("k_vec_index_sum", C.c_int32),
+        ("omega_update_terms", C.c_int32), ("k_update_terms", C.c_int32),
         ("omega_nan", C.c_int32), ("k_nan", C.c_int32),
         ("steps_per_lb", C.c_int32), ("time_since_change", C.c_int32),
         ("dt", C.c_double), ("omega_rel_res", C.c_double), ("k_rel_res", C.c_double),

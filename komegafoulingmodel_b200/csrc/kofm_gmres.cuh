@@ -55,6 +55,10 @@ struct GmresSys {
     int iters;      // iterCount
     int kk;         // number of update coefficients used
     int done;       // current cycle finished (no more Krylov vectors needed)
+    int vecs;       // Krylov vectors built (all cycles)
+    int vec_index_sum;  // sum over built vectors of their index k in the cycle
+    int update_terms;   // sum over cycles of the update's coefficient count kk
+    int pad;
     double rho0, norm_rhs, rinv, rho, prev_err;
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||
     double h[KOFM_MAX_KRYLOV];   // Gram-Schmidt coefficients for the next vector
@@ -171,6 +175,7 @@ __device__ void cycle_finish(GmresSys& S, int K, int k, int full) {
     for (int i = 0; i < k; ++i) S.xi[i] *= S.rho0;
     for (int i = 0; i < K; ++i) S.c[i] = S.xi[i];
     S.kk = k;
+    S.update_terms += k;
     S.prev_err = fabs(S.rho * S.rho0 / S.norm_rhs);
     S.done = 1;
 }
@@ -204,6 +209,7 @@ __device__ void cycle_logic(GmresSys& S, int K, double rel_tol) {
     for (int i = 0; i < k; ++i) S.xi[i] *= S.rho0;
     for (int i = 0; i < K; ++i) S.c[i] = S.xi[i];
     S.kk = k;
+    S.update_terms += k;
     S.prev_err = fabs(S.rho * S.rho0 / S.norm_rhs);
     S.done = 1;
 }
@@ -248,6 +254,8 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
                 // t[0] = ||u_k||^2, t[1] = <r_raw, u_k>, t[2 + j] = <A u_k, u_j> (j <= k)
                 const int k = kcur, K = a.K;
                 const double nk = sqrt(t[0]);
+                S.vecs += 1;
+                S.vec_index_sum += k;
                 S.s[k] = 1.0 / nk;
                 if (k == 0) {
                     for (int i = 0; i < K * K; ++i) S.R[i] = 0.0;
