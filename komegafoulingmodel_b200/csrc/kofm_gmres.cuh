@@ -13,14 +13,13 @@
 //    k are independent in the reference, kOmega.cpp:68-70) with no host
 //    round-trip; the reference needs >= 4 blocking host synchronisations and
 //    ~40 kernel launches per restart.
-//  * One fused sweep per Krylov vector.  A block marches down a strip of
-//    columns keeping rolling rows of u_{k-1} and u_k in shared memory; per
-//    row it recomputes z_k = A u_{k-1}, orthogonalises
+//  * One fused sweep per Krylov vector.  A warp marches down a strip of 32
+//    columns; per row it computes z_k = A u_{k-1}, orthogonalises
 //    u_k = s_{k-1} z_k - sum_j h_j s_j u_j (classical Gram-Schmidt, the
-//    reference's order), writes u_k, and one row behind applies the stencil
-//    to u_k to get w = A u_k for the NEXT vector's Gram-Schmidt dot
-//    products -- so each vector costs one sweep and one grid barrier instead
-//    of the reference's product / two Gram-Schmidt stages / normalise.
+//    reference's order), writes u_k, and accumulates the dot products
+//    <A u_k, u_j> of the NEXT vector's Gram-Schmidt step row by row -- so
+//    each vector costs one sweep and one grid barrier instead of the
+//    reference's product / two Gram-Schmidt stages / normalise.
 //    Krylov vectors are kept un-normalised; the scales 1/||u_j|| are applied
 //    lazily.  Vectors and matrix are FP64 (an FP32 basis stalls the first
 //    cycle near 1e-5 relative residual on the omega wall rows).
@@ -39,7 +38,7 @@
 
 namespace kofm {
 
-constexpr int GM_THREADS = 128;
+constexpr int GM_THREADS = 256;
 #ifndef KOFM_GM_MINBLOCKS
 #define KOFM_GM_MINBLOCKS 2  // resident blocks per SM the register budget targets
 #endif
@@ -94,7 +93,8 @@ struct GmresArgs {
     double rel_tol, abs_tol;
     long long spin_limit;     // barrier spin bound (polls of >= 100 ns)
     int full_cycle;           // 1: build all K vectors before the truncation tests
-    int strips, chunks, chunk_rows;  // row-streaming work units
+    int strips;               // 32-column strips
+    int units_warps;          // warps that take part in a Krylov pass
 };
 
 // ---- coherent access to data written inside the launch (bypass L1) --------
@@ -330,31 +330,42 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
     return ldc(&a.ctl->error) == 0;
 }
 
-// ---- row-streaming Krylov pass ----------------------------------------------
-// A work unit is a strip of RS_W = 256 columns times a chunk of rows.  Each of
-// the 128 threads owns two adjacent columns (16-byte copies); the edge threads
-// also carry the column just outside the strip.  The block marches down the
-// rows keeping rolling rows of u_{k-1} (or r) and of u_k in shared memory:
-//   row y:   u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j on the strip plus one
-//            column each side; store u_k(y);  dots ||u_k||^2, <r, u_k>;
-//   row y-1: w = A u_k on the strip -> dots <w, u_j> for the next vector.
-// The inputs of row y+1 (u_{k-1} of row y+2, the coefficients, the older
-// basis vectors and r of row y+1) are copied into shared memory with
-// cp.async.cg while row y computes.  Vectors and coefficients are zero on
-// every non-fluid node, so no fluid test is needed in the sweep.
-constexpr int RS_W = 2 * GM_THREADS;
-constexpr int RS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
+// ---- warp-strip Krylov pass ---------------------------------------------------
+// A work unit is a strip of 32 columns (lane l <-> column x0 + l) times a
+// range of rows, owned by ONE warp, which marches down the rows:
+//   row y:  u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j; store u_k(y);
+//           dots ||u_k||^2 and <r, u_k>;
+//           <A u_k, u_j> split by rows: row y adds u_j(y) (u_k + W u_k(x-1) +
+//           E u_k(x+1) + S u_k(y-1)) and the N term of row y-1,
+//           u_k(y) N(y-1) u_j(y-1), carried in registers as q_j.
+// x neighbours come from warp shuffles; lanes 0 and 31 also compute u_k on
+// the ghost columns x0-1 and x0+32 (the neighbouring strips' edge columns).
+// Every lane streams its own column's inputs of row y+2 into its own slots of
+// a 3-row shared-memory ring (cp.async, 8 bytes each) while row y computes, so
+// the pass needs no block-level synchronisation and keeps two rows of loads in
+// flight per warp.  Vectors and coefficients are zero on non-fluid nodes and
+// rows outside the lattice read as zero.  Columns are taken modulo nx
+// (periodic x; the padding columns of the last strip alias real columns and
+// are neither stored nor counted).
+constexpr int WS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
+constexpr int WS_SLOTS = 3;
+constexpr int GM_WARPS = GM_THREADS / 32;
 
-struct RowWin {
-    double U1[4][RS_W + 4];            // u_{k-1} (or r) rows; column i <-> x0 - 2 + i
-    double UK[4][RS_W + 2];            // u_k rows;             column i <-> x0 - 1 + i
-    double VJ[3][RS_KV][RS_W];         // u_j (j < k-1), own columns
-    double VJH[3][2][RS_KV][2];        // u_j of the halo pairs (left, right)
-    double CF[3][4][RS_W];             // coefficients E, W, N, S, own columns
-    double CFH[3][2][4][2];            // coefficients of the halo pairs
-    double RR[3][RS_W];                // r, own columns
-    double g[KOFM_MAX_KRYLOV];         // h_j s_j
-    double sk1;                        // s_{k-1}
+struct WarpSlot {
+    double cf[4][32];          // E, W, N, S of row y
+    double vj[WS_KV][32];      // u_j(y), j < k-1
+    double r[32];              // r(y) (k >= 1)
+    double up[32];             // u_{k-1}(y+1)
+    double gcf[2][4];          // ghost columns x0-1 (0) and x0+32 (1): coefficients
+    double gvj[2][WS_KV];      // ... u_j(y)
+    double gup[2];             // ... u_{k-1}(y+1)
+    double gout[2];            // u_{k-1}(y) at x0-2 and x0+33
+};
+
+struct SolverSmem {
+    WarpSlot ring[GM_WARPS][WS_SLOTS];
+    double g[KOFM_MAX_KRYLOV];  // h_j s_j
+    double sk1;                 // s_{k-1}
 };
 
 __device__ __forceinline__ int wrap_mod(int x, int n) {
@@ -362,151 +373,177 @@ __device__ __forceinline__ int wrap_mod(int x, int n) {
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ void cp16(void* smem, const void* gmem) {
+__device__ __forceinline__ void cp8(double* smem, const double* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Copy the pair of doubles at (y, columns x, x+1 mod nx) into dst[0..1]:
-// one 16-byte async copy when the pair is contiguous, two 8-byte plain loads
-// at the periodic seam of an odd nx; zeros outside the rows.
-__device__ __forceinline__ void pair_copy(const GmresArgs& a, const double* base, int y, int x,
-                                          double* dst) {
-    if (y < 0 || y >= a.ny) { dst[0] = 0.0; dst[1] = 0.0; return; }
-    const int xa = wrap_mod(x, a.nx), xb = wrap_mod(x + 1, a.nx);
-    const long long row = (long long)y * a.P;
-    if (xb == xa + 1 && (xa & 1) == 0) {
-        cp16(dst, base + row + xa);
-    } else {
-        dst[0] = __ldcg(base + row + xa);
-        dst[1] = __ldcg(base + row + xb);
-    }
+// element (y, x) of a lattice array into shared memory; zero outside the rows
+__device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, int y, int x, double* dst) {
+    if (y < 0 || y >= a.ny) *dst = 0.0;
+    else cp8(dst, base + (long long)y * a.P + x);
 }
 
-// Async copies of everything row y needs, except u_{k-1}(y+1) (own row slot
-// y % 3) plus u_{k-1} row y + 1 (slot (y+1) & 3).
-__device__ __forceinline__ void issue_row(const GmresArgs& a, const KoSystem& S, const vec_t* src,
-                                          const vec_t* rsrc, int k, int y, int x0, RowWin& W) {
-    const int t = threadIdx.x, c = 2 * t;
+// The thread's inputs of row y into slot W: u_{k-1}(y+1), and for rows inside
+// the lattice the coefficients, u_j (j < k-1) and r; lanes 0 / 31 add their
+// ghost column.
+__device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
+                                         const double* rsrc, int k, int y, int xl, int lane,
+                                         int gin, int gout, WarpSlot& W) {
     const long long D = a.D;
-    // u_{k-1} of row y+1 (and the halo pairs)
-    {
-        const int yu = y + 1, su = yu & 3;
-        pair_copy(a, src, yu, x0 + c, &W.U1[su][c + 2]);
-        if (t == 0) pair_copy(a, src, yu, x0 - 2, &W.U1[su][0]);
-        if (t == GM_THREADS - 1) pair_copy(a, src, yu, x0 + RS_W, &W.U1[su][RS_W + 2]);
+    el_copy(a, src, y + 1, xl, &W.up[lane]);
+    const bool ghost = lane == 0 || lane == 31;
+    const int h = lane == 0 ? 0 : 1;
+    if (ghost) {
+        el_copy(a, src, y + 1, gin, &W.gup[h]);
+        el_copy(a, src, y, gout, &W.gout[h]);
     }
-    const int sr = y % 3;
     if (y < 0 || y >= a.ny) {
-        for (int q = 0; q < 4; ++q) { W.CF[sr][q][c] = 0.0; W.CF[sr][q][c + 1] = 0.0; }
-        for (int j = 0; j < RS_KV; ++j) { W.VJ[sr][j][c] = 0.0; W.VJ[sr][j][c + 1] = 0.0; }
-        W.RR[sr][c] = 0.0; W.RR[sr][c + 1] = 0.0;
-        if (t == 0 || t == GM_THREADS - 1) {
-            const int h = t == 0 ? 0 : 1;
-            for (int q = 0; q < 4; ++q) { W.CFH[sr][h][q][0] = 0.0; W.CFH[sr][h][q][1] = 0.0; }
-            for (int j = 0; j < RS_KV; ++j) { W.VJH[sr][h][j][0] = 0.0; W.VJH[sr][h][j][1] = 0.0; }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) W.cf[q][lane] = 0.0;
+        for (int j = 0; j < k - 1; ++j) W.vj[j][lane] = 0.0;
+        W.r[lane] = 0.0;
+        if (ghost) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) W.gcf[h][q] = 0.0;
+            for (int j = 0; j < k - 1; ++j) W.gvj[h][j] = 0.0;
         }
         return;
     }
-    for (int q = 0; q < 4; ++q) pair_copy(a, S.coef + q * D, y, x0 + c, &W.CF[sr][q][c]);
-    for (int j = 0; j < k - 1; ++j) pair_copy(a, S.V + (long long)j * D, y, x0 + c, &W.VJ[sr][j][c]);
-    pair_copy(a, rsrc, y, x0 + c, &W.RR[sr][c]);
-    if (t == 0 || t == GM_THREADS - 1) {
-        const int h = t == 0 ? 0 : 1;
-        const int xh = t == 0 ? x0 - 2 : x0 + RS_W;  // pair holding the halo column
-        for (int q = 0; q < 4; ++q) pair_copy(a, S.coef + q * D, y, xh, &W.CFH[sr][h][q][0]);
-        for (int j = 0; j < k - 1; ++j) pair_copy(a, S.V + (long long)j * D, y, xh, &W.VJH[sr][h][j][0]);
+    const long long row = (long long)y * a.P;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cp8(&W.cf[q][lane], S.coef + q * D + row + xl);
+    for (int j = 0; j < k - 1; ++j) cp8(&W.vj[j][lane], S.V + (long long)j * D + row + xl);
+    if (k > 0) cp8(&W.r[lane], rsrc + row + xl);
+    if (ghost) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cp8(&W.gcf[h][q], S.coef + q * D + row + gin);
+        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj[h][j], S.V + (long long)j * D + row + gin);
     }
 }
 
-// u_k at UK column i of row y; cf(q) and vj(j) give the node's coefficients
-// and older basis vectors.
-template <typename CF, typename VJ>
-__device__ __forceinline__ double uk_at(const RowWin& W, int k, int y, int i, CF cf, VJ vj) {
-    const int c = i + 1;  // same column in U1
-    const int s0 = y & 3, sm = (y - 1) & 3, sp = (y + 1) & 3;
-    // CSR order of an interior row: S, W, C, E, N
-    const double z = cf(3) * W.U1[sm][c] + cf(1) * W.U1[s0][c - 1] + W.U1[s0][c] +
-                     cf(0) * W.U1[s0][c + 1] + cf(2) * W.U1[sp][c];
-    if (k == 0) return rnd(z);
-    double u = W.sk1 * z;
-    for (int j = 0; j < k - 1; ++j) u -= W.g[j] * vj(j);
-    u -= W.g[k - 1] * W.U1[s0][c];
-    return rnd(u);  // the stored value defines u_k
-}
-
-__device__ void krylov_unit(const GmresArgs& a, const KoSystem& S, const vec_t* rsrc, int k,
-                            int unit, RowWin& W, double (&acc)[2 + KOFM_MAX_KRYLOV]) {
-    const int strip = unit % a.strips, chunk = unit / a.strips;
-    const int x0 = strip * RS_W;
-    const int ya = chunk * a.chunk_rows;
-    const int yb = min(ya + a.chunk_rows, a.ny);
-    const int t = threadIdx.x, c = 2 * t;
+// One warp: rows [ya, yb) of the strip starting at column x0.
+__device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc, int k,
+                             int x0, int ya, int yb, SolverSmem& T, WarpSlot* ring,
+                             double (&acc)[2 + KOFM_MAX_KRYLOV]) {
+    const int lane = threadIdx.x & 31;
     const long long D = a.D;
-    const vec_t* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
+    const double* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
     const bool need_w = k < a.K - 1;
-    const bool real0 = x0 + c < a.nx, real1 = x0 + c + 1 < a.nx;  // not padding / alias
-    __syncthreads();  // the window may still be read by the previous unit
-    // prologue: u_{k-1} rows ya-2 and ya-1, then row ya-1's inputs (+ u_{k-1}(ya))
-    {
-        for (int yy = ya - 2; yy <= ya - 1; ++yy) {
-            const int su = yy & 3;
-            pair_copy(a, src, yy, x0 + c, &W.U1[su][c + 2]);
-            if (t == 0) pair_copy(a, src, yy, x0 - 2, &W.U1[su][0]);
-            if (t == GM_THREADS - 1) pair_copy(a, src, yy, x0 + RS_W, &W.U1[su][RS_W + 2]);
-        }
-        issue_row(a, S, src, rsrc, k, ya - 1, x0, W);
-        cp_commit();
-    }
+    const int xl = wrap_mod(x0 + lane, a.nx);
+    const bool own = x0 + lane < a.nx;
+    // lane 0: ghost column x0-1 (outer x0-2); lane 31: x0+32 (outer x0+33)
+    const int gin = wrap_mod(lane == 0 ? x0 - 1 : x0 + 32, a.nx);
+    const int gout = wrap_mod(lane == 0 ? x0 - 2 : x0 + 33, a.nx);
+    const bool ghost = lane == 0 || lane == 31;
+    double* Vk = S.V + (long long)k * D;
+
+    // rolling u_{k-1} window (rows y-1, y) on the own and the ghost column
+    auto ld = [&](int y, int x) -> double {
+        return (y < 0 || y >= a.ny) ? 0.0 : __ldcg(src + (long long)y * a.P + x);
+    };
+    double um = ld(ya - 2, xl), u0 = ld(ya - 1, xl);
+    double gm = 0.0, g0 = 0.0;
+    if (ghost) { gm = ld(ya - 2, gin); g0 = ld(ya - 1, gin); }
+    ws_issue(a, S, src, rsrc, k, ya - 1, xl, lane, gin, gout, ring[(ya - 1 + 3) % 3]);
+    cp_commit();
+    ws_issue(a, S, src, rsrc, k, ya, xl, lane, gin, gout, ring[ya % 3]);
+    cp_commit();
+
+    double q[WS_KV];
+#pragma unroll
+    for (int j = 0; j < WS_KV; ++j) q[j] = 0.0;
+    double nprev = 0.0, ukprev = 0.0;
+    const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        cp_wait_all();
-        __syncthreads();  // row y's inputs visible; row y-2's w phase finished
-        if (y + 1 <= yb) { issue_row(a, S, src, rsrc, k, y + 1, x0, W); }
+        if (y + 2 <= yb) ws_issue(a, S, src, rsrc, k, y + 2, xl, lane, gin, gout, ring[(y + 2) % 3]);
         cp_commit();
-        // ---- u_k(y) on the two own columns and the halo columns -------------------
-        const int sr = y % 3, s0 = y & 3;
-        const bool rowin = y >= ya && y < yb;
-        for (int e = 0; e < 2; ++e) {
-            const int cc = c + e;
-            const double u = uk_at(W, k, y, cc + 1, [&](int q) { return W.CF[sr][q][cc]; },
-                                   [&](int j) { return W.VJ[sr][j][cc]; });
-            W.UK[s0][cc + 1] = u;
-            if (rowin && (e == 0 ? real0 : real1)) {
-                __stcg(S.V + (long long)k * D + (long long)y * a.P + x0 + cc, (vec_t)u);
-                acc[0] += u * u;
-                acc[1] += W.RR[sr][cc] * u;
+        cp_wait<2>();
+        const WarpSlot& W = ring[(y + 3) % 3];
+        const double up = W.up[lane];
+        const double cE = W.cf[0][lane], cW = W.cf[1][lane], cN = W.cf[2][lane], cS = W.cf[3][lane];
+        double v[WS_KV];
+#pragma unroll
+        for (int j = 0; j < WS_KV; ++j) v[j] = j < k - 1 ? W.vj[j][lane] : 0.0;
+        // u_k(y) on the own column
+        double left = __shfl_up_sync(0xffffffffu, u0, 1);
+        double right = __shfl_down_sync(0xffffffffu, u0, 1);
+        if (lane == 0) left = g0;
+        if (lane == 31) right = g0;
+        // CSR order of an interior row: S, W, C, E, N
+        const double z = cS * um + cW * left + u0 + cE * right + cN * up;
+        double uk;
+        if (k == 0) {
+            uk = z;
+        } else {
+            uk = sk1 * z;
+#pragma unroll
+            for (int j = 0; j < WS_KV; ++j)
+                if (j < k - 1) uk -= T.g[j] * v[j];
+            uk -= T.g[k - 1] * u0;
+        }
+        // u_k(y) on the ghost column (lanes 0 and 31)
+        double ukg = 0.0;
+        if (ghost) {
+            const int h = lane == 0 ? 0 : 1;
+            const double gl = lane == 0 ? W.gout[h] : u0;
+            const double gr = lane == 0 ? u0 : W.gout[h];
+            const double gz = W.gcf[h][3] * gm + W.gcf[h][1] * gl + g0 + W.gcf[h][0] * gr +
+                              W.gcf[h][2] * W.gup[h];
+            if (k == 0) {
+                ukg = gz;
+            } else {
+                ukg = sk1 * gz;
+                for (int j = 0; j < k - 1; ++j) ukg -= T.g[j] * W.gvj[h][j];
+                ukg -= T.g[k - 1] * g0;
             }
         }
-        if (t == 0)
-            W.UK[s0][0] = uk_at(W, k, y, 0, [&](int q) { return W.CFH[sr][0][q][1]; },
-                                [&](int j) { return W.VJH[sr][0][j][1]; });
-        if (t == GM_THREADS - 1)
-            W.UK[s0][RS_W + 1] = uk_at(W, k, y, RS_W + 1, [&](int q) { return W.CFH[sr][1][q][0]; },
-                                       [&](int j) { return W.VJH[sr][1][j][0]; });
-        __syncthreads();
-        // ---- w = A u_k at row y-1, dots with u_j(y-1) ----------------------------
-        const int ym = y - 1;
-        if (need_w && ym >= ya && ym < yb) {
-            const int sm = ym & 3, smm = (ym - 1) & 3, sp = y & 3, srm = ym % 3;
-            for (int e = 0; e < 2; ++e) {
-                const int cc = c + e;
-                if (!(e == 0 ? real0 : real1)) continue;
-                const int i = cc + 1;  // UK column
-                const double w = W.CF[srm][3][cc] * W.UK[smm][i] + W.CF[srm][1][cc] * W.UK[sm][i - 1] +
-                                 W.UK[sm][i] + W.CF[srm][0][cc] * W.UK[sm][i + 1] +
-                                 W.CF[srm][2][cc] * W.UK[sp][i];
+        const bool rowin = y >= ya && y < yb;
+        const double rr = k == 0 ? u0 : W.r[lane];
+        if (rowin && own) {
+            __stcg(Vk + (long long)y * a.P + xl, uk);
+            acc[0] += uk * uk;
+            acc[1] += rr * uk;
+        }
+        if (need_w) {
+            double ukl = __shfl_up_sync(0xffffffffu, uk, 1);
+            double ukr = __shfl_down_sync(0xffffffffu, uk, 1);
+            if (lane == 0) ukl = ukg;
+            if (lane == 31) ukr = ukg;
+            if (own && (rowin || y == yb)) {
+                // row y's own part (zero on the halo row yb) plus row y-1's N term
+                const double aw = rowin ? uk + cW * ukl + cE * ukr + cS * ukprev : 0.0;
+                const double am = rowin ? u0 : 0.0, ak = rowin ? uk : 0.0;
 #pragma unroll
                 for (int j = 0; j < KOFM_MAX_KRYLOV; ++j) {
-                    if (j < k - 1) acc[2 + j] += w * W.VJ[srm][j][cc];
-                    else if (j == k - 1) acc[2 + j] += w * W.U1[sm][cc + 2];
-                    else if (j == k) acc[2 + j] += w * W.UK[sm][i];
+                    double t = 0.0;
+                    if (j < WS_KV && j < k - 1)
+                        t = (rowin ? v[j < WS_KV ? j : 0] : 0.0) * aw + uk * q[j < WS_KV ? j : 0];
+                    else if (j == k - 1)
+                        t = am * aw + uk * (nprev * um);
+                    else if (j == k)
+                        t = ak * aw + uk * (nprev * ukprev);
+                    acc[2 + j] += t;
                 }
             }
+            // carry the N terms of row y (zero for rows outside the unit)
+            const double nrow = rowin ? cN : 0.0;
+#pragma unroll
+            for (int j = 0; j < WS_KV; ++j) q[j] = nrow * v[j];
+            nprev = nrow;
+        }
+        ukprev = uk;
+        um = u0;
+        u0 = up;
+        if (ghost) {
+            gm = g0;
+            g0 = W.gup[lane == 0 ? 0 : 1];
         }
     }
-    cp_wait_all();
+    cp_wait<0>();
 }
 
 // ---- the solver kernel ---------------------------------------------------------
@@ -514,13 +551,15 @@ __global__ void __launch_bounds__(GM_THREADS, KOFM_GM_MINBLOCKS)
 gmres_kernel(const GmresArgs a) {
     GmresControl* ctl = a.ctl;
     extern __shared__ __align__(16) unsigned char gm_smem[];
-    RowWin& T = *reinterpret_cast<RowWin*>(gm_smem);  // dynamic: larger than 48 KiB
+    SolverSmem& T = *reinterpret_cast<SolverSmem*>(gm_smem);  // dynamic: larger than 48 KiB
+    WarpSlot* ring = T.ring[threadIdx.x >> 5];
+    const int gwarp = blockIdx.x * GM_WARPS + (threadIdx.x >> 5);
+    const long long nwarps_total = (long long)a.units_warps;
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
     const long long npairs = a.D / 2;
     const long long stride = (long long)gridDim.x * GM_THREADS;
     const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
-    const int nunits = a.strips * a.chunks;
     const int K = a.K;
 
     for (int restart = 0; restart < a.max_restarts; ++restart) {
@@ -593,8 +632,18 @@ gmres_kernel(const GmresArgs a) {
                     if (threadIdx.x == 0 && k > 0) T.sk1 = ldc(&C->s[k - 1]);
                     __syncthreads();
                     const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
-                    for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x)
-                        krylov_unit(a, S, rsrc, k, unit, T, acc);
+                    if (gwarp < nwarps_total) {
+                        // this warp's share of the flattened (strip, row) sequence
+                        const long long total = (long long)a.strips * a.ny;
+                        long long f = total * gwarp / nwarps_total;
+                        const long long f1 = total * (gwarp + 1) / nwarps_total;
+                        while (f < f1) {
+                            const int strip = (int)(f / a.ny), ya = (int)(f - (long long)strip * a.ny);
+                            const int yb = (int)min((long long)a.ny, (long long)ya + (f1 - f));
+                            krylov_strip(a, S, rsrc, k, strip * 32, ya, yb, T, ring, acc);
+                            f += yb - ya;
+                        }
+                    }
                 }
                 block_reduce_slots<2 + KOFM_MAX_KRYLOV>(acc, sh_act[s] ? nslots : 0, a.part,
                                                         GM_SYS_SLOTS * s);
