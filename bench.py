@@ -126,6 +126,23 @@ def solver_bytes_per_node(stats, K):
     return total
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The slowest rank's time: all-reduce MAX over the process group (NCCL
+    on the GPU box; gloo with a CPU tensor in the tests)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(nodes: int, steps: int, world: int, ms: float) -> float:
+    """Whole-job MLUPS of N independent replicas: every rank's node updates
+    over the slowest rank's time."""
+    return nodes * steps * world / (ms * 1e-3) / 1e6
+
+
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90}   # k-omega collide, per node
 ASM_BYTES = 122                                     # fused assembly, per node
 
@@ -173,13 +190,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local_rank}")
     st = L.stats()
-    value = nodes * args.steps * world / (ms * 1e-3) / 1e6
+    value = replica_value(nodes, args.steps, world, ms)
     launches_per_step = 3 + 0  # collide, assembly, solver (per k-omega sub-step)
 
     # ---- per-kernel breakdown (same stream, CUDA events) ------------------------
@@ -239,11 +252,7 @@ def run_ours(args, rank, world, local_rank):
             _abi.check("reduce", lib.kofm_reduce(ctx, _abi.FIELD_UX, _abi.OP_SUM, C.byref(out)))
         _abi.check("get_macro", lib.kofm_get_macro(ctx, dp(hr), dp(hu), None))
         t1 = time.perf_counter()
-        secs = t1 - t0
-        if world > 1:
-            t = torch.tensor([secs], device=f"cuda:{local_rank}")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            secs = float(t.item())
+        secs = max_over_ranks(t1 - t0, world, f"cuda:{local_rank}")
         h2d = 8 * (9 * n + 3 * n + 3 * n)
         d2h = 8 * 2 * args.steps + 8 * 2 * n
         e2e = {"value": nodes * args.steps * world / secs / 1e6, "unit": UNIT,
@@ -284,7 +293,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_sample(w, steps=2, warmup=0):
+def cpu_reference_sample(w, steps=2, warmup=0, budget_s=None):
     """The reference's CPU code of the path on this host's cores: the OpenCL
     kernel sources compiled as C++ (oracle/_ref) for collide and assembly plus
     the C restatement of GMRESSolver::solve; full-lattice steps."""
@@ -331,15 +340,19 @@ def cpu_reference_sample(w, steps=2, warmup=0):
     for _ in range(warmup):
         one_step()
     t0 = time.perf_counter()
+    done = 0
     for _ in range(steps):
         one_step()
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
     secs = time.perf_counter() - t0
     cores = len(os.sched_getaffinity(0))
-    return {"value": w.nodes * steps / secs / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{steps} full steps of {w.name} ({w.nodes} nodes): reference kernels "
-                      "(oracle/_ref) for collide + k-omega assembly, C restatement of its "
-                      "GMRES(10); OpenMP over rows",
-            "seconds": secs}
+    return {"value": w.nodes * done / secs / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{done} of {steps} full steps of {w.name} ({w.nodes} nodes), "
+                      f"after {warmup} untimed: reference kernels (oracle/_ref) for collide + "
+                      "k-omega assembly, C restatement of its GMRES(10); OpenMP over rows",
+            "seconds": secs, "steps_timed": done}
 
 
 def run_reference(args, rank, world):
@@ -347,12 +360,13 @@ def run_reference(args, rank, world):
         return
     from komegafoulingmodel_b200 import workloads as W
     w = W.by_name(args.workload)
-    # warm-up steps and K timed steps, each a full-lattice step
-    res = cpu_reference_sample(w, steps=args.steps, warmup=args.warmup)
+    # W untimed and up to K timed full-lattice steps; the timed loop stops
+    # after ~150 s of host time so the run stays within a few minutes
+    res = cpu_reference_sample(w, steps=args.steps, warmup=args.warmup, budget_s=150.0)
     line = {
         "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": res["seconds"] * 1e3 / args.steps, "higher_is_better": True,
+        "ms_per_step": res["seconds"] * 1e3 / res["steps_timed"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
                    "nodes": w.nodes, "parallelism": "host cores"},
@@ -379,9 +393,6 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        if args.warmup > 1:
-            args.warmup = 1
-        args.steps = min(args.steps, 3)
         run_reference(args, rank, world)
         return
     if world > 1:

@@ -94,7 +94,6 @@ struct GmresArgs {
     long long spin_limit;     // barrier spin bound (polls of >= 100 ns)
     int full_cycle;           // 1: build all K vectors before the truncation tests
     int strips;               // 32-column strips
-    int units_warps;          // warps that take part in a Krylov pass
 };
 
 // ---- coherent access to data written inside the launch (bypass L1) --------
@@ -553,8 +552,7 @@ gmres_kernel(const GmresArgs a) {
     extern __shared__ __align__(16) unsigned char gm_smem[];
     SolverSmem& T = *reinterpret_cast<SolverSmem*>(gm_smem);  // dynamic: larger than 48 KiB
     WarpSlot* ring = T.ring[threadIdx.x >> 5];
-    const int gwarp = blockIdx.x * GM_WARPS + (threadIdx.x >> 5);
-    const long long nwarps_total = (long long)a.units_warps;
+    const int wib = threadIdx.x >> 5;  // warp in block
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
     const long long npairs = a.D / 2;
@@ -632,15 +630,21 @@ gmres_kernel(const GmresArgs a) {
                     if (threadIdx.x == 0 && k > 0) T.sk1 = ldc(&C->s[k - 1]);
                     __syncthreads();
                     const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
-                    if (gwarp < nwarps_total) {
-                        // this warp's share of the flattened (strip, row) sequence
-                        const long long total = (long long)a.strips * a.ny;
-                        long long f = total * gwarp / nwarps_total;
-                        const long long f1 = total * (gwarp + 1) / nwarps_total;
+                    {
+                        // The block takes a share of the flattened (group, row)
+                        // sequence, a group being GM_WARPS adjacent strips; its
+                        // warps march the same rows of neighbouring strips side
+                        // by side, so their ghost-column reads hit L1 / L2.
+                        const int groups = (a.strips + GM_WARPS - 1) / GM_WARPS;
+                        const long long total = (long long)groups * a.ny;
+                        long long f = total * blockIdx.x / gridDim.x;
+                        const long long f1 = total * (blockIdx.x + 1) / gridDim.x;
                         while (f < f1) {
-                            const int strip = (int)(f / a.ny), ya = (int)(f - (long long)strip * a.ny);
+                            const int grp = (int)(f / a.ny), ya = (int)(f - (long long)grp * a.ny);
                             const int yb = (int)min((long long)a.ny, (long long)ya + (f1 - f));
-                            krylov_strip(a, S, rsrc, k, strip * 32, ya, yb, T, ring, acc);
+                            const int strip = grp * GM_WARPS + wib;
+                            if (strip < a.strips)
+                                krylov_strip(a, S, rsrc, k, strip * 32, ya, yb, T, ring, acc);
                             f += yb - ya;
                         }
                     }

@@ -74,6 +74,10 @@ def by_name(name: str) -> Workload:
         return komega_channel(16384, 1024, steps=20000)
     if name == "komega_straight_2048x256":
         return komega_channel(2048, 256, re_height=2.5e4, steps=50000)
+    if name.startswith("komega_straight_"):
+        # other sizes of the same straight channel (profiling cases)
+        nx, ny = (int(v) for v in name[len("komega_straight_"):].split("x"))
+        return komega_channel(nx, ny)
     raise KeyError(name)
 
 
