@@ -151,6 +151,10 @@ void clVariablesLB::ini() {
     }
     check("clVariablesLB::ini (kofm_create)", kofm_create(&d, &ctx));
     const bool ko = p.kOmegaSolverFlag;
+    if (ko && WallD.size() != n)
+        throw Error("clVariablesLB::ini: WallD missing", KOFM_ERR_INITIALIZING_KOMEGA);
+    // link fractions default to whole links (dXArr = 1, no wall cut)
+    if (ko && dXArr.size() != 4 * n) dXArr.assign(4 * n, 1.0);
     check("clVariablesLB::ini (geometry)",
           kofm_set_geometry(ctx, nType.data(), ko && !WallD.empty() ? WallD.data() : nullptr,
                             ko && !dXArr.empty() ? dXArr.data() : nullptr,

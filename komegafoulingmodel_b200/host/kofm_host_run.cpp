@@ -5,7 +5,8 @@
 // <dir>/params.txt   "key value" lines: nX XsizeFull nY tau Fval MuVal
 //                    kOmega (0/1) [maxTurbVisc krylovDim relTol absTol]
 // <dir>/ntype.bin    int16 node flags (XsizeFull * nY)
-// <dir>/wallD.bin    FP64 wall distance (k-omega only; optional)
+// <dir>/wallD.bin    FP64 wall distance (k-omega only)
+// <dir>/dX.bin       FP64 link fractions, 4 planes E,W,N,S (optional; 1)
 // <dir>/lbf.bin, lbkappa.bin, lbomega.bin   restart files (Array::savebin)
 //
 // Loads the restart files, advances nsteps of clProblem::step (Solve_no_TR),
@@ -68,6 +69,8 @@ int main(int argc, char** argv) {
         if (p.kOmegaSolverFlag) {
             vlb.WallD.resize(n);
             if (!loadBin(dir + "/wallD.bin", vlb.WallD.data(), n)) vlb.WallD.clear();
+            vlb.dXArr.resize(4 * n);
+            if (!loadBin(dir + "/dX.bin", vlb.dXArr.data(), 4 * n)) vlb.dXArr.clear();
         }
         if (!vlb.loadRestartFiles(dir)) throw Error("restart files in " + dir, KOFM_ERR_LOADING_PARAMS);
         vlb.ini();

@@ -25,6 +25,7 @@ def write_case(d, ch, f, k=None, o=None, rate=1.25, g=0.0, nu=0.1, komega=False)
     np.asarray(f, dtype=np.float64).tofile(os.path.join(d, "lbf.bin"))
     if komega:
         np.asarray(ch.wallD, dtype=np.float64).tofile(os.path.join(d, "wallD.bin"))
+        np.asarray(ch.dX, dtype=np.float64).tofile(os.path.join(d, "dX.bin"))
         np.asarray(k, dtype=np.float64).tofile(os.path.join(d, "lbkappa.bin"))
         np.asarray(o, dtype=np.float64).tofile(os.path.join(d, "lbomega.bin"))
 
