@@ -60,7 +60,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -223,7 +223,8 @@ def run_ours(args, rank, world, local_rank):
                                    "gbs": ASM_BYTES * nodes / (t_as * 1e-3) / 1e9},
         "gmres_kernel": {"ms": t_sv, "bytes_per_node": b_sv,
                          "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
-                         "passes": sum(passes) / nb},
+                         "passes": sum(passes) / nb,
+                         "bytes_per_node_by_launch": bytes_solver},
     }
     dom = max(kern, key=lambda k: kern[k]["ms"])
     roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak,
@@ -380,7 +381,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
