@@ -84,7 +84,7 @@ struct GmresArgs {
     float* field[2];          // omega, k (FP32 fields, updated in place)
     const int16_t* ntype;
     GmresControl* ctl;
-    double* part;             // [gridDim.x][GM_SLOTS]
+    double* part;             // [GM_SLOTS][gridDim.x] (slot-major)
     GridBarrier* bar;
     int nx, ny, P;
     long long D;
@@ -122,7 +122,7 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     return v;
 }
 
-// ---- block reduction of NS slots into part[blockIdx.x][base + s] ------------
+// ---- block reduction of NS slots into part[base + s][blockIdx.x] ------------
 template <int NS>
 __device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused, double* part, int base) {
     __shared__ double red[GM_THREADS / 32][GM_SYS_SLOTS];
@@ -141,18 +141,18 @@ __device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused,
         double v = 0.0;
 #pragma unroll
         for (int w = 0; w < GM_THREADS / 32; ++w) v += red[w][threadIdx.x];
-        part[(long long)blockIdx.x * GM_SLOTS + base + threadIdx.x] = v;
+        part[(long long)(base + threadIdx.x) * gridDim.x + blockIdx.x] = v;
     }
     __syncthreads();
 }
 
-// Sum slot `slot` of all blocks in block order (deterministic); one warp.
+// Sum slot `slot` of all blocks in a fixed order (deterministic); one warp,
+// lane l adding blocks l, l + 32, ... (coalesced: slot-major partials).
 __device__ __forceinline__ double sum_slot_warp(const double* part, int nblocks, int slot) {
     const int lane = threadIdx.x & 31;
     double v = 0.0;
-    const int per = (nblocks + 31) / 32;
-    const int b0 = lane * per, b1 = min(nblocks, b0 + per);
-    for (int b = b0; b < b1; ++b) v += __ldcg(part + (long long)b * GM_SLOTS + slot);
+    const double* ps = part + (long long)slot * nblocks;
+    for (int b = lane; b < nblocks; b += 32) v += __ldcg(ps + b);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     return __shfl_sync(0xffffffffu, v, 0);
@@ -347,6 +347,7 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
 // (periodic x; the padding columns of the last strip alias real columns and
 // are neither stored nor counted).
 constexpr int WS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
+static_assert(KOFM_MAX_KRYLOV == 10, "krylov_strip is instantiated for k = 0..9");
 constexpr int WS_SLOTS = 3;
 constexpr int GM_WARPS = GM_THREADS / 32;
 
@@ -389,8 +390,9 @@ __device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, 
 // The thread's inputs of row y into slot W: u_{k-1}(y+1), and for rows inside
 // the lattice the coefficients, u_j (j < k-1) and r; lanes 0 / 31 add their
 // ghost column.
+template <int k>
 __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
-                                         const double* rsrc, int k, int y, int xl, int lane,
+                                         const double* rsrc, int y, int xl, int lane,
                                          int gin, int gout, WarpSlot& W) {
     const long long D = a.D;
     el_copy(a, src, y + 1, xl, &W.up[lane]);
@@ -403,11 +405,13 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
     if (y < 0 || y >= a.ny) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) W.cf[q][lane] = 0.0;
+#pragma unroll
         for (int j = 0; j < k - 1; ++j) W.vj[j][lane] = 0.0;
         W.r[lane] = 0.0;
         if (ghost) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) W.gcf[h][q] = 0.0;
+#pragma unroll
             for (int j = 0; j < k - 1; ++j) W.gvj[h][j] = 0.0;
         }
         return;
@@ -415,17 +419,22 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
     const long long row = (long long)y * a.P;
 #pragma unroll
     for (int q = 0; q < 4; ++q) cp8(&W.cf[q][lane], S.coef + q * D + row + xl);
+#pragma unroll
     for (int j = 0; j < k - 1; ++j) cp8(&W.vj[j][lane], S.V + (long long)j * D + row + xl);
     if (k > 0) cp8(&W.r[lane], rsrc + row + xl);
     if (ghost) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) cp8(&W.gcf[h][q], S.coef + q * D + row + gin);
+#pragma unroll
         for (int j = 0; j < k - 1; ++j) cp8(&W.gvj[h][j], S.V + (long long)j * D + row + gin);
     }
 }
 
 // One warp: rows [ya, yb) of the strip starting at column x0.
-__device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc, int k,
+// k (the vector being built) is a template parameter, so every loop over the
+// older basis vectors has its exact length.
+template <int k>
+__device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc,
                              int x0, int ya, int yb, SolverSmem& T, WarpSlot* ring,
                              double (&acc)[2 + KOFM_MAX_KRYLOV]) {
     const int lane = threadIdx.x & 31;
@@ -447,9 +456,9 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double um = ld(ya - 2, xl), u0 = ld(ya - 1, xl);
     double gm = 0.0, g0 = 0.0;
     if (ghost) { gm = ld(ya - 2, gin); g0 = ld(ya - 1, gin); }
-    ws_issue(a, S, src, rsrc, k, ya - 1, xl, lane, gin, gout, ring[(ya - 1 + 3) % 3]);
+    ws_issue<k>(a, S, src, rsrc, ya - 1, xl, lane, gin, gout, ring[(ya - 1 + 3) % 3]);
     cp_commit();
-    ws_issue(a, S, src, rsrc, k, ya, xl, lane, gin, gout, ring[ya % 3]);
+    ws_issue<k>(a, S, src, rsrc, ya, xl, lane, gin, gout, ring[ya % 3]);
     cp_commit();
 
     double q[WS_KV];
@@ -458,7 +467,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double nprev = 0.0, ukprev = 0.0;
     const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        if (y + 2 <= yb) ws_issue(a, S, src, rsrc, k, y + 2, xl, lane, gin, gout, ring[(y + 2) % 3]);
+        if (y + 2 <= yb) ws_issue<k>(a, S, src, rsrc, y + 2, xl, lane, gin, gout, ring[(y + 2) % 3]);
         cp_commit();
         cp_wait<2>();
         const WarpSlot& W = ring[(y + 3) % 3];
@@ -496,6 +505,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
                 ukg = gz;
             } else {
                 ukg = sk1 * gz;
+#pragma unroll
                 for (int j = 0; j < k - 1; ++j) ukg -= T.g[j] * W.gvj[h][j];
                 ukg -= T.g[k - 1] * g0;
             }
@@ -643,8 +653,17 @@ gmres_kernel(const GmresArgs a) {
                             const int grp = (int)(f / a.ny), ya = (int)(f - (long long)grp * a.ny);
                             const int yb = (int)min((long long)a.ny, (long long)ya + (f1 - f));
                             const int strip = grp * GM_WARPS + wib;
-                            if (strip < a.strips)
-                                krylov_strip(a, S, rsrc, k, strip * 32, ya, yb, T, ring, acc);
+                            if (strip < a.strips) {
+                                switch (k) {
+#define KOFM_KSTRIP(n) \
+    case n: krylov_strip<n>(a, S, rsrc, strip * 32, ya, yb, T, ring, acc); break;
+                                    KOFM_KSTRIP(0) KOFM_KSTRIP(1) KOFM_KSTRIP(2) KOFM_KSTRIP(3)
+                                    KOFM_KSTRIP(4) KOFM_KSTRIP(5) KOFM_KSTRIP(6) KOFM_KSTRIP(7)
+                                    KOFM_KSTRIP(8) KOFM_KSTRIP(9)
+#undef KOFM_KSTRIP
+                                    default: break;
+                                }
+                            }
                             f += yb - ya;
                         }
                     }

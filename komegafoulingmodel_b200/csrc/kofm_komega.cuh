@@ -3,11 +3,11 @@
 // One kernel replaces the reference's Update_kOmega_Diffusivities and
 // Update_kOmega_Coeffs_Implicit (Kernels/kOmegaKernels.cl:7-95, 187-480) and
 // the GMRES updateRHS step (gmresKernels.cl:353-420, b -= A x0):
-//   * a 32x8 tile of nodes stages k and omega with a 2-node halo, and rho,
-//     nu_t, wall distance with a 1-node halo, in shared memory;
+//   * a 32x8 tile of nodes stages k and omega with a 2-node halo in shared
+//     memory;
 //   * the blending function F1, the cross-diffusion multipliers and the
-//     diffusivities D_k, D_w are evaluated on the tile plus a 1-node ring
-//     (they are needed at the neighbours for grad D);
+//     diffusivities D_k, D_w are evaluated on the tile plus a 1-node ring,
+//     one node per thread (D_k, D_w are needed at the neighbours for grad D);
 //   * each fluid node of the tile then builds its backward-Euler rows for k and
 //     omega, normalised by the diagonal (which is therefore 1 and not
 //     stored), with the wall-omega Dirichlet row of kOmegaKernels.cl:389-403;
@@ -25,9 +25,9 @@ constexpr int KO_TX = 32, KO_TY = 8;
 // One implicit system (index 0: omega, 1: k) as the solver sees it.  The
 // matrix stays FP64: an FP32-rounded operator would perturb every implicit
 // update by ~1e-8 relative, and that bias accumulates over the time steps.
-// Krylov basis, residual and right-hand side only carry the per-step
-// increment, so they are FP32 (all arithmetic is FP64); the accumulated
-// correction x stays FP64.
+// The Krylov basis, residual and right-hand side are FP64 as well: an FP32
+// basis loses orthogonality and stalls the first omega cycle near 1e-5
+// relative residual.
 #ifndef KOFM_SOLVER_VEC
 #define KOFM_SOLVER_VEC double
 #endif
@@ -113,107 +113,113 @@ __device__ __forceinline__ int wrapx(int x, int nx) {
     return x < 0 ? x + nx : (x >= nx ? x - nx : x);
 }
 
-__global__ void __launch_bounds__(KO_TX * KO_TY)
+// One thread per node of the tile plus its 1-node ring (34 x 10 = 340 of the
+// 352 threads), so the transcendental-heavy diffusivity phase takes one round;
+// the threads of the 32 x 8 interior then build the rows.  Each thread loads
+// its node's fields before the first barrier, so those loads overlap the
+// staging of k and omega.
+constexpr int KO_RX = KO_TX + 2, KO_RY = KO_TY + 2;
+constexpr int KO_THREADS = 352;  // 11 warps >= KO_RX * KO_RY
+
+__global__ void __launch_bounds__(KO_THREADS, 2)
 komega_assemble_kernel(const AsmParams p) {
     constexpr int HX = KO_TX + 4, HY = KO_TY + 4;  // 2-ring halo
-    constexpr int RX = KO_TX + 2, RY = KO_TY + 2;  // 1-ring
     __shared__ float sK[HY][HX];
     __shared__ float sO[HY][HX];
-    __shared__ double sDk[RY][RX];
-    __shared__ double sDo[RY][RX];
-    __shared__ double sF1[RY][RX];
-    __shared__ double sMx[RY][RX];
-    __shared__ double sMy[RY][RX];
+    __shared__ double sDk[KO_RY][KO_RX];
+    __shared__ double sDo[KO_RY][KO_RX];
 
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * KO_TX + tx;
+    const int tid = threadIdx.x;
     const int x0 = blockIdx.x * KO_TX, y0 = blockIdx.y * KO_TY;
     const int nx = p.nx, ny = p.ny, P = p.P;
+    const long long D = p.D;
+
+    // ---- this thread's ring node and its fields ---------------------------------
+    const bool ring = tid < KO_RX * KO_RY;
+    const int rx = ring ? tid % KO_RX : 0, ry = ring ? tid / KO_RX : 0;
+    const int gxu = x0 - 1 + rx;  // unwrapped column
+    const int gx = wrapx(gxu, nx);
+    const int gy = y0 - 1 + ry;
+    const bool inrow = ring && gy >= 0 && gy < ny;
+    const bool interior = inrow && rx >= 1 && rx <= KO_TX && ry >= 1 && ry <= KO_TY && gxu < nx;
+    const long long g = (long long)(inrow ? gy : 0) * P + gx;
+    int t = M_SOLID;
+    double yv = 1.0, rho = 0.0, nt = 0.0, Ux = 0.0, Uy = 0.0, Sxx = 0.0, Sxy = 0.0, Syy = 0.0;
+    if (inrow) {
+        t = (uint16_t)p.ntype[g];
+        if (!(t & M_SOLID)) {
+            yv = p.wallD[g];
+            rho = p.rho[g];
+            nt = p.nut[g];
+            if (interior) {
+                Ux = p.ux[g]; Uy = p.uy[g];
+                Sxx = p.S[g]; Sxy = p.S[D + g]; Syy = p.S[2 * D + g];
+            }
+        }
+    }
 
     // ---- stage k, omega (2-ring; x periodic over nx, rows clamped) -------
-    for (int i = tid; i < HX * HY; i += KO_TX * KO_TY) {
+    for (int i = tid; i < HX * HY; i += KO_THREADS) {
         const int sy = i / HX, sx = i % HX;
-        const int gx = wrapx(x0 - 2 + sx, nx);
-        int gy = y0 - 2 + sy;
-        gy = gy < 0 ? 0 : (gy >= ny ? ny - 1 : gy);
-        const long long g = (long long)gy * P + gx;
-        sK[sy][sx] = p.K[g];
-        sO[sy][sx] = p.O[g];
+        const int hx = wrapx(x0 - 2 + sx, nx);
+        int hy = y0 - 2 + sy;
+        hy = hy < 0 ? 0 : (hy >= ny ? ny - 1 : hy);
+        const long long h = (long long)hy * P + hx;
+        sK[sy][sx] = p.K[h];
+        sO[sy][sx] = p.O[h];
     }
     __syncthreads();
 
     // ---- F1, cross-diffusion, diffusivities on the tile + 1 ring -------------
     // (Update_kOmega_Diffusivities, kOmegaKernels.cl:24-94)
-    for (int i = tid; i < RX * RY; i += KO_TX * KO_TY) {
-        const int ry = i / RX, rx = i % RX;
-        const int gx = wrapx(x0 - 1 + rx, nx);
-        const int gy = y0 - 1 + ry;
-        double Dk = 0.0, Do = 0.0, F1 = 0.0, mxv = 0.0, myv = 0.0;
-        if (gy >= 0 && gy < ny) {
-            const long long g = (long long)gy * P + gx;
-            const int t = (uint16_t)p.ntype[g];
-            if (!(t & M_SOLID)) {
-                Fd3 X, Y, X2, Y2;
-                node_weights(p, t, g, X, X2, Y, Y2);
-                const int sy = ry + 1, sx = rx + 1;  // position in the 2-ring tile
-                const double om = sO[sy][sx], kv = sK[sy][sx];
-                const double yv = p.wallD[g];
-                const double dOdx = X.e * sO[sy][sx + 1] + X.w * sO[sy][sx - 1] + X.c * om;
-                const double dKdx = X.e * sK[sy][sx + 1] + X.w * sK[sy][sx - 1] + X.c * kv;
-                const double dOdy = Y.e * sO[sy + 1][sx] + Y.w * sO[sy - 1][sx] + Y.c * om;
-                const double dKdy = Y.e * sK[sy + 1][sx] + Y.w * sK[sy - 1][sx] + Y.c * kv;
-                const double m = 2. * KO_SIGMA_O2 / om;
-                mxv = m * dKdx;
-                myv = m * dKdy;
-                const double CDkw = dmaxr((double)p.rho[g] * (mxv * dOdx + myv * dOdy), 1.0e-10);
-                double a = dmaxr(sqrt(kv) / (KO_BETA_STAR * om * yv), 500. * p.mu / (yv * yv * om));
-                a = dminr(a, 4. * kv * KO_SIGMA_O2 / (CDkw * yv * yv));
-                const double a2 = a * a;
-                F1 = tanh(a2 * a2);
-                const double nt = p.nut[g];
-                Dk = p.mu + (KO_SIGMA_K1 * F1 + KO_SIGMA_K2 * (1. - F1)) * nt;
-                Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
-            }
-        }
+    const int sy = ry + 1, sx = rx + 1;  // position in the 2-ring tile
+    double Dk = 0.0, Do = 0.0, F1 = 0.0, mxv = 0.0, myv = 0.0;
+    Fd3 X, Y, X2, Y2;
+    if (inrow && !(t & M_SOLID)) {
+        node_weights(p, t, g, X, X2, Y, Y2);
+        const double om = sO[sy][sx], kv = sK[sy][sx];
+        const double dOdx = X.e * sO[sy][sx + 1] + X.w * sO[sy][sx - 1] + X.c * om;
+        const double dKdx = X.e * sK[sy][sx + 1] + X.w * sK[sy][sx - 1] + X.c * kv;
+        const double dOdy = Y.e * sO[sy + 1][sx] + Y.w * sO[sy - 1][sx] + Y.c * om;
+        const double dKdy = Y.e * sK[sy + 1][sx] + Y.w * sK[sy - 1][sx] + Y.c * kv;
+        const double m = 2. * KO_SIGMA_O2 / om;
+        mxv = m * dKdx;
+        myv = m * dKdy;
+        const double CDkw = dmaxr(rho * (mxv * dOdx + myv * dOdy), 1.0e-10);
+        double a = dmaxr(sqrt(kv) / (KO_BETA_STAR * om * yv), 500. * p.mu / (yv * yv * om));
+        a = dminr(a, 4. * kv * KO_SIGMA_O2 / (CDkw * yv * yv));
+        const double a2 = a * a;
+        F1 = tanh(a2 * a2);
+        Dk = p.mu + (KO_SIGMA_K1 * F1 + KO_SIGMA_K2 * (1. - F1)) * nt;
+        Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
+    }
+    if (ring) {
         sDk[ry][rx] = Dk;
         sDo[ry][rx] = Do;
-        sF1[ry][rx] = F1;
-        sMx[ry][rx] = mxv;
-        sMy[ry][rx] = myv;
     }
     __syncthreads();
 
     // ---- rows of the tile's nodes (Update_kOmega_Coeffs_Implicit) ------------
-    const int gx = x0 + tx, gy = y0 + ty;
-    if (gx >= nx || gy >= ny) return;
-    const long long g = (long long)gy * P + gx;
-    const long long D = p.D;
-    const int t = (uint16_t)p.ntype[g];
+    if (!interior) return;
     if (t & M_SOLID) {
         for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
         p.rhs_o[g] = vec_t(0);
         p.rhs_k[g] = vec_t(0);
         return;
     }
-    Fd3 X, Y, X2, Y2;
-    node_weights(p, t, g, X, X2, Y, Y2);
-    const int ry = ty + 1, rx = tx + 1;
-    const double dk = sDk[ry][rx], dom = sDo[ry][rx];
+    const double dk = Dk, dom = Do;
     const double dk_dx = X.e * sDk[ry][rx + 1] + X.w * sDk[ry][rx - 1] + X.c * dk;
     const double do_dx = X.e * sDo[ry][rx + 1] + X.w * sDo[ry][rx - 1] + X.c * dom;
     const double dk_dy = Y.e * sDk[ry + 1][rx] + Y.w * sDk[ry - 1][rx] + Y.c * dk;
     const double do_dy = Y.e * sDo[ry + 1][rx] + Y.w * sDo[ry - 1][rx] + Y.c * dom;
-    const double Ux = p.ux[g], Uy = p.uy[g], Rho = p.rho[g];
-    const double Jxo = Ux - do_dx - sMx[ry][rx];
-    const double Jyo = Uy - do_dy - sMy[ry][rx];
+    const double Jxo = Ux - do_dx - mxv;
+    const double Jyo = Uy - do_dy - myv;
     const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
-    const int sy = ty + 2, sx = tx + 2;
     const double Kraw = sK[sy][sx], Oraw = sO[sy][sx];
     double om = dmaxr(0.0, Oraw);
     const double kv = dmaxr(0.0, Kraw);
-    const double f1 = sF1[ry][rx], nt = p.nut[g];
-    const double Sxx = p.S[g], Sxy = p.S[D + g], Syy = p.S[2 * D + g];
-    double Pk = 2. * nt * (Sxx * Sxx + Syy * Syy + 2. * Sxy * Sxy) - 2. / 3. * kv * Rho * (Sxx + Syy);
+    const double f1 = F1;
+    double Pk = 2. * nt * (Sxx * Sxx + Syy * Syy + 2. * Sxy * Sxy) - 2. / 3. * kv * rho * (Sxx + Syy);
     Pk = dmaxr(dminr(Pk, 10. * KO_BETA_STAR * kv * om), 0.0);
     const double gam = (f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2) / nt;
     double Sc = -KO_BETA_STAR * om;
@@ -231,7 +237,7 @@ komega_assemble_kernel(const AsmParams p) {
     if (t & NESW_BOUNDARY) {
         dt = 0.;
         Sc = 0.;
-        const double yp = p.wallD[g];
+        const double yp = yv;
         const double ovis = (6. * p.mu / 0.075) / (yp * yp);
         const double olog = sqrt(kv) / (KO_C_MU_0_25 * KO_KAPPA * yp);
         om = dminr(1000., sqrt(ovis * ovis + olog * olog));
