@@ -143,7 +143,8 @@ def replica_value(nodes: int, steps: int, world: int, ms: float) -> float:
     return nodes * steps * world / (ms * 1e-3) / 1e6
 
 
-LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90}   # k-omega collide, per node
+LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
+            "fp16neq": 114}                   # + reference moments read and written
 ASM_BYTES = 122                                     # fused assembly, per node
 
 
@@ -160,7 +161,8 @@ def run_ours(args, rank, world, local_rank):
     build.build()
     lib = _abi.load()
     torch.cuda.set_device(local_rank)
-    storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV}[args.storage]
+    storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV,
+               "fp16neq": _abi.STORE_FP16_NEQ}[args.storage]
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
@@ -274,7 +276,10 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.storage == "fp32" else "f32", "data": "synthetic",
             "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
-                       "nodes": nodes, "storage": f"{args.storage} f-w deviation",
+                       "nodes": nodes,
+                       "storage": {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
+                                   "bf16": "bf16 f-w deviation",
+                                   "fp16neq": "fp16 f-feq (FP32 reference moments)"}[args.storage],
                        "krylov_dim": d.krylov_dim, "rel_tol": d.komega_rel_tol,
                        "abs_tol": d.komega_abs_tol, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (1.2 GB populations), no flush"},
@@ -385,7 +390,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

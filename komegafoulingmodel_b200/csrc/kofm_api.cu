@@ -46,6 +46,7 @@ struct kofm_ctx {
 
     // lattice state
     void* g[2] = {nullptr, nullptr};  // population buffers (9 planes each)
+    float* ref[2] = {nullptr, nullptr};  // KOFM_STORE_FP16_NEQ: reference rho, ux, uy of g[b]
     int cur = 0;                      // buffer holding the current state
     int phase = 0;                    // 0: FA form, 1: post-collision (pull)
     int16_t* ntype = nullptr;
@@ -137,13 +138,51 @@ __global__ void k_fa_in(const double* __restrict__ f, ST* __restrict__ g,
     }
 }
 
+// host-layout FP64 FA -> non-equilibrium form: reference = the node's own
+// moments rounded to FP32, e = f - feq(reference), scaled, in FP16
+__global__ void k_fa_in_neq(const double* __restrict__ f, __half* __restrict__ g,
+                            float* __restrict__ ref, const int16_t* __restrict__ nt, int nx,
+                            int nxf, int ny, int P, long long D) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= P) return;
+    const long long node = (long long)y * P + x;
+    const bool fluid = x < nx && !((uint16_t)nt[node] & M_SOLID);
+    const long long Dh = (long long)nxf * ny;
+    double fv[9];
+    double rho = 0.0, jx = 0.0, jy = 0.0;
+    for (int q = 0; q < 9; ++q) {
+        fv[q] = fluid ? f[q * Dh + (long long)y * nxf + x] : 0.0;
+        rho += fv[q];
+        jx += cx_of(q) * fv[q];
+        jy += cy_of(q) * fv[q];
+    }
+    const float r = fluid ? (float)rho : 0.f;
+    const float u = fluid ? (float)(jx / rho) : 0.f, v = fluid ? (float)(jy / rho) : 0.f;
+    ref[node] = r;
+    ref[D + node] = u;
+    ref[2 * D + node] = v;
+    for (int q = 0; q < 9; ++q) {
+        const float e = fluid ? (float)((fv[q] - weight_of(q)) - (double)feq_dev_f32(q, r, u, v)) : 0.f;
+        g[q * D + node] = __float2half_rn(e * NEQ_SCALE);
+    }
+}
+
 // device state -> host-layout FP64 FA.  phase 0: own deviations; phase 1:
 // gather + bounce-back + interpolated bounce-back (the next step's pull).
+// ref != nullptr: non-equilibrium form (decode with the stored reference of
+// the node each value was read from).
 template <typename ST>
 __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ nt,
                          const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
                          int has_ibb, double* __restrict__ f, int nx, int nxf, int ny,
-                         int P, long long D, int phase) {
+                         int P, long long D, int phase, const float* __restrict__ ref) {
+    auto dec = [&](int q, long long n) -> double {
+        const double raw = Store<ST>::to_f64(g[q * D + n]);
+        if (!ref) return raw;
+        return (double)(feq_dev_f32(q, ref[n], ref[D + n], ref[2 * D + n]) +
+                        (float)raw * NEQ_INV_SCALE);
+    };
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= nxf) return;
@@ -158,20 +197,20 @@ __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ n
     double d[9];
     for (int q = 0; q < 9; ++q) {
         if (phase == 0) {
-            d[q] = Store<ST>::to_f64(g[q * D + node]);
+            d[q] = dec(q, node);
         } else {
             int xs = x - cx_of(q);
             xs = xs < 0 ? xs + nx : (xs >= nx ? xs - nx : xs);
             int ys = y - cy_of(q);
             ys = ys < 0 ? 0 : (ys >= ny ? ny - 1 : ys);
-            d[q] = Store<ST>::to_f64(g[q * D + (long long)ys * P + xs]);
+            d[q] = dec(q, (long long)ys * P + xs);
         }
     }
     if (phase == 1 && (type & BOUNDARY)) {
         double pre[9];
         pre[0] = d[0];
         for (int q = 1; q < 9; ++q) {
-            if (type & bound_of(rev_of(q))) d[q] = Store<ST>::to_f64(g[rev_of(q) * D + node]);
+            if (type & bound_of(rev_of(q))) d[q] = dec(rev_of(q), node);
             pre[q] = d[q];
         }
         if (has_ibb && rec[node] >= 0) {
@@ -182,7 +221,7 @@ __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ n
                 const int rd = rev_of(dd);
                 const double q2 = 2.0 * qf;
                 if (q2 <= 1.0) d[rd] = q2 * pre[rd] + (1.0 - q2) * pre[dd];
-                else d[rd] = (1.0 / q2) * (pre[rd] + (q2 - 1.0) * Store<ST>::to_f64(g[rd * D + node]));
+                else d[rd] = (1.0 / q2) * (pre[rd] + (q2 - 1.0) * dec(rd, node));
             }
         }
     }
@@ -273,16 +312,16 @@ __global__ void k_wall_shear(const int16_t* __restrict__ nt, const float* __rest
 }
 
 // ---- LB step dispatch ------------------------------------------------------------
-template <typename ST, typename AT>
+template <typename ST, typename AT, bool NEQ = false>
 cudaError_t launch_lb(kofm_ctx* c, const LbParams& p, bool komega, bool phase0) {
     dim3 block(32, 4);
     dim3 grid(c->P / 128, (c->desc.ny + 3) / 4);
     if (komega) {
-        if (phase0) lb_step_kernel<ST, AT, true, true><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, true, false><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, true, true, NEQ><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, true, false, NEQ><<<grid, block, 0, c->stream>>>(p);
     } else {
-        if (phase0) lb_step_kernel<ST, AT, false, true><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, false, false><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, false, true, NEQ><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, false, false, NEQ><<<grid, block, 0, c->stream>>>(p);
     }
     return cudaGetLastError();
 }
@@ -291,7 +330,7 @@ int validate_desc(const kofm_desc* d) {
     if (!d) return KOFM_ERR_INVALID_ARG;
     if (d->nx < 4 || d->ny < 3 || d->nx_full < d->nx) return KOFM_ERR_LOADING_PARAMS;
     if ((long long)d->nx_full * d->ny > (1LL << 31) - 1) return KOFM_ERR_LOADING_PARAMS;
-    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_BF16_DEV) return KOFM_ERR_LOADING_PARAMS;
+    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP16_NEQ) return KOFM_ERR_LOADING_PARAMS;
     if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
@@ -350,7 +389,7 @@ int kofm_destroy(kofm_ctx* c) {
     if (!c) return KOFM_ERR_INVALID_ARG;
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->g[0], c->g[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
+    void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
                     c->gpart, c->bar};
@@ -400,6 +439,10 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
     for (int b = 0; b < 2; ++b) {
         int _s = dalloc(&c->g[b], (size_t)(9 * D) * c->store_bytes);
         if (_s) { kofm_destroy(c); return _s; }
+    }
+    if (d->storage == KOFM_STORE_FP16_NEQ) {
+        ALLOC(c->ref[0], 3 * D);
+        ALLOC(c->ref[1], 3 * D);
     }
     ALLOC(c->ntype, D);
     ALLOC(c->rec, D);
@@ -563,6 +606,9 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
         case KOFM_STORE_FP16_DEV:
             k_fa_in<__half><<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
+        case KOFM_STORE_FP16_NEQ:
+            k_fa_in_neq<<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ref[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+            break;
         default:
             k_fa_in<__nv_bfloat16><<<grid, 128, 0, c->stream>>>(c->staging, (__nv_bfloat16*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
     }
@@ -596,13 +642,16 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
         const int has_ibb = c->n_ibb_rec > 0;
         switch (d.storage) {
             case KOFM_STORE_FP32:
-                k_fa_out<float><<<grid, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+                k_fa_out<float><<<grid, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
                 break;
             case KOFM_STORE_FP16_DEV:
-                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                break;
+            case KOFM_STORE_FP16_NEQ:
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, c->ref[c->cur]);
                 break;
             default:
-                k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase);
+                k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
         }
         KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
         KOFM_CUDA_TRY(cudaMemcpyAsync(f, c->staging, 9 * Dh * sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
@@ -645,6 +694,8 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
     p.K = c->K; p.O = c->O; p.S = c->S; p.nut = c->nut;
     p.rho = c->rho; p.ux = c->ux; p.uy = c->uy;
     p.partials = c->lb_partials;
+    p.ref_in = c->ref[c->cur];
+    p.ref_out = c->ref[c->cur ^ 1];
     p.nx = d.nx; p.ny = d.ny; p.P = c->P; p.D = c->D;
     p.tau = d.tau; p.fterm = d.fterm; p.mu = d.mu; p.maxnut = d.max_turb_visc;
     p.options = options;
@@ -654,6 +705,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
     switch (d.storage) {
         case KOFM_STORE_FP32: e = launch_lb<float, double>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_DEV: e = launch_lb<__half, float>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, float, true>(c, p, ko, ph0); break;
         default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
     }
     if (e != cudaSuccess) {

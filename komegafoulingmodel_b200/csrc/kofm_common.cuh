@@ -110,6 +110,29 @@ template <> struct Store<__nv_bfloat16> {
     }
 };
 
+// ---- non-equilibrium storage form (KOFM_STORE_FP16_NEQ) ----------------------
+// A stored population is e_q = f_q - feq_q(rho_r, u_r): its distance from the
+// product-form equilibrium of a reference moment triple (rho_r, u_r) that the
+// writing node stores in FP32 beside it (its rho, reported u_x, u_y).  e is
+// O(f_neq), far smaller than the f - w deviation, so FP16 keeps ~3 more
+// decimal digits of the population.  e is scaled by 2^12 before rounding so
+// that the small values stay in FP16's normal range.  Encoder and decoder use
+// the same FP32 function of the same FP32 reference values.
+constexpr float NEQ_SCALE = 4096.0f;
+constexpr float NEQ_INV_SCALE = 1.0f / 4096.0f;
+
+// feq_q(rho, u) - w_q in FP32 (deviation form of the product equilibrium)
+__device__ __forceinline__ float feq_dev_f32(int q, float rho, float ux, float uy) {
+    const int cx = cx_of(q), cy = cy_of(q);
+    const float drho = rho - 1.0f;
+    const float px0 = cx == 0 ? 2.0f / 3.0f : 1.0f / 6.0f;
+    const float py0 = cy == 0 ? 2.0f / 3.0f : 1.0f / 6.0f;
+    const float dpx = cx == 0 ? -ux * ux : 0.5f * ((float)cx * ux + ux * ux);
+    const float dpy = cy == 0 ? -uy * uy : 0.5f * ((float)cy * uy + uy * uy);
+    return __fadd_rn(__fmul_rn(__fmul_rn(drho, __fadd_rn(px0, dpx)), __fadd_rn(py0, dpy)),
+                     __fadd_rn(__fadd_rn(__fmul_rn(dpx, py0), __fmul_rn(px0, dpy)), __fmul_rn(dpx, dpy)));
+}
+
 // Interpolated bounce-back record of one wall-adjacent node: wall fraction q
 // of each link direction 1..8 (q < 0: no interpolated correction on that
 // link).  Built on the host from the reference's ibbArr / ibbDistArr list.

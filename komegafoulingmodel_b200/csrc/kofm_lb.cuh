@@ -51,6 +51,8 @@ struct LbParams {
     float* ux;
     float* uy;
     double* partials;       // per block: sum rho, sum ux, sum uy (FP64)
+    const float* ref_in;    // non-equilibrium form: reference rho, ux, uy of
+    float* ref_out;         //   the populations read / written (3 planes)
     int nx, ny, P;
     long long D;
     double tau, fterm, mu, maxnut;
@@ -79,8 +81,32 @@ __device__ __forceinline__ float ld1(const ST* base, long long idx) {
     return Store<ST>::to_f32(base[idx]);
 }
 
+// The 4 values of an FP32 plane row that the pull of a direction with x
+// component cx brings to nodes x0..x0+3 (periodic in x; same shifts as the
+// population gather).
+__device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane, int x0, int nx,
+                                             float v[4]) {
+    const float4 c4 = __ldg(reinterpret_cast<const float4*>(row + x0));
+    const float c[4] = {c4.x, c4.y, c4.z, c4.w};
+    if (cx == 0) {
+        v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = c[3];
+    } else if (cx == 1) {
+        float left = __shfl_up_sync(0xffffffffu, c[3], 1);
+        if (lane == 0) left = __ldg(row + (x0 > 0 ? x0 - 1 : nx - 1));
+        v[0] = left; v[1] = c[0]; v[2] = c[1]; v[3] = c[2];
+    } else {
+        float right = __shfl_down_sync(0xffffffffu, c[0], 1);
+        if (lane == 31) right = __ldg(row + ((x0 + 4 < nx) ? x0 + 4 : 0));
+        v[0] = c[1]; v[1] = c[2]; v[2] = c[3]; v[3] = right;
+        const int jw = nx - 1 - x0;
+        if (jw >= 0 && jw < 4) v[jw] = __ldg(row);
+    }
+}
+
 // ---------------------------------------------------------------------------
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0>
+// NEQ: populations stored as f - feq(reference moments of the writing node),
+// FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false>
 __global__ void __launch_bounds__(128)
 lb_step_kernel(const LbParams p) {
     const int lane = threadIdx.x;
@@ -115,6 +141,13 @@ lb_step_kernel(const LbParams p) {
     }
 
     AT d[9][4];
+    float own_r[4], own_u[4], own_v[4];  // NEQ: this node's reference moments
+    // own stored population of direction q, decoded
+    auto own_pop = [&](int q, int j) -> AT {
+        const float raw = ld1(gin, q * D + rowoff + x0 + j);
+        if (!NEQ) return AT(raw);
+        return AT(feq_dev_f32(q, own_r[j], own_u[j], own_v[j]) + raw * NEQ_INV_SCALE);
+    };
     // ---- gather (pull) -----------------------------------------------------
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
@@ -148,6 +181,22 @@ lb_step_kernel(const LbParams p) {
                 if (jw >= 0 && jw < 4) v[jw] = ld1(src, 0);
             }
         }
+        if (NEQ) {
+            // reference moments of the 4 upstream nodes
+            int ys = y - (PHASE0 ? 0 : cy);
+            ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);
+            const int sx = PHASE0 ? 0 : cx;
+            float rr[4], ru[4], rv[4];
+            pull_row_f32(p.ref_in + (long long)ys * p.P, sx, lane, x0, p.nx, rr);
+            pull_row_f32(p.ref_in + D + (long long)ys * p.P, sx, lane, x0, p.nx, ru);
+            pull_row_f32(p.ref_in + 2 * D + (long long)ys * p.P, sx, lane, x0, p.nx, rv);
+            if (q == 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) { own_r[j] = rr[j]; own_u[j] = ru[j]; own_v[j] = rv[j]; }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = feq_dev_f32(q, rr[j], ru[j], rv[j]) + v[j] * NEQ_INV_SCALE;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j) d[q][j] = AT(v[j]);
     }
@@ -161,7 +210,7 @@ lb_step_kernel(const LbParams p) {
             AT pre[9];
 #pragma unroll
             for (int q = 1; q < 9; ++q) {
-                if (type[j] & bound_of(rev_of(q))) d[q][j] = AT(ld1(gin, rev_of(q) * D + node));
+                if (type[j] & bound_of(rev_of(q))) d[q][j] = own_pop(rev_of(q), j);
                 pre[q] = d[q][j];
             }
             if (p.has_ibb) {
@@ -177,7 +226,7 @@ lb_step_kernel(const LbParams p) {
                         if (q2 <= AT(1)) {
                             d[rd][j] = q2 * pre[rd] + (AT(1) - q2) * pre[dd];
                         } else {
-                            const AT own = AT(ld1(gin, rd * D + node));
+                            const AT own = own_pop(rd, j);
                             d[rd][j] = (AT(1) / q2) * (pre[rd] + (q2 - AT(1)) * own);
                         }
                     }
@@ -276,8 +325,16 @@ lb_step_kernel(const LbParams p) {
     for (int q = 0; q < 9; ++q) {
         float v[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = (float)d[q][j];
+        for (int j = 0; j < 4; ++j) {
+            v[j] = (float)d[q][j];
+            if (NEQ) v[j] = fl[j] ? (v[j] - feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j])) * NEQ_SCALE : 0.f;
+        }
         Store<ST>::store4(gout + q * D + rowoff + x0, v);
+    }
+    if (NEQ) {
+        *reinterpret_cast<float4*>(p.ref_out + rowoff + x0) = make_float4(o_rho[0], o_rho[1], o_rho[2], o_rho[3]);
+        *reinterpret_cast<float4*>(p.ref_out + D + rowoff + x0) = make_float4(o_ux[0], o_ux[1], o_ux[2], o_ux[3]);
+        *reinterpret_cast<float4*>(p.ref_out + 2 * D + rowoff + x0) = make_float4(o_uy[0], o_uy[1], o_uy[2], o_uy[3]);
     }
     if (p.options & OPTION_SAVE_MACRO_FIELDS) {
         *reinterpret_cast<float4*>(p.rho + rowoff + x0) = make_float4(o_rho[0], o_rho[1], o_rho[2], o_rho[3]);

@@ -1,0 +1,88 @@
+"""Precision study of the population storage forms.
+
+    python -m komegafoulingmodel_b200.precision --workload komega_straight_16384x1024 \
+        --steps 20000 [--forms fp32,fp16,bf16,fp16neq]
+
+Runs the same seeded channel once per storage form (FP32 / FP16 / BF16
+deviations f - w_i; FP16 non-equilibrium parts f - feq) and reports, for every
+16-bit form, the rel-L2 of u_x, k and omega over the fluid nodes against the
+FP32 form (u_y, ~0 in a straight channel, relative to |u|), the mass drift
+(sum rho at the end over sum rho at the start, minus 1) of every form, and each
+form's device-resident throughput.  The FP32 form itself is held to the FP64
+oracle by the test suite (rel-L2 ~1e-7 after 1000 steps), so its difference to
+a 16-bit form is that form's error up to that level.  Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import _abi
+from . import workloads as W
+from .lattice import Lattice
+
+FORMS = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV,
+         "fp16neq": _abi.STORE_FP16_NEQ}
+
+
+def rel_l2(a, b, mask):
+    d = np.linalg.norm((a - b)[mask])
+    n = np.linalg.norm(b[mask])
+    return float(d / n) if n > 0 else float(d)
+
+
+def run_form(w, form: str, steps: int, chunk: int = 500):
+    d = W.descriptor(w, storage=FORMS[form])
+    with Lattice(d) as L:
+        W.apply(L, w)
+        L.step(1)
+        m0 = L.reduce(_abi.FIELD_RHO)
+        L.sync()
+        t0 = time.perf_counter()
+        left = steps - 1
+        while left > 0:
+            n = min(chunk, left)
+            L.step(n)
+            left -= n
+        L.sync()
+        secs = time.perf_counter() - t0
+        m1 = L.reduce(_abi.FIELD_RHO)
+        rho, ux, uy = L.get_macro()
+        _, k, o, _, _ = L.get_state() if w.komega else (None, None, None, None, None)
+    return {"ux": ux, "uy": uy, "k": k, "omega": o, "mass_drift": m1 / m0 - 1.0,
+            "mlups": w.nodes * max(steps - 1, 1) / secs / 1e6}
+
+
+def study(workload: str, steps: int, forms=("fp32", "fp16", "bf16", "fp16neq")) -> dict:
+    w = W.by_name(workload)
+    fl = w.channel.fluid_mask().ravel()
+    res = {f: run_form(w, f, steps) for f in forms}
+    out = {"workload": workload, "steps": steps, "reference_form": "fp32", "forms": {}}
+    base = res.get("fp32")
+    for f, r in res.items():
+        e = {"mass_drift": r["mass_drift"], "mlups_wall": r["mlups"]}
+        if base is not None and f != "fp32":
+            for key in ("ux", "k", "omega"):
+                if r[key] is not None:
+                    e[f"rel_l2_{key}"] = rel_l2(r[key], base[key], fl)
+            # u_y is ~0 in a straight channel: its error relative to |u|
+            e["l2_uy_over_l2_u"] = float(np.linalg.norm((r["uy"] - base["uy"])[fl]) /
+                                         np.linalg.norm(np.hypot(base["ux"], base["uy"])[fl]))
+        out["forms"][f] = e
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="komega_straight_16384x1024")
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--forms", default="fp32,fp16,bf16,fp16neq")
+    args = ap.parse_args()
+    print(json.dumps(study(args.workload, args.steps, tuple(args.forms.split(",")))), flush=True)
+
+
+if __name__ == "__main__":
+    main()
