@@ -1,7 +1,7 @@
 """Host-side set-up of a channel: geometry flags and initial fields.
 
-Covers what the reference computes on the host before its time loop, for the
-straight channel (two straight wall polylines):
+Covers what the reference computes on the host before its time loop, for a
+channel between two wall polylines given by their height at every column:
   * nType bits with fluid / solid / boundary flags and the per-direction wall
     flags (clVariablesLS::iniFillMap0 / iniFillMap / iniNodeBoundaryInfo0 /
     iniNodeBoundaryInfo, clVariablesLS.cpp:686-1000);
@@ -61,40 +61,108 @@ class Channel:
         return 0.5 * (float(np.mean(self.y_top)) - float(np.mean(self.y_bot)))
 
 
-def straight_channel(nx: int, ny: int, nx_full: int | None = None) -> Channel:
-    """Rows 0 and ny-1 solid; half-way walls at y = 0.5 and y = ny - 1.5."""
+def _link_fraction(i, j, q, nx, y_bot, y_top):
+    """Fraction t in (0, 1] of the link from node (i, j) in direction q at
+    which it meets a wall; walls are linear between columns (periodic in x)."""
+    cx, cy = int(CX[q]), int(CY[q])
+    ts = []
+    for y_w, below in ((y_bot, True), (y_top, False)):
+        y0 = float(y_w[i])
+        d = float(y_w[(i + cx) % nx]) - y0 if cx != 0 else 0.0
+        den = cy - d
+        if den == 0.0:
+            continue
+        t = (y0 - j) / den
+        if 0.0 < t <= 1.0 + 1e-12:
+            ts.append(min(t, 1.0))
+    return min(ts) if ts else 0.5
+
+
+def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius):
+    """Distance of every fluid node to the nearest wall polyline (segments
+    between neighbouring columns, periodic in x) within `radius` columns
+    (kOmega::iniWallD / findMinDist, kOmega.cpp:136-193, 330-349)."""
+    wall = np.zeros((ny, nxf))
+    jj, ii = np.nonzero(fluid)
+    best = np.full(jj.shape, np.inf)
+    for y_w in (y_bot, y_top):
+        for off in range(-radius, radius + 1):
+            xa = ii + off                       # segment from column xa to xa + 1
+            ya = y_w[xa % nx]
+            yb = y_w[(xa + 1) % nx]
+            # projection of (ii, jj) onto the segment (xa, ya) - (xa + 1, yb)
+            dx, dy = 1.0, yb - ya
+            t = np.clip(((ii - xa) * dx + (jj - ya) * dy) / (dx * dx + dy * dy), 0.0, 1.0)
+            px, py = xa + t * dx, ya + t * dy
+            best = np.minimum(best, np.hypot(ii - px, jj - py))
+    wall[jj, ii] = best
+    return wall
+
+
+def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = None,
+                       wall_radius: int = 40) -> Channel:
+    """Channel between two walls given by their heights at every column (the
+    wall polylines of clVariablesLS).  Node (i, j) is fluid iff
+    y_bot[i] < j < y_top[i].  Builds the nType flags (per-direction wall bits
+    of the links whose upstream node is solid), the E/W/N/S link fractions
+    dXArr, the interpolated bounce-back list (link from a fluid node into the
+    wall, as node + D * dir, with its wall fraction q; links with q = 1/2 need
+    no correction and are left out) and the wall distance."""
     nxf = nx if nx_full is None else nx_full
-    yb, yt = 0.5, ny - 1.5
+    y_bot = np.asarray(y_bot, float)
+    y_top = np.asarray(y_top, float)
     j = np.arange(ny)
-    solid_row = (j == 0) | (j == ny - 1)
-    t = np.where(solid_row[:, None], M0_SOLID | M_SOLID, M0_FLUID | M_FLUID)
-    t = np.broadcast_to(t, (ny, nxf)).astype(np.int32).copy()
-    solid = (t & M_SOLID) != 0
+    fluid = np.zeros((ny, nxf), bool)
+    fluid[:, :nx] = (j[:, None] > y_bot[None, :]) & (j[:, None] < y_top[None, :])
+    fluid[0, :] = False
+    fluid[ny - 1, :] = False
+    solid = ~fluid
     solid[:, nx:] = False
-    fluid = ~solid
-    fluid[:, nx:] = False
+    t = np.where(fluid, M0_FLUID | M_FLUID, M0_SOLID | M_SOLID).astype(np.int32)
+    dX = np.zeros((4, ny, nxf))
+    dX[:, fluid] = 1.0
+    D = nxf * ny
+    ibb_idx, ibb_q = [], []
     for q in range(1, 9):
-        # neighbour of (i, j) in direction q, periodic in x over nx
-        nb_solid = np.zeros_like(solid)
-        jj = j + CY[q]
-        valid = (jj >= 0) & (jj < ny)
+        nb_solid = np.zeros((ny, nxf), bool)
+        jn = j + CY[q]
+        valid = (jn >= 0) & (jn < ny)
         src = np.roll(solid[:, :nx], -CX[q], axis=1)
         rows = np.where(valid)[0]
-        nb_solid[rows, :nx] = src[jj[rows], :]
+        nb_solid[rows, :nx] = src[jn[rows], :]
         hit = fluid & nb_solid
         t[hit] |= BOUND[q] | BOUNDARY0
         if q < 5:
             t[hit] |= NESW_BOUNDARY0
-            # mark the solid neighbours of NESW links
             ii, jv = np.nonzero(hit.T)
             t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY | SOLID_BOUNDARY0
-    dX = np.zeros((4, ny, nxf))
-    dX[:, fluid] = 1.0
-    dX[2, ny - 2, :nx] = yt - (ny - 2)   # north link of the top fluid row
-    dX[3, 1, :nx] = 1 - yb               # south link of the bottom fluid row
-    wallD = np.where(fluid, np.minimum(j[:, None] - yb, yt - j[:, None]), 0.0)
-    return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(),
-                   dX.ravel(), wallD.ravel(), y_bot=np.full(nx, yb), y_top=np.full(nx, yt))
+        for jv, ii in zip(*np.nonzero(hit)):
+            frac = _link_fraction(int(ii), int(jv), q, nx, y_bot, y_top)
+            if q < 5:
+                dX[q - 1, jv, ii] = frac
+            if abs(frac - 0.5) > 1e-12:
+                ibb_idx.append(q * D + jv * nxf + ii)
+                ibb_q.append(frac)
+    wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, min(wall_radius, nx // 2))
+    order = np.argsort(ibb_idx, kind="stable")
+    return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(), dX.ravel(),
+                   wall.ravel(), np.asarray(ibb_idx, np.int32)[order],
+                   np.asarray(ibb_q, float)[order], y_bot=y_bot, y_top=y_top)
+
+
+def wavy_channel(nx: int, ny: int, amplitude: float, wavelength: int,
+                 nx_full: int | None = None) -> Channel:
+    """Walls displaced by h(x) = A (1 - cos(2 pi x / L)) / 2 from the half-way
+    positions 0.5 and ny - 1.5, mirrored top and bottom.  h and its slope
+    vanish at x = 0, so the links at the periodic seam keep q <= 1/2."""
+    x = np.arange(nx)
+    h = amplitude * 0.5 * (1.0 - np.cos(2.0 * np.pi * x / wavelength))
+    return channel_from_walls(nx, ny, 0.5 + h, ny - 1.5 - h, nx_full)
+
+
+def straight_channel(nx: int, ny: int, nx_full: int | None = None) -> Channel:
+    """Rows 0 and ny-1 solid; half-way walls at y = 0.5 and y = ny - 1.5."""
+    return channel_from_walls(nx, ny, np.full(nx, 0.5), np.full(nx, ny - 1.5), nx_full)
 
 
 # ---------------------------------------------------------------------------

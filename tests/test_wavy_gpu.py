@@ -1,0 +1,106 @@
+"""Curved walls: the wall-polyline geometry builder on CPU, and the GPU step
+on a wavy channel (interpolated bounce-back with wall fractions q != 1/2,
+non-uniform FD weights from the link fractions, curved wall distance) against
+the FP64 oracle."""
+import numpy as np
+import pytest
+
+from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+from komegafoulingmodel_b200 import geometry as G
+from oracle.orc import OracleSim, make_cfg
+from tests.cases import fp32_state, rel_l2
+
+
+def test_straight_walls_need_no_interpolated_records():
+    ch = G.straight_channel(128, 20)
+    assert len(ch.ibb_idx) == 0
+    fl = ch.fluid_mask()
+    assert fl[1:-1, :].all() and not fl[0].any() and not fl[-1].any()
+
+
+def test_wavy_geometry_invariants():
+    ch = G.wavy_channel(256, 66, 8.0, 128)
+    n = ch.n
+    fl = ch.fluid_mask().ravel()
+    t = ch.ntype.astype(np.int32) & 0xFFFF
+    q = ch.ibb_q
+    assert len(q) > 0 and np.all((q > 0) & (q <= 1))
+    d = ch.ibb_idx // n
+    node = ch.ibb_idx % n
+    # every record is a fluid node whose link in direction d ends in a solid node
+    assert np.all(fl[node])
+    bound = np.array(G.BOUND)[d]
+    assert np.all((t[node] & bound) != 0)
+    # link fractions of the E/W/N/S planes: 1 away from walls, (0, 1] at walls
+    dX = ch.dX.reshape(4, -1)
+    assert np.all(dX[:, fl] > 0) and np.all(dX[:, fl] <= 1) and np.all(dX[:, ~fl] == 0)
+    # wall distance is positive in the fluid and at most half the opening
+    assert np.all(ch.wallD[fl] > 0) and ch.wallD.max() < 33
+    # the seam columns have no link with 2q > 1 (those read the upstream node)
+    x = node % ch.nx_full
+    cx = G.CX[d]
+    seam = ((x == 0) & (cx == 1)) | ((x == ch.nx - 1) & (cx == -1))
+    assert not np.any(seam & (q > 0.5))
+
+
+def _lattice(ch, rate, g, mu, komega):
+    d = desc_default()
+    d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
+    d.tau, d.fterm, d.mu = rate, g, mu
+    d.use_komega = 1 if komega else 0
+    L = Lattice(d)
+    L.set_geometry(ch.ntype, ch.wallD if komega else None, ch.dX if komega else None,
+                   ch.ibb_idx, ch.ibb_q)
+    return L
+
+
+@pytest.mark.gpu
+def test_wavy_laminar_matches_oracle(kofm_lib, oracle):
+    nx, ny = 256, 40
+    ch = G.wavy_channel(nx, ny, 6.0, 128)
+    rate, g, mu = 1.25, 2e-6, 0.1
+    (f,) = fp32_state(G.equilibrium_state(ch, ux=0.01))
+    cfg = make_cfg(nx, ny, rate, g, mu)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
+    sim.step(300)
+    with _lattice(ch, rate, g, mu, False) as L:
+        L.set_state(f)
+        L.step(300)
+        rho, ux, uy = L.get_macro()
+    fl = ch.fluid_mask().ravel()
+    errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl))
+    uy_rel = np.linalg.norm((uy - sim.uy)[fl]) / np.linalg.norm(sim.ux[fl])
+    print(errs, uy_rel)
+    assert errs["rho"] < 1e-6 and errs["ux"] < 1e-5 and uy_rel < 1e-5, (errs, uy_rel)
+
+
+@pytest.mark.gpu
+def test_wavy_komega_matches_oracle(kofm_lib, oracle):
+    nx, ny = 256, 66
+    ch = G.wavy_channel(nx, ny, 8.0, 128)
+    nu, u_max = 5e-4, 0.05
+    R = ch.pipe_radius
+    y = np.arange(ny)[:, None] - 0.5
+    ux = np.clip(u_max * (1 - ((y - R) / R) ** 2), 0, None) * np.ones((1, nx))
+    f = G.equilibrium_state(ch, ux=ux)
+    g = G.force_from_re((2.0 / 3.0) * u_max * R / nu, nu, R)
+    k0 = 1.5 * (0.05 * u_max) ** 2
+    o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * 2 * R)
+    k, o, nut = G.komega_fields(ch, k0, o0)
+    f, k, o, nut = fp32_state(f, k, o, nut)
+    rate = 1.0 / (3 * nu + 0.5)
+    cfg = make_cfg(nx, ny, rate, g, nu)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True,
+                    ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
+    sim.step(500)
+    with _lattice(ch, rate, g, nu, True) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        L.step(500)
+        rho, ux2, uy2 = L.get_macro()
+        _, k2, o2, _, _ = L.get_state()
+    fl = ch.fluid_mask().ravel()
+    errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux2, sim.ux, fl),
+                k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
+    print(errs)
+    for key in ("rho", "ux", "k", "omega"):
+        assert errs[key] < 1e-5, errs
