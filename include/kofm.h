@@ -65,7 +65,7 @@ extern "C" {
 #define KOFM_STORE_BF16_DEV 2 /* f_i - w_i in BF16, FP32 collide arithmetic */
 #define KOFM_STORE_FP16_NEQ 3 /* f_i - feq_i(rho_r, u_r) in FP16 (scaled by 2^12),
                                  with the writer's FP32 rho, u as reference;
-                                 FP32 collide arithmetic.  No counterpart in
+                                 FP64 collide arithmetic.  No counterpart in
                                  the reference (its arrays are FP64). */
 
 /* ---- fields for kofm_reduce ---------------------------------------------- */

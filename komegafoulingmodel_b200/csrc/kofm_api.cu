@@ -705,7 +705,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
     switch (d.storage) {
         case KOFM_STORE_FP32: e = launch_lb<float, double>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_DEV: e = launch_lb<__half, float>(c, p, ko, ph0); break;
-        case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, float, true>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, double, true>(c, p, ko, ph0); break;
         default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
     }
     if (e != cudaSuccess) {

@@ -146,7 +146,7 @@ lb_step_kernel(const LbParams p) {
     auto own_pop = [&](int q, int j) -> AT {
         const float raw = ld1(gin, q * D + rowoff + x0 + j);
         if (!NEQ) return AT(raw);
-        return AT(feq_dev_f32(q, own_r[j], own_u[j], own_v[j]) + raw * NEQ_INV_SCALE);
+        return AT(feq_dev_f32(q, own_r[j], own_u[j], own_v[j])) + AT(raw) * AT(NEQ_INV_SCALE);
     };
     // ---- gather (pull) -----------------------------------------------------
 #pragma unroll
@@ -195,10 +195,12 @@ lb_step_kernel(const LbParams p) {
                 for (int j = 0; j < 4; ++j) { own_r[j] = rr[j]; own_u[j] = ru[j]; own_v[j] = rv[j]; }
             }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = feq_dev_f32(q, rr[j], ru[j], rv[j]) + v[j] * NEQ_INV_SCALE;
-        }
+            for (int j = 0; j < 4; ++j)
+                d[q][j] = AT(feq_dev_f32(q, rr[j], ru[j], rv[j])) + AT(v[j]) * AT(NEQ_INV_SCALE);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) d[q][j] = AT(v[j]);
+            for (int j = 0; j < 4; ++j) d[q][j] = AT(v[j]);
+        }
     }
 
     // ---- half-way bounce-back and interpolated bounce-back -----------------
@@ -326,8 +328,11 @@ lb_step_kernel(const LbParams p) {
         float v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            v[j] = (float)d[q][j];
-            if (NEQ) v[j] = fl[j] ? (v[j] - feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j])) * NEQ_SCALE : 0.f;
+            if (NEQ)
+                v[j] = fl[j] ? (float)((d[q][j] - AT(feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j]))) * AT(NEQ_SCALE))
+                             : 0.f;
+            else
+                v[j] = (float)d[q][j];
         }
         Store<ST>::store4(gout + q * D + rowoff + x0, v);
     }

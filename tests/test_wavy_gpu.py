@@ -74,8 +74,7 @@ def test_wavy_laminar_matches_oracle(kofm_lib, oracle):
     assert errs["rho"] < 1e-6 and errs["ux"] < 1e-5 and uy_rel < 1e-5, (errs, uy_rel)
 
 
-@pytest.mark.gpu
-def test_wavy_komega_matches_oracle(kofm_lib, oracle):
+def _wavy_komega_case():
     nx, ny = 256, 66
     ch = G.wavy_channel(nx, ny, 8.0, 128)
     nu, u_max = 5e-4, 0.05
@@ -88,19 +87,47 @@ def test_wavy_komega_matches_oracle(kofm_lib, oracle):
     o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * 2 * R)
     k, o, nut = G.komega_fields(ch, k0, o0)
     f, k, o, nut = fp32_state(f, k, o, nut)
-    rate = 1.0 / (3 * nu + 0.5)
+    return ch, f, k, o, nut, 1.0 / (3 * nu + 0.5), g, nu
+
+
+def _fields(L):
+    rho, ux, _ = L.get_macro()
+    _, k, o, _, _ = L.get_state()
+    return rho, ux, k, o
+
+
+@pytest.mark.gpu
+def test_wavy_komega_matches_oracle(kofm_lib, oracle):
+    """k-omega on the wavy channel.  This flow amplifies perturbations: the
+    oracle started from k perturbed by 1e-7 (FP32 rounding level) differs by
+    1e-7 after 10 steps, 2e-5 after 20 and ~1e-2 in k after 50 (near-wall
+    limiter and clamp switches), in FP64 and with any GMRES tolerance.  So the
+    GPU is held to 1e-5 after 10 steps, and after 100 steps to a few times the
+    oracle's own spread under that perturbation."""
+    ch, f, k, o, nut, rate, g, nu = _wavy_komega_case()
+    nx, ny = ch.nx, ch.ny
     cfg = make_cfg(nx, ny, rate, g, nu)
-    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True,
-                    ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
-    sim.step(500)
+    mk = lambda kk: OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, kk, o, nut,  # noqa: E731
+                              komega=True, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
+    sim, pert = mk(k), mk(k * (1 + 1e-7))
+    fl = ch.fluid_mask().ravel()
     with _lattice(ch, rate, g, nu, True) as L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
-        L.step(500)
-        rho, ux2, uy2 = L.get_macro()
-        _, k2, o2, _, _ = L.get_state()
-    fl = ch.fluid_mask().ravel()
-    errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux2, sim.ux, fl),
-                k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
-    print(errs)
-    for key in ("rho", "ux", "k", "omega"):
-        assert errs[key] < 1e-5, errs
+        sim.step(10)
+        L.step(10)
+        rho, ux, k2, o2 = _fields(L)
+        errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl),
+                    k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
+        print("10 steps", errs)
+        for key in ("rho", "ux", "k", "omega"):
+            assert errs[key] < 1e-5, errs
+        sim.step(90)
+        pert.step(100)
+        L.step(90)
+        rho, ux, k2, o2 = _fields(L)
+    for name, gpu, ref, alt in (("ux", ux, sim.ux, pert.ux), ("k", k2, sim.K, pert.K),
+                                ("omega", o2, sim.O, pert.O)):
+        spread = rel_l2(alt, ref, fl)
+        err = rel_l2(gpu, ref, fl)
+        print("100 steps", name, err, spread)
+        assert err < 5 * spread + 1e-6, (name, err, spread)
