@@ -113,75 +113,113 @@ __device__ __forceinline__ int wrapx(int x, int nx) {
     return x < 0 ? x + nx : (x >= nx ? x - nx : x);
 }
 
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // One thread per node of the tile plus its 1-node ring (34 x 10 = 340 of the
 // 352 threads), so the transcendental-heavy diffusivity phase takes one round;
-// the threads of the 32 x 8 interior then build the rows.  Each thread loads
-// its node's fields before the first barrier, so those loads overlap the
-// staging of k and omega.
+// the threads of the 32 x 8 interior then build the rows.
+//
+// The kernel is persistent: a block walks the tiles tile += gridDim.x and,
+// while it computes one tile, streams the next tile's k, omega halo and every
+// thread's node fields into the other half of a double-buffered shared-memory
+// stage with 4-byte cp.async (the node flag goes into a register), so the
+// loads of a tile overlap the FP64 work of the previous one.
 constexpr int KO_RX = KO_TX + 2, KO_RY = KO_TY + 2;
 constexpr int KO_THREADS = 352;  // 11 warps >= KO_RX * KO_RY
+constexpr int KO_HX = KO_TX + 4, KO_HY = KO_TY + 4;  // 2-ring halo
+constexpr int KO_NF = 8;  // node fields: wallD, rho, nut, ux, uy, Sxx, Sxy, Syy
 
-__global__ void __launch_bounds__(KO_THREADS, 2)
-komega_assemble_kernel(const AsmParams p) {
-    constexpr int HX = KO_TX + 4, HY = KO_TY + 4;  // 2-ring halo
-    __shared__ float sK[HY][HX];
-    __shared__ float sO[HY][HX];
-    __shared__ double sDk[KO_RY][KO_RX];
-    __shared__ double sDo[KO_RY][KO_RX];
+struct AsmStage {
+    float K[KO_HY][KO_HX];
+    float O[KO_HY][KO_HX];
+    float fld[KO_NF][KO_THREADS];
+};
 
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * KO_TX, y0 = blockIdx.y * KO_TY;
-    const int nx = p.nx, ny = p.ny, P = p.P;
-    const long long D = p.D;
+struct AsmSmem {
+    AsmStage st[2];
+    double Dk[KO_RY][KO_RX];
+    double Do[KO_RY][KO_RX];
+};
 
-    // ---- this thread's ring node and its fields ---------------------------------
+__device__ __forceinline__ void ko_cp4(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Geometry of this thread's ring node in tile (x0, y0).
+struct KoNode {
+    int rx, ry, gxu, gx, gy;
+    bool inrow, interior;
+    long long g;
+};
+
+__device__ __forceinline__ KoNode ko_node(const AsmParams& p, int tid, int x0, int y0) {
+    KoNode n;
     const bool ring = tid < KO_RX * KO_RY;
-    const int rx = ring ? tid % KO_RX : 0, ry = ring ? tid / KO_RX : 0;
-    const int gxu = x0 - 1 + rx;  // unwrapped column
-    const int gx = wrapx(gxu, nx);
-    const int gy = y0 - 1 + ry;
-    const bool inrow = ring && gy >= 0 && gy < ny;
-    const bool interior = inrow && rx >= 1 && rx <= KO_TX && ry >= 1 && ry <= KO_TY && gxu < nx;
-    const long long g = (long long)(inrow ? gy : 0) * P + gx;
-    int t = M_SOLID;
-    double yv = 1.0, rho = 0.0, nt = 0.0, Ux = 0.0, Uy = 0.0, Sxx = 0.0, Sxy = 0.0, Syy = 0.0;
-    if (inrow) {
-        t = (uint16_t)p.ntype[g];
-        if (!(t & M_SOLID)) {
-            yv = p.wallD[g];
-            rho = p.rho[g];
-            nt = p.nut[g];
-            if (interior) {
-                Ux = p.ux[g]; Uy = p.uy[g];
-                Sxx = p.S[g]; Sxy = p.S[D + g]; Syy = p.S[2 * D + g];
-            }
-        }
-    }
+    n.rx = ring ? tid % KO_RX : 0;
+    n.ry = ring ? tid / KO_RX : 0;
+    n.gxu = x0 - 1 + n.rx;
+    n.gx = wrapx(n.gxu, p.nx);
+    n.gy = y0 - 1 + n.ry;
+    n.inrow = ring && n.gy >= 0 && n.gy < p.ny;
+    n.interior = n.inrow && n.rx >= 1 && n.rx <= KO_TX && n.ry >= 1 && n.ry <= KO_TY && n.gxu < p.nx;
+    n.g = (long long)(n.inrow ? n.gy : 0) * p.P + n.gx;
+    return n;
+}
 
-    // ---- stage k, omega (2-ring; x periodic over nx, rows clamped) -------
-    for (int i = tid; i < HX * HY; i += KO_THREADS) {
-        const int sy = i / HX, sx = i % HX;
-        const int hx = wrapx(x0 - 2 + sx, nx);
+// Issue the copies of tile (x0, y0) into stage S; returns the node flag.
+__device__ __forceinline__ int ko_issue(const AsmParams& p, int tid, int x0, int y0, AsmStage& S) {
+    for (int i = tid; i < KO_HX * KO_HY; i += KO_THREADS) {
+        const int sy = i / KO_HX, sx = i % KO_HX;
+        const int hx = wrapx(x0 - 2 + sx, p.nx);
         int hy = y0 - 2 + sy;
-        hy = hy < 0 ? 0 : (hy >= ny ? ny - 1 : hy);
-        const long long h = (long long)hy * P + hx;
-        sK[sy][sx] = p.K[h];
-        sO[sy][sx] = p.O[h];
+        hy = hy < 0 ? 0 : (hy >= p.ny ? p.ny - 1 : hy);
+        const long long h = (long long)hy * p.P + hx;
+        ko_cp4(&S.K[sy][sx], p.K + h);
+        ko_cp4(&S.O[sy][sx], p.O + h);
     }
-    __syncthreads();
+    const KoNode n = ko_node(p, tid, x0, y0);
+    if (!n.inrow) return M_SOLID;
+    const long long g = n.g, D = p.D;
+    ko_cp4(&S.fld[0][tid], p.wallD + g);
+    ko_cp4(&S.fld[1][tid], p.rho + g);
+    ko_cp4(&S.fld[2][tid], p.nut + g);
+    if (n.interior) {
+        ko_cp4(&S.fld[3][tid], p.ux + g);
+        ko_cp4(&S.fld[4][tid], p.uy + g);
+        ko_cp4(&S.fld[5][tid], p.S + g);
+        ko_cp4(&S.fld[6][tid], p.S + D + g);
+        ko_cp4(&S.fld[7][tid], p.S + 2 * D + g);
+    }
+    return (uint16_t)__ldg(p.ntype + g);
+}
+
+// Phases 2 and 3 of one tile from stage S (all of S visible to the block).
+__device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int y0, int t,
+                                        const AsmStage& S, AsmSmem& M) {
+    const KoNode n = ko_node(p, tid, x0, y0);
+    const int rx = n.rx, ry = n.ry;
+    const long long g = n.g, D = p.D;
+    const bool ring = tid < KO_RX * KO_RY;
 
     // ---- F1, cross-diffusion, diffusivities on the tile + 1 ring -------------
     // (Update_kOmega_Diffusivities, kOmegaKernels.cl:24-94)
     const int sy = ry + 1, sx = rx + 1;  // position in the 2-ring tile
     double Dk = 0.0, Do = 0.0, F1 = 0.0, mxv = 0.0, myv = 0.0;
+    double yv = 1.0, rho = 0.0, nt = 0.0;
     Fd3 X, Y, X2, Y2;
-    if (inrow && !(t & M_SOLID)) {
+    const bool fluid = n.inrow && !(t & M_SOLID);
+    if (fluid) {
+        yv = S.fld[0][tid];
+        rho = S.fld[1][tid];
+        nt = S.fld[2][tid];
         node_weights(p, t, g, X, X2, Y, Y2);
-        const double om = sO[sy][sx], kv = sK[sy][sx];
-        const double dOdx = X.e * sO[sy][sx + 1] + X.w * sO[sy][sx - 1] + X.c * om;
-        const double dKdx = X.e * sK[sy][sx + 1] + X.w * sK[sy][sx - 1] + X.c * kv;
-        const double dOdy = Y.e * sO[sy + 1][sx] + Y.w * sO[sy - 1][sx] + Y.c * om;
-        const double dKdy = Y.e * sK[sy + 1][sx] + Y.w * sK[sy - 1][sx] + Y.c * kv;
+        const double om = S.O[sy][sx], kv = S.K[sy][sx];
+        const double dOdx = X.e * S.O[sy][sx + 1] + X.w * S.O[sy][sx - 1] + X.c * om;
+        const double dKdx = X.e * S.K[sy][sx + 1] + X.w * S.K[sy][sx - 1] + X.c * kv;
+        const double dOdy = Y.e * S.O[sy + 1][sx] + Y.w * S.O[sy - 1][sx] + Y.c * om;
+        const double dKdy = Y.e * S.K[sy + 1][sx] + Y.w * S.K[sy - 1][sx] + Y.c * kv;
         const double m = 2. * KO_SIGMA_O2 / om;
         mxv = m * dKdx;
         myv = m * dKdy;
@@ -194,28 +232,30 @@ komega_assemble_kernel(const AsmParams p) {
         Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
     }
     if (ring) {
-        sDk[ry][rx] = Dk;
-        sDo[ry][rx] = Do;
+        M.Dk[ry][rx] = Dk;
+        M.Do[ry][rx] = Do;
     }
     __syncthreads();
 
     // ---- rows of the tile's nodes (Update_kOmega_Coeffs_Implicit) ------------
-    if (!interior) return;
+    if (!n.interior) return;
     if (t & M_SOLID) {
         for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
         p.rhs_o[g] = vec_t(0);
         p.rhs_k[g] = vec_t(0);
         return;
     }
+    const double Ux = S.fld[3][tid], Uy = S.fld[4][tid];
+    const double Sxx = S.fld[5][tid], Sxy = S.fld[6][tid], Syy = S.fld[7][tid];
     const double dk = Dk, dom = Do;
-    const double dk_dx = X.e * sDk[ry][rx + 1] + X.w * sDk[ry][rx - 1] + X.c * dk;
-    const double do_dx = X.e * sDo[ry][rx + 1] + X.w * sDo[ry][rx - 1] + X.c * dom;
-    const double dk_dy = Y.e * sDk[ry + 1][rx] + Y.w * sDk[ry - 1][rx] + Y.c * dk;
-    const double do_dy = Y.e * sDo[ry + 1][rx] + Y.w * sDo[ry - 1][rx] + Y.c * dom;
+    const double dk_dx = X.e * M.Dk[ry][rx + 1] + X.w * M.Dk[ry][rx - 1] + X.c * dk;
+    const double do_dx = X.e * M.Do[ry][rx + 1] + X.w * M.Do[ry][rx - 1] + X.c * dom;
+    const double dk_dy = Y.e * M.Dk[ry + 1][rx] + Y.w * M.Dk[ry - 1][rx] + Y.c * dk;
+    const double do_dy = Y.e * M.Do[ry + 1][rx] + Y.w * M.Do[ry - 1][rx] + Y.c * dom;
     const double Jxo = Ux - do_dx - mxv;
     const double Jyo = Uy - do_dy - myv;
     const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
-    const double Kraw = sK[sy][sx], Oraw = sO[sy][sx];
+    const double Kraw = S.K[sy][sx], Oraw = S.O[sy][sx];
     double om = dmaxr(0.0, Oraw);
     const double kv = dmaxr(0.0, Kraw);
     const double f1 = F1;
@@ -252,14 +292,41 @@ komega_assemble_kernel(const AsmParams p) {
     We *= iWc; Ww *= iWc; Wn *= iWc; Ws *= iWc; Wsrc *= iWc;
 
     // b' = b - A x0, summed in the CSR order of an interior row (S, W, C, E, N)
-    const double kS = sK[sy - 1][sx], kW = sK[sy][sx - 1], kE = sK[sy][sx + 1], kN = sK[sy + 1][sx];
-    const double oS = sO[sy - 1][sx], oW = sO[sy][sx - 1], oE = sO[sy][sx + 1], oN = sO[sy + 1][sx];
+    const double kS = S.K[sy - 1][sx], kW = S.K[sy][sx - 1], kE = S.K[sy][sx + 1], kN = S.K[sy + 1][sx];
+    const double oS = S.O[sy - 1][sx], oW = S.O[sy][sx - 1], oE = S.O[sy][sx + 1], oN = S.O[sy + 1][sx];
     const double Axk = Ks * kS + Kw * kW + Kraw + Ke * kE + Kn * kN;
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
     p.coef_o[g] = We; p.coef_o[D + g] = Ww; p.coef_o[2 * D + g] = Wn; p.coef_o[3 * D + g] = Ws;
     p.coef_k[g] = Ke; p.coef_k[D + g] = Kw; p.coef_k[2 * D + g] = Kn; p.coef_k[3 * D + g] = Ks;
     p.rhs_o[g] = (vec_t)(Wsrc - Axo);
     p.rhs_k[g] = (vec_t)(Ksrc - Axk);
+}
+
+__global__ void __launch_bounds__(KO_THREADS, 2)
+komega_assemble_kernel(const AsmParams p) {
+    extern __shared__ __align__(16) unsigned char ko_smem[];
+    AsmSmem& M = *reinterpret_cast<AsmSmem*>(ko_smem);
+    const int tid = threadIdx.x;
+    const int tiles_x = (p.nx + KO_TX - 1) / KO_TX;
+    const int ntiles = tiles_x * ((p.ny + KO_TY - 1) / KO_TY);
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;  // block-uniform
+    int buf = 0;
+    int t_cur = ko_issue(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, M.st[0]);
+    cp_async_commit();
+    for (; tile < ntiles; tile += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();  // stage `buf` complete for every thread; the previous tile is done
+        const int next = tile + gridDim.x;
+        int t_next = M_SOLID;
+        if (next < ntiles)
+            t_next = ko_issue(p, tid, (next % tiles_x) * KO_TX, (next / tiles_x) * KO_TY, M.st[buf ^ 1]);
+        cp_async_commit();
+        ko_tile(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, t_cur, M.st[buf], M);
+        t_cur = t_next;
+        buf ^= 1;
+    }
+    cp_async_wait_all();
 }
 
 }  // namespace kofm
