@@ -348,22 +348,49 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
 // are neither stored nor counted).
 constexpr int WS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
 static_assert(KOFM_MAX_KRYLOV == 10, "krylov_strip is instantiated for k = 0..9");
-constexpr int WS_SLOTS = 3;
 constexpr int GM_WARPS = GM_THREADS / 32;
 
-struct WarpSlot {
-    double cf[4][32];          // E, W, N, S of row y
-    double vj[WS_KV][32];      // u_j(y), j < k-1
-    double r[32];              // r(y) (k >= 1)
-    double up[32];             // u_{k-1}(y+1)
-    double gcf[2][4];          // ghost columns x0-1 (0) and x0+32 (1): coefficients
-    double gvj[2][WS_KV];      // ... u_j(y)
-    double gup[2];             // ... u_{k-1}(y+1)
-    double gout[2];            // u_{k-1}(y) at x0-2 and x0+33
+// One ring slot of a warp: everything row y needs, laid out per k (the
+// number of basis vectors read depends on the vector being built):
+//   cf[4][32]     E, W, N, S of row y
+//   vj[k-1][32]   u_j(y), j < k-1
+//   r[32]         r(y) (k >= 1)
+//   up[32]        u_{k-1}(y+1)
+//   gcf[2][4], gvj[2][k-1], gup[2], gout[2]: the ghost columns x0-1 (0) and
+//                 x0+32 (1): coefficients, u_j(y), u_{k-1}(y+1), and
+//                 u_{k-1}(y) at x0-2 and x0+33.
+// The warp's ring region holds as many slots of that size as fit (up to 6),
+// so small k prefetch deeper.
+constexpr int WS_RING_DOUBLES = 3 * ((4 + WS_KV + 2) * 32 + 2 * 4 + 2 * WS_KV + 4);
+
+template <int k>
+struct SlotView {
+    static constexpr int NV = k > 1 ? k - 1 : 0;
+    static constexpr int NR = k > 0 ? 1 : 0;
+    static constexpr int O_VJ = 4 * 32;
+    static constexpr int O_R = O_VJ + NV * 32;
+    static constexpr int O_UP = O_R + NR * 32;
+    static constexpr int O_GCF = O_UP + 32;
+    static constexpr int O_GVJ = O_GCF + 8;
+    static constexpr int O_GUP = O_GVJ + 2 * (NV > 0 ? NV : 1);
+    static constexpr int O_GOUT = O_GUP + 2;
+    static constexpr int DOUBLES = O_GOUT + 2;
+    static constexpr int FIT = WS_RING_DOUBLES / DOUBLES;
+    static constexpr int SLOTS = FIT > 6 ? 6 : FIT;
+    static_assert(SLOTS >= 3, "ring too small");
+    double* b;
+    __device__ __forceinline__ double& cf(int q, int lane) const { return b[q * 32 + lane]; }
+    __device__ __forceinline__ double& vj(int j, int lane) const { return b[O_VJ + j * 32 + lane]; }
+    __device__ __forceinline__ double& r(int lane) const { return b[O_R + lane]; }
+    __device__ __forceinline__ double& up(int lane) const { return b[O_UP + lane]; }
+    __device__ __forceinline__ double& gcf(int h, int q) const { return b[O_GCF + h * 4 + q]; }
+    __device__ __forceinline__ double& gvj(int h, int j) const { return b[O_GVJ + h * (NV > 0 ? NV : 1) + j]; }
+    __device__ __forceinline__ double& gup(int h) const { return b[O_GUP + h]; }
+    __device__ __forceinline__ double& gout(int h) const { return b[O_GOUT + h]; }
 };
 
 struct SolverSmem {
-    WarpSlot ring[GM_WARPS][WS_SLOTS];
+    double ring[GM_WARPS][WS_RING_DOUBLES];
     double g[KOFM_MAX_KRYLOV];  // h_j s_j
     double sk1;                 // s_{k-1}
 };
@@ -393,40 +420,40 @@ __device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, 
 template <int k>
 __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
                                          const double* rsrc, int y, int xl, int lane,
-                                         int gin, int gout, WarpSlot& W) {
+                                         int gin, int gout, SlotView<k> W) {
     const long long D = a.D;
-    el_copy(a, src, y + 1, xl, &W.up[lane]);
+    el_copy(a, src, y + 1, xl, &W.up(lane));
     const bool ghost = lane == 0 || lane == 31;
     const int h = lane == 0 ? 0 : 1;
     if (ghost) {
-        el_copy(a, src, y + 1, gin, &W.gup[h]);
-        el_copy(a, src, y, gout, &W.gout[h]);
+        el_copy(a, src, y + 1, gin, &W.gup(h));
+        el_copy(a, src, y, gout, &W.gout(h));
     }
     if (y < 0 || y >= a.ny) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) W.cf[q][lane] = 0.0;
+        for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.0;
 #pragma unroll
-        for (int j = 0; j < k - 1; ++j) W.vj[j][lane] = 0.0;
-        W.r[lane] = 0.0;
+        for (int j = 0; j < k - 1; ++j) W.vj(j, lane) = 0.0;
+        W.r(lane) = 0.0;
         if (ghost) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) W.gcf[h][q] = 0.0;
+            for (int q = 0; q < 4; ++q) W.gcf(h, q) = 0.0;
 #pragma unroll
-            for (int j = 0; j < k - 1; ++j) W.gvj[h][j] = 0.0;
+            for (int j = 0; j < k - 1; ++j) W.gvj(h, j) = 0.0;
         }
         return;
     }
     const long long row = (long long)y * a.P;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) cp8(&W.cf[q][lane], S.coef + q * D + row + xl);
+    for (int q = 0; q < 4; ++q) cp8(&W.cf(q, lane), S.coef + q * D + row + xl);
 #pragma unroll
-    for (int j = 0; j < k - 1; ++j) cp8(&W.vj[j][lane], S.V + (long long)j * D + row + xl);
-    if (k > 0) cp8(&W.r[lane], rsrc + row + xl);
+    for (int j = 0; j < k - 1; ++j) cp8(&W.vj(j, lane), S.V + (long long)j * D + row + xl);
+    if (k > 0) cp8(&W.r(lane), rsrc + row + xl);
     if (ghost) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) cp8(&W.gcf[h][q], S.coef + q * D + row + gin);
+        for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + q * D + row + gin);
 #pragma unroll
-        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj[h][j], S.V + (long long)j * D + row + gin);
+        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + (long long)j * D + row + gin);
     }
 }
 
@@ -435,7 +462,7 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
 // older basis vectors has its exact length.
 template <int k>
 __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc,
-                             int x0, int ya, int yb, SolverSmem& T, WarpSlot* ring,
+                             int x0, int ya, int yb, SolverSmem& T, double* ring,
                              double (&acc)[2 + KOFM_MAX_KRYLOV]) {
     const int lane = threadIdx.x & 31;
     const long long D = a.D;
@@ -456,10 +483,14 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double um = ld(ya - 2, xl), u0 = ld(ya - 1, xl);
     double gm = 0.0, g0 = 0.0;
     if (ghost) { gm = ld(ya - 2, gin); g0 = ld(ya - 1, gin); }
-    ws_issue<k>(a, S, src, rsrc, ya - 1, xl, lane, gin, gout, ring[(ya - 1 + 3) % 3]);
-    cp_commit();
-    ws_issue<k>(a, S, src, rsrc, ya, xl, lane, gin, gout, ring[ya % 3]);
-    cp_commit();
+    using SV = SlotView<k>;
+    constexpr int NS = SV::SLOTS;  // rows of loads in flight: NS - 1
+    auto slot = [&](int y) { return SV{ring + ((y + NS) % NS) * SV::DOUBLES}; };
+#pragma unroll
+    for (int i = 0; i < NS - 1; ++i) {
+        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i));
+        cp_commit();
+    }
 
     double q[WS_KV];
 #pragma unroll
@@ -467,15 +498,15 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double nprev = 0.0, ukprev = 0.0;
     const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        if (y + 2 <= yb) ws_issue<k>(a, S, src, rsrc, y + 2, xl, lane, gin, gout, ring[(y + 2) % 3]);
+        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1));
         cp_commit();
-        cp_wait<2>();
-        const WarpSlot& W = ring[(y + 3) % 3];
-        const double up = W.up[lane];
-        const double cE = W.cf[0][lane], cW = W.cf[1][lane], cN = W.cf[2][lane], cS = W.cf[3][lane];
+        cp_wait<NS - 1>();
+        const SV W = slot(y);
+        const double up = W.up(lane);
+        const double cE = W.cf(0, lane), cW = W.cf(1, lane), cN = W.cf(2, lane), cS = W.cf(3, lane);
         double v[WS_KV];
 #pragma unroll
-        for (int j = 0; j < WS_KV; ++j) v[j] = j < k - 1 ? W.vj[j][lane] : 0.0;
+        for (int j = 0; j < WS_KV; ++j) v[j] = j < k - 1 ? W.vj(j, lane) : 0.0;
         // u_k(y) on the own column
         double left = __shfl_up_sync(0xffffffffu, u0, 1);
         double right = __shfl_down_sync(0xffffffffu, u0, 1);
@@ -497,21 +528,21 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
         double ukg = 0.0;
         if (ghost) {
             const int h = lane == 0 ? 0 : 1;
-            const double gl = lane == 0 ? W.gout[h] : u0;
-            const double gr = lane == 0 ? u0 : W.gout[h];
-            const double gz = W.gcf[h][3] * gm + W.gcf[h][1] * gl + g0 + W.gcf[h][0] * gr +
-                              W.gcf[h][2] * W.gup[h];
+            const double gl = lane == 0 ? W.gout(h) : u0;
+            const double gr = lane == 0 ? u0 : W.gout(h);
+            const double gz = W.gcf(h, 3) * gm + W.gcf(h, 1) * gl + g0 + W.gcf(h, 0) * gr +
+                              W.gcf(h, 2) * W.gup(h);
             if (k == 0) {
                 ukg = gz;
             } else {
                 ukg = sk1 * gz;
 #pragma unroll
-                for (int j = 0; j < k - 1; ++j) ukg -= T.g[j] * W.gvj[h][j];
+                for (int j = 0; j < k - 1; ++j) ukg -= T.g[j] * W.gvj(h, j);
                 ukg -= T.g[k - 1] * g0;
             }
         }
         const bool rowin = y >= ya && y < yb;
-        const double rr = k == 0 ? u0 : W.r[lane];
+        const double rr = k == 0 ? u0 : W.r(lane);
         if (rowin && own) {
             __stcg(Vk + (long long)y * a.P + xl, uk);
             acc[0] += uk * uk;
@@ -549,7 +580,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
         u0 = up;
         if (ghost) {
             gm = g0;
-            g0 = W.gup[lane == 0 ? 0 : 1];
+            g0 = W.gup(lane == 0 ? 0 : 1);
         }
     }
     cp_wait<0>();
@@ -561,7 +592,7 @@ gmres_kernel(const GmresArgs a) {
     GmresControl* ctl = a.ctl;
     extern __shared__ __align__(16) unsigned char gm_smem[];
     SolverSmem& T = *reinterpret_cast<SolverSmem*>(gm_smem);  // dynamic: larger than 48 KiB
-    WarpSlot* ring = T.ring[threadIdx.x >> 5];
+    double* ring = T.ring[threadIdx.x >> 5];
     const int wib = threadIdx.x >> 5;  // warp in block
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];

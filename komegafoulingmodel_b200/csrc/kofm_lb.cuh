@@ -34,6 +34,10 @@
 #pragma once
 #include "kofm_common.cuh"
 
+#ifndef KOFM_LB_MINBLOCKS
+#define KOFM_LB_MINBLOCKS 1  // resident 128-thread blocks per SM the register budget targets
+#endif
+
 namespace kofm {
 
 struct LbParams {
@@ -107,7 +111,7 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 // NEQ: populations stored as f - feq(reference moments of the writing node),
 // FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.
 template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, KOFM_LB_MINBLOCKS)
 lb_step_kernel(const LbParams p) {
     const int lane = threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -141,7 +145,7 @@ lb_step_kernel(const LbParams p) {
     }
 
     AT d[9][4];
-    float own_r[4], own_u[4], own_v[4];  // NEQ: this node's reference moments
+    float own_r[4] = {}, own_u[4] = {}, own_v[4] = {};  // NEQ: this node's reference moments
     // own stored population of direction q, decoded
     auto own_pop = [&](int q, int j) -> AT {
         const float raw = ld1(gin, q * D + rowoff + x0 + j);
