@@ -126,6 +126,18 @@ def solver_bytes_per_node(stats, K):
     return total
 
 
+STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
+                 "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)"}
+
+
+def workload_config(w, args, world: int) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny, "nodes": w.nodes,
+            "storage": STORAGE_NAMES[args.storage], "krylov_dim": 10, "rel_tol": 1.0e-4,
+            "abs_tol": 1.0e-7, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (populations and solver vectors), no flush"}
+
+
 def max_over_ranks(value: float, world: int, device=None) -> float:
     """The slowest rank's time: all-reduce MAX over the process group (NCCL
     on the GPU box; gloo with a CPU tensor in the tests)."""
@@ -275,14 +287,7 @@ def run_ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.storage == "fp32" else "f32", "data": "synthetic",
-            "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
-                       "nodes": nodes,
-                       "storage": {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
-                                   "bf16": "bf16 f-w deviation",
-                                   "fp16neq": "fp16 f-feq (FP32 reference moments)"}[args.storage],
-                       "krylov_dim": d.krylov_dim, "rel_tol": d.komega_rel_tol,
-                       "abs_tol": d.komega_abs_tol, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (1.2 GB populations), no flush"},
+            "config": workload_config(w, args, world),
             "roofline": roof,
             "step_roofline": {"bytes_per_node": step_bytes,
                               "achieved": step_bytes * nodes / (step_ms * 1e-3) / 1e9,
@@ -374,8 +379,7 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["seconds"] * 1e3 / res["steps_timed"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny,
-                   "nodes": w.nodes, "parallelism": "host cores"},
+        "config": workload_config(w, args, world),
         "impl": "reference",
         "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
