@@ -61,21 +61,20 @@ class Channel:
         return 0.5 * (float(np.mean(self.y_top)) - float(np.mean(self.y_bot)))
 
 
-def _link_fraction(i, j, q, nx, y_bot, y_top):
-    """Fraction t in (0, 1] of the link from node (i, j) in direction q at
-    which it meets a wall; walls are linear between columns (periodic in x)."""
+def _link_fractions(ii, jj, q, nx, y_bot, y_top):
+    """Fraction t in (0, 1] of the links from nodes (ii, jj) in direction q at
+    which they meet a wall; walls are linear between columns (periodic in x)."""
     cx, cy = int(CX[q]), int(CY[q])
-    ts = []
-    for y_w, below in ((y_bot, True), (y_top, False)):
-        y0 = float(y_w[i])
-        d = float(y_w[(i + cx) % nx]) - y0 if cx != 0 else 0.0
+    best = np.full(ii.shape, np.inf)
+    for y_w in (y_bot, y_top):
+        y0 = y_w[ii]
+        d = (y_w[(ii + cx) % nx] - y0) if cx != 0 else np.zeros_like(y0)
         den = cy - d
-        if den == 0.0:
-            continue
-        t = (y0 - j) / den
-        if 0.0 < t <= 1.0 + 1e-12:
-            ts.append(min(t, 1.0))
-    return min(ts) if ts else 0.5
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = np.where(den != 0.0, (y0 - jj) / np.where(den != 0.0, den, 1.0), np.inf)
+        ok = (t > 0.0) & (t <= 1.0 + 1e-12)
+        best = np.where(ok, np.minimum(best, np.minimum(t, 1.0)), best)
+    return np.where(np.isfinite(best), best, 0.5)
 
 
 def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius):
@@ -136,14 +135,18 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
             t[hit] |= NESW_BOUNDARY0
             ii, jv = np.nonzero(hit.T)
             t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY | SOLID_BOUNDARY0
-        for jv, ii in zip(*np.nonzero(hit)):
-            frac = _link_fraction(int(ii), int(jv), q, nx, y_bot, y_top)
-            if q < 5:
-                dX[q - 1, jv, ii] = frac
-            if abs(frac - 0.5) > 1e-12:
-                ibb_idx.append(q * D + jv * nxf + ii)
-                ibb_q.append(frac)
-    wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, min(wall_radius, nx // 2))
+        jv, ii = np.nonzero(hit)
+        frac = _link_fractions(ii, jv, q, nx, y_bot, y_top)
+        if q < 5:
+            dX[q - 1, jv, ii] = frac
+        keep = np.abs(frac - 0.5) > 1e-12
+        ibb_idx.extend((q * D + jv * nxf + ii)[keep].tolist())
+        ibb_q.extend(frac[keep].tolist())
+    if np.all(y_bot == y_bot[0]) and np.all(y_top == y_top[0]):
+        # straight walls: the nearest wall point is straight above or below
+        wall = np.where(fluid, np.minimum(j[:, None] - y_bot[0], y_top[0] - j[:, None]), 0.0)
+    else:
+        wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, min(wall_radius, nx // 2))
     order = np.argsort(ibb_idx, kind="stable")
     return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(), dX.ravel(),
                    wall.ravel(), np.asarray(ibb_idx, np.int32)[order],
