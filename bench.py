@@ -106,8 +106,8 @@ def solver_bytes_per_node(stats, K):
     * residual pass: restart 0 reads b' (8); a later restart forms
       r = b' - A x from b', x, the four coefficients and stores r (56);
     * Krylov vector k of a cycle: u_{k-1} (or r) and the older basis vectors
-      u_j (j < k-1), the four FP32 coefficients, r for <r, u_k>, and the store
-      of u_k: 32 + 8 k;
+      u_j (j < k-1), the four coefficients, r for <r, u_k>, and the store of
+      u_k: 48 + 8 k;
     * cycle update: r, the kk - 1 basis vectors with a non-zero coefficient,
       x (after the first cycle) and the store of x;
     * write-back: x, the field (FP32 read + write) and the node flag.
@@ -120,7 +120,7 @@ def solver_bytes_per_node(stats, K):
         vsum = getattr(stats, sysname + "_vec_index_sum")
         terms = getattr(stats, sysname + "_update_terms")
         res = 8 + 56 * max(restarts - 1, 0)
-        kry = 32 * vecs + 8 * vsum
+        kry = 48 * vecs + 8 * vsum
         upd = 16 * cycles + 8 * max(terms - cycles, 0) + 8 * max(cycles - 1, 0)
         total += res + kry + upd + 18
     return total
@@ -162,7 +162,7 @@ GMRES_TRAFFIC_BYTES_PER_NODE = 4.3399e9 / 4194304
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
             "fp16neq": 114}                   # + reference moments read and written
-ASM_BYTES = 154                                     # fused assembly, per node
+ASM_BYTES = 122                                     # fused assembly, per node
 
 
 def run_ours(args, rank, world, local_rank):

@@ -21,13 +21,8 @@
 //    each vector costs one sweep and one grid barrier instead of the
 //    reference's product / two Gram-Schmidt stages / normalise.
 //    Krylov vectors are kept un-normalised; the scales 1/||u_j|| are applied
-//    lazily.  Vectors are FP64 (an FP32 basis stalls the first cycle near 1e-5
-//    relative residual on the omega wall rows).  The Krylov sweeps apply an
-//    FP32 copy of the operator (rounded once by the assembly, ~6e-8 relative);
-//    every residual r = b' - A x that decides convergence or restarts a cycle
-//    uses the FP64 operator, so the converged correction is that of the FP64
-//    system (mixed-precision restarted GMRES; the FP32 operator only shapes
-//    the Krylov space of each cycle).
+//    lazily.  Vectors and matrix are FP64 (an FP32 basis stalls the first
+//    cycle near 1e-5 relative residual on the omega wall rows).
 //  * Dot products are reduced per block and combined, in a fixed order, by
 //    the last block to reach the grid barrier, which also runs the scalar
 //    logic (the reference's host code) before releasing the grid.  The
@@ -357,7 +352,7 @@ constexpr int GM_WARPS = GM_THREADS / 32;
 
 // One ring slot of a warp: everything row y needs, laid out per k (the
 // number of basis vectors read depends on the vector being built):
-//   cf[4][32]     E, W, N, S of row y (FP32 copy of the operator)
+//   cf[4][32]     E, W, N, S of row y
 //   vj[k-1][32]   u_j(y), j < k-1
 //   r[32]         r(y) (k >= 1)
 //   up[32]        u_{k-1}(y+1)
@@ -372,11 +367,11 @@ template <int k>
 struct SlotView {
     static constexpr int NV = k > 1 ? k - 1 : 0;
     static constexpr int NR = k > 0 ? 1 : 0;
-    static constexpr int O_VJ = 2 * 32;  // cf: 4 x 32 floats
+    static constexpr int O_VJ = 4 * 32;
     static constexpr int O_R = O_VJ + NV * 32;
     static constexpr int O_UP = O_R + NR * 32;
     static constexpr int O_GCF = O_UP + 32;
-    static constexpr int O_GVJ = O_GCF + 4;  // gcf: 2 x 4 floats
+    static constexpr int O_GVJ = O_GCF + 8;
     static constexpr int O_GUP = O_GVJ + 2 * (NV > 0 ? NV : 1);
     static constexpr int O_GOUT = O_GUP + 2;
     static constexpr int DOUBLES = O_GOUT + 2;
@@ -384,15 +379,11 @@ struct SlotView {
     static constexpr int SLOTS = FIT > 6 ? 6 : FIT;
     static_assert(SLOTS >= 3, "ring too small");
     double* b;
-    __device__ __forceinline__ float& cf(int q, int lane) const {
-        return reinterpret_cast<float*>(b)[q * 32 + lane];
-    }
+    __device__ __forceinline__ double& cf(int q, int lane) const { return b[q * 32 + lane]; }
     __device__ __forceinline__ double& vj(int j, int lane) const { return b[O_VJ + j * 32 + lane]; }
     __device__ __forceinline__ double& r(int lane) const { return b[O_R + lane]; }
     __device__ __forceinline__ double& up(int lane) const { return b[O_UP + lane]; }
-    __device__ __forceinline__ float& gcf(int h, int q) const {
-        return reinterpret_cast<float*>(b + O_GCF)[h * 4 + q];
-    }
+    __device__ __forceinline__ double& gcf(int h, int q) const { return b[O_GCF + h * 4 + q]; }
     __device__ __forceinline__ double& gvj(int h, int j) const { return b[O_GVJ + h * (NV > 0 ? NV : 1) + j]; }
     __device__ __forceinline__ double& gup(int h) const { return b[O_GUP + h]; }
     __device__ __forceinline__ double& gout(int h) const { return b[O_GOUT + h]; }
@@ -412,10 +403,6 @@ __device__ __forceinline__ int wrap_mod(int x, int n) {
 __device__ __forceinline__ void cp8(double* smem, const double* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp4(float* smem, const float* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -444,13 +431,13 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
     }
     if (y < 0 || y >= a.ny) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.f;
+        for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.0;
 #pragma unroll
         for (int j = 0; j < k - 1; ++j) W.vj(j, lane) = 0.0;
         W.r(lane) = 0.0;
         if (ghost) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) W.gcf(h, q) = 0.f;
+            for (int q = 0; q < 4; ++q) W.gcf(h, q) = 0.0;
 #pragma unroll
             for (int j = 0; j < k - 1; ++j) W.gvj(h, j) = 0.0;
         }
@@ -458,13 +445,13 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
     }
     const long long row = (long long)y * a.P;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) cp4(&W.cf(q, lane), S.coef32 + q * D + row + xl);
+    for (int q = 0; q < 4; ++q) cp8(&W.cf(q, lane), S.coef + q * D + row + xl);
 #pragma unroll
     for (int j = 0; j < k - 1; ++j) cp8(&W.vj(j, lane), S.V + (long long)j * D + row + xl);
     if (k > 0) cp8(&W.r(lane), rsrc + row + xl);
     if (ghost) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) cp4(&W.gcf(h, q), S.coef32 + q * D + row + gin);
+        for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + q * D + row + gin);
 #pragma unroll
         for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + (long long)j * D + row + gin);
     }

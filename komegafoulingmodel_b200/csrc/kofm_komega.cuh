@@ -35,7 +35,6 @@ using vec_t = KOFM_SOLVER_VEC;  // storage type of the streamed solver vectors
 
 struct KoSystem {
     double* coef = nullptr;  // [4][D] normalised off-diagonals E, W, N, S
-    float* coef32 = nullptr; // [4][D] the same rounded to FP32 (Krylov sweeps)
     vec_t* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
     vec_t* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
@@ -55,10 +54,8 @@ struct AsmParams {
     const float* uy;
     const float* S;
     double* coef_o;
-    float* coef32_o;
     vec_t* rhs_o;
     double* coef_k;
-    float* coef32_k;
     vec_t* rhs_k;
     int nx, ny, P;
     long long D;
@@ -243,10 +240,7 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     // ---- rows of the tile's nodes (Update_kOmega_Coeffs_Implicit) ------------
     if (!n.interior) return;
     if (t & M_SOLID) {
-        for (int c = 0; c < 4; ++c) {
-            p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0;
-            p.coef32_o[c * D + g] = 0.f; p.coef32_k[c * D + g] = 0.f;
-        }
+        for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
         p.rhs_o[g] = vec_t(0);
         p.rhs_k[g] = vec_t(0);
         return;
@@ -304,8 +298,6 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
     p.coef_o[g] = We; p.coef_o[D + g] = Ww; p.coef_o[2 * D + g] = Wn; p.coef_o[3 * D + g] = Ws;
     p.coef_k[g] = Ke; p.coef_k[D + g] = Kw; p.coef_k[2 * D + g] = Kn; p.coef_k[3 * D + g] = Ks;
-    p.coef32_o[g] = (float)We; p.coef32_o[D + g] = (float)Ww; p.coef32_o[2 * D + g] = (float)Wn; p.coef32_o[3 * D + g] = (float)Ws;
-    p.coef32_k[g] = (float)Ke; p.coef32_k[D + g] = (float)Kw; p.coef32_k[2 * D + g] = (float)Kn; p.coef32_k[3 * D + g] = (float)Ks;
     p.rhs_o[g] = (vec_t)(Wsrc - Axo);
     p.rhs_k[g] = (vec_t)(Ksrc - Axk);
 }
