@@ -279,21 +279,26 @@ lb_step_kernel(const LbParams p) {
 
         AT w = tau0;
         if (KOMEGA) {
-            AT om = AT(oin[j]), kv = AT(kin[j]);
-            const AT yv = AT(win[j]);
+            // SST eddy viscosity (lbKernels.cl:400-451) in FP32: k, omega,
+            // S and wall distance are FP32 fields and nu_t is stored in FP32;
+            // the relaxation rate it sets changes the populations by ~1e-7
+            // of their non-equilibrium part, below the FP32 storage rounding.
+            float om = oin[j], kv = kin[j];
+            const float yv = win[j];
             const long long node = rowoff + x0 + j;
-            if (om < AT(0)) { om = fabs(om); p.O[node] = (float)om; }
-            if (kv < AT(0)) { kv = AT(1e-16); p.K[node] = 1e-16f; }
-            const AT a = AT(2) * sqrt(kv) / (AT(KO_BETA_STAR) * om * yv);
-            const AT b = AT(500) * mu / (yv * yv * om);
-            const AT arg = amax(a, b);
-            AT F2 = tanh(arg * arg);
-            const AT sxx = AT(sin3[0][j]), sxy = AT(sin3[1][j]), syy = AT(sin3[2][j]);
-            F2 *= sqrt(AT(2) * (sxx * sxx + AT(2) * sxy * sxy + syy * syy));
-            const AT nut = amax(amin(AT(p.maxnut), AT(KO_A1) * kv / amax(AT(KO_A1) * om, F2)),
-                                AT(1e-16));
-            o_nut[j] = (float)nut;
-            w = AT(1) / (AT(3) * (nut + mu) + AT(0.5));
+            if (om < 0.f) { om = fabsf(om); p.O[node] = om; }
+            if (kv < 0.f) { kv = 1e-16f; p.K[node] = 1e-16f; }
+            const float mu_f = (float)p.mu;
+            const float a = 2.f * sqrtf(kv) / ((float)KO_BETA_STAR * om * yv);
+            const float b = 500.f * mu_f / (yv * yv * om);
+            const float arg = fmaxf(a, b);
+            float F2 = tanhf(arg * arg);
+            const float sxx = sin3[0][j], sxy = sin3[1][j], syy = sin3[2][j];
+            F2 *= sqrtf(2.f * (sxx * sxx + 2.f * sxy * sxy + syy * syy));
+            const float a1 = (float)KO_A1;
+            const float nut = fmaxf(fminf((float)p.maxnut, a1 * kv / fmaxf(a1 * om, F2)), 1e-16f);
+            o_nut[j] = nut;
+            w = AT(1) / (AT(3) * (AT(nut) + mu) + AT(0.5));
         }
         AT sxx_n = AT(0), sxy_n = AT(0), syy_n = AT(0);
 #pragma unroll
