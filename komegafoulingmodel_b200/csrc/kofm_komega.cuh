@@ -223,11 +223,15 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
         const double m = 2. * KO_SIGMA_O2 / om;
         mxv = m * dKdx;
         myv = m * dKdy;
-        const double CDkw = dmaxr(rho * (mxv * dOdx + myv * dOdy), 1.0e-10);
-        double a = dmaxr(sqrt(kv) / (KO_BETA_STAR * om * yv), 500. * p.mu / (yv * yv * om));
-        a = dminr(a, 4. * kv * KO_SIGMA_O2 / (CDkw * yv * yv));
-        const double a2 = a * a;
-        F1 = tanh(a2 * a2);
+        // blending function F1 (kOmegaKernels.cl:68-87) in FP32: its inputs k,
+        // omega, rho, y are FP32 fields; F1 in [0, 1] enters D_k, D_w with an
+        // error ~1e-7, the size of the FP32 rounding of nu_t beside it
+        const float CDkw = fmaxf((float)(rho * (mxv * dOdx + myv * dOdy)), 1.0e-10f);
+        const float kf = (float)kv, of = (float)om, yf = (float)yv;
+        float a = fmaxf(sqrtf(kf) / ((float)KO_BETA_STAR * of * yf), 500.f * (float)p.mu / (yf * yf * of));
+        a = fminf(a, 4.f * kf * (float)KO_SIGMA_O2 / (CDkw * yf * yf));
+        const float a2 = a * a;
+        F1 = (double)tanhf(a2 * a2);
         Dk = p.mu + (KO_SIGMA_K1 * F1 + KO_SIGMA_K2 * (1. - F1)) * nt;
         Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
     }
