@@ -408,10 +408,12 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// element (y, x) of a lattice array into shared memory; zero outside the rows
-__device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, int y, int x, double* dst) {
+// element (y, x) of vector j of an array of nv vectors (nv = 1: plain
+// layout) into shared memory; zero outside the rows
+__device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, int nv, int j,
+                                        int y, int x, double* dst) {
     if (y < 0 || y >= a.ny) *dst = 0.0;
-    else cp8(dst, base + (long long)y * a.P + x);
+    else cp8(dst, base + (nv == 1 ? (long long)y * a.P + x : ilv(nv, j, (long long)y * a.P + x)));
 }
 
 // The thread's inputs of row y into slot W: u_{k-1}(y+1), and for rows inside
@@ -419,15 +421,15 @@ __device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, 
 // ghost column.
 template <int k>
 __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
+                                         int src_nv, int src_j,
                                          const double* rsrc, int y, int xl, int lane,
                                          int gin, int gout, SlotView<k> W) {
-    const long long D = a.D;
-    el_copy(a, src, y + 1, xl, &W.up(lane));
+    el_copy(a, src, src_nv, src_j, y + 1, xl, &W.up(lane));
     const bool ghost = lane == 0 || lane == 31;
     const int h = lane == 0 ? 0 : 1;
     if (ghost) {
-        el_copy(a, src, y + 1, gin, &W.gup(h));
-        el_copy(a, src, y, gout, &W.gout(h));
+        el_copy(a, src, src_nv, src_j, y + 1, gin, &W.gup(h));
+        el_copy(a, src, src_nv, src_j, y, gout, &W.gout(h));
     }
     if (y < 0 || y >= a.ny) {
 #pragma unroll
@@ -444,16 +446,17 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
         return;
     }
     const long long row = (long long)y * a.P;
+    const long long gl = row + xl, gg = row + gin;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) cp8(&W.cf(q, lane), S.coef + q * D + row + xl);
+    for (int q = 0; q < 4; ++q) cp8(&W.cf(q, lane), S.coef + ilv(4, q, gl));
 #pragma unroll
-    for (int j = 0; j < k - 1; ++j) cp8(&W.vj(j, lane), S.V + (long long)j * D + row + xl);
-    if (k > 0) cp8(&W.r(lane), rsrc + row + xl);
+    for (int j = 0; j < k - 1; ++j) cp8(&W.vj(j, lane), S.V + ilv(a.K, j, gl));
+    if (k > 0) cp8(&W.r(lane), rsrc + gl);
     if (ghost) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + q * D + row + gin);
+        for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + ilv(4, q, gg));
 #pragma unroll
-        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + (long long)j * D + row + gin);
+        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + ilv(a.K, j, gg));
     }
 }
 
@@ -465,8 +468,9 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
                              int x0, int ya, int yb, SolverSmem& T, double* ring,
                              double (&acc)[2 + KOFM_MAX_KRYLOV]) {
     const int lane = threadIdx.x & 31;
-    const long long D = a.D;
-    const double* src = (k == 0) ? rsrc : S.V + (long long)(k - 1) * D;
+    // u_{k-1}: r (plain layout) for k = 0, else basis vector k-1 (interleaved)
+    const double* src = (k == 0) ? rsrc : S.V;
+    const int src_nv = (k == 0) ? 1 : a.K, src_j = (k == 0) ? 0 : k - 1;
     const bool need_w = k < a.K - 1;
     const int xl = wrap_mod(x0 + lane, a.nx);
     const bool own = x0 + lane < a.nx;
@@ -474,11 +478,12 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     const int gin = wrap_mod(lane == 0 ? x0 - 1 : x0 + 32, a.nx);
     const int gout = wrap_mod(lane == 0 ? x0 - 2 : x0 + 33, a.nx);
     const bool ghost = lane == 0 || lane == 31;
-    double* Vk = S.V + (long long)k * D;
 
     // rolling u_{k-1} window (rows y-1, y) on the own and the ghost column
     auto ld = [&](int y, int x) -> double {
-        return (y < 0 || y >= a.ny) ? 0.0 : __ldcg(src + (long long)y * a.P + x);
+        if (y < 0 || y >= a.ny) return 0.0;
+        const long long g = (long long)y * a.P + x;
+        return __ldcg(src + (src_nv == 1 ? g : ilv(src_nv, src_j, g)));
     };
     double um = ld(ya - 2, xl), u0 = ld(ya - 1, xl);
     double gm = 0.0, g0 = 0.0;
@@ -488,7 +493,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     auto slot = [&](int y) { return SV{ring + ((y + NS) % NS) * SV::DOUBLES}; };
 #pragma unroll
     for (int i = 0; i < NS - 1; ++i) {
-        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i));
+        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i));
         cp_commit();
     }
 
@@ -498,7 +503,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double nprev = 0.0, ukprev = 0.0;
     const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1));
+        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1));
         cp_commit();
         cp_wait<NS - 1>();
         const SV W = slot(y);
@@ -544,7 +549,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
         const bool rowin = y >= ya && y < yb;
         const double rr = k == 0 ? u0 : W.r(lane);
         if (rowin && own) {
-            __stcg(Vk + (long long)y * a.P + xl, uk);
+            __stcg(S.V + ilv(a.K, k, (long long)y * a.P + xl), uk);
             acc[0] += uk * uk;
             acc[1] += rr * uk;
         }
@@ -636,11 +641,11 @@ gmres_kernel(const GmresArgs a) {
                             const int xw = xj > 0 ? xj - 1 : a.nx - 1;
                             const int xe = xj + 1 < a.nx ? xj + 1 : 0;
                             const double Ax =
-                                (double)__ldg(S.coef + 3 * a.D + gj) * __ldcg(S.x + gj - a.P) +
-                                (double)__ldg(S.coef + a.D + gj) * __ldcg(S.x + row + xw) +
+                                (double)__ldg(S.coef + ilv(4, 3, gj)) * __ldcg(S.x + gj - a.P) +
+                                (double)__ldg(S.coef + ilv(4, 1, gj)) * __ldcg(S.x + row + xw) +
                                 __ldcg(S.x + gj) +
-                                (double)__ldg(S.coef + gj) * __ldcg(S.x + row + xe) +
-                                (double)__ldg(S.coef + 2 * a.D + gj) * __ldcg(S.x + gj + a.P);
+                                (double)__ldg(S.coef + ilv(4, 0, gj)) * __ldcg(S.x + row + xe) +
+                                (double)__ldg(S.coef + ilv(4, 2, gj)) * __ldcg(S.x + gj + a.P);
                             rr[j] = rnd((double)__ldcg(S.rhs + gj) - Ax);
                         }
                         stvec2(S.r + g, rr[0], rr[1]);
@@ -730,7 +735,7 @@ gmres_kernel(const GmresArgs a) {
                 for (int j = 1; j < K; ++j) {
                     const double cj = sh_c[s][j];
                     if (cj == 0.0) continue;
-                    const double2 u = ldvec2(S.V + (long long)(j - 1) * a.D + g);
+                    const double2 u = ldvec2(S.V + ilv(K, j - 1, g));  // g even: g, g+1 adjacent
                     v0 += cj * u.x;
                     v1 += cj * u.y;
                 }

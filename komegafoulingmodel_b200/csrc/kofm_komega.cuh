@@ -33,12 +33,21 @@ constexpr int KO_TX = 32, KO_TY = 8;
 #endif
 using vec_t = KOFM_SOLVER_VEC;  // storage type of the streamed solver vectors
 
+// Multi-vector arrays (the 4 coefficients, the Krylov basis) are stored
+// tile-interleaved: the NV values of the 32 nodes of one row segment (node
+// index g = x + P y, P a multiple of 32) are contiguous, element (j, g) at
+// ((g / 32) NV + j) 32 + g % 32.  A warp sweeping a 32-column strip then
+// reads one contiguous block per row instead of NV separate row pieces.
+__host__ __device__ __forceinline__ long long ilv(int nv, int j, long long g) {
+    return ((g >> 5) * nv + j) * 32 + (g & 31);
+}
+
 struct KoSystem {
-    double* coef = nullptr;  // [4][D] normalised off-diagonals E, W, N, S
+    double* coef = nullptr;  // [4 x D] normalised off-diagonals E, W, N, S (interleaved)
     vec_t* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
     vec_t* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
-    vec_t* V = nullptr;      // [K][D] Krylov basis (orthogonalised, unscaled)
+    vec_t* V = nullptr;      // [K x D] Krylov basis (orthogonalised, unscaled; interleaved)
 };
 
 struct AsmParams {
@@ -200,7 +209,7 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
                                         const AsmStage& S, AsmSmem& M) {
     const KoNode n = ko_node(p, tid, x0, y0);
     const int rx = n.rx, ry = n.ry;
-    const long long g = n.g, D = p.D;
+    const long long g = n.g;
     const bool ring = tid < KO_RX * KO_RY;
 
     // ---- F1, cross-diffusion, diffusivities on the tile + 1 ring -------------
@@ -244,7 +253,7 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     // ---- rows of the tile's nodes (Update_kOmega_Coeffs_Implicit) ------------
     if (!n.interior) return;
     if (t & M_SOLID) {
-        for (int c = 0; c < 4; ++c) { p.coef_o[c * D + g] = 0.0; p.coef_k[c * D + g] = 0.0; }
+        for (int c = 0; c < 4; ++c) { p.coef_o[ilv(4, c, g)] = 0.0; p.coef_k[ilv(4, c, g)] = 0.0; }
         p.rhs_o[g] = vec_t(0);
         p.rhs_k[g] = vec_t(0);
         return;
@@ -300,8 +309,8 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     const double oS = S.O[sy - 1][sx], oW = S.O[sy][sx - 1], oE = S.O[sy][sx + 1], oN = S.O[sy + 1][sx];
     const double Axk = Ks * kS + Kw * kW + Kraw + Ke * kE + Kn * kN;
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
-    p.coef_o[g] = We; p.coef_o[D + g] = Ww; p.coef_o[2 * D + g] = Wn; p.coef_o[3 * D + g] = Ws;
-    p.coef_k[g] = Ke; p.coef_k[D + g] = Kw; p.coef_k[2 * D + g] = Kn; p.coef_k[3 * D + g] = Ks;
+    p.coef_o[ilv(4, 0, g)] = We; p.coef_o[ilv(4, 1, g)] = Ww; p.coef_o[ilv(4, 2, g)] = Wn; p.coef_o[ilv(4, 3, g)] = Ws;
+    p.coef_k[ilv(4, 0, g)] = Ke; p.coef_k[ilv(4, 1, g)] = Kw; p.coef_k[ilv(4, 2, g)] = Kn; p.coef_k[ilv(4, 3, g)] = Ks;
     p.rhs_o[g] = (vec_t)(Wsrc - Axo);
     p.rhs_k[g] = (vec_t)(Ksrc - Axk);
 }
