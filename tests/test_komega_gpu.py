@@ -41,9 +41,11 @@ def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0):
     return L
 
 
-@pytest.mark.parametrize("full_cycle", [0, 1])
-def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle):
-    ch, f, k, o, nut, rate, g, nu = channel_case(nx=128, ny=34)
+@pytest.mark.parametrize("full_cycle,nx", [(0, 128), (1, 128), (0, 200)])
+def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle, nx):
+    """nx = 200 is not a multiple of the solver's 32-column strips (periodic
+    tail strip) nor of the 128-node padding."""
+    ch, f, k, o, nut, rate, g, nu = channel_case(nx=nx, ny=34)
     cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
     sim.step(2)
