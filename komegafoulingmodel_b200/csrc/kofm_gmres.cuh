@@ -361,7 +361,6 @@ constexpr int GM_WARPS = GM_THREADS / 32;
 //                 u_{k-1}(y) at x0-2 and x0+33.
 // The warp's ring region holds as many slots of that size as fit (up to 6),
 // so small k prefetch deeper.
-constexpr int WS_MAX_SLOTS = 6;
 constexpr int WS_RING_DOUBLES = 3 * ((4 + WS_KV + 2) * 32 + 2 * 4 + 2 * WS_KV + 4);
 
 template <int k>
@@ -377,7 +376,7 @@ struct SlotView {
     static constexpr int O_GOUT = O_GUP + 2;
     static constexpr int DOUBLES = O_GOUT + 2;
     static constexpr int FIT = WS_RING_DOUBLES / DOUBLES;
-    static constexpr int SLOTS = FIT > WS_MAX_SLOTS ? WS_MAX_SLOTS : FIT;
+    static constexpr int SLOTS = FIT > 6 ? 6 : FIT;
     static_assert(SLOTS >= 3, "ring too small");
     double* b;
     __device__ __forceinline__ double& cf(int q, int lane) const { return b[q * 32 + lane]; }
@@ -392,7 +391,6 @@ struct SlotView {
 
 struct SolverSmem {
     double ring[GM_WARPS][WS_RING_DOUBLES];
-    unsigned long long mbar[GM_WARPS][WS_MAX_SLOTS];  // bulk-copy completion per slot
     double g[KOFM_MAX_KRYLOV];  // h_j s_j
     double sk1;                 // s_{k-1}
 };
@@ -407,39 +405,6 @@ __device__ __forceinline__ void cp8(double* smem, const double* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-
-// ---- bulk (TMA engine) copies completing on an mbarrier ----------------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* m, unsigned bytes) {
-    if (bytes)
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes)
-                     : "memory");
-    else
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(m)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* m, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
-                                         unsigned long long* m) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)) : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -458,63 +423,14 @@ template <int k>
 __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
                                          int src_nv, int src_j,
                                          const double* rsrc, int y, int xl, int lane,
-                                         int gin, int gout, SlotView<k> W,
-                                         unsigned long long* mb) {
+                                         int gin, int gout, SlotView<k> W) {
+    el_copy(a, src, src_nv, src_j, y + 1, xl, &W.up(lane));
     const bool ghost = lane == 0 || lane == 31;
     const int h = lane == 0 ? 0 : 1;
     if (ghost) {
         el_copy(a, src, src_nv, src_j, y + 1, gin, &W.gup(h));
         el_copy(a, src, src_nv, src_j, y, gout, &W.gout(h));
     }
-    if (mb) {
-        __syncwarp();  // every lane is done reading this slot's previous row
-        // Whole-strip rows are contiguous 256-byte blocks (x0 is a multiple of
-        // 32 and the strip lies inside the lattice): one lane moves them with
-        // bulk copies that complete on the slot's mbarrier; rows outside the
-        // lattice are zero-filled by the lanes.
-        const int x0 = xl - lane;
-        const bool rin = y >= 0 && y < a.ny, uin = y + 1 >= 0 && y + 1 < a.ny;
-        if (!rin) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.0;
-#pragma unroll
-            for (int j = 0; j < k - 1; ++j) W.vj(j, lane) = 0.0;
-            if (k > 0) W.r(lane) = 0.0;
-        }
-        if (!uin) W.up(lane) = 0.0;
-        if (ghost && !rin) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) W.gcf(h, q) = 0.0;
-#pragma unroll
-            for (int j = 0; j < k - 1; ++j) W.gvj(h, j) = 0.0;
-        }
-        if (lane == 0) {
-            constexpr unsigned ROWB = 32 * sizeof(double);
-            const unsigned bytes = (rin ? (4u + (k > 1 ? k - 1 : 0) + (k > 0 ? 1 : 0)) * ROWB : 0u) +
-                                   (uin ? ROWB : 0u);
-            fence_proxy_async();  // the warp's earlier reads of this slot come first
-            mbar_arrive_tx(mb, bytes);
-            if (rin) {
-                const long long g0 = (long long)y * a.P + x0;
-                bulk_g2s(&W.cf(0, 0), S.coef + ilv(4, 0, g0), 4 * ROWB, mb);
-                if (k > 1) bulk_g2s(&W.vj(0, 0), S.V + ilv(a.K, 0, g0), (k > 1 ? k - 1 : 0) * ROWB, mb);
-                if (k > 0) bulk_g2s(&W.r(0), rsrc + g0, ROWB, mb);
-            }
-            if (uin) {
-                const long long g1 = (long long)(y + 1) * a.P + x0;
-                bulk_g2s(&W.up(0), src + (src_nv == 1 ? g1 : ilv(src_nv, src_j, g1)), ROWB, mb);
-            }
-        }
-        if (ghost && rin) {
-            const long long gg = (long long)y * a.P + gin;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + ilv(4, q, gg));
-#pragma unroll
-            for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + ilv(a.K, j, gg));
-        }
-        return;
-    }
-    el_copy(a, src, src_nv, src_j, y + 1, xl, &W.up(lane));
     if (y < 0 || y >= a.ny) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.0;
@@ -550,7 +466,7 @@ __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, 
 template <int k>
 __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc,
                              int x0, int ya, int yb, SolverSmem& T, double* ring,
-                             double (&acc)[2 + KOFM_MAX_KRYLOV], unsigned& mb_phase) {
+                             double (&acc)[2 + KOFM_MAX_KRYLOV]) {
     const int lane = threadIdx.x & 31;
     // u_{k-1}: r (plain layout) for k = 0, else basis vector k-1 (interleaved)
     const double* src = (k == 0) ? rsrc : S.V;
@@ -575,16 +491,9 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     using SV = SlotView<k>;
     constexpr int NS = SV::SLOTS;  // rows of loads in flight: NS - 1
     auto slot = [&](int y) { return SV{ring + ((y + NS) % NS) * SV::DOUBLES}; };
-    // bulk copies whenever the strip is whole (not the periodic tail of an nx
-    // that is not a multiple of 32)
-    const bool bulk = x0 + 32 <= a.nx;
-    unsigned long long* mbars = T.mbar[threadIdx.x >> 5];
-    auto mbar = [&](int y) { return bulk ? &mbars[(y + NS) % NS] : nullptr; };
 #pragma unroll
     for (int i = 0; i < NS - 1; ++i) {
-        if (ya - 1 + i <= yb)
-            ws_issue<k>(a, S, src, src_nv, src_j, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i),
-                        mbar(ya - 1 + i));
+        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i));
         cp_commit();
     }
 
@@ -594,23 +503,9 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
     double nprev = 0.0, ukprev = 0.0;
     const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        if (y + NS - 1 <= yb)
-            ws_issue<k>(a, S, src, src_nv, src_j, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1),
-                        mbar(y + NS - 1));
+        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1));
         cp_commit();
         cp_wait<NS - 1>();
-        if (bulk) {
-            const int sl = (y + NS) % NS;
-            const unsigned par = (mb_phase >> sl) & 1u;
-            long long it = 0;
-            while (!mbar_try_wait(&mbars[sl], par)) {
-                if (++it > a.spin_limit) {  // never expected: record and go on
-                    atomicExch(&a.ctl->error, 2);
-                    break;
-                }
-            }
-            mb_phase ^= 1u << sl;
-        }
         const SV W = slot(y);
         const double up = W.up(lane);
         const double cE = W.cf(0, lane), cW = W.cf(1, lane), cN = W.cf(2, lane), cS = W.cf(3, lane);
@@ -704,12 +599,6 @@ gmres_kernel(const GmresArgs a) {
     SolverSmem& T = *reinterpret_cast<SolverSmem*>(gm_smem);  // dynamic: larger than 48 KiB
     double* ring = T.ring[threadIdx.x >> 5];
     const int wib = threadIdx.x >> 5;  // warp in block
-    unsigned mb_phase = 0;             // expected parity of each ring slot's mbarrier
-    if ((threadIdx.x & 31) == 0)
-        for (int i = 0; i < WS_MAX_SLOTS; ++i) mbar_init(&T.mbar[wib][i], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    fence_proxy_async();
-    __syncthreads();
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
     const long long npairs = a.D / 2;
@@ -803,7 +692,7 @@ gmres_kernel(const GmresArgs a) {
                             if (strip < a.strips) {
                                 switch (k) {
 #define KOFM_KSTRIP(n) \
-    case n: krylov_strip<n>(a, S, rsrc, strip * 32, ya, yb, T, ring, acc, mb_phase); break;
+    case n: krylov_strip<n>(a, S, rsrc, strip * 32, ya, yb, T, ring, acc); break;
                                     KOFM_KSTRIP(0) KOFM_KSTRIP(1) KOFM_KSTRIP(2) KOFM_KSTRIP(3)
                                     KOFM_KSTRIP(4) KOFM_KSTRIP(5) KOFM_KSTRIP(6) KOFM_KSTRIP(7)
                                     KOFM_KSTRIP(8) KOFM_KSTRIP(9)
