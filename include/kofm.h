@@ -247,6 +247,25 @@ int kofm_reduce_field_noalloc(const float* field, int32_t ncols, int32_t pitch, 
  * callers that order their own work against it. */
 void* kofm_stream(kofm_ctx* ctx);
 
+/* ---- batched lattices ------------------------------------------------------
+ * No counterpart in the reference, which runs one channel per process.
+ * Advances n independent lattices together: two time steps of every lattice
+ * (collide-stream; for k-omega lattices also assembly and solve) are captured
+ * once into one CUDA graph whose per-lattice branches run concurrently, and
+ * kofm_batch_step replays it (one graph launch per two steps).  Requirements
+ * checked by kofm_batch_create: all contexts on one device, each past its
+ * first step (kofm_step / kofm_lb_step called at least once), and for k-omega
+ * lattices steps_per_lb == 1 (no dt halving in progress).  The captured solves
+ * cannot run the host's dt halving: a NaN residual in any of them stops
+ * kofm_batch_step with KOFM_ERR_NAN, after which the contexts are used on
+ * their own (kofm_step).  While the batch exists the contexts may be read
+ * (kofm_get_*, kofm_reduce, kofm_get_stats) but not stepped on their own. */
+typedef struct kofm_batch kofm_batch;
+int kofm_batch_create(kofm_ctx* const* ctxs, int32_t n, kofm_batch** out);
+/* nsteps must be a multiple of 2; returns after the steps completed. */
+int kofm_batch_step(kofm_batch* b, int32_t nsteps);
+int kofm_batch_destroy(kofm_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,140 @@
+"""Batched channels: several lattices advanced by one CUDA graph per two steps
+(kofm_batch_*), and the seeded 48-channel sweep of uneven size and Re.
+
+    python -m komegafoulingmodel_b200.batch [--channels 48] [--steps 20]
+
+prints one JSON line with the aggregate throughput of the sweep advanced as a
+batch (one graph launch per two steps, the lattices' kernels running
+concurrently) and of the same channels stepped one launch sequence each.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import _abi
+from . import geometry as G
+from . import workloads as W
+from ._abi import check
+from .lattice import Lattice
+
+
+class Batch:
+    """kofm_batch over existing Lattice objects (each already stepped once)."""
+
+    def __init__(self, lattices):
+        self.lib = _abi.load()
+        self.lattices = list(lattices)
+        arr = (C.c_void_p * len(self.lattices))(*[L._ctx for L in self.lattices])
+        out = C.c_void_p()
+        check("kofm_batch_create", self.lib.kofm_batch_create(arr, len(self.lattices), C.byref(out)))
+        self._b = out
+
+    def step(self, nsteps: int = 2) -> None:
+        check("kofm_batch_step", self.lib.kofm_batch_step(self._b, nsteps))
+
+    def close(self) -> None:
+        if self._b:
+            self.lib.kofm_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def sweep_channels(n: int = 48, seed: int = 0, u_mean: float = 0.05):
+    """The batched-sweep channels: nx from {512, 1024, 2048, 4096}, ny from
+    {64, 128, 256}, Re log-uniform in [500, 30000] on the opening, a
+    sinusoidal wall of amplitude uniform in [0, 0.15 ny] and wavelength from
+    {128, 256, 512}; laminar below Re = 2000, k-omega above (the rule used
+    here).  Velocity scale u_mean = 0.05; nu = u_mean H / Re."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = int(rng.choice([512, 1024, 2048, 4096]))
+        ny = int(rng.choice([64, 128, 256]))
+        re = float(np.exp(rng.uniform(np.log(500.0), np.log(30000.0))))
+        amp = float(rng.uniform(0.0, 0.15 * ny))
+        lam = int(rng.choice([128, 256, 512]))
+        ch = G.wavy_channel(nx, ny, amp, lam)
+        R = ch.pipe_radius
+        H = 2.0 * R
+        nu = u_mean * H / re
+        komega = re >= 2000.0
+        u_max = 1.5 * u_mean
+        yb, yt = ch.y_bot[None, :], ch.y_top[None, :]
+        y = np.arange(ny)[:, None]
+        ux = np.clip(u_max * 4.0 * (y - yb) * (yt - y) / np.maximum(yt - yb, 1.0) ** 2, 0.0, None)
+        f = G.equilibrium_state(ch, ux=ux)
+        g = G.force_from_re(u_mean * R / nu, nu, R)
+        w = W.Workload(f"sweep{i}_{nx}x{ny}_re{re:.0f}", ch, 1.0 / (3.0 * nu + 0.5), g, nu, komega, f)
+        if komega:
+            k0 = 1.5 * (0.05 * u_max) ** 2
+            o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * H)
+            w.k, w.omega, w.nut = G.komega_fields(ch, k0, o0)
+            w.sxy = np.zeros(3 * ch.n)
+        out.append(w)
+    return out
+
+
+def open_lattices(workloads, storage=_abi.STORE_FP16_NEQ):
+    lats = []
+    for w in workloads:
+        L = Lattice(W.descriptor(w, storage=storage))
+        W.apply(L, w)
+        L.step(1)
+        lats.append(L)
+    return lats
+
+
+def measure(channels: int = 48, steps: int = 20, seed: int = 0, storage=_abi.STORE_FP16_NEQ):
+    ws = sweep_channels(channels, seed)
+    nodes = sum(w.nodes for w in ws)
+    lats = open_lattices(ws, storage)
+    try:
+        # one launch sequence per channel per step (each lattice on its own)
+        for L in lats:
+            L.step(2)
+        for L in lats:
+            L.sync()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for L in lats:
+                L.step(1)
+        for L in lats:
+            L.sync()
+        t_seq = time.perf_counter() - t0
+        with Batch(lats) as B:
+            B.step(2)
+            t0 = time.perf_counter()
+            B.step(steps)
+            t_bat = time.perf_counter() - t0
+    finally:
+        for L in lats:
+            L.close()
+    return {"channels": channels, "komega_channels": sum(w.komega for w in ws), "nodes": nodes,
+            "steps": steps, "unit": "MLUPS",
+            "batched_mlups": nodes * steps / t_bat / 1e6,
+            "one_by_one_mlups": nodes * steps / t_seq / 1e6,
+            "storage": {0: "fp32", 1: "fp16", 2: "bf16", 3: "fp16neq"}[storage],
+            "timing": "host wall clock around the steps, synchronised at both ends"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--channels", type=int, default=48)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args()
+    print(json.dumps(measure(args.channels, args.steps, args.seed)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -782,3 +782,5 @@ int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
 
 // k-omega entry points live in kofm_komega_api.inc (same translation unit).
 #include "kofm_komega_api.inc"
+// batched lattices (CUDA graph over several contexts)
+#include "kofm_batch.inc"

@@ -77,23 +77,37 @@ def _link_fractions(ii, jj, q, nx, y_bot, y_top):
     return np.where(np.isfinite(best), best, 0.5)
 
 
-def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius):
+def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius=None):
     """Distance of every fluid node to the nearest wall polyline (segments
-    between neighbouring columns, periodic in x) within `radius` columns
-    (kOmega::iniWallD / findMinDist, kOmega.cpp:136-193, 330-349)."""
+    between neighbouring columns, periodic in x) -- the quantity of
+    kOmega::iniWallD / findMinDist (kOmega.cpp:136-193, 330-349), computed
+    exactly: a k-d tree over points sampled every 1/4 column along both walls
+    finds the nearest wall sample, and the exact distances to the three
+    segments around it give the result."""
+    from scipy.spatial import cKDTree
     wall = np.zeros((ny, nxf))
     jj, ii = np.nonzero(fluid)
+    if len(jj) == 0:
+        return wall
+    pts = (ii.astype(float), jj.astype(float))
     best = np.full(jj.shape, np.inf)
+    sub = 4
+    margin = min(nx, ny)                                   # periodic wrap in x
+    xs = np.arange(-margin * sub, (nx + margin) * sub) / sub
     for y_w in (y_bot, y_top):
-        for off in range(-radius, radius + 1):
-            xa = ii + off                       # segment from column xa to xa + 1
+        x0 = np.floor(xs).astype(np.int64)
+        t = xs - x0
+        ys = (1 - t) * y_w[x0 % nx] + t * y_w[(x0 + 1) % nx]
+        tree = cKDTree(np.column_stack([xs, ys]))
+        _, idx = tree.query(np.column_stack(pts), workers=-1)
+        seg0 = np.floor(xs[idx]).astype(np.int64)
+        for o in (-1, 0, 1):
+            xa = seg0 + o
             ya = y_w[xa % nx]
             yb = y_w[(xa + 1) % nx]
-            # projection of (ii, jj) onto the segment (xa, ya) - (xa + 1, yb)
-            dx, dy = 1.0, yb - ya
-            t = np.clip(((ii - xa) * dx + (jj - ya) * dy) / (dx * dx + dy * dy), 0.0, 1.0)
-            px, py = xa + t * dx, ya + t * dy
-            best = np.minimum(best, np.hypot(ii - px, jj - py))
+            dy = yb - ya
+            tt = np.clip(((pts[0] - xa) + (pts[1] - ya) * dy) / (1.0 + dy * dy), 0.0, 1.0)
+            best = np.minimum(best, np.hypot(pts[0] - (xa + tt), pts[1] - (ya + tt * dy)))
     wall[jj, ii] = best
     return wall
 
@@ -146,7 +160,7 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
         # straight walls: the nearest wall point is straight above or below
         wall = np.where(fluid, np.minimum(j[:, None] - y_bot[0], y_top[0] - j[:, None]), 0.0)
     else:
-        wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, min(wall_radius, nx // 2))
+        wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top)
     order = np.argsort(ibb_idx, kind="stable")
     return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(), dX.ravel(),
                    wall.ravel(), np.asarray(ibb_idx, np.int32)[order],

@@ -1,0 +1,86 @@
+"""Batched lattices (kofm_batch_*): several channels advanced by one CUDA
+graph per two steps give exactly the results of stepping them one by one, and
+the seeded sweep of uneven channels is reproducible."""
+import numpy as np
+import pytest
+
+from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+from komegafoulingmodel_b200 import geometry as G
+from komegafoulingmodel_b200.batch import Batch, sweep_channels
+from tests.test_komega_gpu import channel_case
+
+
+def test_sweep_is_seeded_and_follows_its_rules():
+    a = sweep_channels(6, seed=3)
+    b = sweep_channels(6, seed=3)
+    for wa, wb in zip(a, b):
+        assert wa.name == wb.name and np.array_equal(wa.f, wb.f)
+        nx, ny = wa.channel.nx, wa.channel.ny
+        assert nx in (512, 1024, 2048, 4096) and ny in (64, 128, 256)
+        re = float(wa.name.split("_re")[1])
+        assert 500 <= re <= 30000 and wa.komega == (re >= 2000)
+
+
+def _cases():
+    out = []
+    ch = G.straight_channel(256, 40)
+    out.append(("laminar", ch, G.equilibrium_state(ch, ux=0.01), None, None, None, 1.25, 1e-6, 0.1))
+    for nx, ny, amp in ((128, 34, 0.0), (256, 66, 8.0)):
+        c, f, k, o, nut, rate, g, nu = channel_case(nx=nx, ny=ny)
+        if amp > 0:
+            c = G.wavy_channel(nx, ny, amp, 128)
+            f = G.equilibrium_state(c, ux=0.02)
+            k, o, nut = G.komega_fields(c, 1.5 * (0.05 * 0.05) ** 2, 0.003)
+        out.append(("komega", c, f, k, o, nut, rate, g, nu))
+    return out
+
+
+def _open(case):
+    kind, ch, f, k, o, nut, rate, g, nu = case
+    d = desc_default()
+    d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
+    d.tau, d.fterm, d.mu = rate, g, nu
+    d.use_komega = 1 if kind == "komega" else 0
+    L = Lattice(d)
+    ko = kind == "komega"
+    L.set_geometry(ch.ntype, ch.wallD if ko else None, ch.dX if ko else None,
+                   ch.ibb_idx if len(ch.ibb_idx) else None, ch.ibb_q if len(ch.ibb_q) else None)
+    L.set_state(f, k, o, nut, np.zeros(3 * ch.n) if ko else None)
+    return L
+
+
+@pytest.mark.gpu
+def test_batch_matches_one_by_one(kofm_lib):
+    cases = _cases()
+    solo = [_open(c) for c in cases]
+    both = [_open(c) for c in cases]
+    try:
+        for L in solo + both:
+            L.step(1)
+        with pytest.raises(_abi.KofmError):
+            Batch([both[0], both[0]])          # the same context twice
+        with Batch(both) as B:
+            B.step(4)
+            with pytest.raises(_abi.KofmError):
+                B.step(3)                      # odd step counts are rejected
+        for L in solo:
+            L.step(4)
+        for a, b in zip(solo, both):
+            sa, sb = a.get_state(), b.get_state()
+            for x, y in zip(sa, sb):
+                if x is not None:
+                    assert np.array_equal(x, y)
+            assert a.stats().steps == b.stats().steps == 5
+    finally:
+        for L in solo + both:
+            L.close()
+
+
+@pytest.mark.gpu
+def test_batch_needs_stepped_contexts(kofm_lib):
+    L = _open(_cases()[0])
+    try:
+        with pytest.raises(_abi.KofmError):
+            Batch([L])                          # populations still in the set_state form
+    finally:
+        L.close()
