@@ -107,6 +107,10 @@ typedef struct kofm_desc {
                                  restart cycle, as GMRESSolver::solve does;
                                  0 (default): end the cycle as soon as its
                                  truncation tests fire (see kofm_komega_solve) */
+    int32_t solver_max_blocks;/* cap on the k-omega solver's grid (0: two
+                                 blocks per SM, fewer on small lattices);
+                                 lattices advanced together (kofm_batch_*)
+                                 may share the GPU better with a cap */
 } kofm_desc;
 
 /* Per-context counters of the last k-omega update (kOmega::Solve). */

@@ -45,6 +45,7 @@ class KofmDesc(C.Structure):
         ("komega_rel_tol", C.c_double), ("komega_abs_tol", C.c_double),
         ("komega_dt", C.c_double),
         ("komega_full_cycle", C.c_int32),
+        ("solver_max_blocks", C.c_int32),
     ]
 
 

@@ -5,7 +5,9 @@
 
 prints one JSON line with the aggregate throughput of the sweep advanced as a
 batch (one graph launch per two steps, the lattices' kernels running
-concurrently) and of the same channels stepped one launch sequence each.
+concurrently) and of the same channels stepped one launch sequence each.  The
+batch's solver grid sizes come from `autotune`, which times a few batched
+steps under each sizing policy and keeps the fastest.
 """
 from __future__ import annotations
 
@@ -84,20 +86,65 @@ def sweep_channels(n: int = 48, seed: int = 0, u_mean: float = 0.05):
     return out
 
 
-def open_lattices(workloads, storage=_abi.STORE_FP16_NEQ):
+def open_lattices(workloads, storage=_abi.STORE_FP16_NEQ, caps=None):
     lats = []
-    for w in workloads:
-        L = Lattice(W.descriptor(w, storage=storage))
+    for i, w in enumerate(workloads):
+        d = W.descriptor(w, storage=storage)
+        if caps is not None:
+            d.solver_max_blocks = int(caps[i])
+        L = Lattice(d)
         W.apply(L, w)
         L.step(1)
         lats.append(L)
     return lats
 
 
-def measure(channels: int = 48, steps: int = 20, seed: int = 0, storage=_abi.STORE_FP16_NEQ):
+def solver_caps(workloads, policy, sms: int):
+    """Per-lattice caps on the solver grid for one tuning policy:
+    "auto" -- none (each solver may take two blocks per SM);
+    "share" -- two blocks per SM split over the k-omega lattices in proportion
+    to their node counts (at least 8 each), so concurrent solvers fit side by
+    side; an integer -- that cap for every lattice."""
+    if policy == "auto":
+        return [0] * len(workloads)
+    if policy == "share":
+        tot = sum(w.nodes for w in workloads if w.komega) or 1
+        return [max(8, int(2 * sms * w.nodes / tot)) if w.komega else 0 for w in workloads]
+    return [int(policy)] * len(workloads)
+
+
+def autotune(workloads, policies=("auto", "share", 148, 74), steps: int = 4,
+             storage=_abi.STORE_FP16_NEQ):
+    """Times `steps` batched steps per policy and returns (best, {policy: MLUPS})."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    nodes = sum(w.nodes for w in workloads)
+    res = {}
+    for pol in policies:
+        lats = open_lattices(workloads, storage, solver_caps(workloads, pol, sms))
+        try:
+            with Batch(lats) as B:
+                B.step(2)
+                t0 = time.perf_counter()
+                B.step(steps)
+                res[str(pol)] = nodes * steps / (time.perf_counter() - t0) / 1e6
+        finally:
+            for L in lats:
+                L.close()
+    best = max(res, key=res.get)
+    pol = next(p for p in policies if str(p) == best)
+    return pol, res
+
+
+def measure(channels: int = 48, steps: int = 20, seed: int = 0, storage=_abi.STORE_FP16_NEQ,
+            tune: bool = True):
+    import torch
     ws = sweep_channels(channels, seed)
     nodes = sum(w.nodes for w in ws)
+    tuned, table = autotune(ws, storage=storage) if tune else ("auto", {})
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
     lats = open_lattices(ws, storage)
+    lats_b = open_lattices(ws, storage, solver_caps(ws, tuned, sms))
     try:
         # one launch sequence per channel per step (each lattice on its own)
         for L in lats:
@@ -111,19 +158,20 @@ def measure(channels: int = 48, steps: int = 20, seed: int = 0, storage=_abi.STO
         for L in lats:
             L.sync()
         t_seq = time.perf_counter() - t0
-        with Batch(lats) as B:
+        with Batch(lats_b) as B:
             B.step(2)
             t0 = time.perf_counter()
             B.step(steps)
             t_bat = time.perf_counter() - t0
     finally:
-        for L in lats:
+        for L in lats + lats_b:
             L.close()
     return {"channels": channels, "komega_channels": sum(w.komega for w in ws), "nodes": nodes,
             "steps": steps, "unit": "MLUPS",
             "batched_mlups": nodes * steps / t_bat / 1e6,
             "one_by_one_mlups": nodes * steps / t_seq / 1e6,
             "storage": {0: "fp32", 1: "fp16", 2: "bf16", 3: "fp16neq"}[storage],
+            "solver_grid_policy": str(tuned), "autotune_mlups": table,
             "timing": "host wall clock around the steps, synchronised at both ends"}
 
 
@@ -132,8 +180,9 @@ def main():
     ap.add_argument("--channels", type=int, default=48)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
-    print(json.dumps(measure(args.channels, args.steps, args.seed)), flush=True)
+    print(json.dumps(measure(args.channels, args.steps, args.seed, tune=not args.no_tune)), flush=True)
 
 
 if __name__ == "__main__":

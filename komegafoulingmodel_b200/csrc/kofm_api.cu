@@ -20,7 +20,7 @@ using namespace kofm;
 
 namespace kofm {
 int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned int** bar,
-                    int* nblocks, int P, int ny, int K, int dev);
+                    int* nblocks, int P, int ny, int K, int dev, int max_blocks);
 void ko_system_free(KoSystem* s);
 }  // namespace kofm
 
@@ -334,6 +334,7 @@ int validate_desc(const kofm_desc* d) {
     if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
+    if (d->solver_max_blocks < 0) return KOFM_ERR_LOADING_PARAMS;
     return KOFM_OK;
 }
 
@@ -461,7 +462,7 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         ALLOC(c->S, 3 * D);
         ALLOC(c->nut, D);
         int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks,
-                                 c->P, d->ny, d->krylov_dim, c->dev);
+                                 c->P, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
         if (s2) { kofm_destroy(c); return s2; }
         if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {
             kofm_destroy(c);
