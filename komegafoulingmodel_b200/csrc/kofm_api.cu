@@ -20,7 +20,7 @@ using namespace kofm;
 
 namespace kofm {
 int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned int** bar,
-                    int* nblocks, int* part_cols, int P, int ny, int K, int dev, int max_blocks);
+                    int* nblocks, int P, int ny, int K, int dev, int max_blocks);
 void ko_system_free(KoSystem* s);
 }  // namespace kofm
 
@@ -80,7 +80,6 @@ struct kofm_ctx {
     double* gpart = nullptr;          // solver partial sums
     unsigned int* bar = nullptr;      // grid barrier words
     int solver_blocks = 0;
-    int solver_part_cols = 0;         // columns of the solver's partial-sum array
     int steps_per_lb = 1;
     int time_since_change = 0;
     double dt = 1.0;
@@ -462,7 +461,7 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         ALLOC(c->O, D);
         ALLOC(c->S, 3 * D);
         ALLOC(c->nut, D);
-        int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks, &c->solver_part_cols,
+        int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks,
                                  c->P, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
         if (s2) { kofm_destroy(c); return s2; }
         if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {

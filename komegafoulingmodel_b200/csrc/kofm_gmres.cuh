@@ -44,16 +44,6 @@ constexpr int GM_THREADS = 256;
 #endif
 constexpr int GM_SLOTS = 32;                    // partial-sum slots per block
 constexpr int GM_SYS_SLOTS = 16;                // per system
-constexpr long long GM_CHUNK_ROWS = 16;         // rows of a dynamically handed-out chunk
-
-// Split of a Krylov sweep over `nb` blocks: 90% of the (group, row) sequence
-// statically, the rest in chunks of GM_CHUNK_ROWS; returns the number of
-// partial-sum columns (blocks + chunks).  Host and device use the same rule.
-__host__ __device__ inline long long gm_static_rows(long long total, int nb) { return total * 9 / (10LL * nb); }
-__host__ __device__ inline int gm_krylov_cols(long long total, int nb) {
-    const long long tail = total - gm_static_rows(total, nb) * nb;
-    return nb + (int)((tail + GM_CHUNK_ROWS - 1) / GM_CHUNK_ROWS);
-}
 
 struct GmresSys {
     int active;     // still iterating this restart
@@ -82,7 +72,6 @@ struct GmresControl {
     int passes;       // grid sweeps performed
     int any_active;
     int pad;
-    int work_next[2]; // next dynamic chunk of a Krylov sweep, per system (reset at each barrier)
 };
 
 struct GridBarrier {
@@ -95,10 +84,7 @@ struct GmresArgs {
     float* field[2];          // omega, k (FP32 fields, updated in place)
     const int16_t* ntype;
     GmresControl* ctl;
-    double* part;             // [GM_SLOTS][part_cols] (slot-major): one column per
-                              // block (residual) or per chunk of a Krylov sweep
-    int part_cols;            // allocated columns
-    int krylov_cols;          // columns of a Krylov sweep: blocks + dynamic chunks
+    double* part;             // [GM_SLOTS][gridDim.x] (slot-major)
     GridBarrier* bar;
     int nx, ny, P;
     long long D;
@@ -136,10 +122,9 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     return v;
 }
 
-// ---- block reduction of NS slots into part[base + s][col] (row stride `stride`)
+// ---- block reduction of NS slots into part[base + s][blockIdx.x] ------------
 template <int NS>
-__device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused, double* part, int base,
-                                                   int col, int stride) {
+__device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused, double* part, int base) {
     __shared__ double red[GM_THREADS / 32][GM_SYS_SLOTS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -156,18 +141,18 @@ __device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused,
         double v = 0.0;
 #pragma unroll
         for (int w = 0; w < GM_THREADS / 32; ++w) v += red[w][threadIdx.x];
-        part[(long long)(base + threadIdx.x) * stride + col] = v;
+        part[(long long)(base + threadIdx.x) * gridDim.x + blockIdx.x] = v;
     }
     __syncthreads();
 }
 
 // Sum slot `slot` of all blocks in a fixed order (deterministic); one warp,
 // lane l adding blocks l, l + 32, ... (coalesced: slot-major partials).
-__device__ __forceinline__ double sum_slot_warp(const double* part, int ncols, int stride, int slot) {
+__device__ __forceinline__ double sum_slot_warp(const double* part, int nblocks, int slot) {
     const int lane = threadIdx.x & 31;
     double v = 0.0;
-    const double* ps = part + (long long)slot * stride;
-    for (int b = lane; b < ncols; b += 32) v += __ldcg(ps + b);
+    const double* ps = part + (long long)slot * nblocks;
+    for (int b = lane; b < nblocks; b += 32) v += __ldcg(ps + b);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     return __shfl_sync(0xffffffffu, v, 0);
@@ -238,7 +223,7 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
     __shared__ int s_any;
     const int warp = threadIdx.x >> 5, nwarps = GM_THREADS / 32;
     for (int slot = warp; slot < GM_SLOTS; slot += nwarps) {
-        const double v = sum_slot_warp(a.part, nblocks, a.part_cols, slot);
+        const double v = sum_slot_warp(a.part, nblocks, slot);
         if ((threadIdx.x & 31) == 0) tot[slot] = v;
     }
     if (threadIdx.x == 0) s_any = 0;
@@ -322,13 +307,10 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
     __syncthreads();
     if (s_last) {
         __threadfence();
-        if (kind != SER_NONE)
-            serial_section(a, kind, kcur, restart, kind == SER_KRYLOV ? a.krylov_cols : nblocks);
+        if (kind != SER_NONE) serial_section(a, kind, kcur, restart, nblocks);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
-            a.ctl->work_next[0] = 0;
-            a.ctl->work_next[1] = 0;
             atomicExch(&a.bar->count, 0u);
             __threadfence();
             atomicAdd(&a.bar->gen, 1u);
@@ -619,7 +601,6 @@ gmres_kernel(const GmresArgs a) {
     const int wib = threadIdx.x >> 5;  // warp in block
     __shared__ double sh_c[2][KOFM_MAX_KRYLOV];
     __shared__ int sh_act[2];
-    __shared__ int sh_chunk;
     const long long npairs = a.D / 2;
     const long long stride = (long long)gridDim.x * GM_THREADS;
     const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
@@ -672,7 +653,7 @@ gmres_kernel(const GmresArgs a) {
                     }
                 }
             }
-            block_reduce_slots<1>(acc, sh_act[s] ? 1 : 0, a.part, GM_SYS_SLOTS * s, blockIdx.x, a.part_cols);
+            block_reduce_slots<1>(acc, sh_act[s] ? 1 : 0, a.part, GM_SYS_SLOTS * s);
         }
         if (!grid_sync(a, SER_RESIDUAL, 0, restart)) return;
         if (!ldc(&ctl->any_active)) break;
@@ -700,55 +681,31 @@ gmres_kernel(const GmresArgs a) {
                         // sequence, a group being GM_WARPS adjacent strips; its
                         // warps march the same rows of neighbouring strips side
                         // by side, so their ghost-column reads hit L1 / L2.
-                        // 90% of the rows are split statically; the rest is
-                        // handed out in chunks of 16 rows to whichever block
-                        // asks first, which evens out the blocks' finishing
-                        // times (they vary by ~10% with the memory system).
                         const int groups = (a.strips + GM_WARPS - 1) / GM_WARPS;
                         const long long total = (long long)groups * a.ny;
-                        const long long stat = gm_static_rows(total, gridDim.x);
-                        const long long tail0 = stat * gridDim.x;
-                        auto run = [&](long long f, long long f1) {
-                            while (f < f1) {
-                                const int grp = (int)(f / a.ny), ya = (int)(f - (long long)grp * a.ny);
-                                const int yb = (int)min((long long)a.ny, (long long)ya + (f1 - f));
-                                const int strip = grp * GM_WARPS + wib;
-                                if (strip < a.strips) {
-                                    switch (k) {
+                        long long f = total * blockIdx.x / gridDim.x;
+                        const long long f1 = total * (blockIdx.x + 1) / gridDim.x;
+                        while (f < f1) {
+                            const int grp = (int)(f / a.ny), ya = (int)(f - (long long)grp * a.ny);
+                            const int yb = (int)min((long long)a.ny, (long long)ya + (f1 - f));
+                            const int strip = grp * GM_WARPS + wib;
+                            if (strip < a.strips) {
+                                switch (k) {
 #define KOFM_KSTRIP(n) \
     case n: krylov_strip<n>(a, S, rsrc, strip * 32, ya, yb, T, ring, acc); break;
-                                        KOFM_KSTRIP(0) KOFM_KSTRIP(1) KOFM_KSTRIP(2) KOFM_KSTRIP(3)
-                                        KOFM_KSTRIP(4) KOFM_KSTRIP(5) KOFM_KSTRIP(6) KOFM_KSTRIP(7)
-                                        KOFM_KSTRIP(8) KOFM_KSTRIP(9)
+                                    KOFM_KSTRIP(0) KOFM_KSTRIP(1) KOFM_KSTRIP(2) KOFM_KSTRIP(3)
+                                    KOFM_KSTRIP(4) KOFM_KSTRIP(5) KOFM_KSTRIP(6) KOFM_KSTRIP(7)
+                                    KOFM_KSTRIP(8) KOFM_KSTRIP(9)
 #undef KOFM_KSTRIP
-                                        default: break;
-                                    }
+                                    default: break;
                                 }
-                                f += yb - ya;
                             }
-                        };
-                        // each piece's dot products go to a column of its own, so the
-                        // sums do not depend on which block took which chunk
-                        auto flush = [&](int col) {
-                            block_reduce_slots<2 + KOFM_MAX_KRYLOV>(acc, nslots, a.part, GM_SYS_SLOTS * s,
-                                                                    col, a.part_cols);
-#pragma unroll
-                            for (int j = 0; j < 2 + KOFM_MAX_KRYLOV; ++j) acc[j] = 0.0;
-                        };
-                        run(stat * blockIdx.x, stat * (blockIdx.x + 1));
-                        flush(blockIdx.x);
-                        for (;;) {
-                            if (threadIdx.x == 0) sh_chunk = atomicAdd(&ctl->work_next[s], 1);
-                            __syncthreads();
-                            const int chunk = sh_chunk;
-                            const long long f0 = tail0 + (long long)chunk * GM_CHUNK_ROWS;
-                            __syncthreads();  // sh_chunk is read before the next grab
-                            if (f0 >= total) break;
-                            run(f0, min(total, f0 + GM_CHUNK_ROWS));
-                            flush(gridDim.x + chunk);
+                            f += yb - ya;
                         }
                     }
                 }
+                block_reduce_slots<2 + KOFM_MAX_KRYLOV>(acc, sh_act[s] ? nslots : 0, a.part,
+                                                        GM_SYS_SLOTS * s);
             }
             if (!grid_sync(a, SER_KRYLOV, k, restart)) return;
         }
