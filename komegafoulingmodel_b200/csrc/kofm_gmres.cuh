@@ -150,9 +150,19 @@ __device__ __forceinline__ void block_reduce_slots(double (&acc)[NS], int nused,
 // lane l adding blocks l, l + 32, ... (coalesced: slot-major partials).
 __device__ __forceinline__ double sum_slot_warp(const double* part, int nblocks, int slot) {
     const int lane = threadIdx.x & 31;
-    double v = 0.0;
     const double* ps = part + (long long)slot * nblocks;
-    for (int b = lane; b < nblocks; b += 32) v += __ldcg(ps + b);
+    // four independent partial sums per lane (loads in flight together),
+    // combined in a fixed order
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    int b = lane;
+    for (; b + 96 < nblocks; b += 128) {
+        v0 += __ldcg(ps + b);
+        v1 += __ldcg(ps + b + 32);
+        v2 += __ldcg(ps + b + 64);
+        v3 += __ldcg(ps + b + 96);
+    }
+    for (; b < nblocks; b += 32) v0 += __ldcg(ps + b);
+    double v = (v0 + v1) + (v2 + v3);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     return __shfl_sync(0xffffffffu, v, 0);
@@ -222,7 +232,11 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
     __shared__ GmresSys sS;
     __shared__ int s_any;
     const int warp = threadIdx.x >> 5, nwarps = GM_THREADS / 32;
-    for (int slot = warp; slot < GM_SLOTS; slot += nwarps) {
+    // only the slots this pass filled: 1 per system after a residual sweep,
+    // 3 + k (2 for the last vector of a cycle) after Krylov sweep k
+    const int used = kind == SER_RESIDUAL ? 1 : (kcur < a.K - 1 ? 3 + kcur : 2);
+    for (int i = warp; i < 2 * used; i += nwarps) {
+        const int slot = (i < used ? 0 : GM_SYS_SLOTS) + (i < used ? i : i - used);
         const double v = sum_slot_warp(a.part, nblocks, slot);
         if ((threadIdx.x & 31) == 0) tot[slot] = v;
     }
