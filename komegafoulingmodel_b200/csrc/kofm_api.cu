@@ -4,7 +4,6 @@
 // host arrays in the reference's padded FP64 layout cross the boundary only in
 // kofm_set_* / kofm_get_*.  All work is enqueued on the context's stream.
 #include "kofm.h"
-#include <type_traits>
 #include "kofm_common.cuh"
 #include "kofm_lb.cuh"
 #include "kofm_komega.cuh"
@@ -64,6 +63,8 @@ struct kofm_ctx {
     float* rho = nullptr;
     float* ux = nullptr;
     float* uy = nullptr;
+    double* lb_partials = nullptr;
+    long long n_lb_partials = 0;
     double* red_partials = nullptr;   // RED_BLOCKS
     double* red_out = nullptr;        // 1
     double* h_red = nullptr;          // pinned, 64 doubles
@@ -313,18 +314,6 @@ __global__ void k_wall_shear(const int16_t* __restrict__ nt, const float* __rest
 // ---- LB step dispatch ------------------------------------------------------------
 template <typename ST, typename AT, bool NEQ = false>
 cudaError_t launch_lb(kofm_ctx* c, const LbParams& p, bool komega, bool phase0) {
-    if (std::is_same<ST, float>::value && !NEQ && !phase0) {
-        // persistent row-marching form: two blocks of 4 warps per SM, each
-        // warp at least ~16 rows
-        const long long rows = (long long)(c->P / 128) * c->desc.ny;
-        long long nb = (rows + 16 * LB_WARPS - 1) / (16 * LB_WARPS);
-        if (nb > 2LL * c->num_sms) nb = 2LL * c->num_sms;
-        if (komega)
-            lb_step_ring_kernel<true><<<(int)nb, 32 * LB_WARPS, sizeof(LbSmem), c->stream>>>(p);
-        else
-            lb_step_ring_kernel<false><<<(int)nb, 32 * LB_WARPS, sizeof(LbSmem), c->stream>>>(p);
-        return cudaGetLastError();
-    }
     dim3 block(32, 4);
     dim3 grid(c->P / 128, (c->desc.ny + 3) / 4);
     if (komega) {
@@ -403,7 +392,7 @@ int kofm_destroy(kofm_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
-                    c->red_partials, c->red_out, c->staging, c->ctl,
+                    c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
                     c->gpart, c->bar};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -462,6 +451,8 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
     ALLOC(c->rho, D);
     ALLOC(c->ux, D);
     ALLOC(c->uy, D);
+    c->n_lb_partials = (long long)(c->P / 128) * ((d->ny + 3) / 4) * 4 * 3;
+    ALLOC(c->lb_partials, c->n_lb_partials);
     ALLOC(c->red_partials, RED_BLOCKS);
     ALLOC(c->red_out, 8);
     if (d->use_komega) {
@@ -482,13 +473,6 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
     if (cudaMallocHost(&c->h_red, 64 * sizeof(double)) != cudaSuccess) {
         kofm_destroy(c);
         return KOFM_ERR_BUFFER_ALLOCATION;
-    }
-    if (cudaFuncSetAttribute(lb_step_ring_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(LbSmem)) != cudaSuccess ||
-        cudaFuncSetAttribute(lb_step_ring_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(LbSmem)) != cudaSuccess) {
-        kofm_destroy(c);
-        return KOFM_ERR_INITIALIZING_VLB;
     }
     // rec / dxrec_idx default to -1 (no record)
     cudaMemset(c->rec, 0xff, D * sizeof(int32_t));
@@ -710,6 +694,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
     p.wallD = c->wallD;
     p.K = c->K; p.O = c->O; p.S = c->S; p.nut = c->nut;
     p.rho = c->rho; p.ux = c->ux; p.uy = c->uy;
+    p.partials = c->lb_partials;
     p.ref_in = c->ref[c->cur];
     p.ref_out = c->ref[c->cur ^ 1];
     p.nx = d.nx; p.ny = d.ny; p.P = c->P; p.D = c->D;

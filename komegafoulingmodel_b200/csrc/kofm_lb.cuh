@@ -33,7 +33,6 @@
 // FP32-stored deviations keep their relative precision.
 #pragma once
 #include "kofm_common.cuh"
-#include <cstddef>
 
 #ifndef KOFM_LB_MINBLOCKS
 #define KOFM_LB_MINBLOCKS 1  // resident 128-thread blocks per SM the register budget targets
@@ -55,6 +54,7 @@ struct LbParams {
     float* rho;
     float* ux;
     float* uy;
+    double* partials;       // per block: sum rho, sum ux, sum uy (FP64)
     const float* ref_in;    // non-equilibrium form: reference rho, ux, uy of
     float* ref_out;         //   the populations read / written (3 planes)
     int nx, ny, P;
@@ -108,30 +108,22 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 }
 
 // ---------------------------------------------------------------------------
-// Inputs of one output row for one warp (128 nodes) staged by the
-// persistent kernel: plane q as pulled from row y - c_y(q) (the warp's 128
-// columns plus the two columns across its edges), and the node fields.
-struct LbSlot {                // 16-byte copies first, then 8- and 4-byte ones
-    float pop[9][128];
-    float K[128], O[128], W[128], S[3][128];
-    short nt[128];
-    float edge[9][2];          // source columns x0 - 1 and x0 + 128 (periodic)
-    float pad[2];
-};
-static_assert(sizeof(LbSlot) % 16 == 0, "ring slots must keep 16-byte alignment");
-static_assert(offsetof(LbSlot, K) % 16 == 0 && offsetof(LbSlot, nt) % 16 == 0, "slot layout");
-constexpr int LB_RING = 3;     // slots per warp: two rows in flight
-constexpr int LB_WARPS = 4;    // warps per block of the persistent kernel
-struct LbSmem {
-    LbSlot ring[LB_WARPS][LB_RING];
-};
-
-// One row segment of 128 nodes (4 per lane) of one step.
 // NEQ: populations stored as f - feq(reference moments of the writing node),
-// FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.  RING: the row's inputs are in
-// the shared-memory slot R (persistent kernel), else read from global memory.
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ, bool RING>
-__device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lane, const LbSlot* R) {
+// FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false>
+__global__ void __launch_bounds__(128, KOFM_LB_MINBLOCKS)
+lb_step_kernel(const LbParams p) {
+    const int lane = threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    // Each warp owns one partial-sum slot; warps that leave early clear it.
+    double* slot = nullptr;
+    if (p.partials && (p.options & OPTION_SAVE_MACRO_FIELDS))
+        slot = p.partials + (((long long)blockIdx.y * gridDim.x + blockIdx.x) * 4 + threadIdx.y) * 3;
+    if (y >= p.ny) {  // warp-uniform
+        if (slot && lane == 0) { slot[0] = 0.0; slot[1] = 0.0; slot[2] = 0.0; }
+        return;
+    }
+    const int x0 = (blockIdx.x * 32 + lane) * 4;
     const ST* gin = static_cast<const ST*>(p.gin);
     ST* gout = static_cast<ST*>(p.gout);
     const long long rowoff = (long long)y * p.P;
@@ -140,15 +132,17 @@ __device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lan
     int type[4];
     bool fl[4];
     {
-        const short4 t4 = RING ? *reinterpret_cast<const short4*>(&R->nt[4 * lane])
-                               : *reinterpret_cast<const short4*>(p.ntype + rowoff + x0);
+        const short4 t4 = *reinterpret_cast<const short4*>(p.ntype + rowoff + x0);
         type[0] = (uint16_t)t4.x; type[1] = (uint16_t)t4.y;
         type[2] = (uint16_t)t4.z; type[3] = (uint16_t)t4.w;
 #pragma unroll
         for (int j = 0; j < 4; ++j) fl[j] = (x0 + j < p.nx) && !(type[j] & M_SOLID);
     }
     const bool any_fluid = fl[0] | fl[1] | fl[2] | fl[3];
-    if (!__any_sync(0xffffffffu, any_fluid)) return;  // whole warp solid
+    if (!__any_sync(0xffffffffu, any_fluid)) {  // whole warp solid
+        if (slot && lane == 0) { slot[0] = 0.0; slot[1] = 0.0; slot[2] = 0.0; }
+        return;
+    }
 
     AT d[9][4];
     float own_r[4] = {}, own_u[4] = {}, own_v[4] = {};  // NEQ: this node's reference moments
@@ -170,26 +164,21 @@ __device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lan
             ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);  // only solid rows clamp
             const ST* src = gin + q * D + (long long)ys * p.P;
             float c[4];
-            if (RING) {
-                const float4 c4 = *reinterpret_cast<const float4*>(&R->pop[q][4 * lane]);
-                c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
-            } else {
-                Store<ST>::load4(src + x0, c);
-            }
+            Store<ST>::load4(src + x0, c);
             if (cx == 0) {
                 v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = c[3];
             } else if (cx == 1) {
                 float left = __shfl_up_sync(0xffffffffu, c[3], 1);
                 if (lane == 0) {
                     const int xs = x0 > 0 ? x0 - 1 : p.nx - 1;
-                    left = RING ? R->edge[q][0] : ld1(src, xs);
+                    left = ld1(src, xs);
                 }
                 v[0] = left; v[1] = c[0]; v[2] = c[1]; v[3] = c[2];
             } else {
                 float right = __shfl_down_sync(0xffffffffu, c[0], 1);
                 if (lane == 31) {
                     const int xs = (x0 + 4 < p.nx) ? x0 + 4 : 0;
-                    right = RING ? R->edge[q][1] : ld1(src, xs);
+                    right = ld1(src, xs);
                 }
                 v[0] = c[1]; v[1] = c[2]; v[2] = c[3]; v[3] = right;
                 const int jw = p.nx - 1 - x0;  // node nx-1 wraps to x = 0
@@ -257,22 +246,19 @@ __device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lan
     float o_rho[4], o_ux[4], o_uy[4], o_nut[4], o_s[3][4];
     float kin[4], oin[4], win[4], sin3[3][4];
     if (KOMEGA) {
-        const float4 k4 = RING ? *reinterpret_cast<const float4*>(&R->K[4 * lane])
-                               : *reinterpret_cast<const float4*>(p.K + rowoff + x0);
-        const float4 o4 = RING ? *reinterpret_cast<const float4*>(&R->O[4 * lane])
-                               : *reinterpret_cast<const float4*>(p.O + rowoff + x0);
-        const float4 w4 = RING ? *reinterpret_cast<const float4*>(&R->W[4 * lane])
-                               : __ldg(reinterpret_cast<const float4*>(p.wallD + rowoff + x0));
+        const float4 k4 = *reinterpret_cast<const float4*>(p.K + rowoff + x0);
+        const float4 o4 = *reinterpret_cast<const float4*>(p.O + rowoff + x0);
+        const float4 w4 = __ldg(reinterpret_cast<const float4*>(p.wallD + rowoff + x0));
         kin[0] = k4.x; kin[1] = k4.y; kin[2] = k4.z; kin[3] = k4.w;
         oin[0] = o4.x; oin[1] = o4.y; oin[2] = o4.z; oin[3] = o4.w;
         win[0] = w4.x; win[1] = w4.y; win[2] = w4.z; win[3] = w4.w;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float4 s4 = RING ? *reinterpret_cast<const float4*>(&R->S[c][4 * lane])
-                                   : *reinterpret_cast<const float4*>(p.S + c * D + rowoff + x0);
+            const float4 s4 = *reinterpret_cast<const float4*>(p.S + c * D + rowoff + x0);
             sin3[c][0] = s4.x; sin3[c][1] = s4.y; sin3[c][2] = s4.z; sin3[c][3] = s4.w;
         }
     }
+    double bsum_rho = 0.0, bsum_ux = 0.0, bsum_uy = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (!fl[j]) {
@@ -340,6 +326,9 @@ __device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lan
         o_rho[j] = (float)rho;
         o_ux[j] = (float)(ux + fterm / AT(2));
         o_uy[j] = (float)uy;
+        bsum_rho += (double)rho;
+        bsum_ux += (double)(ux + fterm / AT(2));
+        bsum_uy += (double)uy;
     }
 
     // ---- stores -----------------------------------------------------------------
@@ -373,98 +362,16 @@ __device__ __forceinline__ void lb_row(const LbParams& p, int y, int x0, int lan
             *reinterpret_cast<float4*>(p.S + c * D + rowoff + x0) =
                 make_float4(o_s[c][0], o_s[c][1], o_s[c][2], o_s[c][3]);
     }
-}
 
-// One launch per step: a warp per 128-node row segment (blocks of 32 x 4).
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false>
-__global__ void __launch_bounds__(128, KOFM_LB_MINBLOCKS)
-lb_step_kernel(const LbParams p) {
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (y >= p.ny) return;  // warp-uniform
-    const int lane = threadIdx.x;
-    lb_row<ST, AT, KOMEGA, PHASE0, NEQ, false>(p, y, (blockIdx.x * 32 + lane) * 4, lane, nullptr);
-}
-
-__device__ __forceinline__ void lb_cp16(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void lb_cp8(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void lb_cp4(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-
-// Copies of everything row y of strip x0s needs into slot R (each lane its
-// own 4 nodes; lanes 0 / 31 the columns across the strip's edges).
-template <bool KOMEGA>
-__device__ __forceinline__ void lb_issue(const LbParams& p, int y, int x0s, int lane, LbSlot& R) {
-    const float* gin = static_cast<const float*>(p.gin);
-    const long long D = p.D;
-    const int x = x0s + 4 * lane;
+    // ---- per-block FP64 partial sums of rho, ux, uy ----------------------------
+    if (slot) {
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const int cx = cx_of(q), cy = cy_of(q);
-        int ys = y - cy;
-        ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);
-        const float* row = gin + q * D + (long long)ys * p.P;
-        lb_cp16(&R.pop[q][4 * lane], row + x);
-        if (cx == 1 && lane == 0) lb_cp4(&R.edge[q][0], row + (x0s > 0 ? x0s - 1 : p.nx - 1));
-        if (cx == -1 && lane == 31) lb_cp4(&R.edge[q][1], row + (x0s + 128 < p.nx ? x0s + 128 : 0));
-    }
-    const long long g = (long long)y * p.P + x;
-    lb_cp8(&R.nt[4 * lane], p.ntype + g);
-    if (KOMEGA) {
-        lb_cp16(&R.K[4 * lane], p.K + g);
-        lb_cp16(&R.O[4 * lane], p.O + g);
-        lb_cp16(&R.W[4 * lane], p.wallD + g);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) lb_cp16(&R.S[c][4 * lane], p.S + c * D + g);
-    }
-}
-
-// Persistent form of the FP32-deviation step (after the first step): each
-// warp marches down its share of the (128-column strip, row) sequence and
-// streams the inputs of the row two ahead into a 3-slot shared-memory ring
-// while it collides the current one, so a warp's loads overlap its own FP64
-// collision work (the one-launch form loads, then computes, in lock-step
-// across the warps of an SM).
-template <bool KOMEGA>
-__global__ void __launch_bounds__(32 * LB_WARPS, 2)
-lb_step_ring_kernel(const LbParams p) {
-    extern __shared__ __align__(16) unsigned char lb_smem[];
-    LbSmem& M = *reinterpret_cast<LbSmem*>(lb_smem);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    LbSlot* ring = M.ring[w];
-    const int strips = p.P / 128;
-    const long long total = (long long)strips * p.ny;
-    const long long nw = (long long)gridDim.x * LB_WARPS;
-    const long long gw = (long long)blockIdx.x * LB_WARPS + w;
-    long long f = total * gw / nw;
-    const long long f1 = total * (gw + 1) / nw;
-    while (f < f1) {
-        const int strip = (int)(f / p.ny), ya = (int)(f - (long long)strip * p.ny);
-        const int yb = (int)min((long long)p.ny, (long long)ya + (f1 - f));
-        const int x0s = strip * 128;
-#pragma unroll
-        for (int i = 0; i < LB_RING - 1; ++i) {
-            if (ya + i < yb) lb_issue<KOMEGA>(p, ya + i, x0s, lane, ring[(ya + i) % LB_RING]);
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        for (int off = 16; off > 0; off >>= 1) {
+            bsum_rho += __shfl_down_sync(0xffffffffu, bsum_rho, off);
+            bsum_ux += __shfl_down_sync(0xffffffffu, bsum_ux, off);
+            bsum_uy += __shfl_down_sync(0xffffffffu, bsum_uy, off);
         }
-        for (int y = ya; y < yb; ++y) {
-            if (y + LB_RING - 1 < yb)
-                lb_issue<KOMEGA>(p, y + LB_RING - 1, x0s, lane, ring[(y + LB_RING - 1) % LB_RING]);
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(LB_RING - 1) : "memory");
-            __syncwarp();  // the edge columns were copied by lanes 0 and 31
-            lb_row<float, double, KOMEGA, false, false, true>(p, y, x0s + 4 * lane, lane, &ring[y % LB_RING]);
-            __syncwarp();  // every lane is done with the slot before it is refilled
-        }
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        f += yb - ya;
+        if (lane == 0) { slot[0] = bsum_rho; slot[1] = bsum_ux; slot[2] = bsum_uy; }
     }
 }
 
