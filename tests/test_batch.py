@@ -35,9 +35,10 @@ def _cases():
     return out
 
 
-def _open(case):
+def _open(case, storage=_abi.STORE_FP32):
     kind, ch, f, k, o, nut, rate, g, nu = case
     d = desc_default()
+    d.storage = storage
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = rate, g, nu
     d.use_komega = 1 if kind == "komega" else 0
@@ -50,10 +51,11 @@ def _open(case):
 
 
 @pytest.mark.gpu
-def test_batch_matches_one_by_one(kofm_lib):
+@pytest.mark.parametrize("storage", [_abi.STORE_FP32, _abi.STORE_FP16_NEQ])
+def test_batch_matches_one_by_one(kofm_lib, storage):
     cases = _cases()
-    solo = [_open(c) for c in cases]
-    both = [_open(c) for c in cases]
+    solo = [_open(c, storage) for c in cases]
+    both = [_open(c, storage) for c in cases]
     try:
         for L in solo + both:
             L.step(1)

@@ -43,11 +43,12 @@ def test_wavy_geometry_invariants():
     assert not np.any(seam & (q > 0.5))
 
 
-def _lattice(ch, rate, g, mu, komega):
+def _lattice(ch, rate, g, mu, komega, storage=_abi.STORE_FP32):
     d = desc_default()
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = rate, g, mu
     d.use_komega = 1 if komega else 0
+    d.storage = storage
     L = Lattice(d)
     L.set_geometry(ch.ntype, ch.wallD if komega else None, ch.dX if komega else None,
                    ch.ibb_idx, ch.ibb_q)
@@ -55,7 +56,11 @@ def _lattice(ch, rate, g, mu, komega):
 
 
 @pytest.mark.gpu
-def test_wavy_laminar_matches_oracle(kofm_lib, oracle):
+@pytest.mark.parametrize("storage,tol", [(_abi.STORE_FP32, 1e-5), (_abi.STORE_FP16_NEQ, 1e-4)])
+def test_wavy_laminar_matches_oracle(kofm_lib, oracle, storage, tol):
+    """Interpolated bounce-back with q from 0.03 to 0.97; the FP16 f - feq
+    form decodes every gathered, bounced and interpolated population with the
+    reference moments of the node it was read from."""
     nx, ny = 256, 40
     ch = G.wavy_channel(nx, ny, 6.0, 128)
     rate, g, mu = 1.25, 2e-6, 0.1
@@ -63,7 +68,7 @@ def test_wavy_laminar_matches_oracle(kofm_lib, oracle):
     cfg = make_cfg(nx, ny, rate, g, mu)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
     sim.step(300)
-    with _lattice(ch, rate, g, mu, False) as L:
+    with _lattice(ch, rate, g, mu, False, storage) as L:
         L.set_state(f)
         L.step(300)
         rho, ux, uy = L.get_macro()
@@ -71,7 +76,7 @@ def test_wavy_laminar_matches_oracle(kofm_lib, oracle):
     errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl))
     uy_rel = np.linalg.norm((uy - sim.uy)[fl]) / np.linalg.norm(sim.ux[fl])
     print(errs, uy_rel)
-    assert errs["rho"] < 1e-6 and errs["ux"] < 1e-5 and uy_rel < 1e-5, (errs, uy_rel)
+    assert errs["rho"] < tol / 10 and errs["ux"] < tol and uy_rel < tol, (errs, uy_rel)
 
 
 def _wavy_komega_case():
