@@ -212,7 +212,9 @@ def run_ours(args, rank, world, local_rank):
     ms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local_rank}")
     st = L.stats()
     value = replica_value(nodes, args.steps, world, ms)
-    launches_per_step = 3 + 0  # collide, assembly, solver (per k-omega sub-step)
+    # kernels of one kofm_step: collide, assembly, solver control-block init,
+    # solver (one k-omega sub-step per LB step here: steps_per_lb stays 1)
+    launches_per_step = 4 if w.komega else 1
 
     # ---- per-kernel breakdown (same stream, CUDA events) ------------------------
     nb = max(3, min(args.steps, 10))
