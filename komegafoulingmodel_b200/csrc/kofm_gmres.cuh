@@ -100,21 +100,13 @@ struct GmresArgs {
 template <typename T>
 __device__ __forceinline__ T ldc(const T* p) { return __ldcg(p); }
 
-// pair loads / stores of solver vectors (FP32 or FP64 storage, FP64 values)
-__device__ __forceinline__ double2 ldvec2(const float* p) {
-    const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
-    return make_double2((double)v.x, (double)v.y);
-}
+// pair loads / stores of solver vectors (coherent: written inside the launch)
 __device__ __forceinline__ double2 ldvec2(const double* p) {
     return __ldcg(reinterpret_cast<const double2*>(p));
-}
-__device__ __forceinline__ void stvec2(float* p, double a, double b) {
-    __stcg(reinterpret_cast<float2*>(p), make_float2((float)a, (float)b));
 }
 __device__ __forceinline__ void stvec2(double* p, double a, double b) {
     __stcg(reinterpret_cast<double2*>(p), make_double2(a, b));
 }
-__device__ __forceinline__ double rnd(double v) { return (double)(vec_t)v; }
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     unsigned int v;
@@ -660,7 +652,7 @@ gmres_kernel(const GmresArgs a) {
                                 __ldcg(S.x + gj) +
                                 (double)__ldg(S.coef + ilv(4, 0, gj)) * __ldcg(S.x + row + xe) +
                                 (double)__ldg(S.coef + ilv(4, 2, gj)) * __ldcg(S.x + gj + a.P);
-                            rr[j] = rnd((double)__ldcg(S.rhs + gj) - Ax);
+                            rr[j] = __ldcg(S.rhs + gj) - Ax;
                         }
                         stvec2(S.r + g, rr[0], rr[1]);
                         acc[0] += rr[0] * rr[0] + rr[1] * rr[1];
@@ -689,7 +681,7 @@ gmres_kernel(const GmresArgs a) {
                     if (threadIdx.x < k) T.g[threadIdx.x] = ldc(&C->h[threadIdx.x]) * ldc(&C->s[threadIdx.x]);
                     if (threadIdx.x == 0 && k > 0) T.sk1 = ldc(&C->s[k - 1]);
                     __syncthreads();
-                    const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
+                    const double* rsrc = restart == 0 ? S.rhs : S.r;
                     {
                         // The block takes a share of the flattened (group, row)
                         // sequence, a group being GM_WARPS adjacent strips; its
@@ -739,7 +731,7 @@ gmres_kernel(const GmresArgs a) {
         for (int s = 0; s < 2; ++s) {
             if (!sh_act[s]) continue;
             const KoSystem& S = a.sys[s];
-            const vec_t* rsrc = restart == 0 ? S.rhs : S.r;
+            const double* rsrc = restart == 0 ? S.rhs : S.r;
             for (long long pr = t0; pr < npairs; pr += stride) {
                 const long long g = pr * 2;
                 double2 xv = make_double2(0.0, 0.0);

@@ -28,10 +28,7 @@ constexpr int KO_TX = 32, KO_TY = 8;
 // The Krylov basis, residual and right-hand side are FP64 as well: an FP32
 // basis loses orthogonality and stalls the first omega cycle near 1e-5
 // relative residual.
-#ifndef KOFM_SOLVER_VEC
-#define KOFM_SOLVER_VEC double
-#endif
-using vec_t = KOFM_SOLVER_VEC;  // storage type of the streamed solver vectors
+
 
 // Multi-vector arrays (the 4 coefficients, the Krylov basis) are stored
 // tile-interleaved: the NV values of the 32 nodes of one row segment (node
@@ -44,10 +41,10 @@ __host__ __device__ __forceinline__ long long ilv(int nv, int j, long long g) {
 
 struct KoSystem {
     double* coef = nullptr;  // [4 x D] normalised off-diagonals E, W, N, S (interleaved)
-    vec_t* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
-    vec_t* r = nullptr;      // [D] residual of restarts >= 1
+    double* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
+    double* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
-    vec_t* V = nullptr;      // [K x D] Krylov basis (orthogonalised, unscaled; interleaved)
+    double* V = nullptr;      // [K x D] Krylov basis (orthogonalised, unscaled; interleaved)
 };
 
 struct AsmParams {
@@ -63,9 +60,9 @@ struct AsmParams {
     const float* uy;
     const float* S;
     double* coef_o;
-    vec_t* rhs_o;
+    double* rhs_o;
     double* coef_k;
-    vec_t* rhs_k;
+    double* rhs_k;
     int nx, ny, P;
     long long D;
     double mu, dt;
@@ -254,8 +251,8 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     if (!n.interior) return;
     if (t & M_SOLID) {
         for (int c = 0; c < 4; ++c) { p.coef_o[ilv(4, c, g)] = 0.0; p.coef_k[ilv(4, c, g)] = 0.0; }
-        p.rhs_o[g] = vec_t(0);
-        p.rhs_k[g] = vec_t(0);
+        p.rhs_o[g] = 0.0;
+        p.rhs_k[g] = 0.0;
         return;
     }
     const double Ux = S.fld[3][tid], Uy = S.fld[4][tid];
@@ -311,8 +308,8 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
     p.coef_o[ilv(4, 0, g)] = We; p.coef_o[ilv(4, 1, g)] = Ww; p.coef_o[ilv(4, 2, g)] = Wn; p.coef_o[ilv(4, 3, g)] = Ws;
     p.coef_k[ilv(4, 0, g)] = Ke; p.coef_k[ilv(4, 1, g)] = Kw; p.coef_k[ilv(4, 2, g)] = Kn; p.coef_k[ilv(4, 3, g)] = Ks;
-    p.rhs_o[g] = (vec_t)(Wsrc - Axo);
-    p.rhs_k[g] = (vec_t)(Ksrc - Axk);
+    p.rhs_o[g] = (Wsrc - Axo);
+    p.rhs_k[g] = (Ksrc - Axk);
 }
 
 __global__ void __launch_bounds__(KO_THREADS, 2)
