@@ -216,6 +216,23 @@ int kofm_step(kofm_ctx* ctx, int32_t nsteps, int32_t options);
  * of this path). */
 int kofm_reduce(kofm_ctx* ctx, int32_t field, int32_t op, double* out);
 
+/* Wall shear set-up: the shear nodes (node indices i + nx_full*j of the
+ * padded host layout; clVariablesLS::fillShearArray, clVariablesLS.cpp:288-320),
+ * their two coefficient rows of 8 (x then y; TR_Find_Shear_Coeffs1,
+ * Kernels/trKernelsShear.cl:333-375), and per boundary link the list indices
+ * of its four nearest shear nodes (-1: none) with their weights
+ * (TR_Find_Shear_Coeffs2, trKernelsShear.cl:414-505).  n_bl may be 0.
+ * komegafoulingmodel_b200/shear.py builds all of them from the walls. */
+int kofm_set_shear(kofm_ctx* ctx, const int32_t* nodes, int32_t n_nodes, const double* cfss,
+                   const int32_t* bl_nodes, const double* bl_weights, int32_t n_bl);
+
+/* Wall shear of the current state at the shear nodes (TR_shear_1,
+ * trKernelsShear.cl:131-222: non-equilibrium part of the node's post-stream
+ * populations against the moments of the last step, (nu + nu_t)-scaled) and
+ * at the boundary links (TR_shear_2, trKernelsShear.cl:300-316).  Either
+ * output may be NULL; synchronises. */
+int kofm_wall_shear(kofm_ctx* ctx, double* node_tau, double* bl_tau);
+
 int kofm_sync(kofm_ctx* ctx);
 int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);
 

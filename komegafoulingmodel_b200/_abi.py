@@ -22,6 +22,8 @@ ERRORS = {
     -202: "NOT_CONVERGED", -203: "NAN", -204: "TIMEOUT", -205: "STATE",
     -206: "TOO_LARGE",
 }
+ERR_INVALID_ARG = -200
+ERR_STATE = -205
 ERR_TOO_LARGE = -206
 NOALLOC_MAX_NODES = 4096 * 65536
 ERR_NOT_CONVERGED = -202
@@ -86,6 +88,8 @@ SIGNATURES = {
     "kofm_step": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "kofm_reduce": (C.c_int, [_vp, C.c_int32, C.c_int32, _dp]),
     "kofm_sync": (C.c_int, [_vp]),
+    "kofm_set_shear": (C.c_int, [_vp, _i32p, C.c_int32, _dp, _i32p, _dp, C.c_int32]),
+    "kofm_wall_shear": (C.c_int, [_vp, _dp, _dp]),
     "kofm_get_stats": (C.c_int, [_vp, C.POINTER(KofmStats)]),
     "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
     "kofm_stream": (_vp, [_vp]),

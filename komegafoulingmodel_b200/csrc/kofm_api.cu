@@ -84,6 +84,15 @@ struct kofm_ctx {
     int time_since_change = 0;
     double dt = 1.0;
     kofm_stats stats{};
+
+    // wall shear (kofm_set_shear / kofm_wall_shear)
+    int32_t* shear_nodes = nullptr;   // [n] node index of the padded host layout
+    double* shear_cfss = nullptr;     // [n][16]
+    double* shear_tau = nullptr;      // [n]
+    int32_t* shear_bl_nodes = nullptr;// [n_bl][4]
+    double* shear_bl_w = nullptr;     // [n_bl][4]
+    double* shear_bl_tau = nullptr;   // [n_bl]
+    int shear_n = 0, shear_nbl = 0;
 };
 
 namespace {
@@ -170,31 +179,24 @@ __global__ void k_fa_in_neq(const double* __restrict__ f, __half* __restrict__ g
 
 // device state -> host-layout FP64 FA.  phase 0: own deviations; phase 1:
 // gather + bounce-back + interpolated bounce-back (the next step's pull).
-// ref != nullptr: non-equilibrium form (decode with the stored reference of
-// the node each value was read from).
+// Deviations f - w of the populations FA of fluid node (x, y) -- the
+// reference's post-stream, bounced and interpolated state -- from the device
+// state: phase 0 holds them at the node; phase 1 gathers the previous step's
+// post-collision values and applies bounce-back and interpolated bounce-back
+// (the next step's pull).  ref != nullptr: non-equilibrium form (decode with
+// the stored reference of the node each value was read from).
 template <typename ST>
-__global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ nt,
-                         const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
-                         int has_ibb, double* __restrict__ f, int nx, int nxf, int ny,
-                         int P, long long D, int phase, const float* __restrict__ ref) {
+__device__ void fa_node(const ST* __restrict__ g, int type, const int32_t* __restrict__ rec,
+                        const IbbRecord* __restrict__ ibb, int has_ibb, int nx, int ny, int P,
+                        long long D, int phase, const float* __restrict__ ref, int x, int y,
+                        double d[9]) {
     auto dec = [&](int q, long long n) -> double {
         const double raw = Store<ST>::to_f64(g[q * D + n]);
         if (!ref) return raw;
         return (double)(feq_dev_f32(q, ref[n], ref[D + n], ref[2 * D + n]) +
                         (float)raw * NEQ_INV_SCALE);
     };
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= nxf) return;
-    const long long Dh = (long long)nxf * ny;
-    const long long hnode = (long long)y * nxf + x;
     const long long node = (long long)y * P + x;
-    const int type = x < nx ? (uint16_t)nt[node] : M_SOLID;
-    if (type & M_SOLID) {
-        for (int q = 0; q < 9; ++q) f[q * Dh + hnode] = 0.0;
-        return;
-    }
-    double d[9];
     for (int q = 0; q < 9; ++q) {
         if (phase == 0) {
             d[q] = dec(q, node);
@@ -225,7 +227,77 @@ __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ n
             }
         }
     }
+}
+
+// device state -> host-layout FP64 FA (see fa_node)
+template <typename ST>
+__global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ nt,
+                         const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
+                         int has_ibb, double* __restrict__ f, int nx, int nxf, int ny,
+                         int P, long long D, int phase, const float* __restrict__ ref) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= nxf) return;
+    const long long Dh = (long long)nxf * ny;
+    const long long hnode = (long long)y * nxf + x;
+    const int type = x < nx ? (uint16_t)nt[(long long)y * P + x] : M_SOLID;
+    if (type & M_SOLID) {
+        for (int q = 0; q < 9; ++q) f[q * Dh + hnode] = 0.0;
+        return;
+    }
+    double d[9];
+    fa_node<ST>(g, type, rec, ibb, has_ibb, nx, ny, P, D, phase, ref, x, y, d);
     for (int q = 0; q < 9; ++q) f[q * Dh + hnode] = d[q] + weight_of(q);
+}
+
+// Wall shear at the shear nodes (TR_shear_1, Kernels/trKernelsShear.cl:131-222):
+// f_neq = FA - feq(rho, u) of the node's populations 1..8 (rho, u the moments
+// the last step wrote), tau = |(f_neq . cx_row, f_neq . cy_row)| (nu + nu_t)
+// / (3 (nu + nu_t) + 1/2) / rho, with the sign of its x component.
+template <typename ST>
+__global__ void k_shear_nodes(const ST* __restrict__ g, const int16_t* __restrict__ nt,
+                              const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
+                              int has_ibb, int nx, int ny, int P, long long D, int phase,
+                              const float* __restrict__ ref, const float* __restrict__ rho,
+                              const float* __restrict__ ux, const float* __restrict__ uy,
+                              const float* __restrict__ nut, double mu, const int32_t* __restrict__ nodes,
+                              const double* __restrict__ cfss, int n, int nxf, double* __restrict__ tau) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int hn = nodes[i];
+    const int y = hn / nxf, x = hn - y * nxf;
+    const long long node = (long long)y * P + x;
+    const int type = (uint16_t)nt[node];
+    double d[9];
+    fa_node<ST>(g, type, rec, ibb, has_ibb, nx, ny, P, D, phase, ref, x, y, d);
+    const double r = rho[node], u = ux[node], v = uy[node];
+    double tx = 0.0, ty = 0.0;
+    for (int q = 1; q < 9; ++q) {
+        const int cx = cx_of(q), cy = cy_of(q);
+        const double phx = cx == 0 ? 2.0 / 3.0 - u * u : 0.5 * (1.0 / 3.0 + cx * u + u * u);
+        const double phy = cy == 0 ? 2.0 / 3.0 - v * v : 0.5 * (1.0 / 3.0 + cy * v + v * v);
+        const double fneq = (d[q] + weight_of(q)) - r * phx * phy;
+        tx += fneq * cfss[16 * (long long)i + (q - 1)];
+        ty += fneq * cfss[16 * (long long)i + 8 + (q - 1)];
+    }
+    double visc = (nut ? (double)nut[node] : 0.0) + mu;
+    visc *= 1.0 / (3.0 * visc + 0.5);
+    const double t = sqrt(tx * tx * visc * visc + ty * ty * visc * visc) / r;
+    tau[i] = tx < 0.0 ? -t : t;
+}
+
+// Shear of every boundary link: weighted mean of its four nearest shear
+// nodes (TR_shear_2, trKernelsShear.cl:300-316); index -1 contributes nothing.
+__global__ void k_shear_links(const double* __restrict__ tau_nodes, const int32_t* __restrict__ sind,
+                              const double* __restrict__ w, int nbl, double* __restrict__ out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbl) return;
+    double acc = 0.0;
+    for (int a = 0; a < 4; ++a) {
+        const int j = sind[4 * b + a];
+        if (j >= 0) acc += w[4 * b + a] * tau_nodes[j];
+    }
+    out[b] = acc;
 }
 
 // FP64 host-layout scalar field <-> FP32 device field
@@ -393,7 +465,8 @@ int kofm_destroy(kofm_ctx* c) {
     void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
-                    c->gpart, c->bar};
+                    c->gpart, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
+                    c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
@@ -666,6 +739,77 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
             for (int s = 0; s < 3; ++s)
                 if ((st = download_field(c, c->S + s * c->D, sxy + s * Dh))) return st;
     }
+    return KOFM_OK;
+}
+
+int kofm_set_shear(kofm_ctx* c, const int32_t* nodes, int32_t n_nodes, const double* cfss,
+                   const int32_t* bl_nodes, const double* bl_weights, int32_t n_bl) {
+    if (!c || n_nodes < 1 || !nodes || !cfss || n_bl < 0 || (n_bl > 0 && (!bl_nodes || !bl_weights)))
+        return KOFM_ERR_INVALID_ARG;
+    if (!c->have_geometry) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    const long long nh = (long long)d.nx_full * d.ny;
+    for (int i = 0; i < n_nodes; ++i) {
+        if (nodes[i] < 0 || nodes[i] >= nh || nodes[i] % d.nx_full >= d.nx) return KOFM_ERR_INVALID_ARG;
+    }
+    for (long long i = 0; i < 4LL * n_bl; ++i)
+        if (bl_nodes[i] < -1 || bl_nodes[i] >= n_nodes) return KOFM_ERR_INVALID_ARG;
+    cudaSetDevice(c->dev);
+    void* old[] = {c->shear_nodes, c->shear_cfss, c->shear_tau, c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau};
+    for (void* b : old)
+        if (b) cudaFree(b);
+    c->shear_nodes = nullptr; c->shear_cfss = nullptr; c->shear_tau = nullptr;
+    c->shear_bl_nodes = nullptr; c->shear_bl_w = nullptr; c->shear_bl_tau = nullptr;
+    c->shear_n = c->shear_nbl = 0;
+    int st;
+    if ((st = dalloc_t(&c->shear_nodes, (size_t)n_nodes))) return st;
+    if ((st = dalloc_t(&c->shear_cfss, (size_t)16 * n_nodes))) return st;
+    if ((st = dalloc_t(&c->shear_tau, (size_t)n_nodes))) return st;
+    if (n_bl > 0) {
+        if ((st = dalloc_t(&c->shear_bl_nodes, (size_t)4 * n_bl))) return st;
+        if ((st = dalloc_t(&c->shear_bl_w, (size_t)4 * n_bl))) return st;
+        if ((st = dalloc_t(&c->shear_bl_tau, (size_t)n_bl))) return st;
+    }
+    KOFM_CUDA_TRY(cudaMemcpy(c->shear_nodes, nodes, sizeof(int32_t) * n_nodes, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaMemcpy(c->shear_cfss, cfss, sizeof(double) * 16 * n_nodes, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    if (n_bl > 0) {
+        KOFM_CUDA_TRY(cudaMemcpy(c->shear_bl_nodes, bl_nodes, sizeof(int32_t) * 4 * n_bl, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+        KOFM_CUDA_TRY(cudaMemcpy(c->shear_bl_w, bl_weights, sizeof(double) * 4 * n_bl, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    }
+    c->shear_n = n_nodes;
+    c->shear_nbl = n_bl;
+    return KOFM_OK;
+}
+
+int kofm_wall_shear(kofm_ctx* c, double* node_tau, double* bl_tau) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    if (!c->have_state || c->shear_n < 1) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    cudaSetDevice(c->dev);
+    const int n = c->shear_n;
+    const int has_ibb = c->n_ibb_rec > 0;
+    const float* ref = d.storage == KOFM_STORE_FP16_NEQ ? c->ref[c->cur] : nullptr;
+    const int nb = (n + 127) / 128;
+    switch (d.storage) {
+        case KOFM_STORE_FP32:
+            k_shear_nodes<float><<<nb, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            break;
+        case KOFM_STORE_BF16_DEV:
+            k_shear_nodes<__nv_bfloat16><<<nb, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            break;
+        default:  // FP16 forms
+            k_shear_nodes<__half><<<nb, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, ref, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+    }
+    KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    if (c->shear_nbl > 0) {
+        k_shear_links<<<(c->shear_nbl + 127) / 128, 128, 0, c->stream>>>(c->shear_tau, c->shear_bl_nodes, c->shear_bl_w, c->shear_nbl, c->shear_bl_tau);
+        KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+    }
+    if (node_tau)
+        KOFM_CUDA_TRY(cudaMemcpyAsync(node_tau, c->shear_tau, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
+    if (bl_tau && c->shear_nbl > 0)
+        KOFM_CUDA_TRY(cudaMemcpyAsync(bl_tau, c->shear_bl_tau, sizeof(double) * c->shear_nbl, cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
+    KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_CALLING_KERNEL);
     return KOFM_OK;
 }
 

@@ -84,6 +84,24 @@ class Lattice:
             self._ctx, _ptr(f), _ptr(k), _ptr(o), _ptr(nut), _ptr(s)))
         return f, k, o, nut, s
 
+    def set_shear(self, sh):
+        """Uploads a shear.ShearSetup (kofm_set_shear)."""
+        nodes = np.ascontiguousarray(sh.nodes, np.int32)
+        cf = np.ascontiguousarray(sh.cfss, np.float64)
+        bn = np.ascontiguousarray(sh.bl_nodes, np.int32)
+        bw = np.ascontiguousarray(sh.bl_weights, np.float64)
+        self._shear_sizes = (len(nodes), len(bn))
+        check("kofm_set_shear", self.lib.kofm_set_shear(
+            self._ctx, _ptr(nodes, C.c_int32), len(nodes), _ptr(cf), _ptr(bn, C.c_int32), _ptr(bw),
+            len(bn)))
+
+    def wall_shear(self):
+        """(tau at the shear nodes, tau at the boundary links) of the current state."""
+        n, nb = self._shear_sizes
+        t, b = np.empty(n), np.empty(nb)
+        check("kofm_wall_shear", self.lib.kofm_wall_shear(self._ctx, _ptr(t), _ptr(b) if nb else None))
+        return t, b
+
     def get_macro(self):
         rho, ux, uy = np.empty(self.n), np.empty(self.n), np.empty(self.n)
         check("kofm_get_macro", self.lib.kofm_get_macro(self._ctx, _ptr(rho), _ptr(ux), _ptr(uy)))

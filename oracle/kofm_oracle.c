@@ -654,3 +654,42 @@ double orc_min(const double* a, int64_t n) {
     for (int64_t t = 1; t < n; ++t) if (a[t] < m) m = a[t];
     return m;
 }
+
+
+/* TR_shear_1 (Kernels/trKernelsShear.cl:131-222): f_neq of populations 1..8
+ * against the product-form equilibrium of the node's moments (calcLBDists),
+ * dotted with the node's two coefficient rows and scaled by
+ * (nu + nu_t) / (3 (nu + nu_t) + 1/2); tau = |.| / rho, signed by x. */
+void orc_wall_shear_nodes(const orc_cfg* c, const double* FA, const double* rho,
+                          const double* ux, const double* uy, const double* nut,
+                          const int32_t* nodes, int n, const double* cfss, double* tau) {
+    const long D = (long)c->nxf * c->ny;
+    for (int i = 0; i < n; ++i) {
+        const long g = nodes[i];
+        double feq[9];
+        orc_feq(rho[g], ux[g], uy[g], feq);
+        double tx = 0.0, ty = 0.0;
+        for (int q = 1; q < 9; ++q) {
+            const double fneq = FA[g + q * D] - feq[q];
+            tx += fneq * cfss[16L * i + q - 1];
+            ty += fneq * cfss[16L * i + 8 + q - 1];
+        }
+        double visc = (nut ? nut[g] : 0.0) + c->mu;
+        visc *= 1.0 / (3.0 * visc + 0.5);
+        const double t = sqrt((tx * visc) * (tx * visc) + (ty * visc) * (ty * visc)) / rho[g];
+        tau[i] = tx < 0.0 ? -t : t;
+    }
+}
+
+/* TR_shear_2 (trKernelsShear.cl:300-316) */
+void orc_wall_shear_links(const double* tau_nodes, const int32_t* sind, const double* w,
+                          int nbl, double* out) {
+    for (int b = 0; b < nbl; ++b) {
+        double acc = 0.0;
+        for (int a = 0; a < 4; ++a) {
+            const int j = sind[4 * b + a];
+            if (j >= 0) acc += w[4 * b + a] * tau_nodes[j];
+        }
+        out[b] = acc;
+    }
+}

@@ -125,6 +125,17 @@ void orc_geom_straight(const orc_cfg* c, int16_t* map, double* dX,
                        double* wallD);
 
 /* ---- reductions ---------------------------------------------------------- */
+/* ---- wall shear (TR_shear_1 / TR_shear_2, Kernels/trKernelsShear.cl:131-222,
+ * 300-316) ------------------------------------------------------------------
+ * tau at every shear node from the post-stream populations FA and the
+ * moments rho, ux, uy of the last collision; nut may be NULL (laminar). */
+void orc_wall_shear_nodes(const orc_cfg* c, const double* FA, const double* rho,
+                          const double* ux, const double* uy, const double* nut,
+                          const int32_t* nodes, int n, const double* cfss, double* tau);
+/* weighted mean of the four nearest shear nodes per boundary link (-1: none) */
+void orc_wall_shear_links(const double* tau_nodes, const int32_t* sind, const double* w,
+                          int nbl, double* out);
+
 double orc_sum(const double* a, int64_t n);
 double orc_min(const double* a, int64_t n);
 

@@ -93,6 +93,9 @@ class Oracle:
                                        _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                        _dp, _dp, _dp]
         L.orc_geom_straight.argtypes = [cp, _i16, _dp, _dp]
+        L.orc_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, C.c_void_p, _i32, C.c_int,
+                                           _dp, _dp]
+        L.orc_wall_shear_links.argtypes = [_dp, _i32, _dp, C.c_int, _dp]
         L.orc_sum.argtypes = [_dp, C.c_int64]
         L.orc_sum.restype = C.c_double
         L.orc_min.argtypes = [_dp, C.c_int64]
@@ -140,6 +143,9 @@ class RefKernels:
         L.ref_komega_coeffs.argtypes = [cp, _i32, _dp, _dp, _dp, _dp, _dp, _dp,
                                         _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         _dp, _dp, _dp, _i16, C.c_double, _dp]
+        if hasattr(L, "ref_wall_shear_nodes"):
+            L.ref_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, C.c_int]
+            L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
 
     @staticmethod
     def available(path: str = LIB_REF) -> bool:

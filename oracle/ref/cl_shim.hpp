@@ -1,5 +1,6 @@
 // OpenCL-C -> C++ shim used ONLY to compile the reference's own kernel
-// sources (source/Kernels/Heading.cl, lbKernels.cl, kOmegaKernels.cl) for the
+// sources (source/Kernels/Heading.cl, lbKernels.cl, kOmegaKernels.cl and the
+// wall-shear functions of trKernelsShear.cl) for the
 // CPU, so the oracle can be checked against the reference code itself.
 //
 // This file is test infrastructure (the checker), never part of the product.
@@ -21,14 +22,36 @@ typedef unsigned char uchar;
 
 struct int2 { int x, y; };
 struct uint2 { uint x, y; };
-struct double2 { double x, y; };
+struct double2 {
+    double x, y;
+    double2() = default;
+    double2(double s) : x(s), y(s) {}          // OpenCL scalar -> vector
+    double2(double a, double b) : x(a), y(b) {}
+};
 struct double4 { double x, y, z, w; };
+// double8 with the .s0 .. .s7 and .lo / .hi views used by the shear kernels
+struct double8 {
+    union {
+        struct { double s0, s1, s2, s3, s4, s5, s6, s7; };
+        struct { double4 lo, hi; };
+    };
+};
 struct float4 { float x, y, z, w; };
 
 static inline int2 make_int2(int a, int b) { return int2{a, b}; }
 static inline uint2 make_uint2(uint a, uint b) { return uint2{a, b}; }
 static inline double2 make_double2(double a, double b) { return double2{a, b}; }
 static inline double4 make_double4(double a, double b, double c, double d) { return double4{a, b, c, d}; }
+static inline double8 make_double8(double a, double b, double c, double d, double e, double f,
+                                   double g, double h) {
+    double8 r;
+    r.s0 = a; r.s1 = b; r.s2 = c; r.s3 = d; r.s4 = e; r.s5 = f; r.s6 = g; r.s7 = h;
+    return r;
+}
+static inline double8 operator*(double8 a, double s) {
+    return make_double8(a.s0 * s, a.s1 * s, a.s2 * s, a.s3 * s, a.s4 * s, a.s5 * s, a.s6 * s, a.s7 * s);
+}
+static inline double dot(double4 a, double4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
 static inline float4 make_float4(float a, float b, float c, float d) { return float4{a, b, c, d}; }
 
 static inline double2 operator+(double2 a, double2 b) { return {a.x + b.x, a.y + b.y}; }
@@ -38,6 +61,7 @@ static inline double2 operator*(double2 a, double s) { return {s * a.x, s * a.y}
 static inline double2 operator/(double2 a, double s) { return {a.x / s, a.y / s}; }
 static inline double2& operator/=(double2& a, double s) { a.x /= s; a.y /= s; return a; }
 static inline double length(double2 a) { return std::sqrt(a.x * a.x + a.y * a.y); }
+static inline double2 normalize(double2 a) { const double l = length(a); return {a.x / l, a.y / l}; }
 static inline double2 ceil(double2 a) { return {std::ceil(a.x), std::ceil(a.y)}; }
 static inline int2 convert_int2(double2 a) { return {(int)a.x, (int)a.y}; }
 static inline double2 convert_double2(int2 a) { return {(double)a.x, (double)a.y}; }
@@ -65,3 +89,5 @@ static inline ulong atom_cmpxchg(volatile ulong* p, ulong cmp, ulong val) {
 // LB/k-omega kernels use no barriers or local memory).
 extern thread_local size_t g_ref_gid[3];
 static inline size_t get_global_id(int d) { return g_ref_gid[d]; }
+// one work-item per work-group slot: local arrays are indexed by slot 0
+static inline size_t get_local_id(int) { return 0; }

@@ -76,6 +76,10 @@ struct RefProgram {
 #include "../_ref/gen/Heading.inc"
 #include "../_ref/gen/lbKernels.inc"
 #include "../_ref/gen/kOmegaKernels.inc"
+#define SHEAR_CUTOFF_RADIUS m_cutoff
+    double m_cutoff = 5.0;
+#include "../_ref/gen/shear.inc"
+#undef SHEAR_CUTOFF_RADIUS
 };
 
 #pragma GCC diagnostic pop
@@ -177,6 +181,29 @@ int ref_komega_coeffs(const RefCfg* c, int* ind, double* K, double* O,
                                         rho, ux, uy, kA, oA, kb, ob, dX, wallD,
                                         nullptr, nullptr, map, dt, dbg);
     });
+    return 0;
+}
+
+// TR_shear_1 (trKernelsShear.cl:175-222) over n shear nodes.
+int ref_wall_shear_nodes(const RefCfg* c, double* rho, double* ux, double* uy, double* cfss,
+                         double* FA, double* tau, int* nodes, double* nut, int n) {
+    RefProgram p = make_prog(c);
+    for (int i = 0; i < n; ++i) {
+        g_ref_gid[0] = (size_t)i; g_ref_gid[1] = 0; g_ref_gid[2] = 0;
+        double8 scratch[1];
+        p.TR_shear_1(rho, ux, uy, reinterpret_cast<double8*>(cfss), FA, tau, nodes, nut, n, scratch);
+    }
+    return 0;
+}
+
+// TR_Find_Shear_Coeffs1 (trKernelsShear.cl:333-375) over n shear nodes.
+int ref_shear_coeffs1(const RefCfg* c, int* nodes, short* map, double* cfss, int n, double cutoff) {
+    RefProgram p = make_prog(c);
+    p.m_cutoff = cutoff;
+    for (int i = 0; i < n; ++i) {
+        g_ref_gid[0] = (size_t)i; g_ref_gid[1] = 0; g_ref_gid[2] = 0;
+        p.TR_Find_Shear_Coeffs1(nodes, map, cfss, n);
+    }
     return 0;
 }
 
