@@ -155,10 +155,12 @@ def replica_value(nodes: int, steps: int, world: int, ms: float) -> float:
     return nodes * steps * world / (ms * 1e-3) / 1e6
 
 
-# DRAM traffic of one solver launch from an ncu capture of the 8192x512 case
-# (profiles/gmres_kernel_komega_straight_8192x512.md): 4.34 GB for 4,194,304
-# nodes; scaled to a launch of the bench's lattice by its node count.
-GMRES_TRAFFIC_BYTES_PER_NODE = 4.3399e9 / 4194304
+# DRAM traffic over algorithmic bytes of one solver launch, from an ncu capture
+# of the 8192x512 case (profiles/gmres_kernel_komega_straight_8192x512.md):
+# 4.797 GB read + written for a launch of 1076 algorithmic B/node x 4,194,304
+# nodes.  Traffic grows with the nodes and the passes of a launch, so the
+# bench's traffic figure is this ratio times its average launch's bytes.
+GMRES_TRAFFIC_RATIO = 4.7967e9 / (1076 * 4194304)
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
             "fp16neq": 114}                   # + reference moments read and written
@@ -250,9 +252,9 @@ def run_ours(args, rank, world, local_rank):
     dom = max(kern, key=lambda k: kern[k]["ms"])
     roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak,
             "unit": "GB/s", "frac": kern[dom]["gbs"] / peak, "peak_kind": peak_kind,
-            "traffic": (GMRES_TRAFFIC_BYTES_PER_NODE * nodes if dom == "gmres_kernel" else None),
-            "traffic_source": "ncu dram bytes of one launch on komega_straight_8192x512, "
-                              "scaled by nodes",
+            "traffic": (GMRES_TRAFFIC_RATIO * b_sv * nodes if dom == "gmres_kernel" else None),
+            "traffic_source": "ncu dram bytes / algorithmic bytes of one launch on "
+                              "komega_straight_8192x512, times this run's average launch",
             "bytes_per_node": kern[dom]["bytes_per_node"]}
     step_bytes = LB_BYTES[args.storage] + ASM_BYTES + b_sv
     step_ms = t_lb + t_as + t_sv
