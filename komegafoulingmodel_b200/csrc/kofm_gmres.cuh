@@ -336,22 +336,26 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
 }
 
 // ---- warp-strip Krylov pass ---------------------------------------------------
-// A work unit is a strip of 32 columns (lane l <-> column x0 + l) times a
-// range of rows, owned by ONE warp, which marches down the rows:
-//   row y:  u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j; store u_k(y);
-//           dots ||u_k||^2 and <r, u_k>;
+// A work unit is a strip of WS_OWN = 30 columns times a range of rows, owned by
+// ONE warp, which marches down the rows.  Lane l holds column x0 - 1 + l: lanes
+// 1..30 are the strip's own columns, lanes 0 and 31 the neighbouring strips'
+// edge columns (x0 - 1 and x0 + 30), computed like any other column so that
+// every lane runs the same instructions:
+//   row y:  u_k(y) = s_{k-1} A u_{k-1} - sum_j g_j u_j; own lanes store u_k(y)
+//           and add ||u_k||^2 and <r, u_k>;
 //           <A u_k, u_j> split by rows: row y adds u_j(y) (u_k + W u_k(x-1) +
 //           E u_k(x+1) + S u_k(y-1)) and the N term of row y-1,
 //           u_k(y) N(y-1) u_j(y-1), carried in registers as q_j.
-// x neighbours come from warp shuffles; lanes 0 and 31 also compute u_k on
-// the ghost columns x0-1 and x0+32 (the neighbouring strips' edge columns).
-// Every lane streams its own column's inputs of row y+2 into its own slots of
-// a 3-row shared-memory ring (cp.async, 8 bytes each) while row y computes, so
-// the pass needs no block-level synchronisation and keeps two rows of loads in
-// flight per warp.  Vectors and coefficients are zero on non-fluid nodes and
-// rows outside the lattice read as zero.  Columns are taken modulo nx
-// (periodic x; the padding columns of the last strip alias real columns and
-// are neither stored nor counted).
+// x neighbours come from warp shuffles; lanes 0 and 31 also read u_{k-1} one
+// column further out (x0 - 2, x0 + 31).  Every lane streams its column's
+// inputs of the rows ahead into its own slots of a shared-memory ring
+// (cp.async, 8 bytes each, addresses advanced by a fixed row stride) while row
+// y computes, so the pass needs no block-level synchronisation.  Vectors and
+// coefficients are zero on non-fluid nodes and rows outside the lattice read
+// as zero.  Columns are taken modulo nx (periodic x; lanes past the last
+// column of the last strip alias real columns and are neither stored nor
+// counted).
+constexpr int WS_OWN = 30;                  // own columns of a strip
 constexpr int WS_KV = KOFM_MAX_KRYLOV - 2;  // u_j for j < k-1 <= K-2
 static_assert(KOFM_MAX_KRYLOV == 10, "krylov_strip is instantiated for k = 0..9");
 constexpr int GM_WARPS = GM_THREADS / 32;
@@ -362,12 +366,10 @@ constexpr int GM_WARPS = GM_THREADS / 32;
 //   vj[k-1][32]   u_j(y), j < k-1
 //   r[32]         r(y) (k >= 1)
 //   up[32]        u_{k-1}(y+1)
-//   gcf[2][4], gvj[2][k-1], gup[2], gout[2]: the ghost columns x0-1 (0) and
-//                 x0+32 (1): coefficients, u_j(y), u_{k-1}(y+1), and
-//                 u_{k-1}(y) at x0-2 and x0+33.
+//   gout[2]       u_{k-1}(y) at x0 - 2 (lane 0) and x0 + 31 (lane 31)
 // The warp's ring region holds as many slots of that size as fit (up to 6),
 // so small k prefetch deeper.
-constexpr int WS_RING_DOUBLES = 3 * ((4 + WS_KV + 2) * 32 + 2 * 4 + 2 * WS_KV + 4);
+constexpr int WS_RING_DOUBLES = 3 * ((4 + WS_KV + 2) * 32 + 2);
 
 template <int k>
 struct SlotView {
@@ -376,23 +378,11 @@ struct SlotView {
     static constexpr int O_VJ = 4 * 32;
     static constexpr int O_R = O_VJ + NV * 32;
     static constexpr int O_UP = O_R + NR * 32;
-    static constexpr int O_GCF = O_UP + 32;
-    static constexpr int O_GVJ = O_GCF + 8;
-    static constexpr int O_GUP = O_GVJ + 2 * (NV > 0 ? NV : 1);
-    static constexpr int O_GOUT = O_GUP + 2;
+    static constexpr int O_GOUT = O_UP + 32;
     static constexpr int DOUBLES = O_GOUT + 2;
     static constexpr int FIT = WS_RING_DOUBLES / DOUBLES;
     static constexpr int SLOTS = FIT > 6 ? 6 : FIT;
     static_assert(SLOTS >= 3, "ring too small");
-    double* b;
-    __device__ __forceinline__ double& cf(int q, int lane) const { return b[q * 32 + lane]; }
-    __device__ __forceinline__ double& vj(int j, int lane) const { return b[O_VJ + j * 32 + lane]; }
-    __device__ __forceinline__ double& r(int lane) const { return b[O_R + lane]; }
-    __device__ __forceinline__ double& up(int lane) const { return b[O_UP + lane]; }
-    __device__ __forceinline__ double& gcf(int h, int q) const { return b[O_GCF + h * 4 + q]; }
-    __device__ __forceinline__ double& gvj(int h, int j) const { return b[O_GVJ + h * (NV > 0 ? NV : 1) + j]; }
-    __device__ __forceinline__ double& gup(int h) const { return b[O_GUP + h]; }
-    __device__ __forceinline__ double& gout(int h) const { return b[O_GOUT + h]; }
 };
 
 struct SolverSmem {
@@ -406,123 +396,126 @@ __device__ __forceinline__ int wrap_mod(int x, int n) {
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ void cp8(double* smem, const double* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+__device__ __forceinline__ void cp8(unsigned saddr, const double* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// element (y, x) of vector j of an array of nv vectors (nv = 1: plain
-// layout) into shared memory; zero outside the rows
-__device__ __forceinline__ void el_copy(const GmresArgs& a, const double* base, int nv, int j,
-                                        int y, int x, double* dst) {
-    if (y < 0 || y >= a.ny) *dst = 0.0;
-    else cp8(dst, base + (nv == 1 ? (long long)y * a.P + x : ilv(nv, j, (long long)y * a.P + x)));
+__device__ __forceinline__ void st_zero(unsigned saddr) {
+    asm volatile("st.shared.f64 [%0], %1;\n" ::"r"(saddr), "d"(0.0) : "memory");
 }
 
-// The thread's inputs of row y into slot W: u_{k-1}(y+1), and for rows inside
-// the lattice the coefficients, u_j (j < k-1) and r; lanes 0 / 31 add their
-// ghost column.
+// Per-lane addressing of one strip: element offsets of the lane's column in
+// the plain, coefficient (4 interleaved) and basis (K interleaved) arrays, and
+// the row strides (P is a multiple of 32, so a row moves every interleaved
+// array by a fixed stride).
+struct StripAddr {
+    long long oP, oC, oV, oSrc, oOut;  // oOut: u_{k-1} one column further out
+    long long sC, sV, sSrc;            // row strides (plain: P)
+};
+
+// The lane's inputs of row y into the slot at shared address sb:
+// u_{k-1}(y+1), u_{k-1}(y) one column out (lanes 0 / 31), and for rows inside
+// the lattice the coefficients, u_j (j < k-1) and r.
 template <int k>
 __device__ __forceinline__ void ws_issue(const GmresArgs& a, const KoSystem& S, const double* src,
-                                         int src_nv, int src_j,
-                                         const double* rsrc, int y, int xl, int lane,
-                                         int gin, int gout, SlotView<k> W) {
-    el_copy(a, src, src_nv, src_j, y + 1, xl, &W.up(lane));
-    const bool ghost = lane == 0 || lane == 31;
-    const int h = lane == 0 ? 0 : 1;
-    if (ghost) {
-        el_copy(a, src, src_nv, src_j, y + 1, gin, &W.gup(h));
-        el_copy(a, src, src_nv, src_j, y, gout, &W.gout(h));
-    }
+                                         const double* rsrc, const StripAddr& A, int y, int lane,
+                                         bool ghost, unsigned sb) {
+    using SV = SlotView<k>;
+    const unsigned sl = sb + 8u * lane;
+    if (y + 1 >= 0 && y + 1 < a.ny) cp8(sl + 8u * SV::O_UP, src + (long long)(y + 1) * A.sSrc + A.oSrc);
+    else st_zero(sl + 8u * SV::O_UP);
+    const unsigned so = sb + 8u * (SV::O_GOUT + (lane == 0 ? 0 : 1));
     if (y < 0 || y >= a.ny) {
+        if (ghost) st_zero(so);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) W.cf(q, lane) = 0.0;
+        for (int q = 0; q < 4; ++q) st_zero(sl + 8u * (q * 32));
 #pragma unroll
-        for (int j = 0; j < k - 1; ++j) W.vj(j, lane) = 0.0;
-        W.r(lane) = 0.0;
-        if (ghost) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) W.gcf(h, q) = 0.0;
-#pragma unroll
-            for (int j = 0; j < k - 1; ++j) W.gvj(h, j) = 0.0;
-        }
+        for (int j = 0; j < k - 1; ++j) st_zero(sl + 8u * (SV::O_VJ + j * 32));
+        if (k > 0) st_zero(sl + 8u * SV::O_R);
         return;
     }
-    const long long row = (long long)y * a.P;
-    const long long gl = row + xl, gg = row + gin;
+    if (ghost) cp8(so, src + (long long)y * A.sSrc + A.oOut);
+    const double* pc = S.coef + (long long)y * A.sC + A.oC;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) cp8(&W.cf(q, lane), S.coef + ilv(4, q, gl));
+    for (int q = 0; q < 4; ++q) cp8(sl + 8u * (q * 32), pc + q * 32);
+    const double* pv = S.V + (long long)y * A.sV + A.oV;
 #pragma unroll
-    for (int j = 0; j < k - 1; ++j) cp8(&W.vj(j, lane), S.V + ilv(a.K, j, gl));
-    if (k > 0) cp8(&W.r(lane), rsrc + gl);
-    if (ghost) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) cp8(&W.gcf(h, q), S.coef + ilv(4, q, gg));
-#pragma unroll
-        for (int j = 0; j < k - 1; ++j) cp8(&W.gvj(h, j), S.V + ilv(a.K, j, gg));
-    }
+    for (int j = 0; j < k - 1; ++j) cp8(sl + 8u * (SV::O_VJ + j * 32), pv + j * 32);
+    if (k > 0) cp8(sl + 8u * SV::O_R, rsrc + (long long)y * a.P + A.oP);
 }
 
-// One warp: rows [ya, yb) of the strip starting at column x0.
+// One warp: rows [ya, yb) of the strip whose own columns start at x0.
 // k (the vector being built) is a template parameter, so every loop over the
 // older basis vectors has its exact length.
 template <int k>
 __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double* rsrc,
                              int x0, int ya, int yb, SolverSmem& T, double* ring,
                              double (&acc)[2 + KOFM_MAX_KRYLOV]) {
-    const int lane = threadIdx.x & 31;
-    // u_{k-1}: r (plain layout) for k = 0, else basis vector k-1 (interleaved)
-    const double* src = (k == 0) ? rsrc : S.V;
-    const int src_nv = (k == 0) ? 1 : a.K, src_j = (k == 0) ? 0 : k - 1;
-    const bool need_w = k < a.K - 1;
-    const int xl = wrap_mod(x0 + lane, a.nx);
-    const bool own = x0 + lane < a.nx;
-    // lane 0: ghost column x0-1 (outer x0-2); lane 31: x0+32 (outer x0+33)
-    const int gin = wrap_mod(lane == 0 ? x0 - 1 : x0 + 32, a.nx);
-    const int gout = wrap_mod(lane == 0 ? x0 - 2 : x0 + 33, a.nx);
-    const bool ghost = lane == 0 || lane == 31;
-
-    // rolling u_{k-1} window (rows y-1, y) on the own and the ghost column
-    auto ld = [&](int y, int x) -> double {
-        if (y < 0 || y >= a.ny) return 0.0;
-        const long long g = (long long)y * a.P + x;
-        return __ldcg(src + (src_nv == 1 ? g : ilv(src_nv, src_j, g)));
-    };
-    double um = ld(ya - 2, xl), u0 = ld(ya - 1, xl);
-    double gm = 0.0, g0 = 0.0;
-    if (ghost) { gm = ld(ya - 2, gin); g0 = ld(ya - 1, gin); }
     using SV = SlotView<k>;
     constexpr int NS = SV::SLOTS;  // rows of loads in flight: NS - 1
-    auto slot = [&](int y) { return SV{ring + ((y + NS) % NS) * SV::DOUBLES}; };
+    const int lane = threadIdx.x & 31;
+    const int K = a.K;
+    // u_{k-1}: r (plain layout) for k = 0, else basis vector k-1 (interleaved)
+    const double* src = (k == 0) ? rsrc : S.V;
+    const bool need_w = k < K - 1;
+    const int xl = wrap_mod(x0 - 1 + lane, a.nx);
+    const bool own = lane >= 1 && lane <= WS_OWN && x0 - 1 + lane < a.nx;
+    const bool ghost = lane == 0 || lane == 31;
+    const int xo = wrap_mod(lane == 0 ? x0 - 2 : x0 + WS_OWN + 1, a.nx);
+    StripAddr A;
+    A.oP = xl;
+    A.oC = (long long)(xl >> 5) * 128 + (xl & 31);
+    A.oV = (long long)(xl >> 5) * (K * 32) + (xl & 31);
+    A.sC = 4LL * a.P;
+    A.sV = (long long)K * a.P;
+    if (k == 0) {
+        A.oSrc = A.oP; A.oOut = xo; A.sSrc = a.P;
+    } else {
+        A.oSrc = A.oV + (k - 1) * 32;
+        A.oOut = (long long)(xo >> 5) * (K * 32) + (xo & 31) + (k - 1) * 32;
+        A.sSrc = A.sV;
+    }
+    auto ld = [&](int y) -> double {
+        if (y < 0 || y >= a.ny) return 0.0;
+        return __ldcg(src + (long long)y * A.sSrc + A.oSrc);
+    };
+    // rolling u_{k-1} window (rows y-1, y) of the lane's column
+    double um = ld(ya - 2), u0 = ld(ya - 1);
+    const unsigned ring_s = (unsigned)__cvta_generic_to_shared(ring);
+    constexpr unsigned SLOT_BYTES = 8u * SV::DOUBLES;
+    int sw = 0;  // slot of the next row to issue
 #pragma unroll
     for (int i = 0; i < NS - 1; ++i) {
-        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, ya - 1 + i, xl, lane, gin, gout, slot(ya - 1 + i));
+        if (ya - 1 + i <= yb) ws_issue<k>(a, S, src, rsrc, A, ya - 1 + i, lane, ghost, ring_s + sw * SLOT_BYTES);
         cp_commit();
+        sw = sw + 1 == NS ? 0 : sw + 1;
     }
+    int sr = 0;  // slot of row y
 
+    const double* g = T.g;  // Gram-Schmidt weights of this vector (shared)
+    const double sk1 = T.sk1;
     double q[WS_KV];
 #pragma unroll
     for (int j = 0; j < WS_KV; ++j) q[j] = 0.0;
     double nprev = 0.0, ukprev = 0.0;
-    const double sk1 = T.sk1;
     for (int y = ya - 1; y <= yb; ++y) {
-        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, src_nv, src_j, rsrc, y + NS - 1, xl, lane, gin, gout, slot(y + NS - 1));
+        if (y + NS - 1 <= yb) ws_issue<k>(a, S, src, rsrc, A, y + NS - 1, lane, ghost, ring_s + sw * SLOT_BYTES);
         cp_commit();
+        sw = sw + 1 == NS ? 0 : sw + 1;
         cp_wait<NS - 1>();
-        const SV W = slot(y);
-        const double up = W.up(lane);
-        const double cE = W.cf(0, lane), cW = W.cf(1, lane), cN = W.cf(2, lane), cS = W.cf(3, lane);
+        const double* W = ring + sr * SV::DOUBLES;
+        sr = sr + 1 == NS ? 0 : sr + 1;
+        const double up = W[SV::O_UP + lane];
+        const double cE = W[lane], cW = W[32 + lane], cN = W[64 + lane], cS = W[96 + lane];
         double v[WS_KV];
 #pragma unroll
-        for (int j = 0; j < WS_KV; ++j) v[j] = j < k - 1 ? W.vj(j, lane) : 0.0;
-        // u_k(y) on the own column
+        for (int j = 0; j < WS_KV; ++j) v[j] = j < k - 1 ? W[SV::O_VJ + j * 32 + lane] : 0.0;
         double left = __shfl_up_sync(0xffffffffu, u0, 1);
         double right = __shfl_down_sync(0xffffffffu, u0, 1);
-        if (lane == 0) left = g0;
-        if (lane == 31) right = g0;
+        if (lane == 0) left = W[SV::O_GOUT];
+        if (lane == 31) right = W[SV::O_GOUT + 1];
         // CSR order of an interior row: S, W, C, E, N
         const double z = cS * um + cW * left + u0 + cE * right + cN * up;
         double uk;
@@ -532,38 +525,19 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
             uk = sk1 * z;
 #pragma unroll
             for (int j = 0; j < WS_KV; ++j)
-                if (j < k - 1) uk -= T.g[j] * v[j];
-            uk -= T.g[k - 1] * u0;
-        }
-        // u_k(y) on the ghost column (lanes 0 and 31)
-        double ukg = 0.0;
-        if (ghost) {
-            const int h = lane == 0 ? 0 : 1;
-            const double gl = lane == 0 ? W.gout(h) : u0;
-            const double gr = lane == 0 ? u0 : W.gout(h);
-            const double gz = W.gcf(h, 3) * gm + W.gcf(h, 1) * gl + g0 + W.gcf(h, 0) * gr +
-                              W.gcf(h, 2) * W.gup(h);
-            if (k == 0) {
-                ukg = gz;
-            } else {
-                ukg = sk1 * gz;
-#pragma unroll
-                for (int j = 0; j < k - 1; ++j) ukg -= T.g[j] * W.gvj(h, j);
-                ukg -= T.g[k - 1] * g0;
-            }
+                if (j < k - 1) uk -= g[j] * v[j];
+            uk -= g[k > 0 ? k - 1 : 0] * u0;
         }
         const bool rowin = y >= ya && y < yb;
-        const double rr = k == 0 ? u0 : W.r(lane);
         if (rowin && own) {
-            __stcg(S.V + ilv(a.K, k, (long long)y * a.P + xl), uk);
+            const double rr = k == 0 ? u0 : W[SV::O_R + lane];
+            __stcg(S.V + (long long)y * A.sV + A.oV + k * 32, uk);
             acc[0] += uk * uk;
             acc[1] += rr * uk;
         }
         if (need_w) {
-            double ukl = __shfl_up_sync(0xffffffffu, uk, 1);
-            double ukr = __shfl_down_sync(0xffffffffu, uk, 1);
-            if (lane == 0) ukl = ukg;
-            if (lane == 31) ukr = ukg;
+            const double ukl = __shfl_up_sync(0xffffffffu, uk, 1);
+            const double ukr = __shfl_down_sync(0xffffffffu, uk, 1);
             if (own && (rowin || y == yb)) {
                 // row y's own part (zero on the halo row yb) plus row y-1's N term
                 const double aw = rowin ? uk + cW * ukl + cE * ukr + cS * ukprev : 0.0;
@@ -589,10 +563,6 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
         ukprev = uk;
         um = u0;
         u0 = up;
-        if (ghost) {
-            gm = g0;
-            g0 = W.gup(lane == 0 ? 0 : 1);
-        }
     }
     cp_wait<0>();
 }
@@ -698,7 +668,7 @@ gmres_kernel(const GmresArgs a) {
                             if (strip < a.strips) {
                                 switch (k) {
 #define KOFM_KSTRIP(n) \
-    case n: krylov_strip<n>(a, S, rsrc, strip * 32, ya, yb, T, ring, acc); break;
+    case n: krylov_strip<n>(a, S, rsrc, strip * WS_OWN, ya, yb, T, ring, acc); break;
                                     KOFM_KSTRIP(0) KOFM_KSTRIP(1) KOFM_KSTRIP(2) KOFM_KSTRIP(3)
                                     KOFM_KSTRIP(4) KOFM_KSTRIP(5) KOFM_KSTRIP(6) KOFM_KSTRIP(7)
                                     KOFM_KSTRIP(8) KOFM_KSTRIP(9)

@@ -41,10 +41,11 @@ def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0):
     return L
 
 
-@pytest.mark.parametrize("full_cycle,nx", [(0, 128), (1, 128), (0, 200)])
+@pytest.mark.parametrize("full_cycle,nx", [(0, 128), (1, 128), (0, 200), (0, 610)])
 def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle, nx):
-    """nx = 200 is not a multiple of the solver's 32-column strips (periodic
-    tail strip) nor of the 128-node padding."""
+    """nx = 200 and 610 are not multiples of the solver's 30-column strips
+    (periodic tail strip) nor of the 128-node padding; at 610 the strips form
+    three groups of eight and the blocks split the rows of a group."""
     ch, f, k, o, nut, rate, g, nu = channel_case(nx=nx, ny=34)
     cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
