@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define KOFM_ABI_VERSION 1
+#define KOFM_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define KOFM_OK 0
@@ -76,6 +76,7 @@ extern "C" {
 #define KOFM_FIELD_OMEGA 4 /* Omega_array (sumOmega/minOmega) */
 #define KOFM_FIELD_NUT 5   /* Nut_array */
 #define KOFM_FIELD_WALL_SHEAR 6 /* wall-shear integral (see kofm_reduce) */
+#define KOFM_FIELD_TEMP 7  /* tempArray (clVariablesFD.cpp:266 sumTemp) */
 #define KOFM_OP_SUM 0
 #define KOFM_OP_MIN 1
 #define KOFM_OP_MAX 2
@@ -111,6 +112,22 @@ typedef struct kofm_desc {
                                  blocks per SM, fewer on small lattices);
                                  lattices advanced together (kofm_batch_*)
                                  may share the GPU better with a cap */
+    /* thermal implicit FD (clVariablesFD::loadParams, clVariablesFD.cpp:444-493) */
+    int32_t use_thermal;      /* thermalSolverFlag (USE_THERMAL_SOLVER) */
+    int32_t thermal_every;    /* tfdSteps: LB steps per thermal update
+                                 (LB_STEPS_PER_FD = 1, LBLS.cpp:197) */
+    double pr_number;         /* Pr (PR_NUMBER 0.708): alpha_fluid = mu / Pr */
+    double pr_turb_number;    /* Pr_t (PR_TURB_NUMBER 0.9) */
+    double alpha_foul;        /* LB_ALPHA_FOUL: diffusivity of fouling-layer
+                                 nodes (M0_FLUID | M_SOLID) */
+    double t_in;              /* TFD_X_IN_VAL (TFD_X_IN 2.0): inlet temperature
+                                 and upper clamp of T in the source term */
+    int32_t thermal_max_iters;/* THERMAL_MAX_ITERS (1000) */
+    int32_t thermal_pad;
+    double thermal_rel_tol;   /* THERMAL_MAX_REL_TOL (1e-4) */
+    double thermal_abs_tol;   /* THERMAL_MAX_ABS_TOL (1e-7) */
+    double thermal_dt;        /* dTtfd (= tfdSteps, 1); sub-steps per update
+                                 start at (int)(1 / thermal_dt) */
 } kofm_desc;
 
 /* Per-context counters of the last k-omega update (kOmega::Solve). */
@@ -129,6 +146,15 @@ typedef struct kofm_stats {
     int64_t steps;                      /* LB steps taken */
     int32_t solver_passes;              /* grid sweeps of the last solve */
     int32_t phase;                      /* 0: populations pre-collision, 1: post */
+    /* last thermal update (clVariablesFD::Solve) */
+    int32_t thermal_iters;              /* BiCGStabSolver::iterCount, last solve */
+    int32_t thermal_checks;             /* residual checks of the last solve */
+    int32_t thermal_solves;             /* solves run by the update */
+    int32_t thermal_resets;             /* dt halvings in the update */
+    int32_t thermal_steps_per_lb;       /* clVariablesFD::stepsPerLB */
+    int32_t thermal_time_since_change;  /* clVariablesFD::timeSinceTimeStepChange */
+    double thermal_dt;                  /* clVariablesFD::timeStep */
+    double thermal_residual;            /* last ||r||_1 / ||b||_1 */
 } kofm_stats;
 
 int kofm_abi_version(void);
@@ -232,6 +258,27 @@ int kofm_set_shear(kofm_ctx* ctx, const int32_t* nodes, int32_t n_nodes, const d
  * at the boundary links (TR_shear_2, trKernelsShear.cl:300-316).  Either
  * output may be NULL; synchronises. */
 int kofm_wall_shear(kofm_ctx* ctx, double* node_tau, double* bl_tau);
+
+/* ---- thermal implicit finite differences ----------------------------------
+ * The temperature update of Solve_no_TR (LBLS.cpp:197-200 -> vfd.Solve,
+ * clVariablesFD.h:343-358): Update_T_Coeffs_Implicit (tfdKernels.cl:122-279)
+ * and BiCGStabSolver::solve (BiCGStabSolver.cpp:628-723) with the dt halving
+ * and doubling of clVariablesFD.cpp:202-228.  Needs desc.use_thermal; kofm_step
+ * runs it after the k-omega update every thermal_every steps.  T lives on the
+ * device in FP64. */
+
+/* tempArray in (host layout, FP64): clVariablesFD::ini fills ROE0 (Tinitial,
+ * 0.5) on M0_FLUID nodes and 0 elsewhere (clVariablesFD.cpp:236-239);
+ * restart files load it instead. */
+int kofm_set_temperature(kofm_ctx* ctx, const double* T);
+int kofm_get_temperature(kofm_ctx* ctx, double* T);
+/* Link fractions of the unfouled walls, vls.dXArr0 (E, W, N, S planes of
+ * nx_full*ny each) that the thermal rows use; without this call the dX4 of
+ * kofm_set_geometry serves (no fouling layer). */
+int kofm_set_thermal_geometry(kofm_ctx* ctx, const double* dX0);
+/* One clVariablesFD::Solve; synchronises once per solve (reads the solver's
+ * exit state for the dt halving). */
+int kofm_thermal_update(kofm_ctx* ctx);
 
 int kofm_sync(kofm_ctx* ctx);
 int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);

@@ -32,7 +32,7 @@ ERR_TIMEOUT = -204
 
 OPTION_SAVE_MACRO_FIELDS = 0x2
 STORE_FP32, STORE_FP16_DEV, STORE_BF16_DEV, STORE_FP16_NEQ = 0, 1, 2, 3
-FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_K, FIELD_OMEGA, FIELD_NUT, FIELD_WALL_SHEAR = range(7)
+FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_K, FIELD_OMEGA, FIELD_NUT, FIELD_WALL_SHEAR, FIELD_TEMP = range(8)
 OP_SUM, OP_MIN, OP_MAX = 0, 1, 2
 
 
@@ -48,6 +48,12 @@ class KofmDesc(C.Structure):
         ("komega_dt", C.c_double),
         ("komega_full_cycle", C.c_int32),
         ("solver_max_blocks", C.c_int32),
+        ("use_thermal", C.c_int32), ("thermal_every", C.c_int32),
+        ("pr_number", C.c_double), ("pr_turb_number", C.c_double),
+        ("alpha_foul", C.c_double), ("t_in", C.c_double),
+        ("thermal_max_iters", C.c_int32), ("thermal_pad", C.c_int32),
+        ("thermal_rel_tol", C.c_double), ("thermal_abs_tol", C.c_double),
+        ("thermal_dt", C.c_double),
     ]
 
 
@@ -63,6 +69,10 @@ class KofmStats(C.Structure):
         ("steps_per_lb", C.c_int32), ("time_since_change", C.c_int32),
         ("dt", C.c_double), ("omega_rel_res", C.c_double), ("k_rel_res", C.c_double),
         ("steps", C.c_int64), ("solver_passes", C.c_int32), ("phase", C.c_int32),
+        ("thermal_iters", C.c_int32), ("thermal_checks", C.c_int32),
+        ("thermal_solves", C.c_int32), ("thermal_resets", C.c_int32),
+        ("thermal_steps_per_lb", C.c_int32), ("thermal_time_since_change", C.c_int32),
+        ("thermal_dt", C.c_double), ("thermal_residual", C.c_double),
     ]
 
 
@@ -98,6 +108,10 @@ SIGNATURES = {
     "kofm_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
     "kofm_batch_step": (C.c_int, [_vp, C.c_int32]),
     "kofm_batch_destroy": (C.c_int, [_vp]),
+    "kofm_set_temperature": (C.c_int, [_vp, _dp]),
+    "kofm_get_temperature": (C.c_int, [_vp, _dp]),
+    "kofm_set_thermal_geometry": (C.c_int, [_vp, _dp]),
+    "kofm_thermal_update": (C.c_int, [_vp]),
 }
 
 _LIB = None

@@ -8,6 +8,7 @@
 #include "kofm_lb.cuh"
 #include "kofm_komega.cuh"
 #include "kofm_gmres.cuh"
+#include "kofm_thermal.cuh"
 
 #include <cuda_runtime.h>
 #include <cstdio>
@@ -18,7 +19,9 @@
 
 using namespace kofm;
 
+struct kofm_ctx;
 namespace kofm {
+int th_solver_alloc(kofm_ctx* c);
 int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned int** bar,
                     int* nblocks, int P, int ny, int K, int dev, int max_blocks);
 void ko_system_free(KoSystem* s);
@@ -93,6 +96,30 @@ struct kofm_ctx {
     double* shear_bl_w = nullptr;     // [n_bl][4]
     double* shear_bl_tau = nullptr;   // [n_bl]
     int shear_n = 0, shear_nbl = 0;
+
+    // thermal implicit FD (kofm_thermal_*)
+    double* T = nullptr;              // [D] temperature (tempArray), FP64
+    double* Tprev = nullptr;          // [D] tempPrev (restored on a dt halving)
+    double* tb = nullptr;             // [D] right-hand side, then the residual
+    double* tr0 = nullptr;            // [D] r0hat
+    double* tp[2] = {nullptr, nullptr};
+    double* tv[2] = {nullptr, nullptr};
+    double* ts = nullptr;
+    double* tt = nullptr;
+    double* tcoef = nullptr;          // [4 x D] interleaved E, W, N, S
+    int32_t* dxrec0_idx = nullptr;    // per-node dXArr0 record (-1: all 1)
+    DxRecord* dxrec0 = nullptr;
+    bool have_dx0 = false;            // kofm_set_thermal_geometry was called
+    bool have_temp = false;
+    ThermalCtl* tctl = nullptr;
+    ThermalCtl* h_tctl = nullptr;     // pinned mirror
+    double* tpart = nullptr;
+    unsigned int* tbar = nullptr;
+    int th_blocks = 0;
+    int th_steps_per_lb = 1;
+    int th_time_since_change = 0;
+    double th_dt = 1.0;
+    long long time_n = 0;             // p.TimeN of the step loop
 };
 
 namespace {
@@ -329,8 +356,8 @@ __device__ __forceinline__ double red_init() {
     return OP == KOFM_OP_SUM ? 0.0 : (OP == KOFM_OP_MIN ? 1.0e308 : -1.0e308);
 }
 
-template <int OP>
-__global__ void k_reduce_field(const float* __restrict__ v, long long nnodes, int P, int nxf,
+template <int OP, typename T = float>
+__global__ void k_reduce_field(const T* __restrict__ v, long long nnodes, int P, int nxf,
                                double* __restrict__ part) {
     __shared__ double sh[32];
     const long long s = (long long)((double)blockIdx.x * nnodes / gridDim.x);
@@ -407,6 +434,11 @@ int validate_desc(const kofm_desc* d) {
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
     if (d->solver_max_blocks < 0) return KOFM_ERR_LOADING_PARAMS;
+    if (d->use_thermal) {
+        if (d->thermal_every < 1 || d->thermal_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
+        if (!(d->pr_number > 0.0) || !(d->pr_turb_number > 0.0) || !(d->thermal_dt > 0.0))
+            return KOFM_ERR_LOADING_PARAMS;
+    }
     return KOFM_OK;
 }
 
@@ -455,6 +487,16 @@ int kofm_desc_default(kofm_desc* d) {
     d->komega_abs_tol = 1.0e-7;   // KOMEGA_MAX_ABS_TOL
     d->komega_dt = 1.0;           // p.dTlb
     d->komega_full_cycle = 0;     // end each cycle at its first truncation
+    d->use_thermal = 0;
+    d->thermal_every = 1;         // LB_STEPS_PER_FD
+    d->pr_number = 0.708;         // PR_NUMBER
+    d->pr_turb_number = 0.9;      // PR_TURB_NUMBER
+    d->alpha_foul = 0.0;          // no fouling layer
+    d->t_in = 2.0;                // TFD_X_IN
+    d->thermal_max_iters = 1000;  // THERMAL_MAX_ITERS
+    d->thermal_rel_tol = 1.0e-4;  // THERMAL_MAX_REL_TOL
+    d->thermal_abs_tol = 1.0e-7;  // THERMAL_MAX_ABS_TOL
+    d->thermal_dt = 1.0;          // dTtfd = tfdSteps
     return KOFM_OK;
 }
 
@@ -466,12 +508,15 @@ int kofm_destroy(kofm_ctx* c) {
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
                     c->gpart, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
-                    c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau};
+                    c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
+                    c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tt, c->tcoef,
+                    c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->h_tctl) cudaFreeHost(c->h_tctl);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return KOFM_OK;
@@ -542,6 +587,23 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
             return KOFM_ERR_BUFFER_ALLOCATION;
         }
     }
+    if (d->use_thermal) {
+        ALLOC(c->T, D);
+        ALLOC(c->Tprev, D);
+        ALLOC(c->tb, D);
+        ALLOC(c->tr0, D);
+        for (int b = 0; b < 2; ++b) { ALLOC(c->tp[b], D); ALLOC(c->tv[b], D); }
+        ALLOC(c->ts, D);
+        ALLOC(c->tt, D);
+        ALLOC(c->tcoef, 4 * D);
+        ALLOC(c->dxrec0_idx, D);
+        int s3 = th_solver_alloc(c);
+        if (s3) { kofm_destroy(c); return s3; }
+        c->th_dt = d->thermal_dt;
+        c->th_steps_per_lb = (int)(1.0 / d->thermal_dt);
+        if (c->th_steps_per_lb < 1) c->th_steps_per_lb = 1;
+        cudaMemset(c->dxrec0_idx, 0xff, D * sizeof(int32_t));
+    }
 #undef ALLOC
     if (cudaMallocHost(&c->h_red, 64 * sizeof(double)) != cudaSuccess) {
         kofm_destroy(c);
@@ -564,6 +626,7 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     if (!c || !ntype) return KOFM_ERR_INVALID_ARG;
     const kofm_desc& d = c->desc;
     if (d.use_komega && (!wallD || !dX4)) return KOFM_ERR_INVALID_ARG;
+    if (d.use_thermal && !dX4) return KOFM_ERR_INVALID_ARG;
     if (n_ibb < 0 || (n_ibb > 0 && (!ibb_idx || !ibb_q))) return KOFM_ERR_INVALID_ARG;
     cudaSetDevice(c->dev);
     const int nx = d.nx, nxf = d.nx_full, ny = d.ny, P = c->P;
@@ -599,14 +662,17 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     std::vector<int32_t> dxi((size_t)c->D, -1);
     std::vector<DxRecord> dxr;
     std::vector<float> wd;
-    if (d.use_komega) {
-        wd.assign((size_t)c->D, 0.f);
+    if (d.use_komega || d.use_thermal) {
+        if (d.use_komega) wd.assign((size_t)c->D, 0.f);
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
                 const long long h = (long long)y * nxf + x;
                 const size_t node = (size_t)y * P + x;
-                wd[node] = (float)wallD[h];
-                if ((uint16_t)ntype[h] & M_SOLID) continue;
+                if (d.use_komega) wd[node] = (float)wallD[h];
+                // records for the LB-fluid nodes (k-omega rows) and, with the
+                // thermal update, for the fouling-layer nodes of its rows
+                const int tt = (uint16_t)ntype[h];
+                if ((tt & M_SOLID) && !(d.use_thermal && !(tt & M0_SOLID))) continue;
                 DxRecord r;
                 bool unit = true;
                 for (int k = 0; k < 4; ++k) {
@@ -876,9 +942,11 @@ int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
         case KOFM_FIELD_OMEGA: v = c->O; break;
         case KOFM_FIELD_NUT: v = c->nut; break;
         case KOFM_FIELD_WALL_SHEAR: break;
+        case KOFM_FIELD_TEMP: break;
         default: return KOFM_ERR_INVALID_ARG;
     }
-    if (field != KOFM_FIELD_WALL_SHEAR && !v) return KOFM_ERR_STATE;
+    if (field == KOFM_FIELD_TEMP && !c->T) return KOFM_ERR_STATE;
+    if (field != KOFM_FIELD_WALL_SHEAR && field != KOFM_FIELD_TEMP && !v) return KOFM_ERR_STATE;
     if (op < KOFM_OP_SUM || op > KOFM_OP_MAX) return KOFM_ERR_INVALID_ARG;
     cudaSetDevice(c->dev);
     const long long n = c->D;
@@ -886,6 +954,13 @@ int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
         if (!d.use_komega || op != KOFM_OP_SUM) return KOFM_ERR_INVALID_ARG;
         k_wall_shear<<<RED_BLOCKS, 256, 0, c->stream>>>(c->ntype, c->rho, c->nut, c->S, n, c->D, c->P, d.nx, d.mu, c->red_partials);
         k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    } else if (field == KOFM_FIELD_TEMP) {
+        if (op == KOFM_OP_SUM) k_reduce_field<KOFM_OP_SUM, double><<<RED_BLOCKS, 256, 0, c->stream>>>(c->T, n, c->P, d.nx_full, c->red_partials);
+        else if (op == KOFM_OP_MIN) k_reduce_field<KOFM_OP_MIN, double><<<RED_BLOCKS, 256, 0, c->stream>>>(c->T, n, c->P, d.nx_full, c->red_partials);
+        else k_reduce_field<KOFM_OP_MAX, double><<<RED_BLOCKS, 256, 0, c->stream>>>(c->T, n, c->P, d.nx_full, c->red_partials);
+        if (op == KOFM_OP_SUM) k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+        else if (op == KOFM_OP_MIN) k_reduce_final<KOFM_OP_MIN><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+        else k_reduce_final<KOFM_OP_MAX><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     } else if (op == KOFM_OP_SUM) {
         k_reduce_field<KOFM_OP_SUM><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
         k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
@@ -919,6 +994,9 @@ int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
     c->stats.steps_per_lb = c->steps_per_lb;
     c->stats.time_since_change = c->time_since_change;
     c->stats.dt = c->dt;
+    c->stats.thermal_steps_per_lb = c->th_steps_per_lb;
+    c->stats.thermal_time_since_change = c->th_time_since_change;
+    c->stats.thermal_dt = c->th_dt;
     *out = c->stats;
     return KOFM_OK;
 }
@@ -929,3 +1007,5 @@ int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
 #include "kofm_komega_api.inc"
 // batched lattices (CUDA graph over several contexts)
 #include "kofm_batch.inc"
+// thermal implicit FD
+#include "kofm_thermal_api.inc"

@@ -19,7 +19,10 @@ namespace kofm {
 // nType bits (reference Kernels/Heading.cl:223-251).
 constexpr int M_SOLID = 0x0001;
 constexpr int M_FLUID = 0x0002;
+constexpr int M0_SOLID = 0x0004;         // wall of the unfouled geometry
+constexpr int M0_FLUID = 0x0008;
 constexpr int SOLID_BOUNDARY = 0x0010;
+constexpr int SOLID_BOUNDARY0 = 0x0020;  // boundary of the unfouled wall
 constexpr int E_BOUND = 0x0100, W_BOUND = 0x0200, N_BOUND = 0x0400, S_BOUND = 0x0800;
 constexpr int NE_BOUND = 0x1000, SW_BOUND = 0x2000, SE_BOUND = 0x4000, NW_BOUND = 0x8000;
 constexpr int NESW_BOUNDARY = 0x0F00;

@@ -1,0 +1,361 @@
+// kofm_thermal.cuh - the thermal implicit finite-difference update
+// (clVariablesFD::Solve, clVariablesFD.h:343-358) on the device (sm_100a).
+//
+//  * thermal_assemble_kernel: Update_T_Coeffs_Implicit (tfdKernels.cl:122-279)
+//    fused with the sparsity pattern of the reference's non-periodic CSR_Inds
+//    (SparseMatrix.cpp:57-209): one thread per node writes the four
+//    off-diagonals (divided by the diagonal, which becomes 1) in the
+//    interleaved layout ilv(4, q, g) and the right-hand side.
+//  * bicgstab_kernel: BiCGStabSolver::solve (BiCGStabSolver.cpp:628-723) as
+//    the reference enqueues it, in ONE cooperative launch.  The reference
+//    never reduces omega (its omegaDotSqr kernels are built but not run), so
+//    omega stays at the 1 its scalar buffer is filled with and the step-f9
+//    reduction recomputes the same alpha; the convergence checks use L1 norms
+//    (the "Norm" reduction, BiCGStabGenerator.cpp:259-262) against ||b||_1,
+//    and the NaN / tenfold-growth test of reduceAndCheckConvergence
+//    (BiCGStabSolver.cpp:509-545) ends the solve for the host's dt halving.
+//    Each iteration is three grid passes instead of the reference's ~25
+//    kernels and 4 host reads:
+//      B: p = r + beta (p - omega v) on the fly at the node and its four
+//         neighbours, v = A p, <v, r0>            -> alpha
+//      C: s = r - alpha v on the fly, t = A s, ||s||_1  -> first check
+//      D: x = (x + alpha p) + omega s, r = s - omega t, ||r||_1, <r, r0>
+//                                                  -> second check, beta
+//    p and v are double-buffered (a pass reads the old values at the
+//    neighbours while it writes the new ones).  Grid barriers, partial sums
+//    and the last-block serial section are those of the k-omega solver.
+#pragma once
+#include "kofm_gmres.cuh"
+
+namespace kofm {
+
+// row kinds of the thermal system (CSR_Inds with M0_SOLID, M0_FLUID,
+// SOLID_BOUNDARY0; clVariablesFD.h:40)
+enum ThRow : int { TH_EMPTY = 0, TH_DIAG = 1, TH_FULL = 2 };
+
+__device__ __forceinline__ int th_row(int t, int x, int nx) {
+    if (x >= nx) return TH_EMPTY;
+    if (t & M0_SOLID) return (t & SOLID_BOUNDARY0) ? TH_DIAG : TH_EMPTY;
+    return TH_FULL;
+}
+
+struct ThermalAsm {
+    const int16_t* ntype;
+    const int32_t* dxidx;     // per-node link-fraction record (-1: all 1)
+    const DxRecord* dxrec;
+    const float* ux;
+    const float* uy;
+    const float* nut;         // nullptr without k-omega
+    const double* T;
+    double* coef;             // [4 x D] E, W, N, S (interleaved)
+    double* b;                // [D]
+    int nx, ny, P;
+    double alpha_fluid, alpha_foul, prt_inv, t_in, dt;
+};
+
+// Update_T_Coeffs_Implicit for node (x, y); rows of unfouled-wall nodes and
+// padding columns are left as they are.
+__global__ void thermal_assemble_kernel(const ThermalAsm p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= p.nx || y >= p.ny) return;
+    const long long g = (long long)y * p.P + x;
+    const int t = (uint16_t)p.ntype[g];
+    if (t & M0_SOLID) return;
+    double dx[4] = {1.0, 1.0, 1.0, 1.0};
+    const int r = p.dxidx[g];
+    if (r >= 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dx[k] = p.dxrec[r].dx[k];
+    }
+    const double dxe = fmax(dx[0], 0.1), dxw = fmax(dx[1], 0.1), dxc = fmax(dxe + dxw, 0.1);
+    const double dyn = fmax(dx[2], 0.1), dys = fmax(dx[3], 0.1), dyc = fmax(dyn + dys, 0.1);
+    double dXe = dxw / (dxe * dxc), dXw = -dxe / (dxw * dxc), dXc = (dxe - dxw) / (dxe * dxw);
+    double dYn = dys / (dyn * dyc), dYs = -dyn / (dys * dyc), dYc = (dyn - dys) / (dyn * dys);
+    const double dX2e = 2. / (dxe * dxc), dX2w = 2. / (dxw * dxc), dX2c = -2. / (dxe * dxw);
+    const double dY2n = 2. / (dyn * dyc), dY2s = 2. / (dys * dyc), dY2c = -2. / (dyn * dys);
+    if (fabs(dXc) > 10.) { dXe = 1.0 / dxc; dXw = -1.0 / dxc; dXc = 0.0; }
+    if (fabs(dYn) > 10.) { dYn = 1.0 / dyc; dYs = -1.0 / dyc; dYc = 0.0; }
+    double alpha = (t & M_SOLID) ? p.alpha_foul : p.alpha_fluid;
+    const long long row = (long long)y * p.P;
+    const long long gw = row + (x > 0 ? x - 1 : p.nx - 1), ge = row + (x < p.nx - 1 ? x + 1 : 0);
+    double nu_c = 0.0, nu_e = 0.0, nu_w = 0.0, nu_n = 0.0, nu_s = 0.0;
+    if (p.nut) {
+        nu_c = p.nut[g]; nu_e = p.nut[ge]; nu_w = p.nut[gw];
+        nu_n = p.nut[g + p.P]; nu_s = p.nut[g - p.P];
+    }
+    const double alphat = nu_c * p.prt_inv;
+    const double Jx = (double)p.ux[g] - (p.prt_inv * (dXe * nu_e + dXw * nu_w + dXc * alphat));
+    const double Jy = (double)p.uy[g] - (p.prt_inv * (dYn * nu_n + dYs * nu_s + dYc * alphat));
+    alpha += alphat;
+    double Tsrc = fmin(fmax(0.0, p.T[g]), p.t_in);
+    double Cc = 1. + p.dt * (Jx * dXc + Jy * dYc - alpha * (dX2c + dY2c));
+    const double Sc = p.dt * (Jy * dYs - alpha * dY2s);
+    const double Wc = p.dt * (Jx * dXw - alpha * dX2w);
+    if (x == 0) Tsrc -= p.t_in * Wc;           // inlet: fixed temperature
+    const double Ec = p.dt * (Jx * dXe - alpha * dX2e);
+    if (x == p.nx - 1) Cc += Ec;                // outlet: zero gradient
+    Cc = 1. / Cc;
+    p.coef[ilv(4, 0, g)] = x < p.nx - 1 ? Ec * Cc : 0.0;
+    p.coef[ilv(4, 1, g)] = x > 0 ? Wc * Cc : 0.0;
+    p.coef[ilv(4, 2, g)] = p.dt * (Jy * dYn - alpha * dY2n) * Cc;
+    p.coef[ilv(4, 3, g)] = Sc * Cc;
+    p.b[g] = Tsrc * Cc;
+}
+
+// ---- BiCGStab -------------------------------------------------------------------
+struct ThermalCtl {
+    int error;        // 1: barrier timeout
+    int state;        // TH_RUNNING / TH_CONV / TH_RESET / TH_MAXIT / TH_TRIVIAL
+    int iter;         // iterCount
+    int checks;
+    int first;        // next check sets the initial residual
+    int exit_after_c; // stopped at the check after the s step (x += alpha p pending)
+    int passes;
+    int pad;
+    double normb, rho, alpha, omega, beta, avg, residual, initial_residual;
+};
+enum ThState : int { TH_RUNNING = 0, TH_CONV = 1, TH_RESET = 2, TH_MAXIT = 3, TH_TRIVIAL = 4 };
+
+struct ThermalArgs {
+    const int16_t* ntype;
+    const double* coef;
+    double* x;                // T
+    double* b;                // right-hand side, then the residual r (as the reference)
+    double* r0;
+    double* p[2];
+    double* v[2];
+    double* s;
+    double* t;
+    ThermalCtl* ctl;
+    double* part;             // [GM_SLOTS][gridDim.x]
+    GridBarrier* bar;
+    int nx, ny, P;
+    long long D;
+    int max_iters;
+    double rel_tol, abs_tol;
+    int reset_flag;
+    long long spin_limit;
+};
+
+enum ThSerial : int { TS_NONE = 0, TS_NORMB, TS_RHO0, TS_ALPHA, TS_CHECK1, TS_CHECK2 };
+
+// reduceAndCheckConvergence on the summed L1 norm of the current residual
+__device__ void th_check(const ThermalArgs& a, ThermalCtl& C, double l1) {
+    const double res = l1 / C.normb;
+    C.checks += 1;
+    C.residual = res;
+    if (C.first) C.initial_residual = res;
+    C.first = 0;
+    if (a.reset_flag && (isnan(res) || (C.iter > 1 && res > 10. * C.avg))) { C.state = TH_RESET; return; }
+    if (res <= a.rel_tol || res <= a.abs_tol * C.initial_residual) { C.state = TH_CONV; return; }
+    C.avg = res;
+}
+
+__device__ void th_serial(const ThermalArgs& a, int kind, int nblocks) {
+    __shared__ double tot[2];
+    const int warp = threadIdx.x >> 5;
+    const int used = kind == TS_CHECK2 ? 2 : 1;
+    if (warp < used) {
+        const double v = sum_slot_warp(a.part, nblocks, warp);
+        if ((threadIdx.x & 31) == 0) tot[warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ThermalCtl C;
+        {
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(a.ctl);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&C);
+            for (int i = 0; i < (int)(sizeof(ThermalCtl) / 8); ++i) dst[i] = __ldcg(src + i);
+        }
+        switch (kind) {
+            case TS_NORMB:
+                C.normb = tot[0];
+                if (C.normb <= 1.0e-16) C.state = TH_TRIVIAL;
+                break;
+            case TS_RHO0: C.rho = tot[0]; break;
+            case TS_ALPHA: C.alpha = C.rho / tot[0]; break;
+            case TS_CHECK1:
+                th_check(a, C, tot[0]);
+                if (C.state != TH_RUNNING) C.exit_after_c = 1;
+                break;
+            case TS_CHECK2:
+                th_check(a, C, tot[0]);
+                if (C.state == TH_RUNNING) {
+                    C.iter += 1;
+                    if (C.iter >= a.max_iters) {
+                        C.state = TH_MAXIT;
+                    } else {  // Sum_Rho_Calc_Beta (BiCGStabGenerator.cpp:128-142)
+                        const double rho_new = tot[1];
+                        C.beta = (rho_new / C.rho) * (C.alpha / C.omega);
+                        C.rho = rho_new;
+                    }
+                }
+                break;
+            default: break;
+        }
+        C.passes += 1;
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&C);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(a.ctl);
+        for (int i = 0; i < (int)(sizeof(ThermalCtl) / 8); ++i) __stcg(dst + i, src[i]);
+    }
+}
+
+// Bounded grid barrier; the last block to arrive runs the serial section.
+__device__ bool th_sync(const ThermalArgs& a, int kind) {
+    __shared__ int s_last;
+    __shared__ unsigned int s_gen;
+    const int nblocks = gridDim.x;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_gen = ld_acquire_u32(&a.bar->gen);
+        const unsigned int ticket = atomicAdd(&a.bar->count, 1u);
+        s_last = (ticket == (unsigned int)nblocks - 1u);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (kind != TS_NONE) th_serial(a, kind, nblocks);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicExch(&a.bar->count, 0u);
+            __threadfence();
+            atomicAdd(&a.bar->gen, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire_u32(&a.bar->gen) == s_gen) {
+            if (++it > a.spin_limit || ldc(&a.ctl->error)) {
+                atomicExch(&a.ctl->error, 1);
+                break;
+            }
+            __nanosleep(100);
+        }
+    }
+    __syncthreads();
+    return ldc(&a.ctl->error) == 0;
+}
+
+// One row of A times a vector whose entries come from `val(node)` (CSR
+// order of an interior row: S, W, C, E, N).
+template <typename F>
+__device__ __forceinline__ double th_apply(const ThermalArgs& a, int kind, long long g, int x,
+                                           F&& val) {
+    if (kind == TH_EMPTY) return 0.0;
+    if (kind == TH_DIAG) return val(g);
+    double acc = __ldg(a.coef + ilv(4, 3, g)) * val(g - a.P);
+    if (x > 0) acc += __ldg(a.coef + ilv(4, 1, g)) * val(g - 1);
+    acc += val(g);
+    if (x < a.nx - 1) acc += __ldg(a.coef + ilv(4, 0, g)) * val(g + 1);
+    acc += __ldg(a.coef + ilv(4, 2, g)) * val(g + a.P);
+    return acc;
+}
+
+__global__ void __launch_bounds__(GM_THREADS, 2) bicgstab_kernel(const ThermalArgs a) {
+    const long long stride = (long long)gridDim.x * GM_THREADS;
+    const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
+    auto node_x = [&](long long g) { return (int)(g % a.P); };
+    auto kind_of = [&](long long g, int x) { return th_row((uint16_t)a.ntype[g], x, a.nx); };
+
+    // ---- step 1: ||b||_1 --------------------------------------------------------
+    {
+        double acc[1] = {0.0};
+        for (long long g = t0; g < a.D; g += stride) acc[0] += fabs(__ldcg(a.b + g));
+        block_reduce_slots<1>(acc, 1, a.part, 0);
+    }
+    if (!th_sync(a, TS_NORMB)) return;
+    if (ldc(&a.ctl->state) == TH_TRIVIAL) {
+        for (long long g = t0; g < a.D; g += stride) a.x[g] = __ldcg(a.b + g);
+        return;
+    }
+    // ---- steps 2-4: r = b - A x; r0 = p = r; rho = <r, r> ------------------------
+    {
+        double acc[1] = {0.0};
+        for (long long g = t0; g < a.D; g += stride) {
+            const int x = node_x(g);
+            const double ax = th_apply(a, kind_of(g, x), g, x, [&](long long n) { return __ldcg(a.x + n); });
+            const double r = __ldcg(a.b + g) - ax;
+            __stcg(a.b + g, r);
+            __stcg(a.r0 + g, r);
+            __stcg(a.p[0] + g, r);
+            acc[0] += r * r;
+        }
+        block_reduce_slots<1>(acc, 1, a.part, 0);
+    }
+    if (!th_sync(a, TS_RHO0)) return;
+
+    int pc = 0, vc = 0;  // current p and v buffers
+    for (int it = 0; it < a.max_iters; ++it) {
+        // ---- B: p = r + beta (p - omega v) (iteration 0: p), v = A p, <v, r0> ----
+        {
+            const double beta = ldc(&a.ctl->beta), omega = ldc(&a.ctl->omega);
+            const double* pold = a.p[pc];
+            const double* vold = a.v[vc];
+            double* pnew = a.p[pc ^ 1];
+            double* vnew = a.v[vc ^ 1];
+            auto pval = [&](long long n) -> double {
+                return it == 0 ? __ldcg(pold + n)
+                               : __ldcg(a.b + n) + beta * (__ldcg(pold + n) - omega * __ldcg(vold + n));
+            };
+            double acc[1] = {0.0};
+            for (long long g = t0; g < a.D; g += stride) {
+                const int x = node_x(g);
+                const double v = th_apply(a, kind_of(g, x), g, x, pval);
+                __stcg(pnew + g, pval(g));
+                __stcg(vnew + g, v);
+                acc[0] += v * __ldcg(a.r0 + g);
+            }
+            block_reduce_slots<1>(acc, 1, a.part, 0);
+        }
+        pc ^= 1;
+        vc ^= 1;
+        if (!th_sync(a, TS_ALPHA)) return;
+        // ---- C: s = r - alpha v, t = A s, ||s||_1 ----------------------------------
+        const double alpha = ldc(&a.ctl->alpha);
+        {
+            const double* v = a.v[vc];
+            auto sval = [&](long long n) -> double { return __ldcg(a.b + n) - alpha * __ldcg(v + n); };
+            double acc[1] = {0.0};
+            for (long long g = t0; g < a.D; g += stride) {
+                const int x = node_x(g);
+                const double tv = th_apply(a, kind_of(g, x), g, x, sval);
+                const double s = sval(g);
+                __stcg(a.s + g, s);
+                __stcg(a.t + g, tv);
+                acc[0] += fabs(s);
+            }
+            block_reduce_slots<1>(acc, 1, a.part, 0);
+        }
+        if (!th_sync(a, TS_CHECK1)) return;
+        if (ldc(&a.ctl->state) != TH_RUNNING) {
+            // shCalc's x += alpha p and r = s stand (BiCGStabSolver.cpp:694-701)
+            for (long long g = t0; g < a.D; g += stride) {
+                a.x[g] = __ldcg(a.x + g) + alpha * __ldcg(a.p[pc] + g);
+                __stcg(a.b + g, __ldcg(a.s + g));
+            }
+            return;
+        }
+        // ---- D: x = (x + alpha p) + omega s, r = s - omega t, ||r||_1, <r, r0> -----
+        {
+            const double omega = ldc(&a.ctl->omega);
+            double acc[2] = {0.0, 0.0};
+            for (long long g = t0; g < a.D; g += stride) {
+                const double s = __ldcg(a.s + g);
+                const double xh = __ldcg(a.x + g) + alpha * __ldcg(a.p[pc] + g);
+                __stcg(a.x + g, xh + omega * s);
+                const double r = s - omega * __ldcg(a.t + g);
+                __stcg(a.b + g, r);
+                acc[0] += fabs(r);
+                acc[1] += r * __ldcg(a.r0 + g);
+            }
+            block_reduce_slots<2>(acc, 2, a.part, 0);
+        }
+        if (!th_sync(a, TS_CHECK2)) return;
+        if (ldc(&a.ctl->state) != TH_RUNNING) return;
+    }
+}
+
+}  // namespace kofm

@@ -202,6 +202,16 @@ def equilibrium_state(ch: Channel, rho=1.0, ux=0.0, uy=0.0) -> np.ndarray:
     return f.reshape(9, -1).ravel()
 
 
+def temperature_field(ch: Channel, t0: float = 0.5) -> np.ndarray:
+    """tempArray start: Tinitial (TFD_INI_TEMP, 0.5) on M0_FLUID nodes, 0
+    elsewhere (tempArray.fillByNodeType, clVariablesFD.cpp:236-239)."""
+    m = ch.ntype.astype(np.int32) & 0xFFFF
+    T = np.where((m & M0_FLUID) != 0, t0, 0.0)
+    T = T.reshape(ch.ny, ch.nx_full)
+    T[:, ch.nx:] = 0.0
+    return T.ravel()
+
+
 def komega_fields(ch: Channel, k0: float, omega0: float):
     """k, omega, nu_t = k/omega on fluid nodes (fillByNodeType, kOmega.cpp:567-569)."""
     fl = ch.fluid_mask().ravel()

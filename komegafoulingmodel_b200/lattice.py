@@ -84,6 +84,25 @@ class Lattice:
             self._ctx, _ptr(f), _ptr(k), _ptr(o), _ptr(nut), _ptr(s)))
         return f, k, o, nut, s
 
+    def set_temperature(self, T):
+        """tempArray in (host layout, FP64; kofm_set_temperature)."""
+        T = np.ascontiguousarray(T, np.float64)
+        check("kofm_set_temperature", self.lib.kofm_set_temperature(self._ctx, _ptr(T)))
+
+    def get_temperature(self):
+        T = np.empty(self.n)
+        check("kofm_get_temperature", self.lib.kofm_get_temperature(self._ctx, _ptr(T)))
+        return T
+
+    def set_thermal_geometry(self, dX0):
+        """Link fractions of the unfouled walls (dXArr0) for the thermal rows."""
+        dX0 = np.ascontiguousarray(dX0, np.float64)
+        check("kofm_set_thermal_geometry", self.lib.kofm_set_thermal_geometry(self._ctx, _ptr(dX0)))
+
+    def thermal_update(self):
+        """One clVariablesFD::Solve (kofm_thermal_update)."""
+        check("kofm_thermal_update", self.lib.kofm_thermal_update(self._ctx))
+
     def set_shear(self, sh):
         """Uploads a shear.ShearSetup (kofm_set_shear)."""
         nodes = np.ascontiguousarray(sh.nodes, np.int32)

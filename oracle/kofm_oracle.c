@@ -693,3 +693,258 @@ void orc_wall_shear_links(const double* tau_nodes, const int32_t* sind, const do
         out[b] = acc;
     }
 }
+
+/* ======================================================================== */
+/* Thermal implicit finite differences (clVariablesFD::Solve,
+ * clVariablesFD.h:343-358; Update_T_Coeffs_Implicit, tfdKernels.cl:122-279;
+ * BiCGStabSolver::solve, BiCGStabSolver.cpp:628-723).                      */
+
+/* CSR_Inds with flags (M0_SOLID, M0_FLUID, SOLID_BOUNDARY0) and no periodic
+ * wrap (SparseMatrix.cpp:57-209, SparseMatrix.h:120-128; clVariablesFD.h:40):
+ * rows of unfouled-wall boundary nodes hold only the diagonal, other wall
+ * rows are empty, rows of the thermal domain (fluid and fouling layer) hold
+ * S, W, C, E, N with the neighbours outside the lattice (x < 0, x >= nx)
+ * left out. */
+static int csr_th_neigh_ok(const orc_cfg* c, const int16_t* map, int i, int j) {
+    if (i < 0 || i >= c->nx || j < 0 || j >= c->ny) return 0;
+    const int t = (uint16_t)map[i + (long)c->nxf * j];
+    return (t & (ORC_SOLID_BOUNDARY0 | ORC_M0_FLUID)) != 0;
+}
+
+int orc_csr_build_thermal(const orc_cfg* c, const int16_t* map, int32_t* IA,
+                          int32_t* JA, int32_t* ind) {
+    const int nx = c->nx, nxf = c->nxf, ny = c->ny;
+    const long n = (long)nxf * ny;
+    enum { iC = 0, iE = 1, iW = 2, iN = 3, iS = 4 };
+    int nnz = 0;
+    if (IA) IA[0] = 0;
+    if (ind) for (long t = 0; t < 5 * n; ++t) ind[t] = -1;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nxf; ++i) {
+            const long g = i + (long)nxf * j;
+            if (i < nx) {
+                const int t = (uint16_t)map[g];
+                if (t & ORC_M0_SOLID) {
+                    if (t & ORC_SOLID_BOUNDARY0) {
+                        if (JA) JA[nnz] = (int32_t)g;
+                        if (ind) ind[g + n * iC] = nnz;
+                        ++nnz;
+                    }
+                } else {
+                    const long nb[5] = {g, g + 1, g - 1, g + nxf, g - nxf};
+                    const int ok[5] = {1, csr_th_neigh_ok(c, map, i + 1, j),
+                                       csr_th_neigh_ok(c, map, i - 1, j),
+                                       csr_th_neigh_ok(c, map, i, j + 1),
+                                       csr_th_neigh_ok(c, map, i, j - 1)};
+                    const int order[5] = {iS, iW, iC, iE, iN};
+                    for (int k = 0; k < 5; ++k) {
+                        const int d = order[k];
+                        if (!ok[d]) continue;
+                        if (JA) JA[nnz] = (int32_t)nb[d];
+                        if (ind) ind[g + n * d] = nnz;
+                        ++nnz;
+                    }
+                }
+            }
+            if (IA) IA[g + 1] = nnz;
+        }
+    return nnz;
+}
+
+void orc_csr_fill_solid_boundary_thermal(const orc_cfg* c, const int16_t* map,
+                                         const int32_t* ind, double* A) {
+    for (int j = 0; j < c->ny; ++j)
+        for (int i = 0; i < c->nx; ++i) {
+            const long g = i + (long)c->nxf * j;
+            const int t = (uint16_t)map[g];
+            if ((t & ORC_M0_SOLID) && (t & ORC_SOLID_BOUNDARY0)) A[ind[g]] = 1.;
+        }
+}
+
+/* Update_T_Coeffs_Implicit (tfdKernels.cl:122-279): backward-Euler rows of
+ * the advection-diffusion equation of T with non-uniform 3-point differences
+ * from the link fractions dX0 (floored at 0.1), the advecting flux
+ * J = u - grad(nu_t)/Pr_t, diffusivity alpha (+ nu_t/Pr_t), fixed inlet
+ * temperature on x = 0 (its W term moved to the right-hand side) and a
+ * zero-gradient outlet on x = nx-1 (its E term added to the diagonal); every
+ * row is divided by its diagonal.  Rows of unfouled-wall nodes are left as
+ * they are. */
+void orc_thermal_coeffs(const orc_cfg* c, const orc_thermal_cfg* th, const int32_t* ind,
+                        const int16_t* map, const double* dX0, double* A, double* b,
+                        const double* T, const double* ux, const double* uy,
+                        const double* nut, double dt) {
+    const int nx = c->nx, nxf = c->nxf, ny = c->ny;
+    const long D = (long)nxf * ny;
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const long g = i + (long)nxf * j;
+            const int t = (uint16_t)map[g];
+            if (t & ORC_M0_SOLID) continue;
+            const double dxe = dmax(dX0[g], 0.1), dxw = dmax(dX0[g + D], 0.1);
+            const double dxc = dmax(dxe + dxw, 0.1);
+            const double dyn = dmax(dX0[g + 2 * D], 0.1), dys = dmax(dX0[g + 3 * D], 0.1);
+            const double dyc = dmax(dyn + dys, 0.1);
+            double dXe = dxw / (dxe * dxc), dXw = -dxe / (dxw * dxc), dXc = (dxe - dxw) / (dxe * dxw);
+            double dYn = dys / (dyn * dyc), dYs = -dyn / (dys * dyc), dYc = (dyn - dys) / (dyn * dys);
+            const double dX2e = 2. / (dxe * dxc), dX2w = 2. / (dxw * dxc), dX2c = -2. / (dxe * dxw);
+            const double dY2n = 2. / (dyn * dyc), dY2s = 2. / (dys * dyc), dY2c = -2. / (dyn * dys);
+            if (fabs(dXc) > 10.) { dXe = 1.0 / dxc; dXw = -1.0 / dxc; dXc = 0.0; }
+            if (fabs(dYn) > 10.) { dYn = 1.0 / dyc; dYs = -1.0 / dyc; dYc = 0.0; }
+            double alpha = (t & ORC_M_SOLID) ? th->alpha_foul : th->alpha_fluid;
+            const double nu_c = nut ? nut[g] : 0.0;
+            const double alphat = nu_c * th->pr_turb_inv;
+            const long gw = (i > 0 ? -1 : nx - 1) + g;
+            const long ge = (i < nx - 1 ? 1 : 1 - nxf) + g;
+            const double nu_e = nut ? nut[ge] : 0.0, nu_w = nut ? nut[gw] : 0.0;
+            const double nu_n = nut ? nut[g + nxf] : 0.0, nu_s = nut ? nut[g - nxf] : 0.0;
+            const double Jx = ux[g] - (th->pr_turb_inv * (dXe * nu_e + dXw * nu_w + dXc * alphat));
+            const double Jy = uy[g] - (th->pr_turb_inv * (dYn * nu_n + dYs * nu_s + dYc * alphat));
+            alpha += alphat;
+            double Tsrc = dmin(dmax(0.0, T[g]), th->t_in);
+            double Cc = 1. + dt * (Jx * dXc + Jy * dYc - alpha * (dX2c + dY2c));
+            const double Sc = dt * (Jy * dYs - alpha * dY2s);
+            const double Wc = dt * (Jx * dXw - alpha * dX2w);
+            if (i == 0) Tsrc -= th->t_in * Wc;
+            const double Ec = dt * (Jx * dXe - alpha * dX2e);
+            if (i == nx - 1) Cc += Ec;
+            Cc = 1. / Cc;
+            A[ind[g + 4 * D]] = Sc * Cc;
+            if (i > 0) A[ind[g + 2 * D]] = Wc * Cc;
+            if (i < nx - 1) A[ind[g + D]] = Ec * Cc;
+            A[ind[g]] = 1.;
+            A[ind[g + 3 * D]] = dt * (Jy * dYn - alpha * dY2n) * Cc;
+            b[g] = Tsrc * Cc;
+        }
+}
+
+static double sum_abs_chunked(const double* a, long n) {
+    double part[ORC_CHUNKS];
+#pragma omp parallel for schedule(static)
+    for (int cidx = 0; cidx < ORC_CHUNKS; ++cidx) {
+        const long s = (long)((cidx * (double)n) / ORC_CHUNKS);
+        const long e = (long)(((cidx + 1) * (double)n) / ORC_CHUNKS);
+        double acc = 0.;
+        for (long t = s; t < e; ++t) acc += fabs(a[t]);
+        part[cidx] = acc;
+    }
+    double sum = 0.;
+    for (int cidx = 0; cidx < ORC_CHUNKS; ++cidx) sum += part[cidx];
+    return sum;
+}
+
+/* reduceAndCheckConvergence (BiCGStabSolver.cpp:509-545): the residual is
+ * the L1 norm of r over the L1 norm of b ("Norm" reduction,
+ * BiCGStabGenerator.cpp:259-262). */
+static int bicg_check(orc_bicgstab_stats* st, const double* r, long n, double normb,
+                      int first, int iter, double* avg, double rel_tol, double abs_tol,
+                      int reset_flag) {
+    const double res = sum_abs_chunked(r, n) / normb;
+    st->checks++;
+    st->residual = res;
+    if (first) st->initial_residual = res;
+    if (reset_flag && (isnan(res) || (iter > 1 && res > 10. * *avg))) {
+        st->reset = 1;
+        return 1;
+    }
+    if (res <= rel_tol || res <= abs_tol * st->initial_residual) {
+        st->conv = 1;
+        return 1;
+    }
+    *avg = res;
+    return 0;
+}
+
+/* BiCGStabSolver::solve (BiCGStabSolver.cpp:628-723) as the reference
+ * enqueues it.  The scalars start at 1 on every call (scalarBuf.FillBuffer);
+ * omega is never reduced (the omegaDotSqr list is built but not run), so
+ * every "omega" update uses 1; step f9 recomputes alpha from the same
+ * vectors.  b is overwritten with the residual; x holds the initial guess on
+ * entry.  With reset_flag, a NaN residual or one that grew tenfold since the
+ * previous check (after the second iteration) stops the solve with
+ * st->reset = 1 (the resetTimeFunc path). */
+void orc_bicgstab_solve(int n, const int32_t* IA, const int32_t* JA, const double* A,
+                        double* b, double* x, int max_iters, double rel_tol, double abs_tol,
+                        int reset_flag, orc_bicgstab_stats* st) {
+    memset(st, 0, sizeof(*st));
+    double* r0 = (double*)malloc(sizeof(double) * n);
+    double* p = (double*)malloc(sizeof(double) * n);
+    double* v = (double*)malloc(sizeof(double) * n);
+    double* t = (double*)malloc(sizeof(double) * n);
+    double rho = 1., alpha = 1., omega = 1., beta = 1., avg = 0.;
+    const double normb = sum_abs_chunked(b, n);
+    int iter = 0;
+    if (normb <= 1.0e-16) {
+        memcpy(x, b, sizeof(double) * n);
+        st->conv = 1;
+        goto done;
+    }
+    spmv(n, IA, JA, A, x, t);
+    for (int k = 0; k < n; ++k) b[k] -= t[k];
+    memcpy(r0, b, sizeof(double) * n);
+    memcpy(p, b, sizeof(double) * n);
+    rho = dot_chunked(b, b, n);
+    int first = 1;
+    while (iter < max_iters) {
+        if (iter > 0) {
+            const double rho_new = dot_chunked(b, r0, n);
+            beta = (rho_new / rho) * (alpha / omega);
+            rho = rho_new;
+            for (int k = 0; k < n; ++k) p[k] = b[k] + beta * (p[k] - omega * v[k]);
+        }
+        spmv(n, IA, JA, A, p, v);
+        alpha = rho / dot_chunked(v, r0, n);
+        for (int k = 0; k < n; ++k) {
+            x[k] += alpha * p[k];
+            b[k] -= alpha * v[k];
+        }
+        if (bicg_check(st, b, n, normb, first, iter, &avg, rel_tol, abs_tol, reset_flag)) break;
+        first = 0;
+        spmv(n, IA, JA, A, b, t);
+        alpha = rho / dot_chunked(v, r0, n);
+        for (int k = 0; k < n; ++k) {
+            x[k] += omega * b[k];
+            b[k] -= omega * t[k];
+        }
+        if (bicg_check(st, b, n, normb, first, iter, &avg, rel_tol, abs_tol, reset_flag)) break;
+        iter++;
+    }
+done:
+    st->iters = iter;
+    free(r0); free(p); free(v); free(t);
+}
+
+/* clVariablesFD::Solve (clVariablesFD.h:343-358) with halveTimeStep /
+ * doubleTimeStep (clVariablesFD.cpp:202-228): T is saved before the
+ * sub-steps; a reset restores it, doubles the sub-step count and halves dt,
+ * and the sub-step loop continues from its counter's restart. */
+void orc_thermal_solve(const orc_cfg* c, const orc_thermal_cfg* th, orc_thermal_state* s,
+                       const int16_t* map, const int32_t* IA, const int32_t* JA,
+                       const int32_t* ind, const double* dX0, double* T, double* Tprev,
+                       const double* ux, const double* uy, const double* nut, double* A,
+                       double* b) {
+    const int n = c->nxf * c->ny;
+    s->time_since_change++;
+    if (s->time_since_change >= 20) {
+        s->time_since_change = 0;
+        if (s->steps_per_lb != 1) { s->steps_per_lb /= 2; s->dt *= 2.0; }
+    }
+    memcpy(Tprev, T, sizeof(double) * n);
+    int cur = 0;
+    s->solves = 0;
+    while (cur < s->steps_per_lb) {
+        orc_thermal_coeffs(c, th, ind, map, dX0, A, b, T, ux, uy, nut, s->dt);
+        orc_bicgstab_solve(n, IA, JA, A, b, T, s->max_iters, s->rel_tol, s->abs_tol, 1, &s->last);
+        s->solves++;
+        if (s->last.reset) {
+            s->steps_per_lb *= 2;
+            s->dt /= 2.0;
+            memcpy(T, Tprev, sizeof(double) * n);
+            cur = 0;
+            s->time_since_change = 0;
+            s->resets++;
+        }
+        if (s->steps_per_lb > (1 << 20)) break;
+        cur++;
+    }
+}

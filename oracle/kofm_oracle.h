@@ -136,6 +136,53 @@ void orc_wall_shear_nodes(const orc_cfg* c, const double* FA, const double* rho,
 void orc_wall_shear_links(const double* tau_nodes, const int32_t* sind, const double* w,
                           int nbl, double* out);
 
+/* ---- thermal implicit FD (clVariablesFD::Solve, clVariablesFD.h:343-358) -- */
+typedef struct orc_thermal_cfg {
+    double alpha_fluid;   /* LB_ALPHA_FLUID = MU / Pr (clVariablesFD.cpp:457) */
+    double alpha_foul;    /* LB_ALPHA_FOUL, fouling-layer diffusivity */
+    double pr_turb_inv;   /* PR_TURB_NUMBER_INV = 1 / Pr_t */
+    double t_in;          /* TFD_X_IN_VAL: inlet temperature, upper clamp of T */
+} orc_thermal_cfg;
+
+typedef struct orc_bicgstab_stats {
+    int iters;        /* iterCount at exit */
+    int checks;       /* convergence checks run */
+    int conv;         /* converged (or b == 0) */
+    int reset;        /* resetTimeFunc path taken */
+    double residual;  /* last checked ||r||_1 / ||b||_1 */
+    double initial_residual;
+} orc_bicgstab_stats;
+
+typedef struct orc_thermal_state {
+    int steps_per_lb;          /* stepsPerLB */
+    int time_since_change;     /* timeSinceTimeStepChange */
+    double dt;                 /* timeStep */
+    int max_iters;
+    double rel_tol, abs_tol;
+    int solves, resets;        /* of the last orc_thermal_solve */
+    orc_bicgstab_stats last;
+} orc_thermal_state;
+
+/* CSR_Inds (non-periodic) with the thermal flags; same conventions as
+ * orc_csr_build. */
+int orc_csr_build_thermal(const orc_cfg* c, const int16_t* map, int32_t* IA,
+                          int32_t* JA, int32_t* ind);
+void orc_csr_fill_solid_boundary_thermal(const orc_cfg* c, const int16_t* map,
+                                         const int32_t* ind, double* A);
+/* Update_T_Coeffs_Implicit; nut may be NULL (no eddy diffusivity). */
+void orc_thermal_coeffs(const orc_cfg* c, const orc_thermal_cfg* th, const int32_t* ind,
+                        const int16_t* map, const double* dX0, double* A, double* b,
+                        const double* T, const double* ux, const double* uy,
+                        const double* nut, double dt);
+void orc_bicgstab_solve(int n, const int32_t* IA, const int32_t* JA, const double* A,
+                        double* b, double* x, int max_iters, double rel_tol, double abs_tol,
+                        int reset_flag, orc_bicgstab_stats* st);
+void orc_thermal_solve(const orc_cfg* c, const orc_thermal_cfg* th, orc_thermal_state* s,
+                       const int16_t* map, const int32_t* IA, const int32_t* JA,
+                       const int32_t* ind, const double* dX0, double* T, double* Tprev,
+                       const double* ux, const double* uy, const double* nut, double* A,
+                       double* b);
+
 double orc_sum(const double* a, int64_t n);
 double orc_min(const double* a, int64_t n);
 

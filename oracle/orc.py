@@ -61,6 +61,23 @@ class KOmegaState(C.Structure):
     ]
 
 
+class ThermalCfg(C.Structure):
+    _fields_ = [("alpha_fluid", C.c_double), ("alpha_foul", C.c_double),
+                ("pr_turb_inv", C.c_double), ("t_in", C.c_double)]
+
+
+class BicgStats(C.Structure):
+    _fields_ = [("iters", C.c_int), ("checks", C.c_int), ("conv", C.c_int), ("reset", C.c_int),
+                ("residual", C.c_double), ("initial_residual", C.c_double)]
+
+
+class ThermalState(C.Structure):
+    _fields_ = [("steps_per_lb", C.c_int), ("time_since_change", C.c_int),
+                ("dt", C.c_double), ("max_iters", C.c_int),
+                ("rel_tol", C.c_double), ("abs_tol", C.c_double),
+                ("solves", C.c_int), ("resets", C.c_int), ("last", BicgStats)]
+
+
 def make_cfg(nx, ny, tau0, fterm, mu, max_turb_visc=10.0, nxf=None) -> _Cfg:
     return _Cfg(nx, nxf or nx, ny, tau0, fterm, mu, max_turb_visc)
 
@@ -96,6 +113,16 @@ class Oracle:
         L.orc_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, C.c_void_p, _i32, C.c_int,
                                            _dp, _dp]
         L.orc_wall_shear_links.argtypes = [_dp, _i32, _dp, C.c_int, _dp]
+        L.orc_csr_build_thermal.argtypes = [cp, _i16, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_csr_build_thermal.restype = C.c_int
+        L.orc_csr_fill_solid_boundary_thermal.argtypes = [cp, _i16, _i32, _dp]
+        tp = C.POINTER(ThermalCfg)
+        L.orc_thermal_coeffs.argtypes = [cp, tp, _i32, _i16, _dp, _dp, _dp, _dp, _dp, _dp,
+                                         C.c_void_p, C.c_double]
+        L.orc_bicgstab_solve.argtypes = [C.c_int, _i32, _i32, _dp, _dp, _dp, C.c_int, C.c_double,
+                                         C.c_double, C.c_int, C.POINTER(BicgStats)]
+        L.orc_thermal_solve.argtypes = [cp, tp, C.POINTER(ThermalState), _i16, _i32, _i32, _i32,
+                                        _dp, _dp, _dp, _dp, _dp, C.c_void_p, _dp, _dp]
         L.orc_sum.argtypes = [_dp, C.c_int64]
         L.orc_sum.restype = C.c_double
         L.orc_min.argtypes = [_dp, C.c_int64]
@@ -125,6 +152,17 @@ class Oracle:
                              ind.ctypes.data)
         return IA, JA, ind
 
+    def csr_thermal(self, cfg, m):
+        """CSR_Inds (non-periodic) with the thermal flags."""
+        n = cfg.nxf * cfg.ny
+        nnz = self.L.orc_csr_build_thermal(C.byref(cfg), m, None, None, None)
+        IA = np.zeros(n + 1, np.int32)
+        JA = np.zeros(nnz, np.int32)
+        ind = np.zeros(5 * n, np.int32)
+        self.L.orc_csr_build_thermal(C.byref(cfg), m, IA.ctypes.data, JA.ctypes.data,
+                                     ind.ctypes.data)
+        return IA, JA, ind
+
 
 class RefKernels:
     """The reference's kernels compiled for the CPU (oracle/_ref)."""
@@ -143,6 +181,9 @@ class RefKernels:
         L.ref_komega_coeffs.argtypes = [cp, _i32, _dp, _dp, _dp, _dp, _dp, _dp,
                                         _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                         _dp, _dp, _dp, _i16, C.c_double, _dp]
+        if hasattr(L, "ref_thermal_coeffs"):
+            L.ref_thermal_coeffs.argtypes = [cp, _dp, _i32, _i16, _dp, _dp, _dp, _dp, _dp, _dp,
+                                             _dp, C.c_double]
         if hasattr(L, "ref_wall_shear_nodes"):
             L.ref_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, C.c_int]
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
@@ -161,7 +202,7 @@ class OracleSim:
 
     def __init__(self, orc: Oracle, cfg, ntype, dX, wallD, f, k=None, omega=None,
                  nut=None, sxy=None, komega=False, ibb_idx=None, ibb_q=None,
-                 max_iters=1000, rel_tol=1e-4, abs_tol=1e-7, dt=1.0):
+                 max_iters=1000, rel_tol=1e-4, abs_tol=1e-7, dt=1.0, thermal=None):
         self.o, self.cfg, self.komega = orc, cfg, komega
         n = cfg.nxf * cfg.ny
         self.n = n
@@ -190,10 +231,26 @@ class OracleSim:
             self.F1 = np.zeros(n)
             self.dkdo = np.zeros(2 * n)
             self.kst = KOmegaState(1, 0, dt, max_iters, rel_tol, abs_tol)
+        # thermal: dict(T=..., cfg=ThermalCfg, dX0=..., max_iters, rel_tol, abs_tol, dt,
+        # every=LB steps per thermal solve)
+        self.thermal = thermal
+        if thermal is not None:
+            self.T = np.array(thermal["T"], np.float64)
+            self.Tprev = np.zeros(n)
+            self.tcfg = thermal["cfg"]
+            self.dX0 = np.ascontiguousarray(thermal.get("dX0", self.dX), np.float64)
+            self.tIA, self.tJA, self.tind = orc.csr_thermal(cfg, self.m)
+            self.tA = np.zeros(len(self.tJA))
+            orc.L.orc_csr_fill_solid_boundary_thermal(C.byref(cfg), self.m, self.tind, self.tA)
+            self.tb = np.zeros(n)
+            self.tst = ThermalState(1, 0, thermal.get("dt", 1.0), thermal.get("max_iters", 1000),
+                                    thermal.get("rel_tol", 1e-4), thermal.get("abs_tol", 1e-7))
+            self.t_every = thermal.get("every", 1)
+            self.time_n = 0
 
     def step(self, nsteps=1, options=OPTION_SAVE_MACRO_FIELDS):
         L, cp = self.o.L, C.byref(self.cfg)
-        opt = options | (OPTION_SAVE_MACRO_FIELDS if self.komega else 0)
+        opt = options | (OPTION_SAVE_MACRO_FIELDS if self.komega or self.thermal is not None else 0)
         for _ in range(nsteps):
             L.orc_collide_push(cp, self.FA, self.FB, self.m, self.rho, self.ux, self.uy,
                                self.K, self.O, self.wallD, self.nut, self.S, opt,
@@ -203,6 +260,10 @@ class OracleSim:
             self.FA, self.FB = self.FB, self.FA
             if self.komega:
                 self.komega_solve()
+            if self.thermal is not None:
+                if self.time_n % self.t_every == 0:
+                    self.thermal_solve()
+                self.time_n += 1
 
     def komega_solve(self):
         L, cp = self.o.L, C.byref(self.cfg)
@@ -210,3 +271,9 @@ class OracleSim:
                            self.K, self.O, self.nut, self.wallD, self.rho, self.ux,
                            self.uy, self.S, self.dX, self.Dk, self.Do, self.F1,
                            self.dkdo, self.kA, self.oA, self.kb, self.ob)
+
+    def thermal_solve(self):
+        L, cp = self.o.L, C.byref(self.cfg)
+        L.orc_thermal_solve(cp, C.byref(self.tcfg), C.byref(self.tst), self.m, self.tIA,
+                            self.tJA, self.tind, self.dX0, self.T, self.Tprev, self.ux, self.uy,
+                            self.nut.ctypes.data if self.komega else None, self.tA, self.tb)

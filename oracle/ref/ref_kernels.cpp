@@ -80,6 +80,20 @@ struct RefProgram {
     double m_cutoff = 5.0;
 #include "../_ref/gen/shear.inc"
 #undef SHEAR_CUTOFF_RADIUS
+// thermal program defines (clVariablesFD::setSourceDefines,
+// clVariablesFD.cpp:684-698); the k-omega build adds USING_KOMEGA_SOLVER
+#define LB_ALPHA_FLUID m_alpha_fluid
+#define LB_ALPHA_FOUL m_alpha_foul
+#define PR_TURB_NUMBER_INV m_prt_inv
+#define TFD_X_IN_VAL m_tin
+#define USING_KOMEGA_SOLVER
+    double m_alpha_fluid = 0.0, m_alpha_foul = 0.0, m_prt_inv = 1.0, m_tin = 0.0;
+#include "../_ref/gen/thermal.inc"
+#undef USING_KOMEGA_SOLVER
+#undef LB_ALPHA_FLUID
+#undef LB_ALPHA_FOUL
+#undef PR_TURB_NUMBER_INV
+#undef TFD_X_IN_VAL
 };
 
 #pragma GCC diagnostic pop
@@ -204,6 +218,18 @@ int ref_shear_coeffs1(const RefCfg* c, int* nodes, short* map, double* cfss, int
         g_ref_gid[0] = (size_t)i; g_ref_gid[1] = 0; g_ref_gid[2] = 0;
         p.TR_Find_Shear_Coeffs1(nodes, map, cfss, n);
     }
+    return 0;
+}
+
+// Update_T_Coeffs_Implicit (tfdKernels.cl:122-279) over XsizeFull x nY.
+int ref_thermal_coeffs(const RefCfg* c, const double* th4, int* ind, short* map, double* dX0,
+                       double* A, double* b, double* T, double* ux, double* uy, double* nut,
+                       double dt) {
+    RefProgram p = make_prog(c);
+    p.m_alpha_fluid = th4[0]; p.m_alpha_foul = th4[1]; p.m_prt_inv = th4[2]; p.m_tin = th4[3];
+    ndrange2d(c->nxf, c->ny, [&] {
+        p.Update_T_Coeffs_Implicit(ind, map, dX0, A, b, T, nullptr, ux, uy, nut, dt);
+    });
     return 0;
 }
 
