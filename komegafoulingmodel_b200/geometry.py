@@ -203,13 +203,13 @@ def equilibrium_state(ch: Channel, rho=1.0, ux=0.0, uy=0.0) -> np.ndarray:
 
 
 def temperature_field(ch: Channel, t0: float = 0.5) -> np.ndarray:
-    """tempArray start: Tinitial (TFD_INI_TEMP, 0.5) on M0_FLUID nodes, 0
-    elsewhere (tempArray.fillByNodeType, clVariablesFD.cpp:236-239)."""
-    m = ch.ntype.astype(np.int32) & 0xFFFF
-    T = np.where((m & M0_FLUID) != 0, t0, 0.0)
-    T = T.reshape(ch.ny, ch.nx_full)
-    T[:, ch.nx:] = 0.0
-    return T.ravel()
+    """tempArray at the start of a run that loads no temperature file:
+    Tinitial (TFD_INI_TEMP, 0.5) on every node -- clVariablesFD::testRestartRun
+    fills the whole array (clVariablesFD.cpp:813-823) and ini's
+    fillByNodeType(ROE0, nType, M0_FLUID_NODE) (236-239) leaves the wall nodes
+    as they are.  The wall-boundary rows of the thermal system (x = 0) pull
+    those values to 0 over the first solves."""
+    return np.full(ch.n, float(t0))
 
 
 def komega_fields(ch: Channel, k0: float, omega0: float):

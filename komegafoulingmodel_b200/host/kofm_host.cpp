@@ -145,6 +145,16 @@ void clVariablesLB::ini() {
     d.komega_rel_tol = p.relTol;
     d.komega_abs_tol = p.absTol;
     d.komega_dt = p.dTlb;
+    d.use_thermal = p.thermalSolverFlag ? 1 : 0;
+    d.thermal_every = p.tfdSteps;
+    d.pr_number = p.PrNum;
+    d.pr_turb_number = p.PrTurbNum;
+    d.alpha_foul = p.AlphaFoul;
+    d.t_in = p.ROE_INX;
+    d.thermal_max_iters = p.tempMaxIters;
+    d.thermal_rel_tol = p.tempMaxRelTol;
+    d.thermal_abs_tol = p.tempMaxAbsTol;
+    d.thermal_dt = (double)p.tfdSteps;  // dTtfd (clProblem.cpp:510)
     if (ctx) {
         kofm_destroy(ctx);
         ctx = nullptr;
@@ -154,10 +164,11 @@ void clVariablesLB::ini() {
     if (ko && WallD.size() != n)
         throw Error("clVariablesLB::ini: WallD missing", KOFM_ERR_INITIALIZING_KOMEGA);
     // link fractions default to whole links (dXArr = 1, no wall cut)
-    if (ko && dXArr.size() != 4 * n) dXArr.assign(4 * n, 1.0);
+    const bool th = p.thermalSolverFlag;
+    if ((ko || th) && dXArr.size() != 4 * n) dXArr.assign(4 * n, 1.0);
     check("clVariablesLB::ini (geometry)",
           kofm_set_geometry(ctx, nType.data(), ko && !WallD.empty() ? WallD.data() : nullptr,
-                            ko && !dXArr.empty() ? dXArr.data() : nullptr,
+                            (ko || th) && !dXArr.empty() ? dXArr.data() : nullptr,
                             ibbArr.empty() ? nullptr : ibbArr.data(),
                             ibbDistArr.empty() ? nullptr : ibbDistArr.data(),
                             (int32_t)ibbArr.size()));
@@ -239,7 +250,50 @@ bool clVariablesLB::loadRestartFiles(const std::string& dir) {
 // ---- clProblem ----------------------------------------------------------------
 void clProblem::step() {
     // collide + IBB, then kOmega::Solve (which ends with the queue drained)
+    const long long timeN = vlb_.TimeN;
     vlb_.Solve(KOFM_OPTION_SAVE_MACRO_FIELDS);
+    if (vfd_ && vfd_->thermalSolverFlag && timeN % vlb_.p.tfdSteps == 0) vfd_->Solve();
+}
+
+clVariablesFD::clVariablesFD(clVariablesLB& vlb)
+    : thermalSolverFlag(vlb.p.thermalSolverFlag), sumTemp(&vlb.ctx, KOFM_FIELD_TEMP, KOFM_OP_SUM), lb_(vlb) {}
+
+void clVariablesFD::ini() {
+    if (!thermalSolverFlag) return;
+    if (!lb_.ctx) throw Error("clVariablesFD::ini: clVariablesLB::ini first", KOFM_ERR_STATE);
+    const size_t n = lb_.fullSize();
+    if (tempArray.size() != n) tempArray.assign(n, lb_.p.ROE0);
+    if (!dXArr0.empty()) {
+        if (dXArr0.size() != 4 * n) throw Error("clVariablesFD::ini: dXArr0 size", KOFM_ERR_INVALID_ARG);
+        check("clVariablesFD::ini (dXArr0)", kofm_set_thermal_geometry(lb_.ctx, dXArr0.data()));
+    }
+    check("clVariablesFD::ini (temperature)", kofm_set_temperature(lb_.ctx, tempArray.data()));
+}
+
+void clVariablesFD::Solve() {
+    check("clVariablesFD::Solve", kofm_thermal_update(lb_.ctx));
+    kofm_stats st;
+    check("kofm_get_stats", kofm_get_stats(lb_.ctx, &st));
+    stepsPerLB = st.thermal_steps_per_lb;
+    timeSinceTimeStepChange = st.thermal_time_since_change;
+    timeStep = st.thermal_dt;
+    lastIters = st.thermal_iters;
+}
+
+void clVariablesFD::saveRestartFiles(const std::string& dir) {
+    const size_t n = lb_.fullSize();
+    tempArray.resize(n);
+    check("kofm_get_temperature", kofm_get_temperature(lb_.ctx, tempArray.data()));
+    if (!saveBin(dir + "/temp.bin", tempArray.data(), n))
+        throw Error("clVariablesFD::saveRestartFiles", KOFM_ERR_MEMORY_COPY);
+}
+
+bool clVariablesFD::loadRestartFiles(const std::string& dir) {
+    const size_t n = lb_.fullSize();
+    std::vector<double> t(n);
+    if (!loadBin(dir + "/temp.bin", t.data(), n)) return false;
+    tempArray.swap(t);
+    return true;
 }
 
 }  // namespace host

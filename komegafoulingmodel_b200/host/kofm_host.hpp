@@ -48,6 +48,17 @@ struct Params {
     double relTol = 1.0e-4;      // KOMEGA_MAX_REL_TOL
     double absTol = 1.0e-7;      // KOMEGA_MAX_ABS_TOL
     double dTlb = 1.0;           // p.dTlb
+    // thermal solver (clVariablesFD::loadParams, clVariablesFD.cpp:444-493)
+    bool thermalSolverFlag = false;  // "Thermal Solver"
+    int tfdSteps = 1;                // "LB Steps Per T" (LB_STEPS_PER_FD)
+    double PrNum = 0.708;            // "Pr Number"
+    double PrTurbNum = 0.9;          // PR_TURB_NUMBER
+    double AlphaFoul = 0.0;          // LB_ALPHA_FOUL (fouling-layer diffusivity)
+    double ROE0 = 0.5;               // "Tinitial" (TFD_INI_TEMP)
+    double ROE_INX = 2.0;            // "Tinlet Sim" (TFD_X_IN)
+    int tempMaxIters = 1000;         // "Temp Max Iterations"
+    double tempMaxRelTol = 1.0e-4;   // "Temp Max Rel Tol"
+    double tempMaxAbsTol = 1.0e-7;   // "Temp Max Abs Tol"
     int storage = KOFM_STORE_FP32;
     int device = 0;
 };
@@ -149,16 +160,47 @@ class clVariablesLB {
     size_t fullSize() const { return (size_t)p.XsizeFull * (size_t)p.nY; }
 };
 
-// One time step of the reference's step loop without particles or heat
-// transfer: Solve_no_TR (LBLS.cpp:185-205).
+// The thermal solver of the reference (clVariablesFD.h:20-452): the
+// temperature field and its implicit finite-difference update over the
+// context that clVariablesLB::ini created (Params::thermalSolverFlag on).
+class clVariablesFD {
+  public:
+    explicit clVariablesFD(clVariablesLB& vlb);
+    bool thermalSolverFlag = false;
+    int stepsPerLB = 1, timeSinceTimeStepChange = 0;
+    double timeStep = 1.0;
+    int lastIters = 0;
+    std::vector<double> tempArray;   // XsizeFull * nY, FP64
+    std::vector<double> dXArr0;      // unfouled link fractions (may be empty)
+    Reducer sumTemp;                 // clVariablesFD.cpp:266
+
+    // clVariablesFD::ini (clVariablesFD.cpp:230-280): Tinitial everywhere
+    // unless a temperature was loaded, then the upload
+    void ini();
+    // clVariablesFD::Solve (clVariablesFD.h:343-358)
+    void Solve();
+    // clVariablesFD::calcAverageT (clVariablesFD.cpp:139-142): the sum
+    double calcAverageT() const { return sumTemp.reduceSingle(); }
+    // dir/temp.bin (the "load/temp" file testRestartRun reads)
+    void saveRestartFiles(const std::string& dir);
+    bool loadRestartFiles(const std::string& dir);
+
+  private:
+    clVariablesLB& lb_;
+};
+
+// One time step of the reference's step loop without particles:
+// Solve_no_TR (LBLS.cpp:185-205): collide + IBB, kOmega::Solve, and
+// vfd.Solve() every tfdSteps steps when a thermal solver is attached.
 class clProblem {
   public:
-    explicit clProblem(clVariablesLB& vlb) : vlb_(vlb) {}
+    explicit clProblem(clVariablesLB& vlb, clVariablesFD* vfd = nullptr) : vlb_(vlb), vfd_(vfd) {}
     void step();
     void Solve_no_TR() { step(); }
 
   private:
     clVariablesLB& vlb_;
+    clVariablesFD* vfd_;
 };
 
 // Raw binary array files as Array::savebin writes them (Array.h:1178-1193).

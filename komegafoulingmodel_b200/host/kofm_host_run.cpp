@@ -4,10 +4,14 @@
 //
 // <dir>/params.txt   "key value" lines: nX XsizeFull nY tau Fval MuVal
 //                    kOmega (0/1) [maxTurbVisc krylovDim relTol absTol]
+//                    [thermal (0/1) tempRelTol tempAbsTol]
 // <dir>/ntype.bin    int16 node flags (XsizeFull * nY)
 // <dir>/wallD.bin    FP64 wall distance (k-omega only)
 // <dir>/dX.bin       FP64 link fractions, 4 planes E,W,N,S (optional; 1)
 // <dir>/lbf.bin, lbkappa.bin, lbomega.bin   restart files (Array::savebin)
+// <dir>/temp.bin     FP64 temperature (thermal only; Tinitial when absent)
+// <dir>/ibbArr.bin, ibbDistArr.bin   interpolated bounce-back links (int32
+//                    link index, FP64 wall fraction; optional)
 //
 // Loads the restart files, advances nsteps of clProblem::step (Solve_no_TR),
 // writes the restart files of the final state to <dir>/out/ and prints one
@@ -56,6 +60,9 @@ int main(int argc, char** argv) {
         p.krylovDim = std::stoi(get("krylovDim", "10"));
         p.relTol = std::stod(get("relTol", "1e-4"));
         p.absTol = std::stod(get("absTol", "1e-7"));
+        p.thermalSolverFlag = std::stoi(get("thermal", "0")) != 0;
+        p.tempMaxRelTol = std::stod(get("tempRelTol", "1e-4"));
+        p.tempMaxAbsTol = std::stod(get("tempAbsTol", "1e-7"));
 
         clVariablesLB vlb(p);
         const size_t n = vlb.fullSize();
@@ -66,19 +73,39 @@ int main(int argc, char** argv) {
             if (s.gcount() != (std::streamsize)(n * sizeof(int16_t)))
                 throw Error("ntype.bin", KOFM_ERR_LOADING_PARAMS);
         }
-        if (p.kOmegaSolverFlag) {
-            vlb.WallD.resize(n);
-            if (!loadBin(dir + "/wallD.bin", vlb.WallD.data(), n)) vlb.WallD.clear();
+        if (p.kOmegaSolverFlag || p.thermalSolverFlag) {
             vlb.dXArr.resize(4 * n);
             if (!loadBin(dir + "/dX.bin", vlb.dXArr.data(), 4 * n)) vlb.dXArr.clear();
         }
+        if (p.kOmegaSolverFlag) {
+            vlb.WallD.resize(n);
+            if (!loadBin(dir + "/wallD.bin", vlb.WallD.data(), n)) vlb.WallD.clear();
+        }
+        {
+            std::ifstream s(dir + "/ibbArr.bin", std::ios::binary | std::ios::ate);
+            if (s) {
+                const size_t nb = (size_t)s.tellg() / sizeof(int32_t);
+                s.seekg(0);
+                vlb.ibbArr.resize(nb);
+                s.read(reinterpret_cast<char*>(vlb.ibbArr.data()), (std::streamsize)(nb * sizeof(int32_t)));
+                vlb.ibbDistArr.resize(nb);
+                if (!loadBin(dir + "/ibbDistArr.bin", vlb.ibbDistArr.data(), nb))
+                    throw Error("ibbDistArr.bin", KOFM_ERR_LOADING_PARAMS);
+            }
+        }
         if (!vlb.loadRestartFiles(dir)) throw Error("restart files in " + dir, KOFM_ERR_LOADING_PARAMS);
         vlb.ini();
-        clProblem prob(vlb);
+        clVariablesFD vfd(vlb);
+        if (p.thermalSolverFlag) {
+            vfd.loadRestartFiles(dir);
+            vfd.ini();
+        }
+        clProblem prob(vlb, &vfd);
         for (int t = 0; t < nsteps; ++t) prob.step();
         const std::string out = dir + "/out";
         mkdir(out.c_str(), 0755);
         vlb.saveRestartFiles(out);
+        if (p.thermalSolverFlag) vfd.saveRestartFiles(out);
         const double rho = vlb.sumRo.reduceSingle();
         std::printf("{\"steps\": %d, \"sum_rho\": %.17g, \"umean\": %.17g", nsteps, rho, vlb.calcUmean());
         if (p.kOmegaSolverFlag)
@@ -88,6 +115,9 @@ int main(int argc, char** argv) {
                         vlb.kOmegaClass.minKappa.reduceSingle(), vlb.kOmegaClass.minOmega.reduceSingle(),
                         vlb.kOmegaClass.stepsPerLB, vlb.kOmegaClass.lastOmegaIters,
                         vlb.kOmegaClass.lastKappaIters);
+        if (p.thermalSolverFlag)
+            std::printf(", \"sum_temp\": %.17g, \"temp_steps_per_lb\": %d, \"temp_iters\": %d",
+                        vfd.calcAverageT(), vfd.stepsPerLB, vfd.lastIters);
         std::printf("}\n");
     } catch (const Error& e) {
         std::fprintf(stderr, "kofm_host_run: %s\n", e.what());

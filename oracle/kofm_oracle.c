@@ -932,6 +932,7 @@ void orc_thermal_solve(const orc_cfg* c, const orc_thermal_cfg* th, orc_thermal_
     memcpy(Tprev, T, sizeof(double) * n);
     int cur = 0;
     s->solves = 0;
+    s->resets = 0;
     while (cur < s->steps_per_lb) {
         orc_thermal_coeffs(c, th, ind, map, dX0, A, b, T, ux, uy, nut, s->dt);
         orc_bicgstab_solve(n, IA, JA, A, b, T, s->max_iters, s->rel_tol, s->abs_tol, 1, &s->last);

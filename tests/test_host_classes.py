@@ -16,16 +16,20 @@ from tests.test_komega_gpu import channel_case, make_lattice
 RUN = build.HOST_RUN
 
 
-def write_case(d, ch, f, k=None, o=None, rate=1.25, g=0.0, nu=0.1, komega=False):
+def write_case(d, ch, f, k=None, o=None, rate=1.25, g=0.0, nu=0.1, komega=False, thermal=False):
     os.makedirs(d, exist_ok=True)
     with open(os.path.join(d, "params.txt"), "w") as fh:
         fh.write(f"nX {ch.nx}\nXsizeFull {ch.nx_full}\nnY {ch.ny}\ntau {rate!r}\n"
-                 f"Fval {g!r}\nMuVal {nu!r}\nkOmega {int(komega)}\n")
+                 f"Fval {g!r}\nMuVal {nu!r}\nkOmega {int(komega)}\nthermal {int(thermal)}\n")
     ch.ntype.astype(np.int16).tofile(os.path.join(d, "ntype.bin"))
     np.asarray(f, dtype=np.float64).tofile(os.path.join(d, "lbf.bin"))
+    if komega or thermal:
+        np.asarray(ch.dX, dtype=np.float64).tofile(os.path.join(d, "dX.bin"))
     if komega:
         np.asarray(ch.wallD, dtype=np.float64).tofile(os.path.join(d, "wallD.bin"))
-        np.asarray(ch.dX, dtype=np.float64).tofile(os.path.join(d, "dX.bin"))
+    if ch.ibb_idx is not None and len(ch.ibb_idx):
+        np.asarray(ch.ibb_idx, dtype=np.int32).tofile(os.path.join(d, "ibbArr.bin"))
+        np.asarray(ch.ibb_q, dtype=np.float64).tofile(os.path.join(d, "ibbDistArr.bin"))
         np.asarray(k, dtype=np.float64).tofile(os.path.join(d, "lbkappa.bin"))
         np.asarray(o, dtype=np.float64).tofile(os.path.join(d, "lbomega.bin"))
 
@@ -82,3 +86,32 @@ def test_host_step_loop_matches_python_path(tmp_path, kofm_lib):
     r2 = subprocess.run([RUN, os.path.join(d, "again"), "1"], capture_output=True, text=True,
                         timeout=300)
     assert r2.returncode == 0, r2.stderr
+
+
+@pytest.mark.gpu
+def test_host_thermal_step_loop_matches_python_path(tmp_path, kofm_lib):
+    """clProblem::step with a clVariablesFD attached (collide, kOmega::Solve,
+    clVariablesFD::Solve) against kofm_step with use_thermal: identical
+    temperature, and temp.bin restarts."""
+    from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+    from tests.test_thermal import _wavy_case
+    ch, f, k, o, nut, rate, g, nu = _wavy_case()
+    d = str(tmp_path)
+    write_case(d, ch, f, k, o, rate, g, nu, komega=True, thermal=True)
+    r = subprocess.run([RUN, d, "8"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    desc = desc_default()
+    desc.nx, desc.nx_full, desc.ny = ch.nx, ch.nx_full, ch.ny
+    desc.tau, desc.fterm, desc.mu = rate, g, nu
+    desc.use_komega = desc.use_thermal = 1
+    with Lattice(desc) as L:
+        L.set_geometry(ch.ntype, ch.wallD, ch.dX, ch.ibb_idx, ch.ibb_q)
+        L.set_state(f, k, o, None, np.zeros(3 * ch.n))
+        L.set_temperature(G.temperature_field(ch))
+        L.step(8)
+        T = L.get_temperature()
+        tsum = L.reduce(_abi.FIELD_TEMP)
+    To = np.fromfile(os.path.join(d, "out", "temp.bin"))
+    assert np.array_equal(To, T)
+    assert res["sum_temp"] == tsum

@@ -235,19 +235,22 @@ TIGHT_KO = dict(komega_rel_tol=1e-10, komega_abs_tol=1e-30)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tol,dt", [(1e-4, 1.0), (1e-12, 1.0), (1e-12, 8.0)])
-def test_gpu_thermal_update_of_device_state(kofm_lib, oracle, tol, dt):
+@pytest.mark.parametrize("tol,dt,npre", [(1e-4, 1.0, 5), (1e-12, 1.0, 5), (1e-12, 64.0, 0)])
+def test_gpu_thermal_update_of_device_state(kofm_lib, oracle, tol, dt, npre):
     """kofm_thermal_update against orc_thermal_solve on the state the device
     holds (T, the step's u and nu_t, the sub-step count and dt): one
-    clVariablesFD::Solve.  At dt = 8 the residual growth test halves the
-    time step (the resetTimeFunc path) in both."""
+    clVariablesFD::Solve after npre full steps and one LB + k-omega step.  At
+    dt = 64 the residual growth test halves the time step twice (the
+    resetTimeFunc path: T restored, sub-steps doubled) in both."""
     ch, f, k, o, nut, rate, g, nu = _wavy_case()
     cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
     L, d = _thermal_lattice(ch, rate, g, nu, True, thermal_rel_tol=tol, thermal_dt=dt, **TIGHT_KO)
     with L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
         L.set_temperature(G.temperature_field(ch))
-        L.step(5)
+        L.step(npre)
+        L.lb_step()
+        L.komega_update()
         T5 = L.get_temperature()
         _, ux, uy = L.get_macro()
         nut5 = L.get_state()[3]
@@ -272,6 +275,7 @@ def test_gpu_thermal_update_of_device_state(kofm_lib, oracle, tol, dt):
     print(dict(solves=(st6.thermal_solves, ts.solves), resets=(st6.thermal_resets, ts.resets),
                dt=(st6.thermal_dt, ts.dt), steps5=(st5.thermal_steps_per_lb, st5.thermal_dt)))
     assert (st6.thermal_solves, st6.thermal_resets) == (ts.solves, ts.resets)
+    assert ts.resets == (2 if dt > 32 else 0)
     assert (st6.thermal_steps_per_lb, st6.thermal_dt) == (ts.steps_per_lb, ts.dt)
     assert abs(st6.thermal_iters - ts.last.iters) <= (0 if tol < 1e-8 else 1)
     # both solves meet the tolerance; at 1e-4 they may stop an iteration apart
