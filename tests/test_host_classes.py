@@ -27,11 +27,11 @@ def write_case(d, ch, f, k=None, o=None, rate=1.25, g=0.0, nu=0.1, komega=False,
         np.asarray(ch.dX, dtype=np.float64).tofile(os.path.join(d, "dX.bin"))
     if komega:
         np.asarray(ch.wallD, dtype=np.float64).tofile(os.path.join(d, "wallD.bin"))
+        np.asarray(k, dtype=np.float64).tofile(os.path.join(d, "lbkappa.bin"))
+        np.asarray(o, dtype=np.float64).tofile(os.path.join(d, "lbomega.bin"))
     if ch.ibb_idx is not None and len(ch.ibb_idx):
         np.asarray(ch.ibb_idx, dtype=np.int32).tofile(os.path.join(d, "ibbArr.bin"))
         np.asarray(ch.ibb_q, dtype=np.float64).tofile(os.path.join(d, "ibbDistArr.bin"))
-        np.asarray(k, dtype=np.float64).tofile(os.path.join(d, "lbkappa.bin"))
-        np.asarray(o, dtype=np.float64).tofile(os.path.join(d, "lbomega.bin"))
 
 
 def test_driver_builds_and_fails_loudly_without_a_device(tmp_path):
