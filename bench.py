@@ -132,10 +132,30 @@ STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
 
 def workload_config(w, args, world: int) -> dict:
     """The `config` object of both arms' JSON lines."""
-    return {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny, "nodes": w.nodes,
-            "storage": STORAGE_NAMES[args.storage], "krylov_dim": 10, "rel_tol": 1.0e-4,
-            "abs_tol": 1.0e-7, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (populations and solver vectors), no flush"}
+    cfg = {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny, "nodes": w.nodes,
+           "storage": STORAGE_NAMES[args.storage], "krylov_dim": 10, "rel_tol": 1.0e-4,
+           "abs_tol": 1.0e-7, "parallelism": f"replicas x{world}",
+           "l2": "inputs larger than L2 (populations and solver vectors), no flush"}
+    if getattr(args, "thermal", False):
+        cfg["thermal"] = "implicit FD temperature update every step (BiCGStab to 1e-4)"
+    return cfg
+
+
+def thermal_bytes_per_node(checks: int) -> float:
+    """Algorithmic bytes per node of one thermal update (one solve): the
+    assembly (ntype, link-fraction index, u, v, nu_t, T in; 4 coefficients
+    and b out: 66), the copy of T for a halving (16), ||b||_1 (8), the
+    residual pass (b, x, coefficients, ntype in; r, r0, p out: 74), then per
+    iteration pass B (r, p, v, coefficients, ntype, r0 in; p, v out: 82, 66 in
+    the first), pass C (r, v, coefficients, ntype in; s, t out: 66) and pass D
+    (s, x, p, t, r0 in; x, r out: 56); a solve that stops at the check after
+    pass C ends with x += alpha p, r = s (40)."""
+    n_c = (checks + 1) // 2
+    n_d = checks // 2
+    b = 66 + 16 + 8 + 74 + n_c * (82 + 66) - 16 + n_d * 56
+    if checks % 2 == 1:
+        b += 40
+    return float(b)
 
 
 def max_over_ranks(value: float, world: int, device=None) -> float:
@@ -185,8 +205,12 @@ def run_ours(args, rank, world, local_rank):
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
+    d.use_thermal = 1 if args.thermal else 0
     L = Lattice(d)
     W.apply(L, w)
+    if args.thermal:
+        from komegafoulingmodel_b200 import geometry as G
+        L.set_temperature(G.temperature_field(w.channel))
     stream = torch.cuda.ExternalStream(L.stream, device=local_rank)
     nodes = w.nodes
 
@@ -217,6 +241,8 @@ def run_ours(args, rank, world, local_rank):
     # kernels of one kofm_step: collide, assembly, solver control-block init,
     # solver (one k-omega sub-step per LB step here: steps_per_lb stays 1)
     launches_per_step = 4 if w.komega else 1
+    if args.thermal:  # assembly, control-block init and BiCGStab per solve
+        launches_per_step += 3 * max(1, st.thermal_solves)
 
     # ---- per-kernel breakdown (same stream, CUDA events) ------------------------
     nb = max(3, min(args.steps, 10))
@@ -238,6 +264,23 @@ def run_ours(args, rank, world, local_rank):
     t_as = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(nb)) / nb
     t_sv = sum(ev[i][2].elapsed_time(ev[i][3]) for i in range(nb)) / nb
     b_sv = sum(bytes_solver) / nb
+    thermal = None
+    if args.thermal:
+        tev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(nb)]
+        tchecks = []
+        for i in range(nb):
+            L.lb_step(_abi.OPTION_SAVE_MACRO_FIELDS)
+            L.komega_update()
+            tev[i][0].record(stream)
+            L.thermal_update()
+            tev[i][1].record(stream)
+            tchecks.append(L.stats().thermal_checks)
+        torch.cuda.synchronize()
+        t_th = sum(tev[i][0].elapsed_time(tev[i][1]) for i in range(nb)) / nb
+        b_th = sum(thermal_bytes_per_node(c) for c in tchecks) / nb
+        thermal = {"ms": t_th, "bytes_per_node": b_th, "gbs": b_th * nodes / (t_th * 1e-3) / 1e9,
+                   "checks_by_update": tchecks,
+                   "kernels": "thermal_assemble_kernel + bicgstab_kernel (+ T copy, control init)"}
     peak, peak_kind = measured_peaks()
     kern = {
         "lb_step_kernel": {"ms": t_lb, "bytes_per_node": LB_BYTES[args.storage],
@@ -290,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.thermal:
         cpu = cpu_reference_sample(w, steps=args.cpu_steps, warmup=0)
 
     if rank == 0:
@@ -305,6 +348,7 @@ def run_ours(args, rank, world, local_rank):
                               "achieved": step_bytes * nodes / (step_ms * 1e-3) / 1e9,
                               "frac": step_bytes * nodes / (step_ms * 1e-3) / 1e9 / peak},
             "kernels": kern,
+            **({"thermal": thermal} if thermal else {}),
             "solver": {"omega_iters": st.omega_iters, "k_iters": st.k_iters,
                        "omega_restarts": st.omega_restarts, "k_restarts": st.k_restarts,
                        "omega_vectors": st.omega_vectors, "k_vectors": st.k_vectors,
@@ -410,6 +454,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--thermal", action="store_true",
+                    help="add the thermal implicit FD update to every step (reported apart)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
