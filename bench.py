@@ -142,17 +142,17 @@ def workload_config(w, args, world: int) -> dict:
 
 
 def thermal_bytes_per_node(checks: int) -> float:
-    """Algorithmic bytes per node of one thermal update (one solve): the
-    assembly (ntype, link-fraction index, u, v, nu_t, T in; 4 coefficients
-    and b out: 66), the copy of T for a halving (16), ||b||_1 (8), the
-    residual pass (b, x, coefficients, ntype in; r, r0, p out: 74), then per
-    iteration pass B (r, p, v, coefficients, ntype, r0 in; p, v out: 82, 66 in
-    the first), pass C (r, v, coefficients, ntype in; s, t out: 66) and pass D
-    (s, x, p, t, r0 in; x, r out: 56); a solve that stops at the check after
-    pass C ends with x += alpha p, r = s (40)."""
+    """Algorithmic bytes per node of one thermal update (one solve ending
+    after `checks` residual checks): the assembly (ntype, link-fraction index,
+    u, v, nu_t, T in; 4 coefficients, b and the saved T out: 74), pass R (b,
+    x, coefficients, ntype in; r, r0 out: 66), per iteration pass B (r, p, v,
+    coefficients, ntype, r0 in; p, v out: 82; 50 in the first, where p = r0),
+    pass C (r, v in; s out: 24) and pass D (s, coefficients, ntype, x, p, r0
+    in; x, r out: 82); a solve that stops at the check after pass C ends with
+    x += alpha p, r = s (40)."""
     n_c = (checks + 1) // 2
     n_d = checks // 2
-    b = 66 + 16 + 8 + 74 + n_c * (82 + 66) - 16 + n_d * 56
+    b = 74 + 66 + 50 + (n_c - 1) * 82 + n_c * 24 + n_d * 82
     if checks % 2 == 1:
         b += 40
     return float(b)

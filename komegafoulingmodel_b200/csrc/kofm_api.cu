@@ -105,7 +105,6 @@ struct kofm_ctx {
     double* tp[2] = {nullptr, nullptr};
     double* tv[2] = {nullptr, nullptr};
     double* ts = nullptr;
-    double* tt = nullptr;
     double* tcoef = nullptr;          // [4 x D] interleaved E, W, N, S
     int32_t* dxrec0_idx = nullptr;    // per-node dXArr0 record (-1: all 1)
     DxRecord* dxrec0 = nullptr;
@@ -509,7 +508,7 @@ int kofm_destroy(kofm_ctx* c) {
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
                     c->gpart, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
                     c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
-                    c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tt, c->tcoef,
+                    c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
                     c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -594,7 +593,6 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         ALLOC(c->tr0, D);
         for (int b = 0; b < 2; ++b) { ALLOC(c->tp[b], D); ALLOC(c->tv[b], D); }
         ALLOC(c->ts, D);
-        ALLOC(c->tt, D);
         ALLOC(c->tcoef, 4 * D);
         ALLOC(c->dxrec0_idx, D);
         int s3 = th_solver_alloc(c);

@@ -14,16 +14,18 @@
 //    (the "Norm" reduction, BiCGStabGenerator.cpp:259-262) against ||b||_1,
 //    and the NaN / tenfold-growth test of reduceAndCheckConvergence
 //    (BiCGStabSolver.cpp:509-545) ends the solve for the host's dt halving.
-//    Each iteration is three grid passes instead of the reference's ~25
-//    kernels and 4 host reads:
+//    Instead of the reference's ~25 kernels and 4 host reads per iteration:
+//      R: r = b - A x, r0 = r, ||b||_1, <r, r>         (once)
 //      B: p = r + beta (p - omega v) on the fly at the node and its four
-//         neighbours, v = A p, <v, r0>            -> alpha
-//      C: s = r - alpha v on the fly, t = A s, ||s||_1  -> first check
-//      D: x = (x + alpha p) + omega s, r = s - omega t, ||r||_1, <r, r0>
-//                                                  -> second check, beta
+//         neighbours (iteration 0: p = r0), v = A p, <v, r0>   -> alpha
+//      C: s = r - alpha v, ||s||_1                     -> first check
+//      D: t = A s on the fly, x = (x + alpha p) + omega s, r = s - omega t,
+//         ||r||_1, <r, r0>                             -> second check, beta
 //    p and v are double-buffered (a pass reads the old values at the
-//    neighbours while it writes the new ones).  Grid barriers, partial sums
-//    and the last-block serial section are those of the k-omega solver.
+//    neighbours while it writes the new ones); p of iteration 0 is r0 itself.
+//    Threads take node pairs (16-byte loads and stores; the pair shares its
+//    row neighbours).  Grid barriers, partial sums and the last-block serial
+//    section are those of the k-omega solver.
 #pragma once
 #include "kofm_gmres.cuh"
 
@@ -47,6 +49,7 @@ struct ThermalAsm {
     const float* uy;
     const float* nut;         // nullptr without k-omega
     const double* T;
+    double* Tprev;            // copy of T (first sub-step of an update), or nullptr
     double* coef;             // [4 x D] E, W, N, S (interleaved)
     double* b;                // [D]
     int nx, ny, P;
@@ -58,8 +61,10 @@ struct ThermalAsm {
 __global__ void thermal_assemble_kernel(const ThermalAsm p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
-    if (x >= p.nx || y >= p.ny) return;
+    if (x >= p.P || y >= p.ny) return;
     const long long g = (long long)y * p.P + x;
+    if (p.Tprev) p.Tprev[g] = p.T[g];  // copyToPrevSolution (BiCGStabSolver.cpp:572-578)
+    if (x >= p.nx) return;
     const int t = (uint16_t)p.ntype[g];
     if (t & M0_SOLID) return;
     double dx[4] = {1.0, 1.0, 1.0, 1.0};
@@ -126,7 +131,6 @@ struct ThermalArgs {
     double* p[2];
     double* v[2];
     double* s;
-    double* t;
     ThermalCtl* ctl;
     double* part;             // [GM_SLOTS][gridDim.x]
     GridBarrier* bar;
@@ -138,7 +142,7 @@ struct ThermalArgs {
     long long spin_limit;
 };
 
-enum ThSerial : int { TS_NONE = 0, TS_NORMB, TS_RHO0, TS_ALPHA, TS_CHECK1, TS_CHECK2 };
+enum ThSerial : int { TS_NONE = 0, TS_RES0, TS_ALPHA, TS_CHECK1, TS_CHECK2 };
 
 // reduceAndCheckConvergence on the summed L1 norm of the current residual
 __device__ void th_check(const ThermalArgs& a, ThermalCtl& C, double l1) {
@@ -155,7 +159,7 @@ __device__ void th_check(const ThermalArgs& a, ThermalCtl& C, double l1) {
 __device__ void th_serial(const ThermalArgs& a, int kind, int nblocks) {
     __shared__ double tot[2];
     const int warp = threadIdx.x >> 5;
-    const int used = kind == TS_CHECK2 ? 2 : 1;
+    const int used = (kind == TS_CHECK2 || kind == TS_RES0) ? 2 : 1;
     if (warp < used) {
         const double v = sum_slot_warp(a.part, nblocks, warp);
         if ((threadIdx.x & 31) == 0) tot[warp] = v;
@@ -169,11 +173,11 @@ __device__ void th_serial(const ThermalArgs& a, int kind, int nblocks) {
             for (int i = 0; i < (int)(sizeof(ThermalCtl) / 8); ++i) dst[i] = __ldcg(src + i);
         }
         switch (kind) {
-            case TS_NORMB:
+            case TS_RES0:  // step 1 (||b||_1, the b == 0 exit) and step 4 (rho)
                 C.normb = tot[0];
                 if (C.normb <= 1.0e-16) C.state = TH_TRIVIAL;
+                C.rho = tot[1];
                 break;
-            case TS_RHO0: C.rho = tot[0]; break;
             case TS_ALPHA: C.alpha = C.rho / tot[0]; break;
             case TS_CHECK1:
                 th_check(a, C, tot[0]);
@@ -239,117 +243,184 @@ __device__ bool th_sync(const ThermalArgs& a, int kind) {
     return ldc(&a.ctl->error) == 0;
 }
 
-// One row of A times a vector whose entries come from `val(node)` (CSR
-// order of an interior row: S, W, C, E, N).
-template <typename F>
-__device__ __forceinline__ double th_apply(const ThermalArgs& a, int kind, long long g, int x,
-                                           F&& val) {
-    if (kind == TH_EMPTY) return 0.0;
-    if (kind == TH_DIAG) return val(g);
-    double acc = __ldg(a.coef + ilv(4, 3, g)) * val(g - a.P);
-    if (x > 0) acc += __ldg(a.coef + ilv(4, 1, g)) * val(g - 1);
-    acc += val(g);
-    if (x < a.nx - 1) acc += __ldg(a.coef + ilv(4, 0, g)) * val(g + 1);
-    acc += __ldg(a.coef + ilv(4, 2, g)) * val(g + a.P);
-    return acc;
+__device__ __forceinline__ double2 ld2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ void st2(double* p, double u, double v) {
+    __stcg(reinterpret_cast<double2*>(p), make_double2(u, v));
+}
+
+// A times a vector on the node pair (g, g+1), g even: val2(n) gives the
+// vector on nodes n, n+1 (n even), val1(n) on one node.  Rows in CSR order
+// (S, W, C, E, N); wall-boundary rows are the identity, inner-wall and
+// padding rows are empty.
+template <typename F2, typename F1>
+__device__ __forceinline__ double2 th_apply2(const ThermalArgs& a, long long g, int x, int k0, int k1,
+                                             F2&& val2, F1&& val1) {
+    if (k0 == TH_EMPTY && k1 == TH_EMPTY) return make_double2(0.0, 0.0);
+    const double2 c = val2(g);
+    double r0 = k0 == TH_DIAG ? c.x : 0.0, r1 = k1 == TH_DIAG ? c.y : 0.0;
+    if (k0 == TH_FULL || k1 == TH_FULL) {
+        const double2 sv = val2(g - a.P), nv = val2(g + a.P);
+        if (k0 == TH_FULL) {
+            double acc = __ldg(a.coef + ilv(4, 3, g)) * sv.x;
+            if (x > 0) acc += __ldg(a.coef + ilv(4, 1, g)) * val1(g - 1);
+            acc += c.x;
+            if (x < a.nx - 1) acc += __ldg(a.coef + ilv(4, 0, g)) * c.y;
+            acc += __ldg(a.coef + ilv(4, 2, g)) * nv.x;
+            r0 = acc;
+        }
+        if (k1 == TH_FULL) {
+            const long long g1 = g + 1;
+            double acc = __ldg(a.coef + ilv(4, 3, g1)) * sv.y;
+            acc += __ldg(a.coef + ilv(4, 1, g1)) * c.x;  // x + 1 > 0
+            acc += c.y;
+            if (x + 1 < a.nx - 1) acc += __ldg(a.coef + ilv(4, 0, g1)) * val1(g + 2);
+            acc += __ldg(a.coef + ilv(4, 2, g1)) * nv.y;
+            r1 = acc;
+        }
+    }
+    return make_double2(r0, r1);
 }
 
 __global__ void __launch_bounds__(GM_THREADS, 2) bicgstab_kernel(const ThermalArgs a) {
+    const long long npairs = a.D / 2;
     const long long stride = (long long)gridDim.x * GM_THREADS;
     const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
-    auto node_x = [&](long long g) { return (int)(g % a.P); };
-    auto kind_of = [&](long long g, int x) { return th_row((uint16_t)a.ntype[g], x, a.nx); };
+    auto kinds = [&](long long g, int x, int& k0, int& k1) {
+        const unsigned int t2 = *reinterpret_cast<const unsigned int*>(a.ntype + g);
+        k0 = th_row((int)(t2 & 0xffff), x, a.nx);
+        k1 = th_row((int)(t2 >> 16), x + 1, a.nx);
+    };
 
-    // ---- step 1: ||b||_1 --------------------------------------------------------
+    // ---- R: steps 1-4: ||b||_1; r = b - A x; r0 = r; rho = <r, r> -------------------
     {
-        double acc[1] = {0.0};
-        for (long long g = t0; g < a.D; g += stride) acc[0] += fabs(__ldcg(a.b + g));
-        block_reduce_slots<1>(acc, 1, a.part, 0);
+        double acc[2] = {0.0, 0.0};
+        auto x2 = [&](long long n) { return ld2(a.x + n); };
+        auto x1 = [&](long long n) { return __ldcg(a.x + n); };
+        for (long long pr = t0; pr < npairs; pr += stride) {
+            const long long g = 2 * pr;
+            const int x = (int)(g % a.P);
+            int k0, k1;
+            kinds(g, x, k0, k1);
+            const double2 ax = th_apply2(a, g, x, k0, k1, x2, x1);
+            const double2 b = ld2(a.b + g);
+            const double r0 = b.x - ax.x, r1 = b.y - ax.y;
+            st2(a.b + g, r0, r1);
+            st2(a.r0 + g, r0, r1);
+            acc[0] += fabs(b.x) + fabs(b.y);
+            acc[1] += r0 * r0 + r1 * r1;
+        }
+        block_reduce_slots<2>(acc, 2, a.part, 0);
     }
-    if (!th_sync(a, TS_NORMB)) return;
+    if (!th_sync(a, TS_RES0)) return;
     if (ldc(&a.ctl->state) == TH_TRIVIAL) {
-        for (long long g = t0; g < a.D; g += stride) a.x[g] = __ldcg(a.b + g);
+        // b == 0: x = b (BiCGStabSolver.cpp:654-658); b holds r = b - A x now,
+        // so b is rebuilt as r + A x into s first, then copied to x and b
+        auto x2 = [&](long long n) { return ld2(a.x + n); };
+        auto x1 = [&](long long n) { return __ldcg(a.x + n); };
+        for (long long pr = t0; pr < npairs; pr += stride) {
+            const long long g = 2 * pr;
+            const int x = (int)(g % a.P);
+            int k0, k1;
+            kinds(g, x, k0, k1);
+            const double2 ax = th_apply2(a, g, x, k0, k1, x2, x1);
+            const double2 r = ld2(a.b + g);
+            st2(a.s + g, r.x + ax.x, r.y + ax.y);
+        }
+        if (!th_sync(a, TS_NONE)) return;
+        for (long long pr = t0; pr < npairs; pr += stride) {
+            const long long g = 2 * pr;
+            const double2 v = ld2(a.s + g);
+            st2(a.x + g, v.x, v.y);
+            st2(a.b + g, v.x, v.y);
+        }
         return;
     }
-    // ---- steps 2-4: r = b - A x; r0 = p = r; rho = <r, r> ------------------------
-    {
-        double acc[1] = {0.0};
-        for (long long g = t0; g < a.D; g += stride) {
-            const int x = node_x(g);
-            const double ax = th_apply(a, kind_of(g, x), g, x, [&](long long n) { return __ldcg(a.x + n); });
-            const double r = __ldcg(a.b + g) - ax;
-            __stcg(a.b + g, r);
-            __stcg(a.r0 + g, r);
-            __stcg(a.p[0] + g, r);
-            acc[0] += r * r;
-        }
-        block_reduce_slots<1>(acc, 1, a.part, 0);
-    }
-    if (!th_sync(a, TS_RHO0)) return;
 
-    int pc = 0, vc = 0;  // current p and v buffers
+    const double* pcur = a.r0;  // p of the last iteration (iteration 0: r0 = r)
+    int vc = 0;                 // v of the last iteration
     for (int it = 0; it < a.max_iters; ++it) {
-        // ---- B: p = r + beta (p - omega v) (iteration 0: p), v = A p, <v, r0> ----
+        // ---- B: p = r + beta (p - omega v), v = A p, <v, r0> -------------------------
+        double* pnew = (pcur == a.p[0]) ? a.p[1] : a.p[0];
         {
             const double beta = ldc(&a.ctl->beta), omega = ldc(&a.ctl->omega);
-            const double* pold = a.p[pc];
             const double* vold = a.v[vc];
-            double* pnew = a.p[pc ^ 1];
             double* vnew = a.v[vc ^ 1];
-            auto pval = [&](long long n) -> double {
-                return it == 0 ? __ldcg(pold + n)
-                               : __ldcg(a.b + n) + beta * (__ldcg(pold + n) - omega * __ldcg(vold + n));
+            auto p2 = [&](long long n) -> double2 {
+                const double2 po = ld2(pcur + n);
+                if (it == 0) return po;
+                const double2 r = ld2(a.b + n), vo = ld2(vold + n);
+                return make_double2(r.x + beta * (po.x - omega * vo.x), r.y + beta * (po.y - omega * vo.y));
+            };
+            auto p1 = [&](long long n) -> double {
+                const double po = __ldcg(pcur + n);
+                if (it == 0) return po;
+                return __ldcg(a.b + n) + beta * (po - omega * __ldcg(vold + n));
             };
             double acc[1] = {0.0};
-            for (long long g = t0; g < a.D; g += stride) {
-                const int x = node_x(g);
-                const double v = th_apply(a, kind_of(g, x), g, x, pval);
-                __stcg(pnew + g, pval(g));
-                __stcg(vnew + g, v);
-                acc[0] += v * __ldcg(a.r0 + g);
+            for (long long pr = t0; pr < npairs; pr += stride) {
+                const long long g = 2 * pr;
+                const int x = (int)(g % a.P);
+                int k0, k1;
+                kinds(g, x, k0, k1);
+                const double2 v = th_apply2(a, g, x, k0, k1, p2, p1);
+                if (it > 0) {
+                    const double2 pv = p2(g);
+                    st2(pnew + g, pv.x, pv.y);
+                }
+                st2(vnew + g, v.x, v.y);
+                const double2 rr = ld2(a.r0 + g);
+                acc[0] += v.x * rr.x + v.y * rr.y;
             }
             block_reduce_slots<1>(acc, 1, a.part, 0);
         }
-        pc ^= 1;
+        if (it > 0) pcur = pnew;
         vc ^= 1;
         if (!th_sync(a, TS_ALPHA)) return;
-        // ---- C: s = r - alpha v, t = A s, ||s||_1 ----------------------------------
+        // ---- C: s = r - alpha v, ||s||_1 ---------------------------------------------
         const double alpha = ldc(&a.ctl->alpha);
         {
             const double* v = a.v[vc];
-            auto sval = [&](long long n) -> double { return __ldcg(a.b + n) - alpha * __ldcg(v + n); };
             double acc[1] = {0.0};
-            for (long long g = t0; g < a.D; g += stride) {
-                const int x = node_x(g);
-                const double tv = th_apply(a, kind_of(g, x), g, x, sval);
-                const double s = sval(g);
-                __stcg(a.s + g, s);
-                __stcg(a.t + g, tv);
-                acc[0] += fabs(s);
+            for (long long pr = t0; pr < npairs; pr += stride) {
+                const long long g = 2 * pr;
+                const double2 r = ld2(a.b + g), vv = ld2(v + g);
+                const double s0 = r.x - alpha * vv.x, s1 = r.y - alpha * vv.y;
+                st2(a.s + g, s0, s1);
+                acc[0] += fabs(s0) + fabs(s1);
             }
             block_reduce_slots<1>(acc, 1, a.part, 0);
         }
         if (!th_sync(a, TS_CHECK1)) return;
         if (ldc(&a.ctl->state) != TH_RUNNING) {
             // shCalc's x += alpha p and r = s stand (BiCGStabSolver.cpp:694-701)
-            for (long long g = t0; g < a.D; g += stride) {
-                a.x[g] = __ldcg(a.x + g) + alpha * __ldcg(a.p[pc] + g);
-                __stcg(a.b + g, __ldcg(a.s + g));
+            for (long long pr = t0; pr < npairs; pr += stride) {
+                const long long g = 2 * pr;
+                const double2 xv = ld2(a.x + g), pv = ld2(pcur + g), sv = ld2(a.s + g);
+                st2(a.x + g, xv.x + alpha * pv.x, xv.y + alpha * pv.y);
+                st2(a.b + g, sv.x, sv.y);
             }
             return;
         }
-        // ---- D: x = (x + alpha p) + omega s, r = s - omega t, ||r||_1, <r, r0> -----
+        // ---- D: t = A s, x = (x + alpha p) + omega s, r = s - omega t ------------------
         {
             const double omega = ldc(&a.ctl->omega);
+            auto s2 = [&](long long n) { return ld2(a.s + n); };
+            auto s1 = [&](long long n) { return __ldcg(a.s + n); };
             double acc[2] = {0.0, 0.0};
-            for (long long g = t0; g < a.D; g += stride) {
-                const double s = __ldcg(a.s + g);
-                const double xh = __ldcg(a.x + g) + alpha * __ldcg(a.p[pc] + g);
-                __stcg(a.x + g, xh + omega * s);
-                const double r = s - omega * __ldcg(a.t + g);
-                __stcg(a.b + g, r);
-                acc[0] += fabs(r);
-                acc[1] += r * __ldcg(a.r0 + g);
+            for (long long pr = t0; pr < npairs; pr += stride) {
+                const long long g = 2 * pr;
+                const int x = (int)(g % a.P);
+                int k0, k1;
+                kinds(g, x, k0, k1);
+                const double2 t = th_apply2(a, g, x, k0, k1, s2, s1);
+                const double2 sv = ld2(a.s + g), xv = ld2(a.x + g), pv = ld2(pcur + g);
+                const double xh0 = xv.x + alpha * pv.x, xh1 = xv.y + alpha * pv.y;
+                st2(a.x + g, xh0 + omega * sv.x, xh1 + omega * sv.y);
+                const double r0 = sv.x - omega * t.x, r1 = sv.y - omega * t.y;
+                st2(a.b + g, r0, r1);
+                const double2 rr = ld2(a.r0 + g);
+                acc[0] += fabs(r0) + fabs(r1);
+                acc[1] += r0 * rr.x + r1 * rr.y;
             }
             block_reduce_slots<2>(acc, 2, a.part, 0);
         }
