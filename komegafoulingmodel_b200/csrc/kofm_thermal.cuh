@@ -67,20 +67,22 @@ __global__ void thermal_assemble_kernel(const ThermalAsm p) {
     if (x >= p.nx) return;
     const int t = (uint16_t)p.ntype[g];
     if (t & M0_SOLID) return;
-    double dx[4] = {1.0, 1.0, 1.0, 1.0};
+    // 3-point weights of the first and second derivatives; whole links (no
+    // record) give the exact constants 1/2, -1/2, 0 and 1, 1, -2
+    double dXe = 0.5, dXw = -0.5, dXc = 0.0, dYn = 0.5, dYs = -0.5, dYc = 0.0;
+    double dX2e = 1.0, dX2w = 1.0, dX2c = -2.0, dY2n = 1.0, dY2s = 1.0, dY2c = -2.0;
     const int r = p.dxidx[g];
     if (r >= 0) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) dx[k] = p.dxrec[r].dx[k];
+        const DxRecord rec = p.dxrec[r];
+        const double dxe = fmax(rec.dx[0], 0.1), dxw = fmax(rec.dx[1], 0.1), dxc = fmax(dxe + dxw, 0.1);
+        const double dyn = fmax(rec.dx[2], 0.1), dys = fmax(rec.dx[3], 0.1), dyc = fmax(dyn + dys, 0.1);
+        dXe = dxw / (dxe * dxc); dXw = -dxe / (dxw * dxc); dXc = (dxe - dxw) / (dxe * dxw);
+        dYn = dys / (dyn * dyc); dYs = -dyn / (dys * dyc); dYc = (dyn - dys) / (dyn * dys);
+        dX2e = 2. / (dxe * dxc); dX2w = 2. / (dxw * dxc); dX2c = -2. / (dxe * dxw);
+        dY2n = 2. / (dyn * dyc); dY2s = 2. / (dys * dyc); dY2c = -2. / (dyn * dys);
+        if (fabs(dXc) > 10.) { dXe = 1.0 / dxc; dXw = -1.0 / dxc; dXc = 0.0; }
+        if (fabs(dYn) > 10.) { dYn = 1.0 / dyc; dYs = -1.0 / dyc; dYc = 0.0; }
     }
-    const double dxe = fmax(dx[0], 0.1), dxw = fmax(dx[1], 0.1), dxc = fmax(dxe + dxw, 0.1);
-    const double dyn = fmax(dx[2], 0.1), dys = fmax(dx[3], 0.1), dyc = fmax(dyn + dys, 0.1);
-    double dXe = dxw / (dxe * dxc), dXw = -dxe / (dxw * dxc), dXc = (dxe - dxw) / (dxe * dxw);
-    double dYn = dys / (dyn * dyc), dYs = -dyn / (dys * dyc), dYc = (dyn - dys) / (dyn * dys);
-    const double dX2e = 2. / (dxe * dxc), dX2w = 2. / (dxw * dxc), dX2c = -2. / (dxe * dxw);
-    const double dY2n = 2. / (dyn * dyc), dY2s = 2. / (dys * dyc), dY2c = -2. / (dyn * dys);
-    if (fabs(dXc) > 10.) { dXe = 1.0 / dxc; dXw = -1.0 / dxc; dXc = 0.0; }
-    if (fabs(dYn) > 10.) { dYn = 1.0 / dyc; dYs = -1.0 / dyc; dYc = 0.0; }
     double alpha = (t & M_SOLID) ? p.alpha_foul : p.alpha_fluid;
     const long long row = (long long)y * p.P;
     const long long gw = row + (x > 0 ? x - 1 : p.nx - 1), ge = row + (x < p.nx - 1 ? x + 1 : 0);
@@ -281,7 +283,7 @@ __device__ __forceinline__ double2 th_apply2(const ThermalArgs& a, long long g, 
     return make_double2(r0, r1);
 }
 
-__global__ void __launch_bounds__(GM_THREADS, 2) bicgstab_kernel(const ThermalArgs a) {
+__global__ void __launch_bounds__(GM_THREADS, 4) bicgstab_kernel(const ThermalArgs a) {
     const long long npairs = a.D / 2;
     const long long stride = (long long)gridDim.x * GM_THREADS;
     const long long t0 = (long long)blockIdx.x * GM_THREADS + threadIdx.x;
