@@ -167,6 +167,44 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
                    np.asarray(ibb_q, float)[order], y_bot=y_bot, y_top=y_top)
 
 
+def read_reference_walls(directory: str):
+    """The wall polylines of a reference run directory: lbsize.txt ("nX nY"),
+    lsc0.txt (one "x y" point per line) and lsbl.txt (one "i j" segment per
+    line, 0-based point indices) -- the files clVariablesLS::allocateArrays
+    loads (clVariablesLS.cpp:45-50) and MakeChannel_Test.m writes.  Returns
+    (nx, ny, y_bot, y_top): the two walls' heights at every column, where
+    each column crosses exactly two segments (the lower wall and the upper)."""
+    import os
+    size = np.loadtxt(os.path.join(directory, "lbsize.txt")).ravel()
+    nx, ny = int(size[0]), int(size[1])
+    pts = np.loadtxt(os.path.join(directory, "lsc0.txt"), ndmin=2)
+    segs = np.loadtxt(os.path.join(directory, "lsbl.txt"), ndmin=2).astype(np.int64)
+    xa, ya = pts[segs[:, 0], 0], pts[segs[:, 0], 1]
+    xb, yb = pts[segs[:, 1], 0], pts[segs[:, 1], 1]
+    lo, hi = np.minimum(xa, xb), np.maximum(xa, xb)
+    y_bot = np.full(nx, np.inf)
+    y_top = np.full(nx, -np.inf)
+    for x in range(nx):
+        on = (lo <= x) & (x <= hi) & (hi > lo)
+        if not np.any(on):
+            raise ValueError(f"column {x} crosses no wall segment")
+        t = (x - xa[on]) / (xb[on] - xa[on])
+        y = ya[on] + t * (yb[on] - ya[on])
+        y_bot[x], y_top[x] = y.min(), y.max()
+        if not y_top[x] > y_bot[x]:
+            raise ValueError(f"column {x} crosses only one wall")
+    return nx, ny, y_bot, y_top
+
+
+def channel_from_reference_files(directory: str, nx_full: int | None = None) -> Channel:
+    """channel_from_walls on the wall polylines of a reference run directory
+    (read_reference_walls).  The polylines are sampled at the integer
+    columns, so walls whose vertices lie between columns are represented by
+    the straight segments between those samples."""
+    nx, ny, y_bot, y_top = read_reference_walls(directory)
+    return channel_from_walls(nx, ny, y_bot, y_top, nx_full)
+
+
 def wavy_channel(nx: int, ny: int, amplitude: float, wavelength: int,
                  nx_full: int | None = None) -> Channel:
     """Walls displaced by h(x) = A (1 - cos(2 pi x / L)) / 2 from the half-way

@@ -150,3 +150,46 @@ def test_wavy_komega_matches_oracle(kofm_lib, oracle):
         err = rel_l2(gpu, ref, fl)
         print("100 steps", name, err, spread)
         assert err < 5 * spread + 1e-6, (name, err, spread)
+
+
+def _write_reference_walls(d, nx, ny, bottom, top, dx=1.0):
+    """Wall files in the layout of a reference run directory: points every dx
+    from x = -0.75 along the lower wall to past nx - 0.5, then back along the
+    upper wall; segments join consecutive points of each wall."""
+    import os
+    xs = [-0.75]
+    while xs[-1] <= nx - 0.5:
+        xs.append(xs[-1] + dx)
+    xs = np.array(xs)
+    pts = [(x, bottom(x)) for x in xs] + [(x, top(x)) for x in xs[::-1]]
+    n = len(xs)
+    segs = [(i, i + 1) for i in range(n - 1)] + [(n + i, n + i + 1) for i in range(n - 1)]
+    os.makedirs(d, exist_ok=True)
+    np.savetxt(os.path.join(d, "lsc0.txt"), np.array(pts))
+    np.savetxt(os.path.join(d, "lsbl.txt"), np.array(segs), fmt="%d")
+    np.savetxt(os.path.join(d, "lbsize.txt"), np.array([[nx, ny]]), fmt="%d")
+
+
+def test_reference_wall_files(tmp_path):
+    """lsc0 / lsbl / lbsize files (straight walls of the reference's channel
+    script: y = nY/2 - 1 + 0.5 -/+ H) and a wavy pair give the channel that
+    channel_from_walls builds from the same heights."""
+    nx, H = 96, 20
+    ny = 2 * H + 4
+    yini = ny / 2 - 1 + 0.5
+    _write_reference_walls(str(tmp_path / "s"), nx, ny, lambda x: yini - H, lambda x: yini + H)
+    ch = G.channel_from_reference_files(str(tmp_path / "s"))
+    ref = G.channel_from_walls(nx, ny, np.full(nx, yini - H), np.full(nx, yini + H))
+    assert np.array_equal(ch.ntype, ref.ntype) and np.array_equal(ch.dX, ref.dX)
+    assert np.array_equal(ch.ibb_idx, ref.ibb_idx) and np.allclose(ch.wallD, ref.wallD)
+    # wavy walls with vertices at the columns (dx = 1 from x = -0.75 misses
+    # them; dx = 0.25 from -0.75 hits every column)
+    amp, lam = 4.0, 48
+    h = lambda x: amp * 0.5 * (1 - np.cos(2 * np.pi * x / lam))  # noqa: E731
+    _write_reference_walls(str(tmp_path / "w"), nx, ny, lambda x: 0.5 + h(x),
+                           lambda x: ny - 1.5 - h(x), dx=0.25)
+    ch = G.channel_from_reference_files(str(tmp_path / "w"))
+    x = np.arange(nx)
+    ref = G.channel_from_walls(nx, ny, 0.5 + h(x), ny - 1.5 - h(x))
+    assert np.array_equal(ch.ntype, ref.ntype)
+    assert np.allclose(ch.dX, ref.dX, atol=1e-12) and np.allclose(ch.ibb_q, ref.ibb_q, atol=1e-12)
