@@ -38,12 +38,15 @@ class Channel:
     """Geometry arrays of one channel (reference padded layout)."""
 
     def __init__(self, nx, ny, nx_full, ntype, dX, wallD, ibb_idx=None, ibb_q=None,
-                 y_bot=None, y_top=None):
+                 y_bot=None, y_top=None, dX0=None):
         self.nx, self.ny, self.nx_full = nx, ny, nx_full
         self.ntype, self.dX, self.wallD = ntype, dX, wallD
         self.ibb_idx = np.zeros(0, np.int32) if ibb_idx is None else ibb_idx
         self.ibb_q = np.zeros(0) if ibb_q is None else ibb_q
         self.y_bot, self.y_top = y_bot, y_top
+        # link fractions of the unfouled walls (dXArr0); the same as dX when
+        # the channel has no fouling layer
+        self.dX0 = dX if dX0 is None else dX0
 
     @property
     def n(self):
@@ -112,43 +115,80 @@ def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius=None):
     return wall
 
 
+def _fluid(nx, ny, nxf, y_bot, y_top):
+    j = np.arange(ny)
+    fluid = np.zeros((ny, nxf), bool)
+    fluid[:, :nx] = (j[:, None] > y_bot[None, :]) & (j[:, None] < y_top[None, :])
+    fluid[0, :] = False
+    fluid[ny - 1, :] = False
+    return fluid
+
+
+def _wall_links(nx, ny, nxf, fluid, q):
+    """Fluid nodes whose link in direction q ends in a solid node."""
+    solid = ~fluid
+    solid[:, nx:] = False
+    j = np.arange(ny)
+    nb_solid = np.zeros((ny, nxf), bool)
+    jn = j + CY[q]
+    valid = (jn >= 0) & (jn < ny)
+    src = np.roll(solid[:, :nx], -CX[q], axis=1)
+    rows = np.where(valid)[0]
+    nb_solid[rows, :nx] = src[jn[rows], :]
+    return fluid & nb_solid
+
+
 def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = None,
-                       wall_radius: int = 40) -> Channel:
+                       wall_radius: int = 40, y_bot0=None, y_top0=None) -> Channel:
     """Channel between two walls given by their heights at every column (the
     wall polylines of clVariablesLS).  Node (i, j) is fluid iff
     y_bot[i] < j < y_top[i].  Builds the nType flags (per-direction wall bits
     of the links whose upstream node is solid), the E/W/N/S link fractions
     dXArr, the interpolated bounce-back list (link from a fluid node into the
     wall, as node + D * dir, with its wall fraction q; links with q = 1/2 need
-    no correction and are left out) and the wall distance."""
+    no correction and are left out) and the wall distance.
+
+    y_bot0 / y_top0 give unfouled walls outside the fouled ones: the nodes
+    between them are the fouling layer (M0_FLUID | M_SOLID), the *0 flags and
+    dX0 (dXArr0) follow the unfouled walls (iniFillMap0 /
+    iniNodeBoundaryInfo0, clVariablesLS.cpp:920-951), everything the flow
+    uses follows the fouled ones (iniNodeBoundaryInfo, 953-998)."""
     nxf = nx if nx_full is None else nx_full
     y_bot = np.asarray(y_bot, float)
     y_top = np.asarray(y_top, float)
+    fouled = y_bot0 is not None or y_top0 is not None
+    y_bot0 = y_bot if y_bot0 is None else np.asarray(y_bot0, float)
+    y_top0 = y_top if y_top0 is None else np.asarray(y_top0, float)
+    if np.any(y_bot0 > y_bot) or np.any(y_top0 < y_top):
+        raise ValueError("the unfouled walls must lie outside the fouled ones")
     j = np.arange(ny)
-    fluid = np.zeros((ny, nxf), bool)
-    fluid[:, :nx] = (j[:, None] > y_bot[None, :]) & (j[:, None] < y_top[None, :])
-    fluid[0, :] = False
-    fluid[ny - 1, :] = False
-    solid = ~fluid
-    solid[:, nx:] = False
-    t = np.where(fluid, M0_FLUID | M_FLUID, M0_SOLID | M_SOLID).astype(np.int32)
+    fluid = _fluid(nx, ny, nxf, y_bot, y_top)
+    fluid0 = _fluid(nx, ny, nxf, y_bot0, y_top0)
+    t = np.where(fluid0, M0_FLUID, M0_SOLID) | np.where(fluid, M_FLUID, M_SOLID)
+    t = t.astype(np.int32)
+    t[:, nx:] = M0_SOLID | M_SOLID
     dX = np.zeros((4, ny, nxf))
     dX[:, fluid] = 1.0
+    dX0 = np.zeros((4, ny, nxf))
+    dX0[:, fluid0] = 1.0
     D = nxf * ny
     ibb_idx, ibb_q = [], []
     for q in range(1, 9):
-        nb_solid = np.zeros((ny, nxf), bool)
-        jn = j + CY[q]
-        valid = (jn >= 0) & (jn < ny)
-        src = np.roll(solid[:, :nx], -CX[q], axis=1)
-        rows = np.where(valid)[0]
-        nb_solid[rows, :nx] = src[jn[rows], :]
-        hit = fluid & nb_solid
-        t[hit] |= BOUND[q] | BOUNDARY0
+        # unfouled domain
+        hit0 = _wall_links(nx, ny, nxf, fluid0, q)
+        t[hit0] |= BOUNDARY0
         if q < 5:
-            t[hit] |= NESW_BOUNDARY0
+            t[hit0] |= NESW_BOUNDARY0
+            ii, jv = np.nonzero(hit0.T)
+            t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY0
+            jv, ii = np.nonzero(hit0)
+            dX0[q - 1, jv, ii] = _link_fractions(ii, jv, q, nx, y_bot0, y_top0)
+        # fouled domain (the flow)
+        hit = _wall_links(nx, ny, nxf, fluid, q)
+        t[hit] |= BOUND[q]
+        if q < 5:
             ii, jv = np.nonzero(hit.T)
-            t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY | SOLID_BOUNDARY0
+            t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY
         jv, ii = np.nonzero(hit)
         frac = _link_fractions(ii, jv, q, nx, y_bot, y_top)
         if q < 5:
@@ -164,7 +204,8 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
     order = np.argsort(ibb_idx, kind="stable")
     return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(), dX.ravel(),
                    wall.ravel(), np.asarray(ibb_idx, np.int32)[order],
-                   np.asarray(ibb_q, float)[order], y_bot=y_bot, y_top=y_top)
+                   np.asarray(ibb_q, float)[order], y_bot=y_bot, y_top=y_top,
+                   dX0=dX0.ravel() if fouled else None)
 
 
 def read_reference_walls(directory: str):

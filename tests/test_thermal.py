@@ -319,3 +319,88 @@ def test_gpu_thermal_run_matches_oracle(kofm_lib, oracle, komega):
     assert change > 1e-3            # the inlet front has moved in
     assert err < 1e-6 * max(change, 1.0)
     assert abs(tsum - T.sum()) <= 1e-12 * abs(T.sum()) and tmin == T.min()
+
+
+# ---- fouling layer: conjugate heat transfer ----------------------------------------
+
+def _fouled_channel(nx=160, ny=40):
+    """Straight unfouled walls at 0.5 and ny - 1.5 with a deposit 2.5-5.5
+    cells thick on both: the nodes between are the fouling layer
+    (M0_FLUID | M_SOLID), where T diffuses with LB_ALPHA_FOUL."""
+    x = np.arange(nx)
+    d = 4.0 + 1.5 * np.sin(2 * np.pi * x / 80.0)
+    return G.channel_from_walls(nx, ny, 0.5 + d, ny - 1.5 - d,
+                                y_bot0=np.full(nx, 0.5), y_top0=np.full(nx, ny - 1.5))
+
+
+def test_fouled_channel_flags():
+    ch = _fouled_channel()
+    t = (ch.ntype.astype(np.int32) & 0xFFFF)
+    foul = (t & G.M0_FLUID != 0) & (t & G.M_SOLID != 0)
+    assert foul.sum() > 2 * ch.nx * 2
+    clean = G.straight_channel(ch.nx, ch.ny)
+    ct = clean.ntype.astype(np.int32) & 0xFFFF
+    m0 = G.M0_SOLID | G.M0_FLUID | G.SOLID_BOUNDARY0 | G.NESW_BOUNDARY0 | G.BOUNDARY0
+    # the unfouled flags and link fractions are those of the clean channel
+    assert np.array_equal(t & m0, ct & m0)
+    assert np.array_equal(ch.dX0, clean.dX)
+    # the flow sees the deposit: its surface nodes are solid boundaries of the
+    # flow, fluid nodes next to it carry wall bits, and its links are cut
+    fl = ((t & G.M_FLUID) != 0).reshape(ch.ny, ch.nx_full)
+    tt = t.reshape(ch.ny, ch.nx_full)
+    assert np.any(foul & ((t & G.SOLID_BOUNDARY) != 0))
+    below_solid = fl[1:, :] & ~fl[:-1, :]
+    assert np.all((tt[1:, :][below_solid] & G.BOUND[4]) != 0)
+    assert len(ch.ibb_idx) > 0 and not np.array_equal(ch.dX, ch.dX0)
+
+
+def test_thermal_coeffs_fouling_layer_match_reference(oracle, refk):
+    ch = _fouled_channel()
+    cfg = make_cfg(ch.nx, ch.ny, 1.4, 1e-5, 0.02)
+    th = ThermalCfg(0.02 / 0.708, 0.003, 1 / 0.9, 2.0)
+    rng = np.random.default_rng(51)
+    fl = ch.fluid_mask().ravel()
+    T = 2.2 * rng.random(ch.n)
+    ux = np.where(fl, 0.04 * rng.random(ch.n), 0.0)
+    uy = np.where(fl, 0.004 * rng.standard_normal(ch.n), 0.0)
+    _, _, nut, _ = komega_state(ch, seed=52)
+    IA, JA, ind = oracle.csr_thermal(cfg, ch.ntype)
+    A, A2 = np.zeros(len(JA)), np.zeros(len(JA))
+    oracle.L.orc_csr_fill_solid_boundary_thermal(C.byref(cfg), ch.ntype, ind, A)
+    A2[:] = A
+    b, b2 = np.zeros(ch.n), np.zeros(ch.n)
+    oracle.L.orc_thermal_coeffs(C.byref(cfg), C.byref(th), ind, ch.ntype, ch.dX0, A, b, T, ux, uy,
+                                nut.ctypes.data, 1.0)
+    refk.L.ref_thermal_coeffs(C.byref(cfg), np.array([th.alpha_fluid, th.alpha_foul, th.pr_turb_inv,
+                                                      th.t_in]),
+                              ind, ch.ntype, ch.dX0.copy(), A2, b2, T.copy(), ux.copy(), uy.copy(),
+                              nut.copy(), 1.0)
+    assert np.array_equal(A, A2) and np.array_equal(b, b2)
+
+
+@pytest.mark.gpu
+def test_gpu_thermal_fouling_layer_matches_oracle(kofm_lib, oracle):
+    """Laminar flow over the deposit, heat conducted through it: the device
+    update with the unfouled link fractions (kofm_set_thermal_geometry) and
+    the fouling-layer diffusivity against the oracle run."""
+    ch = _fouled_channel()
+    rate, g, nu = 1.25, 2e-6, 0.1
+    (f,) = fp32_state(G.equilibrium_state(ch, ux=0.01))
+    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+    L, d = _thermal_lattice(ch, rate, g, nu, False, thermal_rel_tol=1e-12, alpha_foul=0.02)
+    T0 = G.temperature_field(ch)
+    th = ThermalCfg(nu / d.pr_number, d.alpha_foul, 1.0 / d.pr_turb_number, d.t_in)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q,
+                    thermal=dict(T=T0, cfg=th, dX0=ch.dX0, rel_tol=1e-12, abs_tol=d.thermal_abs_tol))
+    sim.step(40)
+    with L:
+        L.set_thermal_geometry(ch.dX0)
+        L.set_state(f)
+        L.set_temperature(T0)
+        L.step(40)
+        T = L.get_temperature()
+    t = ch.ntype.astype(np.int32) & 0xFFFF
+    dom = (t & G.M0_FLUID) != 0
+    err = rel_l2(T, sim.T, dom)
+    print(dict(err=err, change=rel_l2(sim.T, T0, dom)))
+    assert err < 1e-8
