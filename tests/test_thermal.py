@@ -324,11 +324,13 @@ def test_gpu_thermal_run_matches_oracle(kofm_lib, oracle, komega):
 # ---- fouling layer: conjugate heat transfer ----------------------------------------
 
 def _fouled_channel(nx=160, ny=40):
-    """Straight unfouled walls at 0.5 and ny - 1.5 with a deposit 2.5-5.5
-    cells thick on both: the nodes between are the fouling layer
-    (M0_FLUID | M_SOLID), where T diffuses with LB_ALPHA_FOUL."""
+    """Straight unfouled walls at 0.5 and ny - 1.5 with a deposit 3-6 cells
+    thick on both: the nodes between are the fouling layer (M0_FLUID |
+    M_SOLID), where T diffuses with LB_ALPHA_FOUL.  The deposit is flat and
+    half-way between rows at x = 0, so no link at the periodic seam has
+    2q > 1 (where the reference's lbIBB reads an unwrapped neighbour)."""
     x = np.arange(nx)
-    d = 4.0 + 1.5 * np.sin(2 * np.pi * x / 80.0)
+    d = 3.0 + 1.5 * (1.0 - np.cos(2 * np.pi * x / 80.0))
     return G.channel_from_walls(nx, ny, 0.5 + d, ny - 1.5 - d,
                                 y_bot0=np.full(nx, 0.5), y_top0=np.full(nx, ny - 1.5))
 
