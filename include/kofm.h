@@ -289,6 +289,20 @@ int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);
  * the fields unchanged.  No counterpart in the reference. */
 int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
 
+/* ---- discrete adjoint of the laminar step -----------------------------------
+ * No counterpart in the reference.  From the current state (a stepped FP32
+ * laminar context without thermal update), takes T steps and returns
+ *   J = sum over the T steps of j(FA), FA the populations a step gathers,
+ *   j = (mean rho of the fluid nodes of column 0 - that of column nx-1) / 3
+ *       + sum of the wall shear of TR_shear_1 (trKernelsShear.cl:175-222) at
+ *         the shear nodes of kofm_set_shear (none: the pressure term only),
+ *       computed from FA and its own moments,
+ * and dJ/dq for every interpolated bounce-back link given to
+ * kofm_set_geometry (its wall fraction q; dJdq may be NULL), by the hand-written
+ * adjoint of the gather + collide with states recomputed from sqrt(T)
+ * checkpoints.  The lattice ends T steps ahead. */
+int kofm_adjoint(kofm_ctx* ctx, int32_t T, double* J, double* dJdq);
+
 /* ---- reduction without device allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not let the library
  * allocate device memory (an application that owns a fixed device-memory

@@ -13,8 +13,10 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <new>
+#include <utility>
 #include <vector>
 
 using namespace kofm;
@@ -56,6 +58,7 @@ struct kofm_ctx {
     int32_t* rec = nullptr;           // per-node IBB record index
     IbbRecord* ibb = nullptr;
     int n_ibb_rec = 0;
+    std::vector<std::pair<long long, int>> ibb_links;  // input order: (device node, direction)
     int32_t* dxrec_idx = nullptr;     // per-node dX record index
     DxRecord* dxrec = nullptr;
     float* wallD = nullptr;
@@ -640,6 +643,7 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     // interpolated bounce-back records, one per node that owns a link
     std::vector<int32_t> rec((size_t)c->D, -1);
     std::vector<IbbRecord> recs;
+    std::vector<std::pair<long long, int>> links;
     for (int i = 0; i < n_ibb; ++i) {
         const long long loc = ibb_idx[i];
         const int dir = (int)(loc / Dh);
@@ -655,6 +659,7 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
             recs.push_back(r);
         }
         recs[rec[node]].q[dir - 1] = ibb_q[i];
+        links.emplace_back((long long)node, dir);
     }
     // FD link-fraction records for nodes whose dX differs from 1
     std::vector<int32_t> dxi((size_t)c->D, -1);
@@ -686,6 +691,7 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     if (c->ibb) { cudaFree(c->ibb); c->ibb = nullptr; }
     if (c->dxrec) { cudaFree(c->dxrec); c->dxrec = nullptr; }
     c->n_ibb_rec = (int)recs.size();
+    c->ibb_links.swap(links);
     if (!recs.empty()) {
         if (dalloc_t(&c->ibb, recs.size())) return KOFM_ERR_BUFFER_ALLOCATION;
         KOFM_CUDA_TRY(cudaMemcpy(c->ibb, recs.data(), recs.size() * sizeof(IbbRecord), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
@@ -1007,3 +1013,5 @@ int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
 #include "kofm_batch.inc"
 // thermal implicit FD
 #include "kofm_thermal_api.inc"
+// discrete adjoint of the laminar step
+#include "kofm_adjoint.inc"

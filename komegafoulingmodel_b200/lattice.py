@@ -68,6 +68,7 @@ class Lattice:
         check("kofm_set_geometry", self.lib.kofm_set_geometry(
             self._ctx, _ptr(ntype, C.c_int16), _ptr(wallD), _ptr(dX),
             _ptr(ii, C.c_int32), _ptr(qq), n_ibb))
+        self._n_ibb = n_ibb
 
     def set_state(self, f, k=None, omega=None, nut=None, sxy=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float64)
@@ -102,6 +103,15 @@ class Lattice:
     def thermal_update(self):
         """One clVariablesFD::Solve (kofm_thermal_update)."""
         check("kofm_thermal_update", self.lib.kofm_thermal_update(self._ctx))
+
+    def adjoint(self, nsteps, n_ibb=None):
+        """(J, dJ/dq) over nsteps from the current state (kofm_adjoint); dJ/dq
+        in the order of the IBB links given to set_geometry."""
+        n = self._n_ibb if n_ibb is None else n_ibb
+        J = C.c_double()
+        dq = np.zeros(max(n, 1))
+        check("kofm_adjoint", self.lib.kofm_adjoint(self._ctx, nsteps, C.byref(J), _ptr(dq)))
+        return J.value, dq[:n]
 
     def set_shear(self, sh):
         """Uploads a shear.ShearSetup (kofm_set_shear)."""

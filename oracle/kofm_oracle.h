@@ -183,6 +183,18 @@ void orc_thermal_solve(const orc_cfg* c, const orc_thermal_cfg* th, orc_thermal_
                        const double* ux, const double* uy, const double* nut, double* A,
                        double* b);
 
+/* ---- discrete adjoint of the laminar step (kofm_adjoint.c) --------------- */
+void orc_adj_collide(const orc_cfg* c, const int16_t* map, const double* FA, double* fstar);
+void orc_adj_stream(const orc_cfg* c, const int16_t* map, const int32_t* ibb, const double* q,
+                    int nibb, const double* fstar, double* FA);
+void orc_adj_stream_T(const orc_cfg* c, const int16_t* map, const int32_t* ibb, const double* q,
+                      int nibb, const double* lam, const double* fstar, double* nu, double* dq);
+double orc_adj_j(const orc_cfg* c, const int16_t* map, const double* FA, const int32_t* snodes,
+                 const double* cfss, int nshear, double* grad);
+double orc_adj_run(const orc_cfg* c, const int16_t* map, const int32_t* ibb, const double* q,
+                   int nibb, const double* FA0, int T, const int32_t* snodes, const double* cfss,
+                   int nshear, double* dq, double* dF0);
+
 double orc_sum(const double* a, int64_t n);
 double orc_min(const double* a, int64_t n);
 

@@ -123,6 +123,14 @@ class Oracle:
                                          C.c_double, C.c_int, C.POINTER(BicgStats)]
         L.orc_thermal_solve.argtypes = [cp, tp, C.POINTER(ThermalState), _i16, _i32, _i32, _i32,
                                         _dp, _dp, _dp, _dp, _dp, C.c_void_p, _dp, _dp]
+        L.orc_adj_collide.argtypes = [cp, _i16, _dp, _dp]
+        L.orc_adj_stream.argtypes = [cp, _i16, _i32, _dp, C.c_int, _dp, _dp]
+        L.orc_adj_stream_T.argtypes = [cp, _i16, _i32, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_adj_j.argtypes = [cp, _i16, _dp, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_adj_j.restype = C.c_double
+        L.orc_adj_run.argtypes = [cp, _i16, _i32, _dp, C.c_int, _dp, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_adj_run.restype = C.c_double
         L.orc_sum.argtypes = [_dp, C.c_int64]
         L.orc_sum.restype = C.c_double
         L.orc_min.argtypes = [_dp, C.c_int64]
@@ -162,6 +170,28 @@ class Oracle:
         self.L.orc_csr_build_thermal(C.byref(cfg), m, IA.ctypes.data, JA.ctypes.data,
                                      ind.ctypes.data)
         return IA, JA, ind
+
+
+def adj_run(orc, cfg, ch, FA0, T, q=None, shear_setup=None, want_dF0=False):
+    """orc_adj_run: (J, dJ/dq per IBB entry, dJ/dFA0 or None)."""
+    q = np.ascontiguousarray(ch.ibb_q if q is None else q, np.float64)
+    ibb = np.ascontiguousarray(ch.ibb_idx, np.int32)
+    dq = np.zeros(len(ibb))
+    dF0 = np.zeros_like(FA0) if want_dF0 else None
+    if shear_setup is not None:
+        sn = np.ascontiguousarray(shear_setup.nodes, np.int32)
+        cf = np.ascontiguousarray(shear_setup.cfss.ravel(), np.float64)
+        sp, cpp, ns = sn.ctypes.data, cf.ctypes.data, len(sn)
+    else:
+        sn = cf = None
+        sp = cpp = None
+        ns = 0
+    J = orc.L.orc_adj_run(C.byref(cfg), np.ascontiguousarray(ch.ntype, np.int16), ibb, q, len(ibb),
+                          np.ascontiguousarray(FA0, np.float64), T, sp, cpp, ns,
+                          dq.ctypes.data if len(dq) else None,
+                          dF0.ctypes.data if dF0 is not None else None)
+    del sn, cf
+    return J, dq, dF0
 
 
 class RefKernels:
