@@ -80,6 +80,64 @@ def _link_fractions(ii, jj, q, nx, y_bot, y_top):
     return np.where(np.isfinite(best), best, 0.5)
 
 
+def wall_fraction_jacobian(ch: Channel):
+    """d q / d (wall heights) of every interpolated bounce-back link of ch, in
+    the order of ch.ibb_idx: arrays (wall, col0, dq_dy0, col1, dq_dy1) with
+    wall 0 = bottom, 1 = top, q = (y0 - j) / (c_y - (y1 - y0)) the crossing
+    of the link from node (i, j) with the wall segment from (i, y0) to
+    (i + c_x, y1) (y1 = y0 for the vertical links).  Links whose fraction was
+    clamped to 1 get zero derivatives."""
+    D = ch.n
+    d = ch.ibb_idx // D
+    node = ch.ibb_idx % D
+    ii = node % ch.nx_full
+    jj = node // ch.nx_full
+    nx = ch.nx
+    n = len(d)
+    wall = np.zeros(n, np.int32)
+    col0 = ii.astype(np.int64)
+    col1 = np.zeros(n, np.int64)
+    g0 = np.zeros(n)
+    g1 = np.zeros(n)
+    for k in range(n):
+        q = int(d[k])
+        cx, cy = int(CX[q]), int(CY[q])
+        best, pick = np.inf, None
+        for w, y_w in enumerate((ch.y_bot, ch.y_top)):
+            y0 = y_w[ii[k]]
+            y1 = y_w[(ii[k] + cx) % nx] if cx != 0 else y0
+            den = cy - (y1 - y0)
+            if den == 0.0:
+                continue
+            t = (y0 - jj[k]) / den
+            if 0.0 < t <= 1.0 + 1e-12 and t < best:
+                best, pick = t, (w, y0, y1, den)
+        if pick is None:
+            continue
+        w, y0, y1, den = pick
+        wall[k] = w
+        col1[k] = (ii[k] + cx) % nx
+        if best > 1.0:
+            continue
+        N = y0 - jj[k]
+        if cx == 0:
+            g0[k] = 1.0 / den
+        else:
+            g0[k] = (den - N) / den ** 2
+            g1[k] = N / den ** 2
+    return wall, col0, g0, col1, g1
+
+
+def shape_gradient(ch: Channel, dJdq):
+    """dJ/d(wall heights) from dJ/dq (kofm_adjoint): (dJ/dy_bot, dJ/dy_top),
+    one value per column."""
+    wall, c0, g0, c1, g1 = wall_fraction_jacobian(ch)
+    out = np.zeros((2, ch.nx))
+    np.add.at(out, (wall, c0), np.asarray(dJdq) * g0)
+    np.add.at(out, (wall, c1), np.asarray(dJdq) * g1)
+    return out[0], out[1]
+
+
 def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius=None):
     """Distance of every fluid node to the nearest wall polyline (segments
     between neighbouring columns, periodic in x) -- the quantity of
