@@ -40,6 +40,16 @@ struct DevBuf {
 
 }  // namespace
 
+// device work memory of kofm_adjoint, kept between calls
+struct AdjWork {
+    float* cps = nullptr;  size_t cps_b = 0;   // checkpoints
+    float* seg = nullptr;  size_t seg_b = 0;   // recomputed states of a segment
+    double* lam = nullptr; size_t lam_b = 0;
+    double* nu = nullptr;  size_t nu_b = 0;
+    double* jpart = nullptr; size_t jpart_b = 0;
+    double* dq = nullptr;  size_t dq_b = 0;
+};
+
 struct kofm_ctx {
     kofm_desc desc{};
     int P = 0;            // device row pitch (nodes)
@@ -99,6 +109,8 @@ struct kofm_ctx {
     double* shear_bl_w = nullptr;     // [n_bl][4]
     double* shear_bl_tau = nullptr;   // [n_bl]
     int shear_n = 0, shear_nbl = 0;
+    int32_t* shear_idx = nullptr;     // per device node: shear-node index or -1
+    AdjWork adj;
 
     // thermal implicit FD (kofm_thermal_*)
     double* T = nullptr;              // [D] temperature (tempArray), FP64
@@ -512,7 +524,8 @@ int kofm_destroy(kofm_ctx* c) {
                     c->gpart, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
                     c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
                     c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
-                    c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar};
+                    c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar, c->shear_idx,
+                    c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
@@ -825,10 +838,11 @@ int kofm_set_shear(kofm_ctx* c, const int32_t* nodes, int32_t n_nodes, const dou
     for (long long i = 0; i < 4LL * n_bl; ++i)
         if (bl_nodes[i] < -1 || bl_nodes[i] >= n_nodes) return KOFM_ERR_INVALID_ARG;
     cudaSetDevice(c->dev);
-    void* old[] = {c->shear_nodes, c->shear_cfss, c->shear_tau, c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau};
+    void* old[] = {c->shear_nodes, c->shear_cfss, c->shear_tau, c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau,
+                   c->shear_idx};
     for (void* b : old)
         if (b) cudaFree(b);
-    c->shear_nodes = nullptr; c->shear_cfss = nullptr; c->shear_tau = nullptr;
+    c->shear_nodes = nullptr; c->shear_cfss = nullptr; c->shear_tau = nullptr; c->shear_idx = nullptr;
     c->shear_bl_nodes = nullptr; c->shear_bl_w = nullptr; c->shear_bl_tau = nullptr;
     c->shear_n = c->shear_nbl = 0;
     int st;
@@ -845,6 +859,16 @@ int kofm_set_shear(kofm_ctx* c, const int32_t* nodes, int32_t n_nodes, const dou
     if (n_bl > 0) {
         KOFM_CUDA_TRY(cudaMemcpy(c->shear_bl_nodes, bl_nodes, sizeof(int32_t) * 4 * n_bl, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
         KOFM_CUDA_TRY(cudaMemcpy(c->shear_bl_w, bl_weights, sizeof(double) * 4 * n_bl, cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    }
+    {
+        std::vector<int32_t> idx((size_t)c->D, -1);
+        for (int i = 0; i < n_nodes; ++i) {
+            const int yy = nodes[i] / d.nx_full, xx = nodes[i] - yy * d.nx_full;
+            idx[(size_t)yy * c->P + xx] = i;
+        }
+        if ((st = dalloc_t(&c->shear_idx, (size_t)c->D))) return st;
+        KOFM_CUDA_TRY(cudaMemcpy(c->shear_idx, idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+                      KOFM_ERR_MEMORY_COPY);
     }
     c->shear_n = n_nodes;
     c->shear_nbl = n_bl;

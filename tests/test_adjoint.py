@@ -184,3 +184,24 @@ def test_torch_wrapper_gradient(kofm_lib, oracle):
     assert np.array_equal(c2.ntype, ch.ntype)
     J2 = WallShapeObjective.apply(yb2, yt2, F0, T, nx, ny)
     assert J2.item() < J.item()
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_c4_against_fp64_adjoint(kofm_lib, oracle):
+    """The adjoint case's lattice (1024 x 256, wall h(x) = sum_{m<=64} a_m
+    cos(2 pi m x / nx), a_m ~ N(0, (4/m)^2), seed 0) over 20 steps: device J
+    and dJ/dq against the FP64 oracle adjoint of the same run."""
+    from komegafoulingmodel_b200.adjoint import Case
+    case = Case(1024, 256)
+    ch = case.channel()
+    (F0,) = fp32_state(case.start(ch))
+    sh = shear.setup(ch)
+    T = 20
+    cfg = make_cfg(ch.nx, ch.ny, case.rate, case.fterm, case.nu)
+    J, dq, _ = adj_run(oracle, cfg, ch, F0, T, shear_setup=sh)
+    with case.lattice(ch) as L:
+        L.set_state(F0)
+        L.step(1)
+        Jg, dqg = L.adjoint(T)
+    print(dict(J=(J, Jg), dq_err=rel_l2(dqg, dq)))
+    assert abs(Jg - J) <= 1e-6 * abs(J) and rel_l2(dqg, dq) < 1e-4
