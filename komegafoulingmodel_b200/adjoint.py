@@ -30,14 +30,19 @@ def coefficients(n_modes: int = 64, seed: int = 0) -> np.ndarray:
 
 
 def walls(a: np.ndarray, nx: int, ny: int):
-    """Bottom wall 0.8 + h(x) - min h (above the half-way position, so no
-    link at the periodic seam needs the upstream neighbour), top wall
-    mirrored."""
+    """Bottom wall y = b + h(x) - h(0), top wall mirrored (ny - 1 - y).  The
+    offset b puts the wall at x = 0 (where every cosine is flat) 0.6 above a
+    row, so the first fluid row there is 0.4 away and no link across the
+    periodic seam has 2q > 1 (those read an unwrapped upstream neighbour in
+    the reference's lbIBB); b is the smallest such value that keeps the wall
+    at least 0.8 above row 0.  b is piecewise constant in a."""
     x = np.arange(nx)
     m = np.arange(1, len(a) + 1)
     h = (a[:, None] * np.cos(2 * np.pi * m[:, None] * x[None, :] / nx)).sum(0)
-    h = h - h.min()
-    return 0.8 + h, ny - 1.8 - h
+    h = h - h[0]
+    b = np.ceil(0.8 - h.min() - 0.6) + 0.6
+    yb = b + h
+    return yb, (ny - 1) - yb
 
 
 def modes(nx: int, n_modes: int) -> np.ndarray:
@@ -61,6 +66,15 @@ class Case:
     def channel(self, a=None):
         yb, yt = walls(self.a if a is None else a, self.nx, self.ny)
         return G.channel_from_walls(self.nx, self.ny, yb, yt, ibb_all=True)
+
+    def seam_ok(self, ch) -> bool:
+        """No interpolated link across the periodic seam has 2q > 1."""
+        D = ch.n
+        d = ch.ibb_idx // D
+        x = (ch.ibb_idx % D) % ch.nx_full
+        cx = G.CX[d]
+        seam = ((x == 0) & (cx == 1)) | ((x == ch.nx - 1) & (cx == -1))
+        return not np.any(seam & (ch.ibb_q > 0.5))
 
     def start(self, ch):
         y = np.arange(self.ny)[:, None]
@@ -122,11 +136,9 @@ def main(argv=None):
         adj_ms = (time.perf_counter() - t0) * 1e3
     gb, gt = G.shape_gradient(ch, dq)
     M = modes(args.nx, len(case.a))
-    # d y_bot / d a_m = cos(...) - [m-th mode at argmin h]; the min shift moves
-    # both walls by the same amount, so differentiate through walls() directly
-    yb0, yt0 = walls(case.a, args.nx, args.ny)
-    ib = int(np.argmin(yb0))
-    dyb = M - M[:, ib:ib + 1]
+    # y_bot = b + h(x) - h(0): d y_bot / d a_m = cos(2 pi m x / nx) - 1,
+    # y_top = ny - 1 - y_bot
+    dyb = M - 1.0
     dJda = dyb @ gb - dyb @ gt
     rng = np.random.default_rng(1)
     checks = []
@@ -134,9 +146,12 @@ def main(argv=None):
         d = rng.standard_normal(len(case.a))
         d /= np.linalg.norm(d)
         h = args.h
+        b0 = walls(case.a, args.nx, args.ny)[0][0]
         while True:
             cp, cm = case.channel(case.a + h * d), case.channel(case.a - h * d)
-            if (np.array_equal(cp.ntype, ch.ntype) and np.array_equal(cm.ntype, ch.ntype)
+            same_b = (walls(case.a + h * d, args.nx, args.ny)[0][0] == b0
+                      and walls(case.a - h * d, args.nx, args.ny)[0][0] == b0)
+            if (same_b and np.array_equal(cp.ntype, ch.ntype) and np.array_equal(cm.ntype, ch.ntype)
                     and np.array_equal(cp.ibb_idx, ch.ibb_idx) and np.array_equal(cm.ibb_idx, ch.ibb_idx)):
                 break
             h *= 0.25

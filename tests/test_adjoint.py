@@ -194,6 +194,7 @@ def test_gpu_adjoint_c4_against_fp64_adjoint(kofm_lib, oracle):
     from komegafoulingmodel_b200.adjoint import Case
     case = Case(1024, 256)
     ch = case.channel()
+    assert case.seam_ok(ch)   # the oracle follows the reference's unwrapped seam read
     (F0,) = fp32_state(case.start(ch))
     sh = shear.setup(ch)
     T = 20
