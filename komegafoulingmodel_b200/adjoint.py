@@ -29,19 +29,36 @@ def coefficients(n_modes: int = 64, seed: int = 0) -> np.ndarray:
     return rng.standard_normal(n_modes) * (4.0 / m)
 
 
-def walls(a: np.ndarray, nx: int, ny: int):
-    """Bottom wall y = b + h(x) - h(0), top wall mirrored (ny - 1 - y).  The
-    offset b puts the wall at x = 0 (where every cosine is flat) 0.6 above a
-    row, so the first fluid row there is 0.4 away and no link across the
-    periodic seam has 2q > 1 (those read an unwrapped upstream neighbour in
-    the reference's lbIBB); b is the smallest such value that keeps the wall
-    at least 0.8 above row 0.  b is piecewise constant in a."""
+def walls(a: np.ndarray, nx: int, ny: int, with_source: bool = False):
+    """Bottom wall y = b + h(x) - h(0), top wall mirrored (ny - 1 - y).
+
+    The offset b puts the wall at x = 0 (where every cosine is flat) 0.6
+    above a row, so the first fluid row there is 0.4 away and no link across
+    the periodic seam has 2q > 1 (those read an unwrapped upstream neighbour
+    in the reference's lbIBB); b is the smallest such value that keeps the
+    wall at least 0.8 above row 0 (piecewise constant in a).
+
+    A column that dips below both neighbours across a lattice row would leave
+    a one-node notch whose fluid node has wall links on both sides; there the
+    reference's lbIBB reads populations of a solid node (2q > 1 needs the
+    upstream neighbour, which is wall).  Such columns are lifted to their
+    lower neighbour's height; with_source also returns, per column, the
+    column whose height it carries."""
     x = np.arange(nx)
     m = np.arange(1, len(a) + 1)
     h = (a[:, None] * np.cos(2 * np.pi * m[:, None] * x[None, :] / nx)).sum(0)
     h = h - h[0]
     b = np.ceil(0.8 - h.min() - 0.6) + 0.6
     yb = b + h
+    src = np.arange(nx)
+    for i in range(nx):
+        lo = min(yb[(i - 1) % nx], yb[(i + 1) % nx])
+        if yb[i] < lo and np.floor(lo) > np.floor(yb[i]) and np.floor(lo) != lo:
+            j = (i - 1) % nx if yb[(i - 1) % nx] <= yb[(i + 1) % nx] else (i + 1) % nx
+            yb[i] = yb[j]
+            src[i] = j
+    if with_source:
+        return yb, (ny - 1) - yb, src
     return yb, (ny - 1) - yb
 
 
@@ -66,6 +83,16 @@ class Case:
     def channel(self, a=None):
         yb, yt = walls(self.a if a is None else a, self.nx, self.ny)
         return G.channel_from_walls(self.nx, self.ny, yb, yt, ibb_all=True)
+
+    @staticmethod
+    def notches(ch) -> int:
+        """Fluid nodes with wall links in two opposite directions."""
+        t = ch.ntype.astype(np.int32) & 0xFFFF
+        fl = (t & G.M_SOLID) == 0
+        n = 0
+        for q in (1, 3, 5, 7):
+            n += int(np.sum(fl & ((t & G.BOUND[q]) != 0) & ((t & G.BOUND[G.REV[q]]) != 0)))
+        return n
 
     def seam_ok(self, ch) -> bool:
         """No interpolated link across the periodic seam has 2q > 1."""
@@ -136,9 +163,10 @@ def main(argv=None):
         adj_ms = (time.perf_counter() - t0) * 1e3
     gb, gt = G.shape_gradient(ch, dq)
     M = modes(args.nx, len(case.a))
-    # y_bot = b + h(x) - h(0): d y_bot / d a_m = cos(2 pi m x / nx) - 1,
-    # y_top = ny - 1 - y_bot
-    dyb = M - 1.0
+    # y_bot = b + h(x) - h(0): d y_bot / d a_m = cos(2 pi m x / nx) - 1 (a
+    # lifted column follows the column it copies), y_top = ny - 1 - y_bot
+    src = walls(case.a, args.nx, args.ny, with_source=True)[2]
+    dyb = (M - 1.0)[:, src]
     dJda = dyb @ gb - dyb @ gt
     rng = np.random.default_rng(1)
     checks = []

@@ -27,6 +27,7 @@ NESW_BOUNDARY = 0x0F00
 CX = np.array([0, 1, -1, 0, 0, 1, -1, 1, -1])
 CY = np.array([0, 0, 0, 1, -1, 1, -1, -1, 1])
 W = np.array([4 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 9, 1 / 36, 1 / 36, 1 / 36, 1 / 36])
+REV = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7])
 
 
 def xsize_full(nx: int) -> int:

@@ -194,7 +194,10 @@ def test_gpu_adjoint_c4_against_fp64_adjoint(kofm_lib, oracle):
     from komegafoulingmodel_b200.adjoint import Case
     case = Case(1024, 256)
     ch = case.channel()
-    assert case.seam_ok(ch)   # the oracle follows the reference's unwrapped seam read
+    # the oracle follows the reference's lbIBB where it reads outside the
+    # fluid (the unwrapped seam neighbour, the wall node of a one-node notch);
+    # the case's walls have neither
+    assert case.seam_ok(ch) and case.notches(ch) == 0
     (F0,) = fp32_state(case.start(ch))
     sh = shear.setup(ch)
     T = 20
