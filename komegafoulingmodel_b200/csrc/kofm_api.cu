@@ -44,8 +44,8 @@ struct DevBuf {
 struct AdjWork {
     float* cps = nullptr;  size_t cps_b = 0;   // checkpoints
     float* seg = nullptr;  size_t seg_b = 0;   // recomputed states of a segment
-    double* lam = nullptr; size_t lam_b = 0;
-    double* nu = nullptr;  size_t nu_b = 0;
+    float* lam = nullptr;  size_t lam_b = 0;   // adjoint of the gathered populations
+    float* nu = nullptr;   size_t nu_b = 0;    // adjoint of the post-collision state
     double* jpart = nullptr; size_t jpart_b = 0;
     double* dq = nullptr;  size_t dq_b = 0;
 };
