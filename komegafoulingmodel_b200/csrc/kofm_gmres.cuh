@@ -93,7 +93,7 @@ struct GmresArgs {
     double rel_tol, abs_tol;
     long long spin_limit;     // barrier spin bound (polls of >= 100 ns)
     int full_cycle;           // 1: build all K vectors before the truncation tests
-    int strips;               // 32-column strips
+    int strips;               // strips of WS_OWN (30) own columns
 };
 
 // ---- coherent access to data written inside the launch (bypass L1) --------

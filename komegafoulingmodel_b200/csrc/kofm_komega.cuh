@@ -33,8 +33,9 @@ constexpr int KO_TX = 32, KO_TY = 8;
 // Multi-vector arrays (the 4 coefficients, the Krylov basis) are stored
 // tile-interleaved: the NV values of the 32 nodes of one row segment (node
 // index g = x + P y, P a multiple of 32) are contiguous, element (j, g) at
-// ((g / 32) NV + j) 32 + g % 32.  A warp sweeping a 32-column strip then
-// reads one contiguous block per row instead of NV separate row pieces.
+// ((g / 32) NV + j) 32 + g % 32.  A warp sweeping a strip of columns then
+// reads one or two contiguous blocks per row instead of NV separate row
+// pieces.
 __host__ __device__ __forceinline__ long long ilv(int nv, int j, long long g) {
     return ((g >> 5) * nv + j) * 32 + (g & 31);
 }
