@@ -299,9 +299,19 @@ int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
  *       computed from FA and its own moments,
  * and dJ/dq for every interpolated bounce-back link given to
  * kofm_set_geometry (its wall fraction q; dJdq may be NULL), by the hand-written
- * adjoint of the gather + collide with states recomputed from sqrt(T)
- * checkpoints.  The lattice ends T steps ahead. */
+ * adjoint of the gather + collide.  The forward's states are kept on the
+ * device as far as the cap of kofm_set_adjoint_memory allows; the rest are
+ * recomputed from checkpoints (one per segment of s steps, s >= ceil(sqrt(T))).
+ * The work buffers stay with the context for the next call.  The lattice ends
+ * T steps ahead. */
 int kofm_adjoint(kofm_ctx* ctx, int32_t T, double* J, double* dJdq);
+
+/* Device memory kofm_adjoint may hold for stored states: bytes < 0 (the
+ * default) = half of the free device memory at the call; 0 = only the
+ * checkpoints and one segment of ceil(sqrt(T)) steps; otherwise that many
+ * bytes (never fewer than the sqrt(T) minimum).  Results do not depend on it.
+ * No counterpart in the reference. */
+int kofm_set_adjoint_memory(kofm_ctx* ctx, int64_t bytes);
 
 /* ---- reduction without device allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not let the library

@@ -113,6 +113,7 @@ SIGNATURES = {
     "kofm_set_thermal_geometry": (C.c_int, [_vp, _dp]),
     "kofm_thermal_update": (C.c_int, [_vp]),
     "kofm_adjoint": (C.c_int, [_vp, C.c_int32, _dp, _dp]),
+    "kofm_set_adjoint_memory": (C.c_int, [_vp, C.c_int64]),
 }
 
 _LIB = None

@@ -48,6 +48,9 @@ struct AdjWork {
     float* nu = nullptr;   size_t nu_b = 0;    // adjoint of the post-collision state
     double* jpart = nullptr; size_t jpart_b = 0;
     double* dq = nullptr;  size_t dq_b = 0;
+    double* sgrad = nullptr; size_t sgrad_b = 0;  // shear-term gradients of a segment
+    int8_t* cls = nullptr; size_t cls_b = 0;      // node classes of the transposed gather
+    long long cap = -1;    // bytes for stored states (< 0: half the free memory)
 };
 
 struct kofm_ctx {
@@ -525,7 +528,7 @@ int kofm_destroy(kofm_ctx* c) {
                     c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
                     c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
                     c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar, c->shear_idx,
-                    c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq};
+                    c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq, c->adj.sgrad, c->adj.cls};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);

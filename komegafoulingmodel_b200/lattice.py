@@ -113,6 +113,11 @@ class Lattice:
         check("kofm_adjoint", self.lib.kofm_adjoint(self._ctx, nsteps, C.byref(J), _ptr(dq)))
         return J.value, dq[:n]
 
+    def set_adjoint_memory(self, nbytes):
+        """Cap on the device memory adjoint() keeps states in (< 0: half the
+        free memory; 0: sqrt(T) checkpoints only) (kofm_set_adjoint_memory)."""
+        check("kofm_set_adjoint_memory", self.lib.kofm_set_adjoint_memory(self._ctx, int(nbytes)))
+
     def set_shear(self, sh):
         """Uploads a shear.ShearSetup (kofm_set_shear)."""
         nodes = np.ascontiguousarray(sh.nodes, np.int32)

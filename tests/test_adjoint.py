@@ -64,7 +64,7 @@ def test_oracle_adjoint_matches_finite_differences(oracle):
         assert abs(fd - dF0 @ d) <= 1e-7 * abs(fd)
 
 
-def _gpu_adjoint(ch, sh, F0, T, q=None):
+def _gpu_adjoint(ch, sh, F0, T, q=None, mem=None):
     d = desc_default()
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = RATE, FTERM, MU
@@ -72,6 +72,8 @@ def _gpu_adjoint(ch, sh, F0, T, q=None):
         L.set_geometry(ch.ntype, None, None, ch.ibb_idx, ch.ibb_q if q is None else q)
         if sh is not None:
             L.set_shear(sh)
+        if mem is not None:
+            L.set_adjoint_memory(mem)
         L.set_state(F0)
         L.step(1)   # g^0 = collide(FA^0)
         return L.adjoint(T)
@@ -90,6 +92,22 @@ def test_gpu_adjoint_matches_oracle(kofm_lib, oracle, T):
     print(dict(T=T, J=(J, Jg), dq_err=rel_l2(dqg, dq)))
     assert abs(Jg - J) <= 1e-6 * abs(J)
     assert rel_l2(dqg, dq) < 1e-4
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_memory_cap_does_not_change_results(kofm_lib, oracle):
+    """Every state stored (default cap), sqrt(T) checkpoints only (cap 0) and a
+    cap between (segments of 6 states + 2 checkpoints for T = 17): the same
+    kernels on the same states, so J and dJ/dq agree bit for bit."""
+    ch, cfg, sh = _case(96, 40, 5.0, 48)
+    (F0,) = fp32_state(perturbed_state(ch, seed=6, u_mean=0.02))
+    T = 17
+    state = 4 * 9 * (-(-ch.nx_full // 128) * 128) * ch.ny   # FP32 state at the device row pitch
+    runs = [_gpu_adjoint(ch, sh, F0, T, mem=m) for m in (None, 0, 7 * state + 6 * 9 * 8 * len(sh.nodes))]
+    for J, dq in runs[1:]:
+        assert J == runs[0][0] and np.array_equal(dq, runs[0][1])
+    J, dq, _ = adj_run(oracle, cfg, ch, F0, T, shear_setup=sh)
+    assert abs(runs[0][0] - J) <= 1e-6 * abs(J) and rel_l2(runs[0][1], dq) < 1e-4
 
 
 @pytest.mark.gpu

@@ -81,9 +81,8 @@ def test_wavy_laminar_matches_oracle(kofm_lib, oracle, storage, tol):
     assert errs["rho"] < tol / 10 and errs["ux"] < tol and uy_rel < tol, (errs, uy_rel)
 
 
-def _wavy_komega_case():
-    nx, ny = 256, 66
-    ch = G.wavy_channel(nx, ny, 8.0, 128)
+def _wavy_komega_case(nx=256, ny=66, amp=8.0, lam=128):
+    ch = G.wavy_channel(nx, ny, amp, lam)
     nu, u_max = 5e-4, 0.05
     R = ch.pipe_radius
     y = np.arange(ny)[:, None] - 0.5
@@ -149,6 +148,48 @@ def test_wavy_komega_matches_oracle(kofm_lib, oracle):
         spread = rel_l2(alt, ref, fl)
         err = rel_l2(gpu, ref, fl)
         print("100 steps", name, err, spread)
+        assert err < 5 * spread + 1e-6, (name, err, spread)
+
+
+@pytest.mark.gpu
+def test_wavy_komega_2048x256_matches_oracle(kofm_lib, oracle):
+    """The 2048 x 256 wavy k-omega channel (walls 0.5 + 16 (1 - cos(2 pi x /
+    512)) and mirrored: a +-16 sine of wavelength 512 phased so that the
+    periodic seam sits at a crest, where no interpolated link has 2q > 1),
+    body-forced and periodic, nu = 5e-4, GMRES solves run to 1e-10: 10 steps
+    within 1e-5 of the FP64 oracle, 40 within a few times the oracle's own
+    spread under a 1e-7 perturbation of k."""
+    ch, f, k, o, nut, rate, g, nu = _wavy_komega_case(2048, 256, 32.0, 512)
+    from komegafoulingmodel_b200.adjoint import Case
+    assert Case.notches(ch) == 0
+    x = (ch.ibb_idx % ch.n) % ch.nx_full
+    cx = G.CX[ch.ibb_idx // ch.n]
+    assert not np.any((((x == 0) & (cx == 1)) | ((x == ch.nx - 1) & (cx == -1))) & (ch.ibb_q > 0.5))
+    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+    mk = lambda kk: OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, kk, o, nut,  # noqa: E731
+                              komega=True, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q, **TIGHT)
+    sim, pert = mk(k), mk(k * (1 + 1e-7))
+    fl = ch.fluid_mask().ravel()
+    with _lattice(ch, rate, g, nu, True, komega_rel_tol=TIGHT["rel_tol"],
+                  komega_abs_tol=TIGHT["abs_tol"], komega_max_iters=TIGHT["max_iters"]) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        sim.step(10)
+        L.step(10)
+        rho, ux, k2, o2 = _fields(L)
+        errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl),
+                    k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
+        print("10 steps", errs)
+        for key in ("rho", "ux", "k", "omega"):
+            assert errs[key] < 1e-5, errs
+        sim.step(30)
+        pert.step(40)
+        L.step(30)
+        rho, ux, k2, o2 = _fields(L)
+    for name, gpu, ref, alt in (("ux", ux, sim.ux, pert.ux), ("k", k2, sim.K, pert.K),
+                                ("omega", o2, sim.O, pert.O)):
+        spread = rel_l2(alt, ref, fl)
+        err = rel_l2(gpu, ref, fl)
+        print("40 steps", name, err, spread)
         assert err < 5 * spread + 1e-6, (name, err, spread)
 
 
