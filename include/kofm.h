@@ -182,6 +182,34 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
                       const double* dX4, const int32_t* ibb_idx,
                       const double* ibb_q, int32_t n_ibb);
 
+/* Geometry built on the device from the wall heights at every column: node
+ * (x, y) is fluid iff y_bot[x] < y < y_top[x] (rows 0 and ny-1 never), the
+ * walls being polylines through (x, y_w[x]), periodic in x.  Builds what
+ * kofm_set_geometry takes -- the nType flags, the E/W/N/S link fractions, the
+ * interpolated bounce-back links (wall fraction q = first crossing of the link
+ * with a wall; links with q = 1/2 left out unless KOFM_WALLS_IBB_ALL) and, with
+ * k-omega, the exact distance to the nearest wall segment -- plus, with the
+ * thermal update, what kofm_set_thermal_geometry takes (fractions of the
+ * unfouled walls y_bot0 / y_top0, NULL = the fouled ones).  Replaces the
+ * host set-up of clVariablesLS::ini (clVariablesLS.cpp:650-1000) and
+ * kOmega::iniWallD (kOmega.cpp:136-193, 330-349) for such walls, and can be
+ * called again on a live context when the walls move (clVariablesLS::update,
+ * clVariablesLS.cpp:1020-1033).  Requires y_bot0 <= y_bot and
+ * y_top0 >= y_top, all finite. */
+#define KOFM_WALLS_IBB_ALL 1
+int kofm_set_walls(kofm_ctx* ctx, const double* y_bot, const double* y_top,
+                   const double* y_bot0, const double* y_top0, int32_t flags);
+
+/* The context's geometry in the layouts kofm_set_geometry / _thermal_geometry
+ * take (any output may be NULL): ntype [nx_full*ny], wallD (k-omega
+ * contexts), dX4 and dX04 [4][nx_full*ny] (dX04: thermal contexts), and the
+ * interpolated links ordered by (direction, node) with their q (*n_ibb gets
+ * the count; cap = room in ibb_idx / ibb_q).  No counterpart in the
+ * reference. */
+int kofm_get_geometry(kofm_ctx* ctx, int16_t* ntype, double* wallD, double* dX4,
+                      double* dX04, int32_t* ibb_idx, double* ibb_q, int32_t cap,
+                      int32_t* n_ibb);
+
 /* State upload: f = FA (9 planes), k, omega, nut (1 plane each), sxy (3
  * planes Sxx,Sxy,Syy).  The k-omega arrays may be NULL when use_komega = 0;
  * nut may be NULL (it is recomputed by the next step).  Replaces the

@@ -33,6 +33,7 @@ ERR_TIMEOUT = -204
 OPTION_SAVE_MACRO_FIELDS = 0x2
 STORE_FP32, STORE_FP16_DEV, STORE_BF16_DEV, STORE_FP16_NEQ = 0, 1, 2, 3
 FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_K, FIELD_OMEGA, FIELD_NUT, FIELD_WALL_SHEAR, FIELD_TEMP = range(8)
+WALLS_IBB_ALL = 1
 OP_SUM, OP_MIN, OP_MAX = 0, 1, 2
 
 
@@ -88,6 +89,8 @@ SIGNATURES = {
     "kofm_create": (C.c_int, [C.POINTER(KofmDesc), C.POINTER(_vp)]),
     "kofm_destroy": (C.c_int, [_vp]),
     "kofm_set_geometry": (C.c_int, [_vp, _i16p, _dp, _dp, _i32p, _dp, C.c_int32]),
+    "kofm_set_walls": (C.c_int, [_vp, _dp, _dp, _dp, _dp, C.c_int32]),
+    "kofm_get_geometry": (C.c_int, [_vp, _i16p, _dp, _dp, _dp, _i32p, _dp, C.c_int32, _i32p]),
     "kofm_set_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "kofm_get_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "kofm_get_macro": (C.c_int, [_vp, _dp, _dp, _dp]),

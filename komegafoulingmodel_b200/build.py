@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libkofm.so")
 SOURCES = ["kofm_api.cu", "kofm_noalloc.cu"]
 DEPS = ["kofm_api.cu", "kofm_noalloc.cu", "kofm_common.cuh", "kofm_lb.cuh",
         "kofm_komega.cuh", "kofm_gmres.cuh", "kofm_komega_api.inc", "kofm_batch.inc",
-        "kofm_thermal.cuh", "kofm_thermal_api.inc", "kofm_adjoint.inc"]
+        "kofm_thermal.cuh", "kofm_thermal_api.inc", "kofm_adjoint.inc", "kofm_geometry.inc"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

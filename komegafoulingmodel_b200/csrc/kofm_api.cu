@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <utility>
@@ -114,6 +115,13 @@ struct kofm_ctx {
     int shear_n = 0, shear_nbl = 0;
     int32_t* shear_idx = nullptr;     // per device node: shear-node index or -1
     AdjWork adj;
+    int n_dxrec = -1, n_dxrec0 = -1;  // FD records (-1: not built)
+    // room in the record tables, and the device builder's work buffers (kept
+    // so that a builder call on a live context allocates nothing)
+    size_t ibb_cap = 0, dxrec_cap = 0, dxrec0_cap = 0;
+    int32_t* ibb_node = nullptr;  // host-layout node of each IBB record [ibb_cap]
+    double* geo_walls = nullptr;  size_t geo_walls_n = 0;
+    int* geo_rows = nullptr;      size_t geo_rows_n = 0;
 
     // thermal implicit FD (kofm_thermal_*)
     double* T = nullptr;              // [D] temperature (tempArray), FP64
@@ -528,7 +536,8 @@ int kofm_destroy(kofm_ctx* c) {
                     c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
                     c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
                     c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar, c->shear_idx,
-                    c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq, c->adj.sgrad, c->adj.cls};
+                    c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq, c->adj.sgrad, c->adj.cls,
+                    c->ibb_node, c->geo_walls, c->geo_rows};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
@@ -707,6 +716,10 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     if (c->ibb) { cudaFree(c->ibb); c->ibb = nullptr; }
     if (c->dxrec) { cudaFree(c->dxrec); c->dxrec = nullptr; }
     c->n_ibb_rec = (int)recs.size();
+    c->ibb_cap = recs.size();
+    c->dxrec_cap = dxr.size();
+    if (c->ibb_node) { cudaFree(c->ibb_node); c->ibb_node = nullptr; }
+    c->n_dxrec = (d.use_komega || d.use_thermal) ? (int)dxr.size() : -1;
     c->ibb_links.swap(links);
     if (!recs.empty()) {
         if (dalloc_t(&c->ibb, recs.size())) return KOFM_ERR_BUFFER_ALLOCATION;
@@ -1042,3 +1055,4 @@ int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
 #include "kofm_thermal_api.inc"
 // discrete adjoint of the laminar step
 #include "kofm_adjoint.inc"
+#include "kofm_geometry.inc"

@@ -380,3 +380,55 @@ def komega_reference_initial(re: float, mu: float, pipe_radius: float, umean: fl
 def force_from_re(re: float, mu: float, pipe_radius: float) -> float:
     """Fval = Re * 3 mu^2 / R^3 (clVariablesLB.cpp:584-600)."""
     return re * 3.0 * mu * mu / pipe_radius ** 3
+
+
+def main(argv=None):
+    """Times the geometry set-up of a wavy k-omega channel: the device builder
+    (kofm_set_walls, median of 5 calls on a live context after one warm-up)
+    and, with --host, this module's host builder plus kofm_set_geometry.
+
+        python -m komegafoulingmodel_b200.geometry [--nx 16384 --ny 1024 --host]
+    """
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=16384)
+    ap.add_argument("--ny", type=int, default=1024)
+    ap.add_argument("--amplitude", type=float, default=32.0)
+    ap.add_argument("--wavelength", type=int, default=512)
+    ap.add_argument("--host", action="store_true")
+    args = ap.parse_args(argv)
+    from .lattice import Lattice, desc_default
+    nx, ny = args.nx, args.ny
+    h = args.amplitude * 0.5 * (1.0 - np.cos(2.0 * np.pi * np.arange(nx) / args.wavelength))
+    yb, yt = 0.5 + h, ny - 1.5 - h
+    d = desc_default()
+    d.nx, d.nx_full, d.ny = nx, nx, ny
+    d.use_komega = 1
+    out = {"case": f"wavy k-omega channel {nx}x{ny}, amplitude {args.amplitude}, "
+                   f"wavelength {args.wavelength}"}
+    with Lattice(d) as L:
+        L.set_walls(yb, yt)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            L.set_walls(yb, yt)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        out["device_ms"] = sorted(ts)[2]
+        out["device_runs_ms"] = ts
+        out["n_ibb"] = L._n_ibb
+        if args.host:
+            t0 = time.perf_counter()
+            ch = wavy_channel(nx, ny, args.amplitude, args.wavelength)
+            t1 = time.perf_counter()
+            L.set_geometry(ch.ntype, ch.wallD, ch.dX, ch.ibb_idx, ch.ibb_q)
+            t2 = time.perf_counter()
+            out["host_builder_ms"] = (t1 - t0) * 1e3
+            out["set_geometry_ms"] = (t2 - t1) * 1e3
+            out["host_over_device"] = (t2 - t0) * 1e3 / out["device_ms"]
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

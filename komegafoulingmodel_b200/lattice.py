@@ -70,6 +70,40 @@ class Lattice:
             _ptr(ii, C.c_int32), _ptr(qq), n_ibb))
         self._n_ibb = n_ibb
 
+    def set_walls(self, y_bot, y_top, y_bot0=None, y_top0=None, ibb_all=False):
+        """Geometry built on the device from the wall heights at every column
+        (kofm_set_walls): what geometry.channel_from_walls builds on the host,
+        plus, with the thermal update, the unfouled-wall fractions."""
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64)
+                for a in (y_bot, y_top, y_bot0, y_top0)]
+        for a in arrs:
+            if a is not None and a.shape != (self.desc.nx,):
+                raise ValueError("wall heights need one value per column")
+        check("kofm_set_walls", self.lib.kofm_set_walls(
+            self._ctx, *[_ptr(a) for a in arrs], _abi.WALLS_IBB_ALL if ibb_all else 0))
+        n = C.c_int32()
+        check("kofm_get_geometry", self.lib.kofm_get_geometry(
+            self._ctx, None, None, None, None, None, None, 0, C.byref(n)))
+        self._n_ibb = n.value
+
+    def get_geometry(self):
+        """The context's geometry in the host layout: dict with ntype, dX,
+        ibb_idx, ibb_q, and wallD (k-omega) / dX0 (thermal) (kofm_get_geometry)."""
+        d = self.desc
+        n = C.c_int32()
+        check("kofm_get_geometry", self.lib.kofm_get_geometry(
+            self._ctx, None, None, None, None, None, None, 0, C.byref(n)))
+        out = dict(ntype=np.empty(self.n, np.int16), dX=np.empty(4 * self.n),
+                   ibb_idx=np.empty(max(n.value, 1), np.int32), ibb_q=np.empty(max(n.value, 1)))
+        out["wallD"] = np.empty(self.n) if d.use_komega else None
+        out["dX0"] = np.empty(4 * self.n) if d.use_thermal else None
+        check("kofm_get_geometry", self.lib.kofm_get_geometry(
+            self._ctx, _ptr(out["ntype"], C.c_int16), _ptr(out["wallD"]), _ptr(out["dX"]),
+            _ptr(out["dX0"]), _ptr(out["ibb_idx"], C.c_int32), _ptr(out["ibb_q"]),
+            len(out["ibb_idx"]), C.byref(n)))
+        out["ibb_idx"], out["ibb_q"] = out["ibb_idx"][:n.value], out["ibb_q"][:n.value]
+        return out
+
     def set_state(self, f, k=None, omega=None, nut=None, sxy=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float64)
                 for a in (f, k, omega, nut, sxy)]
