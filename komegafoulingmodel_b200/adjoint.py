@@ -129,8 +129,10 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--directions", type=int, default=8)
     ap.add_argument("--h", type=float, default=1e-3)
+    ap.add_argument("--nu", type=float, default=0.01,
+                    help="viscosity (0.01: Re ~ 1.3e3 on the height at 1024x256; 1.27e-3: ~1e4)")
     args = ap.parse_args(argv)
-    case = Case(args.nx, args.ny)
+    case = Case(args.nx, args.ny, nu=args.nu)
     ch = case.channel()
     F0 = case.start(ch)
     T = args.steps
@@ -208,7 +210,8 @@ def main(argv=None):
         fd = (Jp - Jm) / (2 * h)
         ad = float(dJda @ d)
         checks.append({"h": h, "fd": fd, "adjoint": ad, "rel": abs(fd - ad) / max(abs(fd), 1e-300)})
-    line = {"case": f"laminar wall-shape gradient {args.nx}x{args.ny}, T={T}",
+    line = {"case": f"laminar wall-shape gradient {args.nx}x{args.ny}, T={T}, nu={args.nu}",
+            "re_height": case.u_mean * (args.ny - 2) / args.nu,
             "J": J, "n_links": len(dq), "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
             "adjoint_over_forward": adj_ms / fwd_ms, "adjoint_runs_ms": adj_runs,
             "adjoint_first_call_ms": cold_ms, "adjoint_sqrt_checkpoints_ms": ckpt_ms,
