@@ -187,7 +187,9 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
  * walls being polylines through (x, y_w[x]), periodic in x.  Builds what
  * kofm_set_geometry takes -- the nType flags, the E/W/N/S link fractions, the
  * interpolated bounce-back links (wall fraction q = first crossing of the link
- * with a wall; links with q = 1/2 left out unless KOFM_WALLS_IBB_ALL) and, with
+ * with a wall; links with q = 1/2 left out unless KOFM_WALLS_IBB_ALL; none on
+ * columns 0 and nx-1, as updateIBBOnly, lsKernels.cl:455-466, unless
+ * KOFM_WALLS_SEAM_IBB) and, with
  * k-omega, the exact distance to the nearest wall segment -- plus, with the
  * thermal update, what kofm_set_thermal_geometry takes (fractions of the
  * unfouled walls y_bot0 / y_top0, NULL = the fouled ones).  Replaces the
@@ -197,6 +199,7 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
  * clVariablesLS.cpp:1020-1033).  Requires y_bot0 <= y_bot and
  * y_top0 >= y_top, all finite. */
 #define KOFM_WALLS_IBB_ALL 1
+#define KOFM_WALLS_SEAM_IBB 2   /* interpolated links on columns 0 and nx-1 too */
 int kofm_set_walls(kofm_ctx* ctx, const double* y_bot, const double* y_top,
                    const double* y_bot0, const double* y_top0, int32_t flags);
 

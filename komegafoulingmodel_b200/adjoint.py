@@ -35,9 +35,10 @@ def walls(a: np.ndarray, nx: int, ny: int, with_source: bool = False):
 
     The offset b puts the wall at x = 0 (where every cosine is flat) 0.6
     above a row, so the first fluid row there is 0.4 away and no link across
-    the periodic seam has 2q > 1 (those read an unwrapped upstream neighbour
-    in the reference's lbIBB); b is the smallest such value that keeps the
-    wall at least 0.8 above row 0 (piecewise constant in a).
+    the periodic seam has 2q > 1 even when the seam columns are given
+    interpolated links (seam_ibb; such links read an unwrapped upstream
+    neighbour in the reference's lbIBB); b is the smallest such value that
+    keeps the wall at least 0.8 above row 0 (piecewise constant in a).
 
     A column that dips below both neighbours across a lattice row would leave
     a one-node notch whose fluid node has wall links on both sides; there the

@@ -199,7 +199,7 @@ def _wall_links(nx, ny, nxf, fluid, q):
 
 def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = None,
                        wall_radius: int = 40, y_bot0=None, y_top0=None,
-                       ibb_all: bool = False) -> Channel:
+                       ibb_all: bool = False, seam_ibb: bool = False) -> Channel:
     """Channel between two walls given by their heights at every column (the
     wall polylines of clVariablesLS).  Node (i, j) is fluid iff
     y_bot[i] < j < y_top[i].  Builds the nType flags (per-direction wall bits
@@ -216,7 +216,11 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
 
     ibb_all keeps the links with q = 1/2 in the interpolated bounce-back list
     too (they give the half-way value exactly), so that every wall link has a
-    wall fraction to differentiate (kofm_adjoint)."""
+    wall fraction to differentiate (kofm_adjoint).
+
+    As the reference's list builder (updateIBBOnly, lsKernels.cl:455-466),
+    the nodes of columns 0 and nx-1 get no interpolated links: their wall
+    links bounce back half-way.  seam_ibb = True lists them too."""
     nxf = nx if nx_full is None else nx_full
     y_bot = np.asarray(y_bot, float)
     y_top = np.asarray(y_top, float)
@@ -258,6 +262,8 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
         if q < 5:
             dX[q - 1, jv, ii] = frac
         keep = np.abs(frac - 0.5) > 1e-12 if not ibb_all else np.ones(frac.shape, bool)
+        if not seam_ibb:
+            keep &= (ii != 0) & (ii != nx - 1)
         ibb_idx.extend((q * D + jv * nxf + ii)[keep].tolist())
         ibb_q.extend(frac[keep].tolist())
     if np.all(y_bot == y_bot[0]) and np.all(y_top == y_top[0]):
@@ -311,13 +317,14 @@ def channel_from_reference_files(directory: str, nx_full: int | None = None) -> 
 
 
 def wavy_channel(nx: int, ny: int, amplitude: float, wavelength: int,
-                 nx_full: int | None = None, ibb_all: bool = False) -> Channel:
+                 nx_full: int | None = None, ibb_all: bool = False,
+                 seam_ibb: bool = False) -> Channel:
     """Walls displaced by h(x) = A (1 - cos(2 pi x / L)) / 2 from the half-way
     positions 0.5 and ny - 1.5, mirrored top and bottom.  h and its slope
     vanish at x = 0, so the links at the periodic seam keep q <= 1/2."""
     x = np.arange(nx)
     h = amplitude * 0.5 * (1.0 - np.cos(2.0 * np.pi * x / wavelength))
-    return channel_from_walls(nx, ny, 0.5 + h, ny - 1.5 - h, nx_full, ibb_all=ibb_all)
+    return channel_from_walls(nx, ny, 0.5 + h, ny - 1.5 - h, nx_full, ibb_all=ibb_all, seam_ibb=seam_ibb)
 
 
 def straight_channel(nx: int, ny: int, nx_full: int | None = None) -> Channel:

@@ -46,13 +46,15 @@ def _walls(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["straight", "wavy", "wavy_all", "random", "fouled", "c2"])
-def test_device_builder_matches_host_builder(kofm_lib, name):
+@pytest.mark.parametrize("name,seam", [("straight", False), ("wavy", False), ("wavy", True),
+                                       ("wavy_all", False), ("random", False), ("random", True),
+                                       ("fouled", False), ("c2", False)])
+def test_device_builder_matches_host_builder(kofm_lib, name, seam):
     nx, ny, yb, yt, yb0, yt0, ibb_all = _walls(name)
     thermal = yb0 is not None
-    ch = G.channel_from_walls(nx, ny, yb, yt, y_bot0=yb0, y_top0=yt0, ibb_all=ibb_all)
+    ch = G.channel_from_walls(nx, ny, yb, yt, y_bot0=yb0, y_top0=yt0, ibb_all=ibb_all, seam_ibb=seam)
     with Lattice(_desc(nx, ny, komega=True, thermal=thermal)) as L:
-        L.set_walls(yb, yt, yb0, yt0, ibb_all=ibb_all)
+        L.set_walls(yb, yt, yb0, yt0, ibb_all=ibb_all, seam_ibb=seam)
         geo = L.get_geometry()
     assert np.array_equal(geo["ntype"], ch.ntype)
     assert np.array_equal(geo["ibb_idx"], ch.ibb_idx)

@@ -18,6 +18,21 @@ def test_straight_walls_need_no_interpolated_records():
     assert fl[1:-1, :].all() and not fl[0].any() and not fl[-1].any()
 
 
+def test_no_interpolated_links_on_the_seam_columns():
+    """As the reference's updateIBBOnly (lsKernels.cl:455-466): no interpolated
+    links from the nodes of columns 0 and nx-1 unless asked for."""
+    for ibb_all in (False, True):
+        ch = G.wavy_channel(256, 66, 8.0, 100, ibb_all=ibb_all)
+        x = (ch.ibb_idx % ch.n) % ch.nx_full
+        assert len(x) > 0 and not np.any((x == 0) | (x == ch.nx - 1))
+        cs = G.wavy_channel(256, 66, 8.0, 100, ibb_all=ibb_all, seam_ibb=True)
+        xs = (cs.ibb_idx % cs.n) % cs.nx_full
+        assert np.any(xs == ch.nx - 1)
+        inner = (xs != 0) & (xs != ch.nx - 1)
+        assert np.array_equal(cs.ibb_idx[inner], ch.ibb_idx) and np.array_equal(cs.ibb_q[inner], ch.ibb_q)
+        assert np.array_equal(cs.ntype, ch.ntype) and np.array_equal(cs.dX, ch.dX)
+
+
 def test_wavy_geometry_invariants():
     ch = G.wavy_channel(256, 66, 8.0, 128)
     n = ch.n
