@@ -205,10 +205,11 @@ int kofm_set_walls(kofm_ctx* ctx, const double* y_bot, const double* y_top,
 
 /* The context's geometry in the layouts kofm_set_geometry / _thermal_geometry
  * take (any output may be NULL): ntype [nx_full*ny], wallD (k-omega
- * contexts), dX4 and dX04 [4][nx_full*ny] (dX04: thermal contexts), and the
+ * contexts), dX4 and dX04 [4][nx_full*ny] (dX4: k-omega or thermal contexts,
+ * or any geometry from kofm_set_walls; dX04: thermal contexts), and the
  * interpolated links ordered by (direction, node) with their q (*n_ibb gets
- * the count; cap = room in ibb_idx / ibb_q).  No counterpart in the
- * reference. */
+ * the count; cap = room in ibb_idx / ibb_q).  KOFM_ERR_STATE for an output
+ * the context does not hold.  No counterpart in the reference. */
 int kofm_get_geometry(kofm_ctx* ctx, int16_t* ntype, double* wallD, double* dX4,
                       double* dX04, int32_t* ibb_idx, double* ibb_q, int32_t cap,
                       int32_t* n_ibb);
