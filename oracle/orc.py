@@ -217,6 +217,27 @@ class RefKernels:
         if hasattr(L, "ref_wall_shear_nodes"):
             L.ref_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, C.c_int]
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
+        if hasattr(L, "ref_update_ibb_only"):
+            L.ref_update_ibb_only.argtypes = [cp, _dp, C.c_int, _i16, _i32, _dp, C.c_int,
+                                              C.POINTER(C.c_int)]
+
+    def ibb_list(self, cfg, ntype, y_bot, y_top, cap=1 << 20):
+        """The reference's interpolated-link list (updateIBBOnly) for walls
+        through (x, y_w[x]), x = -1 .. nx (periodic heights): (population
+        index, wall fraction) in the builder's order, duplicates kept."""
+        nx = cfg.nx
+        xs = np.arange(-1, nx + 1)
+        bot = np.column_stack([xs, np.asarray(y_bot)[xs % nx]])
+        top = np.column_stack([xs[::-1], np.asarray(y_top)[xs[::-1] % nx]])
+        pts = np.ascontiguousarray(np.vstack([bot, top]), np.float64)
+        ibb = np.zeros(cap, np.int32)
+        dist = np.zeros(cap)
+        n = C.c_int()
+        self.L.ref_update_ibb_only(C.byref(cfg), pts.ravel(), len(pts),
+                                   np.ascontiguousarray(ntype, np.int16), ibb, dist, cap, C.byref(n))
+        if n.value > cap:
+            raise RuntimeError("reference link list larger than cap")
+        return ibb[:n.value], dist[:n.value]
 
     @staticmethod
     def available(path: str = LIB_REF) -> bool:

@@ -1,6 +1,7 @@
 // OpenCL-C -> C++ shim used ONLY to compile the reference's own kernel
-// sources (source/Kernels/Heading.cl, lbKernels.cl, kOmegaKernels.cl and the
-// wall-shear functions of trKernelsShear.cl) for the
+// sources (source/Kernels/Heading.cl, lbKernels.cl, kOmegaKernels.cl, the
+// wall-shear functions of trKernelsShear.cl, the implicit thermal assembly of
+// tfdKernels.cl and the interpolated-link list builder of lsKernels.cl) for the
 // CPU, so the oracle can be checked against the reference code itself.
 //
 // This file is test infrastructure (the checker), never part of the product.
@@ -60,6 +61,8 @@ static inline double2 operator*(double s, double2 a) { return {s * a.x, s * a.y}
 static inline double2 operator*(double2 a, double s) { return {s * a.x, s * a.y}; }
 static inline double2 operator/(double2 a, double s) { return {a.x / s, a.y / s}; }
 static inline double2& operator/=(double2& a, double s) { a.x /= s; a.y /= s; return a; }
+static inline double2& operator*=(double2& a, double s) { a.x *= s; a.y *= s; return a; }
+static inline double dot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
 static inline double length(double2 a) { return std::sqrt(a.x * a.x + a.y * a.y); }
 static inline double2 normalize(double2 a) { const double l = length(a); return {a.x / l, a.y / l}; }
 static inline double2 ceil(double2 a) { return {std::ceil(a.x), std::ceil(a.y)}; }
@@ -80,6 +83,8 @@ using std::isfinite;
 static inline uint mad_hi(uint a, uint b, uint c) {
     return (uint)(((unsigned long long)a * (unsigned long long)b) >> 32) + c;
 }
+// the list builder's slot counter; its work-items run one after another
+static inline int atomic_add(int* p, int v) { const int old = *p; *p += v; return old; }
 static inline ulong atom_cmpxchg(volatile ulong* p, ulong cmp, ulong val) {
     return __sync_val_compare_and_swap(p, cmp, val);
 }

@@ -13,6 +13,7 @@
 // slot from exactly one work-item, so row-parallel OpenMP is race-free.
 #include "cl_shim.hpp"
 #include <cstdio>
+#include <vector>
 
 thread_local size_t g_ref_gid[3];
 
@@ -89,6 +90,15 @@ struct RefProgram {
 #define USING_KOMEGA_SOLVER
     double m_alpha_fluid = 0.0, m_alpha_foul = 0.0, m_prt_inv = 1.0, m_tin = 0.0;
 #include "../_ref/gen/thermal.inc"
+// level-set module: the polyline has LSC_UPDATE_M_NN + 1 points, the
+// segment LSC_UPDATE_M_SKIP (bottom wall end -> top wall start) is not a
+// wall (clVariablesLS.cpp:464-466)
+#define LSC_UPDATE_M_NN m_lsc_nn1
+#define LSC_UPDATE_M_SKIP m_lsc_skip
+    int m_lsc_nn1 = 0, m_lsc_skip = -1;
+#include "../_ref/gen/ls.inc"
+#undef LSC_UPDATE_M_NN
+#undef LSC_UPDATE_M_SKIP
 #undef USING_KOMEGA_SOLVER
 #undef LB_ALPHA_FLUID
 #undef LB_ALPHA_FOUL
@@ -230,6 +240,27 @@ int ref_thermal_coeffs(const RefCfg* c, const double* th4, int* ind, short* map,
     ndrange2d(c->nxf, c->ny, [&] {
         p.Update_T_Coeffs_Implicit(ind, map, dX0, A, b, T, nullptr, ux, uy, nut, dt);
     });
+    return 0;
+}
+
+// updateIBBOnly (lsKernels.cl:428-492): one work-item per polyline segment
+// i = 0 .. npts-2 (clVariablesLS.cpp:1085-1110), run in segment order.  C2
+// holds the points (x, y) of the bottom wall left to right, then of the top
+// wall right to left; writes up to cap links (population index, wall
+// fraction) and returns the number the builder found in *count.
+int ref_update_ibb_only(const RefCfg* c, const double* C2, int npts, short* map, int* ibb,
+                        double* dist, int cap, int* count) {
+    RefProgram p = make_prog(c);
+    p.m_lsc_nn1 = npts - 1;
+    p.m_lsc_skip = npts / 2 - 1;
+    std::vector<double2> C((size_t)npts);
+    for (int i = 0; i < npts; ++i) C[(size_t)i] = double2(C2[2 * i], C2[2 * i + 1]);
+    int cnt = 0;
+    for (int i = 0; i < npts - 1; ++i) {
+        g_ref_gid[0] = (size_t)i; g_ref_gid[1] = 0; g_ref_gid[2] = 0;
+        p.updateIBBOnly(C.data(), map, ibb, dist, &cnt, cap);
+    }
+    *count = cnt;
     return 0;
 }
 

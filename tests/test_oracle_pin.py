@@ -161,3 +161,47 @@ def test_oracle_assembly_against_golden_fixtures(oracle):
                                ch.wallD, ch.ntype, 1.0)
     for key, v in dict(Dk=Dk, Do=Do, F1=F1, dkdo=dk, kA=kA, oA=oA, kb=kb, ob=ob).items():
         assert np.array_equal(v, g[key]), key
+
+
+# ---- interpolated bounce-back list of the geometry builders ------------------------
+
+def _same_list(idx, dist, ch):
+    """The reference's list (duplicates included) against a builder's: every
+    link once, the same wall fractions.  The reference lists a link twice
+    where it meets the wall at a polyline point (both segments' tests accept
+    it, lsKernels.cl:199-206): the two entries carry the same fraction."""
+    uniq, first, inv = np.unique(idx, return_index=True, return_inverse=True)
+    spread = np.zeros(len(uniq))
+    np.maximum.at(spread, inv, np.abs(dist - dist[first][inv]))
+    assert spread.max() <= 1e-15
+    assert np.array_equal(uniq, ch.ibb_idx)   # the builder's list is sorted
+    assert np.abs(dist[first] - ch.ibb_q).max() <= 1e-15
+    return len(idx) - len(uniq)
+
+
+@pytest.mark.parametrize("name", ["wavy", "sine", "random"])
+def test_ibb_list_matches_reference_builder(refk, name):
+    """channel_from_walls (and, through the GPU tests, kofm_set_walls) against
+    the reference's updateIBBOnly on the same walls: the same links from the
+    same nodes (none on columns 0 and nx-1) with the same wall fractions."""
+    from komegafoulingmodel_b200 import adjoint as A
+    if name == "random":
+        nx, ny = 1024, 256
+        yb, yt = A.walls(A.coefficients(), nx, ny)
+    else:
+        import tests.golden.make_golden_ibb as mk
+        nx, ny = mk.NX, mk.NY
+        yb, yt = mk.walls(name)
+    ch = G.channel_from_walls(nx, ny, yb, yt, ibb_all=True)
+    idx, dist = refk.ibb_list(make_cfg(nx, ny, 1.0, 0.0, 0.1), ch.ntype, yb, yt)
+    dups = _same_list(idx, dist, ch)
+    print(name, len(ch.ibb_idx), "links;", dups, "listed twice by the reference")
+
+
+def test_ibb_list_against_golden_fixture():
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ibb.npz"))
+    nx, ny = int(z["nx"]), int(z["ny"])
+    for name in ("wavy", "sine"):
+        ch = G.channel_from_walls(nx, ny, z[f"{name}_yb"], z[f"{name}_yt"], ibb_all=True)
+        assert np.array_equal(ch.ntype, z[f"{name}_ntype"])
+        _same_list(z[f"{name}_idx"], z[f"{name}_dist"], ch)
