@@ -196,12 +196,16 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
  * host set-up of clVariablesLS::ini (clVariablesLS.cpp:650-1000) and
  * kOmega::iniWallD (kOmega.cpp:136-193, 330-349) for such walls, and can be
  * called again on a live context when the walls move (clVariablesLS::update,
- * clVariablesLS.cpp:1020-1033).  Requires y_bot0 <= y_bot and
+ * clVariablesLS.cpp:1020-1033).  min_dx is the smallest E/W/N/S link
+ * fraction ("Min dX Dist", reference default MINIMUM_DX_DIST = 0.001,
+ * bcSetdXArr, clVariablesLS.cpp:248-286), in [0, 1]; the interpolated list
+ * keeps the unclamped fraction.  Requires y_bot0 <= y_bot and
  * y_top0 >= y_top, all finite. */
 #define KOFM_WALLS_IBB_ALL 1
 #define KOFM_WALLS_SEAM_IBB 2   /* interpolated links on columns 0 and nx-1 too */
 int kofm_set_walls(kofm_ctx* ctx, const double* y_bot, const double* y_top,
-                   const double* y_bot0, const double* y_top0, int32_t flags);
+                   const double* y_bot0, const double* y_top0, double min_dx,
+                   int32_t flags);
 
 /* The context's geometry in the layouts kofm_set_geometry / _thermal_geometry
  * take (any output may be NULL): ntype [nx_full*ny], wallD (k-omega

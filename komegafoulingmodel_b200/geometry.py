@@ -199,7 +199,8 @@ def _wall_links(nx, ny, nxf, fluid, q):
 
 def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = None,
                        wall_radius: int = 40, y_bot0=None, y_top0=None,
-                       ibb_all: bool = False, seam_ibb: bool = False) -> Channel:
+                       ibb_all: bool = False, seam_ibb: bool = False,
+                       min_dx: float = 0.001) -> Channel:
     """Channel between two walls given by their heights at every column (the
     wall polylines of clVariablesLS).  Node (i, j) is fluid iff
     y_bot[i] < j < y_top[i].  Builds the nType flags (per-direction wall bits
@@ -220,7 +221,11 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
 
     As the reference's list builder (updateIBBOnly, lsKernels.cl:455-466),
     the nodes of columns 0 and nx-1 get no interpolated links: their wall
-    links bounce back half-way.  seam_ibb = True lists them too."""
+    links bounce back half-way.  seam_ibb = True lists them too.
+
+    min_dx is the smallest link fraction dXArr / dXArr0 take ("Min dX Dist",
+    MINIMUM_DX_DIST = 0.001: bcSetdXArr, clVariablesLS.cpp:248-286); the
+    interpolated list keeps the unclamped fraction, as updateIBBOnly."""
     nxf = nx if nx_full is None else nx_full
     y_bot = np.asarray(y_bot, float)
     y_top = np.asarray(y_top, float)
@@ -250,7 +255,7 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
             ii, jv = np.nonzero(hit0.T)
             t[jv + CY[q], (ii + CX[q]) % nx] |= SOLID_BOUNDARY0
             jv, ii = np.nonzero(hit0)
-            dX0[q - 1, jv, ii] = _link_fractions(ii, jv, q, nx, y_bot0, y_top0)
+            dX0[q - 1, jv, ii] = np.maximum(_link_fractions(ii, jv, q, nx, y_bot0, y_top0), min_dx)
         # fouled domain (the flow)
         hit = _wall_links(nx, ny, nxf, fluid, q)
         t[hit] |= BOUND[q]
@@ -260,7 +265,7 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
         jv, ii = np.nonzero(hit)
         frac = _link_fractions(ii, jv, q, nx, y_bot, y_top)
         if q < 5:
-            dX[q - 1, jv, ii] = frac
+            dX[q - 1, jv, ii] = np.maximum(frac, min_dx)
         keep = np.abs(frac - 0.5) > 1e-12 if not ibb_all else np.ones(frac.shape, bool)
         if not seam_ibb:
             keep &= (ii != 0) & (ii != nx - 1)

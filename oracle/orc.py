@@ -217,6 +217,8 @@ class RefKernels:
         if hasattr(L, "ref_wall_shear_nodes"):
             L.ref_wall_shear_nodes.argtypes = [cp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, C.c_int]
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
+        if hasattr(L, "ref_update_node_boundary_info"):
+            L.ref_update_node_boundary_info.argtypes = [cp, _i16]
         if hasattr(L, "ref_update_ibb_only"):
             L.ref_update_ibb_only.argtypes = [cp, _dp, C.c_int, _i16, _i32, _dp, C.c_int,
                                               C.POINTER(C.c_int)]

@@ -264,6 +264,20 @@ int ref_update_ibb_only(const RefCfg* c, const double* C2, int npts, short* map,
     return 0;
 }
 
+// updateNodeBoundaryInfo (lsKernels.cl:511-583) over nX x nY, in place:
+// recomputes the per-direction wall bits and SOLID_BOUNDARY from the
+// M_SOLID / M_FLUID bits, which it does not change (so the serial in-place
+// run equals the reference's parallel one).
+int ref_update_node_boundary_info(const RefCfg* c, short* map) {
+    RefProgram p = make_prog(c);
+    for (int gy = 0; gy < c->ny; ++gy)
+        for (int gx = 0; gx < c->nx; ++gx) {
+            g_ref_gid[0] = (size_t)gx; g_ref_gid[1] = (size_t)gy; g_ref_gid[2] = 0;
+            p.updateNodeBoundaryInfo(map);
+        }
+    return 0;
+}
+
 int ref_abi_version(void) { return 1; }
 
 }  // extern "C"

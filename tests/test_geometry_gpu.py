@@ -38,6 +38,9 @@ def _walls(name):
         nx, ny = 160, 40
         dep = 3.0 + 1.5 * (1.0 - np.cos(2 * np.pi * np.arange(nx) / 80.0))
         return nx, ny, 0.5 + dep, ny - 1.5 - dep, np.full(nx, 0.5), np.full(nx, ny - 1.5), False
+    if name == "near":     # walls 5e-4 below / above a row: fractions under min_dx
+        nx, ny = 64, 20
+        return nx, ny, np.full(nx, 0.9995), np.full(nx, ny - 1.9995), None, None, False
     if name == "c2":
         nx, ny = 2048, 256
         h = 32.0 * 0.5 * (1 - np.cos(2 * np.pi * np.arange(nx) / 512))
@@ -48,7 +51,7 @@ def _walls(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,seam", [("straight", False), ("wavy", False), ("wavy", True),
                                        ("wavy_all", False), ("random", False), ("random", True),
-                                       ("fouled", False), ("c2", False)])
+                                       ("fouled", False), ("near", False), ("c2", False)])
 def test_device_builder_matches_host_builder(kofm_lib, name, seam):
     nx, ny, yb, yt, yb0, yt0, ibb_all = _walls(name)
     thermal = yb0 is not None

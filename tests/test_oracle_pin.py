@@ -205,3 +205,44 @@ def test_ibb_list_against_golden_fixture():
         ch = G.channel_from_walls(nx, ny, z[f"{name}_yb"], z[f"{name}_yt"], ibb_all=True)
         assert np.array_equal(ch.ntype, z[f"{name}_ntype"])
         _same_list(z[f"{name}_idx"], z[f"{name}_dist"], ch)
+
+
+@pytest.mark.parametrize("name", ["wavy", "sine", "random", "fouled"])
+def test_boundary_flags_match_reference_kernel(refk, name):
+    """The builders' nType against the reference's updateNodeBoundaryInfo
+    (lsKernels.cl:511-583): cleared to the bits it keeps and recomputed by it,
+    the fouled-wall flags come back unchanged; run on the unfouled map, it
+    gives the *0 flags the builders set (BOUNDARY_NODE0 for any wall link,
+    NESW_BOUNDARY_NODE0 for an E/W/N/S one, SOLID_BOUNDARY_NODE0 from its
+    SOLID_BOUNDARY_NODE, as iniNodeBoundaryInfo0, clVariablesLS.cpp:920-951)."""
+    from komegafoulingmodel_b200 import adjoint as A
+    import tests.golden.make_golden_ibb as mk
+    yb0 = yt0 = None
+    if name == "random":
+        nx, ny = 1024, 256
+        yb, yt = A.walls(A.coefficients(), nx, ny)
+    elif name == "fouled":
+        nx, ny = 160, 40
+        dep = 3.0 + 1.5 * (1.0 - np.cos(2 * np.pi * np.arange(nx) / 80.0))
+        yb, yt = 0.5 + dep, ny - 1.5 - dep
+        yb0, yt0 = np.full(nx, 0.5), np.full(nx, ny - 1.5)
+    else:
+        nx, ny = mk.NX, mk.NY
+        yb, yt = mk.walls(name)
+    ch = G.channel_from_walls(nx, ny, yb, yt, y_bot0=yb0, y_top0=yt0)
+    cfg = make_cfg(nx, ny, 1.0, 0.0, 0.1)
+    t = ch.ntype.astype(np.int32) & 0xFFFF
+    m = (t & 0x00EF).astype(np.uint16).view(np.int16)
+    refk.L.ref_update_node_boundary_info(C.byref(cfg), m)
+    assert np.array_equal(m, ch.ntype)
+    # the unfouled map: M0 bits in the places of the M bits
+    m0 = np.where(t & G.M0_SOLID, G.M_SOLID, G.M_FLUID).astype(np.uint16).view(np.int16)
+    refk.L.ref_update_node_boundary_info(C.byref(cfg), m0)
+    r = m0.astype(np.int32) & 0xFFFF
+    fl0 = (t & G.M0_SOLID) == 0
+    want = np.zeros_like(t)
+    want |= np.where(fl0 & ((r & 0xFF00) != 0), G.BOUNDARY0, 0)
+    want |= np.where(fl0 & ((r & G.NESW_BOUNDARY) != 0), G.NESW_BOUNDARY0, 0)
+    want |= np.where(~fl0 & ((r & G.SOLID_BOUNDARY) != 0), G.SOLID_BOUNDARY0, 0)
+    got = t & (G.BOUNDARY0 | G.NESW_BOUNDARY0 | G.SOLID_BOUNDARY0)
+    assert np.array_equal(got, want)

@@ -33,6 +33,18 @@ def test_no_interpolated_links_on_the_seam_columns():
         assert np.array_equal(cs.ntype, ch.ntype) and np.array_equal(cs.dX, ch.dX)
 
 
+def test_link_fractions_clamped_for_the_fd_weights_only():
+    """dXArr takes at least "Min dX Dist" (bcSetdXArr, clVariablesLS.cpp:
+    248-286); the interpolated list keeps the fraction itself."""
+    nx, ny = 64, 20
+    ch = G.channel_from_walls(nx, ny, np.full(nx, 0.9995), np.full(nx, ny - 1.9995))
+    dX = ch.dX.reshape(4, ny, nx)
+    assert np.allclose(dX[3, 1, :], 0.001) and np.allclose(dX[2, ny - 2, :], 0.001)
+    assert len(ch.ibb_q) > 0 and np.allclose(ch.ibb_q, 0.0005)
+    c0 = G.channel_from_walls(nx, ny, np.full(nx, 0.9995), np.full(nx, ny - 1.9995), min_dx=0.0)
+    assert np.allclose(c0.dX.reshape(4, ny, nx)[3, 1, :], 0.0005)
+
+
 def test_wavy_geometry_invariants():
     ch = G.wavy_channel(256, 66, 8.0, 128)
     n = ch.n
