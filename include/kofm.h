@@ -189,8 +189,10 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
  * interpolated bounce-back links (wall fraction q = first crossing of the link
  * with a wall; links with q = 1/2 left out unless KOFM_WALLS_IBB_ALL; none on
  * columns 0 and nx-1, as updateIBBOnly, lsKernels.cl:455-466, unless
- * KOFM_WALLS_SEAM_IBB) and, with
- * k-omega, the exact distance to the nearest wall segment -- plus, with the
+ * KOFM_WALLS_SEAM_IBB) and, with k-omega, the wall distance of the
+ * reference's updateWallD (kOmegaKernels.cl:751-840) over the segments within
+ * wall_radius ("Wall D Search Rad", default WALLD_SEARCH_RADIUS = 50) of the
+ * node's column, the walls taken through x = -1 .. nx -- plus, with the
  * thermal update, what kofm_set_thermal_geometry takes (fractions of the
  * unfouled walls y_bot0 / y_top0, NULL = the fouled ones).  Replaces the
  * host set-up of clVariablesLS::ini (clVariablesLS.cpp:650-1000) and
@@ -205,7 +207,7 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
 #define KOFM_WALLS_SEAM_IBB 2   /* interpolated links on columns 0 and nx-1 too */
 int kofm_set_walls(kofm_ctx* ctx, const double* y_bot, const double* y_top,
                    const double* y_bot0, const double* y_top0, double min_dx,
-                   int32_t flags);
+                   int32_t wall_radius, int32_t flags);
 
 /* The context's geometry in the layouts kofm_set_geometry / _thermal_geometry
  * take (any output may be NULL): ntype [nx_full*ny], wallD (k-omega

@@ -89,7 +89,7 @@ SIGNATURES = {
     "kofm_create": (C.c_int, [C.POINTER(KofmDesc), C.POINTER(_vp)]),
     "kofm_destroy": (C.c_int, [_vp]),
     "kofm_set_geometry": (C.c_int, [_vp, _i16p, _dp, _dp, _i32p, _dp, C.c_int32]),
-    "kofm_set_walls": (C.c_int, [_vp, _dp, _dp, _dp, _dp, C.c_double, C.c_int32]),
+    "kofm_set_walls": (C.c_int, [_vp, _dp, _dp, _dp, _dp, C.c_double, C.c_int32, C.c_int32]),
     "kofm_get_geometry": (C.c_int, [_vp, _i16p, _dp, _dp, _dp, _i32p, _dp, C.c_int32, _i32p]),
     "kofm_set_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "kofm_get_state": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),

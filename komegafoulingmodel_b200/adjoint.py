@@ -84,7 +84,7 @@ class Case:
 
     def channel(self, a=None):
         yb, yt = walls(self.a if a is None else a, self.nx, self.ny)
-        return G.channel_from_walls(self.nx, self.ny, yb, yt, ibb_all=True)
+        return G.channel_from_walls(self.nx, self.ny, yb, yt, ibb_all=True, wall_distance=False)
 
     @staticmethod
     def notches(ch) -> int:

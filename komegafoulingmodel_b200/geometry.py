@@ -139,38 +139,63 @@ def shape_gradient(ch: Channel, dJdq):
     return out[0], out[1]
 
 
-def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius=None):
-    """Distance of every fluid node to the nearest wall polyline (segments
-    between neighbouring columns, periodic in x) -- the quantity of
-    kOmega::iniWallD / findMinDist (kOmega.cpp:136-193, 330-349), computed
-    exactly: a k-d tree over points sampled every 1/4 column along both walls
-    finds the nearest wall sample, and the exact distances to the three
-    segments around it give the result."""
-    from scipy.spatial import cKDTree
+def _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, radius=50):
+    """Distance of every fluid node to the walls as the reference computes it
+    (kOmega::iniWallD / findMinDist, kOmega.cpp:136-193, 330-349, and the
+    updateWallD kernel, kOmegaKernels.cl:751-840), for walls given as
+    polylines through (x, y_w[x]) for x = -1 .. nx (periodic heights; the
+    bottom wall left to right, the top wall right to left):
+      * only the segments within `radius` of the segment that starts at the
+        node's column ("Wall D Search Rad", WALLD_SEARCH_RADIUS = 50): bottom
+        segments starting at x - radius .. x + radius - 1, top segments at
+        x - radius + 1 .. x + radius, none outside -1 .. nx - 1;
+      * per segment the distance to its line, |cross| / |P1 - P0|, replaced by
+        the distance to P0 or P1 when the foot of the perpendicular, taken on
+        the side the segment's normal points to, falls beyond that end in x;
+      * the minimum over both walls (starting from 1000).
+    The same floating-point operations in the same order as the reference,
+    so the values agree bit for bit; where the node lies behind a segment's
+    line the "foot" is the mirror image and the line distance can be shorter
+    than the segment's true distance -- kept, as the reference."""
     wall = np.zeros((ny, nxf))
     jj, ii = np.nonzero(fluid)
     if len(jj) == 0:
         return wall
-    pts = (ii.astype(float), jj.astype(float))
-    best = np.full(jj.shape, np.inf)
-    sub = 4
-    margin = min(nx, ny)                                   # periodic wrap in x
-    xs = np.arange(-margin * sub, (nx + margin) * sub) / sub
-    for y_w in (y_bot, y_top):
-        x0 = np.floor(xs).astype(np.int64)
-        t = xs - x0
-        ys = (1 - t) * y_w[x0 % nx] + t * y_w[(x0 + 1) % nx]
-        tree = cKDTree(np.column_stack([xs, ys]))
-        _, idx = tree.query(np.column_stack(pts), workers=-1)
-        seg0 = np.floor(xs[idx]).astype(np.int64)
-        for o in (-1, 0, 1):
-            xa = seg0 + o
-            ya = y_w[xa % nx]
-            yb = y_w[(xa + 1) % nx]
-            dy = yb - ya
-            tt = np.clip(((pts[0] - xa) + (pts[1] - ya) * dy) / (1.0 + dy * dy), 0.0, 1.0)
-            best = np.minimum(best, np.hypot(pts[0] - (xa + tt), pts[1] - (ya + tt * dy)))
-    wall[jj, ii] = best
+    px = ii.astype(float)
+    py = jj.astype(float)
+    dmin = np.full(len(jj), 1000.0)
+    for top, y_w in ((False, y_bot), (True, y_top)):
+        lo, hi = (-radius + 1, radius) if top else (-radius, radius - 1)
+        for o in range(lo, hi + 1):
+            xa = ii + o
+            m = (xa >= -1) & (xa <= nx - 1)
+            if not m.any():
+                continue
+            xa = xa[m]
+            x, y = px[m], py[m]
+            ax = xa.astype(float)
+            ay = y_w[xa % nx]
+            bx = ax + 1.0
+            by = y_w[(xa + 1) % nx]
+            P0x, P0y, P1x, P1y = (bx, by, ax, ay) if top else (ax, ay, bx, by)
+            vTx = P1x - P0x
+            vTy = P1y - P0y
+            vTmag = np.sqrt(vTx * vTx + vTy * vTy)
+            d = np.abs(vTy * x - vTx * y + P1x * P0y - P1y * P0x) / vTmag
+            pcx = x - d * (-(vTy / vTmag))
+            if top:
+                c0 = pcx > P0x
+                c1 = ~c0 & (pcx < P1x)
+            else:
+                c0 = pcx < P0x
+                c1 = ~c0 & (pcx > P1x)
+            e0x, e0y = x - P0x, y - P0y
+            e1x, e1y = x - P1x, y - P1y
+            d = np.where(c0, np.sqrt(e0x * e0x + e0y * e0y), d)
+            d = np.where(c1, np.sqrt(e1x * e1x + e1y * e1y), d)
+            cur = dmin[m]
+            dmin[m] = np.where(d < cur, d, cur)
+    wall[jj, ii] = dmin
     return wall
 
 
@@ -198,9 +223,9 @@ def _wall_links(nx, ny, nxf, fluid, q):
 
 
 def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = None,
-                       wall_radius: int = 40, y_bot0=None, y_top0=None,
+                       wall_radius: int = 50, y_bot0=None, y_top0=None,
                        ibb_all: bool = False, seam_ibb: bool = False,
-                       min_dx: float = 0.001) -> Channel:
+                       min_dx: float = 0.001, wall_distance: bool = True) -> Channel:
     """Channel between two walls given by their heights at every column (the
     wall polylines of clVariablesLS).  Node (i, j) is fluid iff
     y_bot[i] < j < y_top[i].  Builds the nType flags (per-direction wall bits
@@ -225,7 +250,11 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
 
     min_dx is the smallest link fraction dXArr / dXArr0 take ("Min dX Dist",
     MINIMUM_DX_DIST = 0.001: bcSetdXArr, clVariablesLS.cpp:248-286); the
-    interpolated list keeps the unclamped fraction, as updateIBBOnly."""
+    interpolated list keeps the unclamped fraction, as updateIBBOnly.
+
+    The wall distance follows the reference's search (_wall_distance, over
+    the segments within wall_radius columns); wall_distance = False leaves it
+    0 (a laminar run does not read it)."""
     nxf = nx if nx_full is None else nx_full
     y_bot = np.asarray(y_bot, float)
     y_top = np.asarray(y_top, float)
@@ -271,11 +300,15 @@ def channel_from_walls(nx: int, ny: int, y_bot, y_top, nx_full: int | None = Non
             keep &= (ii != 0) & (ii != nx - 1)
         ibb_idx.extend((q * D + jv * nxf + ii)[keep].tolist())
         ibb_q.extend(frac[keep].tolist())
-    if np.all(y_bot == y_bot[0]) and np.all(y_top == y_top[0]):
-        # straight walls: the nearest wall point is straight above or below
+    if not wall_distance:
+        wall = np.zeros((ny, nxf))
+    elif np.all(y_bot == y_bot[0]) and np.all(y_top == y_top[0]):
+        # straight walls: the vertical distance (the reference's line distance
+        # equals it up to the rounding of (x + 1) y_w - x y_w, exactly for
+        # half-way walls)
         wall = np.where(fluid, np.minimum(j[:, None] - y_bot[0], y_top[0] - j[:, None]), 0.0)
     else:
-        wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top)
+        wall = _wall_distance(nx, ny, nxf, fluid, y_bot, y_top, wall_radius)
     order = np.argsort(ibb_idx, kind="stable")
     return Channel(nx, ny, nxf, t.astype(np.uint16).view(np.int16).ravel(), dX.ravel(),
                    wall.ravel(), np.asarray(ibb_idx, np.int32)[order],

@@ -71,7 +71,7 @@ class Lattice:
         self._n_ibb = n_ibb
 
     def set_walls(self, y_bot, y_top, y_bot0=None, y_top0=None, ibb_all=False, seam_ibb=False,
-                  min_dx=0.001):
+                  min_dx=0.001, wall_radius=50):
         """Geometry built on the device from the wall heights at every column
         (kofm_set_walls): what geometry.channel_from_walls builds on the host,
         plus, with the thermal update, the unfouled-wall fractions."""
@@ -81,7 +81,7 @@ class Lattice:
             if a is not None and a.shape != (self.desc.nx,):
                 raise ValueError("wall heights need one value per column")
         check("kofm_set_walls", self.lib.kofm_set_walls(
-            self._ctx, *[_ptr(a) for a in arrs], float(min_dx),
+            self._ctx, *[_ptr(a) for a in arrs], float(min_dx), int(wall_radius),
             (_abi.WALLS_IBB_ALL if ibb_all else 0) | (_abi.WALLS_SEAM_IBB if seam_ibb else 0)))
         n = C.c_int32()
         check("kofm_get_geometry", self.lib.kofm_get_geometry(

@@ -219,19 +219,43 @@ class RefKernels:
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
         if hasattr(L, "ref_update_node_boundary_info"):
             L.ref_update_node_boundary_info.argtypes = [cp, _i16]
+        if hasattr(L, "ref_update_walld"):
+            L.ref_update_walld.argtypes = [cp, _dp, C.c_int,
+                                           np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS"),
+                                           _i16, _dp, C.c_int]
         if hasattr(L, "ref_update_ibb_only"):
             L.ref_update_ibb_only.argtypes = [cp, _dp, C.c_int, _i16, _i32, _dp, C.c_int,
                                               C.POINTER(C.c_int)]
+
+    @staticmethod
+    def wall_points(nx, y_bot, y_top):
+        """The reference's polyline layout for walls through (x, y_w[x]),
+        x = -1 .. nx (periodic heights): bottom wall left to right, then top
+        wall right to left."""
+        xs = np.arange(-1, nx + 1)
+        bot = np.column_stack([xs, np.asarray(y_bot)[xs % nx]])
+        top = np.column_stack([xs[::-1], np.asarray(y_top)[xs[::-1] % nx]])
+        return np.ascontiguousarray(np.vstack([bot, top]), np.float64)
+
+    def wall_distance(self, cfg, ntype, y_bot, y_top, radius=50):
+        """The reference's updateWallD on walls laid out as wall_points; lsMap
+        per iniLSMap (the segment starting at each column)."""
+        nx, nxf, ny = cfg.nx, cfg.nxf, cfg.ny
+        pts = self.wall_points(nx, y_bot, y_top)
+        n2 = len(pts) // 2
+        lsmap = np.zeros((2, nxf), np.uint16)
+        lsmap[0, :nx] = np.arange(nx) + 1                 # bottom segment from x = i
+        lsmap[1, :nx] = n2 + (nx - 1 - np.arange(nx))     # top segment from x = i + 1 to x = i
+        wd = np.zeros(nxf * ny)
+        self.L.ref_update_walld(C.byref(cfg), pts.ravel(), len(pts), lsmap.ravel(),
+                                np.ascontiguousarray(ntype, np.int16), wd, radius)
+        return wd
 
     def ibb_list(self, cfg, ntype, y_bot, y_top, cap=1 << 20):
         """The reference's interpolated-link list (updateIBBOnly) for walls
         through (x, y_w[x]), x = -1 .. nx (periodic heights): (population
         index, wall fraction) in the builder's order, duplicates kept."""
-        nx = cfg.nx
-        xs = np.arange(-1, nx + 1)
-        bot = np.column_stack([xs, np.asarray(y_bot)[xs % nx]])
-        top = np.column_stack([xs[::-1], np.asarray(y_top)[xs[::-1] % nx]])
-        pts = np.ascontiguousarray(np.vstack([bot, top]), np.float64)
+        pts = self.wall_points(cfg.nx, y_bot, y_top)
         ibb = np.zeros(cap, np.int32)
         dist = np.zeros(cap)
         n = C.c_int()

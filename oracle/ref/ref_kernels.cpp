@@ -278,6 +278,19 @@ int ref_update_node_boundary_info(const RefCfg* c, short* map) {
     return 0;
 }
 
+// updateWallD (kOmegaKernels.cl:813-840) over nX x nY: the distance of each
+// fluid node to the wall segments within WALLD_SEARCH_RADIUS of the column's
+// segment (lsMap, clVariablesLS.cpp:895-918).  C2 as ref_update_ibb_only;
+// lsmap [2][nxf] (bottom, top segment index of each column).
+int ref_update_walld(const RefCfg* c, const double* C2, int npts, unsigned short* lsmap, short* map,
+                     double* wallD, int radius) {
+    RefProgram p(c->nx, c->nxf, c->ny, c->tau0, c->fterm, c->mu, c->max_turb_visc, npts, radius);
+    std::vector<double2> C((size_t)npts);
+    for (int i = 0; i < npts; ++i) C[(size_t)i] = double2(C2[2 * i], C2[2 * i + 1]);
+    ndrange2d(c->nxf, c->ny, [&] { p.updateWallD(wallD, lsmap, C.data(), map); });
+    return 0;
+}
+
 int ref_abi_version(void) { return 1; }
 
 }  // extern "C"

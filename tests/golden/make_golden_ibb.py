@@ -1,10 +1,11 @@
-"""Generates tests/golden/ref_ibb.npz from the reference's own list builder.
+"""Generates tests/golden/ref_ibb.npz from the reference's own geometry kernels.
 
 Runs oracle/_ref/libkofm_ref.so (updateIBBOnly and bcFindIntersectionLS of the
-reference's source/Kernels/lsKernels.cl compiled for the CPU by
-oracle/Makefile) on two walls given as polylines through one point per
-column: the interpolated bounce-back list (population index, wall fraction)
-in the builder's order, duplicates included.
+reference's source/Kernels/lsKernels.cl, updateWallD of kOmegaKernels.cl,
+compiled for the CPU by oracle/Makefile) on two walls given as polylines
+through one point per column: the interpolated bounce-back list (population
+index, wall fraction) in the builder's order, duplicates included, and the
+wall distance of every node.
 
     make -C oracle && python tests/golden/make_golden_ibb.py
 """
@@ -43,6 +44,7 @@ def main():
         out[f"{name}_yb"], out[f"{name}_yt"] = yb, yt
         out[f"{name}_ntype"] = ch.ntype
         out[f"{name}_idx"], out[f"{name}_dist"] = idx, dist
+        out[f"{name}_walld"] = rk.wall_distance(make_cfg(NX, NY, 1.0, 0.0, 0.1), ch.ntype, yb, yt)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_ibb.npz")
     np.savez_compressed(path, nx=NX, ny=NY, **out)
     print("wrote", path, {k: v.shape for k, v in out.items() if k.endswith("_idx")})

@@ -198,13 +198,14 @@ def test_ibb_list_matches_reference_builder(refk, name):
     print(name, len(ch.ibb_idx), "links;", dups, "listed twice by the reference")
 
 
-def test_ibb_list_against_golden_fixture():
+def test_geometry_against_golden_fixture():
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ibb.npz"))
     nx, ny = int(z["nx"]), int(z["ny"])
     for name in ("wavy", "sine"):
         ch = G.channel_from_walls(nx, ny, z[f"{name}_yb"], z[f"{name}_yt"], ibb_all=True)
         assert np.array_equal(ch.ntype, z[f"{name}_ntype"])
         _same_list(z[f"{name}_idx"], z[f"{name}_dist"], ch)
+        assert np.array_equal(ch.wallD, z[f"{name}_walld"])
 
 
 @pytest.mark.parametrize("name", ["wavy", "sine", "random", "fouled"])
@@ -246,3 +247,21 @@ def test_boundary_flags_match_reference_kernel(refk, name):
     want |= np.where(~fl0 & ((r & G.SOLID_BOUNDARY) != 0), G.SOLID_BOUNDARY0, 0)
     got = t & (G.BOUNDARY0 | G.NESW_BOUNDARY0 | G.SOLID_BOUNDARY0)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", ["wavy", "sine", "random"])
+def test_wall_distance_matches_reference_kernel(refk, name):
+    """channel_from_walls' wall distance against the reference's updateWallD
+    (kOmegaKernels.cl:751-840) on the same polylines: bit for bit, including
+    the nodes where the reference's line distance undercuts the segment's."""
+    from komegafoulingmodel_b200 import adjoint as A
+    import tests.golden.make_golden_ibb as mk
+    if name == "random":
+        nx, ny = 1024, 256
+        yb, yt = A.walls(A.coefficients(), nx, ny)
+    else:
+        nx, ny = mk.NX, mk.NY
+        yb, yt = mk.walls(name)
+    ch = G.channel_from_walls(nx, ny, yb, yt)
+    wd = refk.wall_distance(make_cfg(nx, ny, 1.0, 0.0, 0.1), ch.ntype, yb, yt)
+    assert np.array_equal(ch.wallD, wd)
