@@ -65,7 +65,10 @@ def sweep_channels(n: int = 48, seed: int = 0, u_mean: float = 0.05):
         re = float(np.exp(rng.uniform(np.log(500.0), np.log(30000.0))))
         amp = float(rng.uniform(0.0, 0.15 * ny))
         lam = int(rng.choice([128, 256, 512]))
-        ch = G.wavy_channel(nx, ny, amp, lam)
+        # the host builds the flags and the start state; the device builds the
+        # geometry the lattice uses (the same, and the wall distance of a
+        # million-node channel in milliseconds instead of seconds)
+        ch = G.wavy_channel(nx, ny, amp, lam, wall_distance=False)
         R = ch.pipe_radius
         H = 2.0 * R
         nu = u_mean * H / re
@@ -76,7 +79,8 @@ def sweep_channels(n: int = 48, seed: int = 0, u_mean: float = 0.05):
         ux = np.clip(u_max * 4.0 * (y - yb) * (yt - y) / np.maximum(yt - yb, 1.0) ** 2, 0.0, None)
         f = G.equilibrium_state(ch, ux=ux)
         g = G.force_from_re(u_mean * R / nu, nu, R)
-        w = W.Workload(f"sweep{i}_{nx}x{ny}_re{re:.0f}", ch, 1.0 / (3.0 * nu + 0.5), g, nu, komega, f)
+        w = W.Workload(f"sweep{i}_{nx}x{ny}_re{re:.0f}", ch, 1.0 / (3.0 * nu + 0.5), g, nu, komega, f,
+                       device_geometry=True)
         if komega:
             k0 = 1.5 * (0.05 * u_max) ** 2
             o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * H)

@@ -356,13 +356,14 @@ def channel_from_reference_files(directory: str, nx_full: int | None = None) -> 
 
 def wavy_channel(nx: int, ny: int, amplitude: float, wavelength: int,
                  nx_full: int | None = None, ibb_all: bool = False,
-                 seam_ibb: bool = False) -> Channel:
+                 seam_ibb: bool = False, wall_distance: bool = True) -> Channel:
     """Walls displaced by h(x) = A (1 - cos(2 pi x / L)) / 2 from the half-way
     positions 0.5 and ny - 1.5, mirrored top and bottom.  h and its slope
     vanish at x = 0, so the links at the periodic seam keep q <= 1/2."""
     x = np.arange(nx)
     h = amplitude * 0.5 * (1.0 - np.cos(2.0 * np.pi * x / wavelength))
-    return channel_from_walls(nx, ny, 0.5 + h, ny - 1.5 - h, nx_full, ibb_all=ibb_all, seam_ibb=seam_ibb)
+    return channel_from_walls(nx, ny, 0.5 + h, ny - 1.5 - h, nx_full, ibb_all=ibb_all, seam_ibb=seam_ibb,
+                              wall_distance=wall_distance)
 
 
 def straight_channel(nx: int, ny: int, nx_full: int | None = None) -> Channel:

@@ -33,6 +33,7 @@ class Workload:
     nut: np.ndarray | None = None
     sxy: np.ndarray | None = None
     steps: int = 1000
+    device_geometry: bool = False  # geometry from the walls on the device (kofm_set_walls)
 
     @property
     def nodes(self) -> int:
@@ -84,8 +85,11 @@ def by_name(name: str) -> Workload:
 def apply(lattice, w: Workload) -> None:
     """Uploads geometry and state of a workload into a Lattice."""
     ch = w.channel
-    lattice.set_geometry(ch.ntype, ch.wallD, ch.dX, ch.ibb_idx if len(ch.ibb_idx) else None,
-                         ch.ibb_q if len(ch.ibb_q) else None)
+    if w.device_geometry:
+        lattice.set_walls(ch.y_bot, ch.y_top)
+    else:
+        lattice.set_geometry(ch.ntype, ch.wallD, ch.dX, ch.ibb_idx if len(ch.ibb_idx) else None,
+                             ch.ibb_q if len(ch.ibb_q) else None)
     lattice.set_state(w.f, w.k, w.omega, w.nut, w.sxy)
 
 

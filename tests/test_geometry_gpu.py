@@ -138,3 +138,28 @@ def test_walls_moving_on_a_live_context(kofm_lib):
             runs.append(L.get_macro())
     for a, b in zip(*runs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_workload_with_device_geometry(kofm_lib):
+    """A workload whose lattice geometry comes from kofm_set_walls (as the
+    batched sweep's) steps exactly as the same workload with the host
+    builder's arrays."""
+    from komegafoulingmodel_b200 import workloads as W
+    nx, ny, yb, yt, _, _, _ = _walls("wavy")
+    full = G.channel_from_walls(nx, ny, yb, yt)
+    bare = G.channel_from_walls(nx, ny, yb, yt, wall_distance=False)
+    nu, u = 5e-4, 0.05
+    f = G.equilibrium_state(full, ux=u)
+    k, o, nut = G.komega_fields(full, 1.5 * (0.05 * u) ** 2, 0.003)
+    out = []
+    for ch, dev in ((full, False), (bare, True)):
+        w = W.Workload("wavy", ch, 1.0 / (3 * nu + 0.5), 1e-7, nu, True, f, k, o, nut,
+                       np.zeros(3 * ch.n), device_geometry=dev)
+        with Lattice(W.descriptor(w)) as L:
+            W.apply(L, w)
+            L.step(10)
+            out.append(L.get_state())
+    for a, b in zip(*out):
+        if a is not None:
+            assert np.array_equal(a, b)
