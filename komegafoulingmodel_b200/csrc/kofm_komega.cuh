@@ -313,7 +313,10 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     p.rhs_k[g] = (Ksrc - Axk);
 }
 
-__global__ void __launch_bounds__(KO_THREADS, 2)
+#ifndef KOFM_ASM_MINBLOCKS
+#define KOFM_ASM_MINBLOCKS 2  // resident blocks per SM (registers and the persistent grid)
+#endif
+__global__ void __launch_bounds__(KO_THREADS, KOFM_ASM_MINBLOCKS)
 komega_assemble_kernel(const AsmParams p) {
     extern __shared__ __align__(16) unsigned char ko_smem[];
     AsmSmem& M = *reinterpret_cast<AsmSmem*>(ko_smem);
