@@ -198,7 +198,10 @@ int kofm_set_geometry(kofm_ctx* ctx, const int16_t* ntype, const double* wallD,
  * host set-up of clVariablesLS::ini (clVariablesLS.cpp:650-1000) and
  * kOmega::iniWallD (kOmega.cpp:136-193, 330-349) for such walls, and can be
  * called again on a live context when the walls move (clVariablesLS::update,
- * clVariablesLS.cpp:1020-1033).  min_dx is the smallest E/W/N/S link
+ * clVariablesLS.cpp:1020-1033); on a stepped context the nodes that turn
+ * from fluid to solid get k, omega, nu_t, the strain rates and the moments
+ * set to 0, as updateNType (lsKernels.cl:47-163) does for a growing deposit
+ * (populations and temperature stay).  min_dx is the smallest E/W/N/S link
  * fraction ("Min dX Dist", reference default MINIMUM_DX_DIST = 0.001,
  * bcSetdXArr, clVariablesLS.cpp:248-286), in [0, 1]; the interpolated list
  * keeps the unclamped fraction.  Requires y_bot0 <= y_bot and

@@ -163,3 +163,34 @@ def test_workload_with_device_geometry(kofm_lib):
     for a, b in zip(*out):
         if a is not None:
             assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_komega_walls_moving_zero_the_new_solid_nodes(kofm_lib):
+    """k-omega channel, deposit grown on the live context: kofm_set_walls sets
+    k, omega, nu_t, the strain rates and the moments of the nodes turned solid
+    to 0 (updateNType) and leaves them unchanged everywhere else."""
+    nx, ny = 256, 48
+    x = np.arange(nx)
+    yb0, yt0 = np.full(nx, 0.5), np.full(nx, ny - 1.5)
+    h = 0.5 + 3.7 * (1 - np.cos(2 * np.pi * x / 128)) / 2
+    ch0 = G.channel_from_walls(nx, ny, yb0, yt0)
+    ch1 = G.channel_from_walls(nx, ny, h, ny - 1 - h, y_bot0=yb0, y_top0=yt0)
+    f = perturbed_state(ch0, seed=8, u_mean=0.02)
+    k, o, nut, s = komega_state(ch0)
+    f, k, o, nut = fp32_state(f, k, o, nut)
+    with Lattice(_desc(nx, ny, komega=True)) as L:
+        L.set_walls(yb0, yt0)
+        L.set_state(f, k, o, nut, s)
+        L.step(5)
+        before = L.get_state()[1:]
+        mbefore = L.get_macro()
+        L.set_walls(h, ny - 1 - h, yb0, yt0)
+        after = L.get_state()[1:]
+        mafter = L.get_macro()
+    gone = ch0.fluid_mask().ravel() & ~ch1.fluid_mask().ravel()
+    assert gone.sum() > 0
+    for b, a in zip(before + tuple(mbefore), after + tuple(mafter)):
+        b, a = np.asarray(b).reshape(-1, ch0.n), np.asarray(a).reshape(-1, ch0.n)
+        assert np.all(a[:, gone] == 0.0)
+        assert np.array_equal(a[:, ~gone], b[:, ~gone])
