@@ -124,10 +124,37 @@ void clVariablesLB::iniDistsFromVel(const double* ux, const double* uy) {
     }
 }
 
+// kofm_set_walls with this object's walls, then the geometry back into nType,
+// WallD, dXArr and the interpolated-link lists
+static void set_walls_and_fetch(clVariablesLB& lb) {
+    const size_t nx = (size_t)lb.p.nX, n = lb.fullSize();
+    if (lb.yBot.size() != nx || lb.yTop.size() != nx ||
+        (!lb.yBot0.empty() && lb.yBot0.size() != nx) || (!lb.yTop0.empty() && lb.yTop0.size() != nx))
+        throw Error("clVariablesLB: wall heights need one value per column", KOFM_ERR_INVALID_ARG);
+    check("clVariablesLB (kofm_set_walls)",
+          kofm_set_walls(lb.ctx, lb.yBot.data(), lb.yTop.data(), lb.yBot0.empty() ? nullptr : lb.yBot0.data(),
+                         lb.yTop0.empty() ? nullptr : lb.yTop0.data(), lb.minDxDist, lb.wallDSearchRad, 0));
+    int32_t nl = 0;
+    check("kofm_get_geometry", kofm_get_geometry(lb.ctx, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, &nl));
+    lb.nType.resize(n);
+    lb.dXArr.resize(4 * n);
+    lb.ibbArr.resize((size_t)nl);
+    lb.ibbDistArr.resize((size_t)nl);
+    if (lb.p.kOmegaSolverFlag) lb.WallD.resize(n);
+    check("kofm_get_geometry",
+          kofm_get_geometry(lb.ctx, lb.nType.data(), lb.p.kOmegaSolverFlag ? lb.WallD.data() : nullptr,
+                            lb.dXArr.data(), nullptr, lb.ibbArr.data(), lb.ibbDistArr.data(), nl, &nl));
+}
+
+void clVariablesLB::update() {
+    if (!ctx) throw Error("clVariablesLB::update before ini", KOFM_ERR_STATE);
+    set_walls_and_fetch(*this);
+}
+
 void clVariablesLB::ini() {
     const size_t n = fullSize();
-    if (nType.size() != n) throw Error("clVariablesLB::ini: nType size", KOFM_ERR_INVALID_ARG);
-    if (FA.size() != 9 * n) iniDists();
+    const bool walls = !yBot.empty();
+    if (!walls && nType.size() != n) throw Error("clVariablesLB::ini: nType size", KOFM_ERR_INVALID_ARG);
     kofm_desc d;
     check("kofm_desc_default", kofm_desc_default(&d));
     d.nx = p.nX;
@@ -161,17 +188,22 @@ void clVariablesLB::ini() {
     }
     check("clVariablesLB::ini (kofm_create)", kofm_create(&d, &ctx));
     const bool ko = p.kOmegaSolverFlag;
-    if (ko && WallD.size() != n)
-        throw Error("clVariablesLB::ini: WallD missing", KOFM_ERR_INITIALIZING_KOMEGA);
-    // link fractions default to whole links (dXArr = 1, no wall cut)
     const bool th = p.thermalSolverFlag;
-    if ((ko || th) && dXArr.size() != 4 * n) dXArr.assign(4 * n, 1.0);
-    check("clVariablesLB::ini (geometry)",
-          kofm_set_geometry(ctx, nType.data(), ko && !WallD.empty() ? WallD.data() : nullptr,
-                            (ko || th) && !dXArr.empty() ? dXArr.data() : nullptr,
-                            ibbArr.empty() ? nullptr : ibbArr.data(),
-                            ibbDistArr.empty() ? nullptr : ibbDistArr.data(),
-                            (int32_t)ibbArr.size()));
+    if (walls) {
+        set_walls_and_fetch(*this);
+    } else {
+        if (ko && WallD.size() != n)
+            throw Error("clVariablesLB::ini: WallD missing", KOFM_ERR_INITIALIZING_KOMEGA);
+        // link fractions default to whole links (dXArr = 1, no wall cut)
+        if ((ko || th) && dXArr.size() != 4 * n) dXArr.assign(4 * n, 1.0);
+        check("clVariablesLB::ini (geometry)",
+              kofm_set_geometry(ctx, nType.data(), ko && !WallD.empty() ? WallD.data() : nullptr,
+                                (ko || th) && !dXArr.empty() ? dXArr.data() : nullptr,
+                                ibbArr.empty() ? nullptr : ibbArr.data(),
+                                ibbDistArr.empty() ? nullptr : ibbDistArr.data(),
+                                (int32_t)ibbArr.size()));
+    }
+    if (FA.size() != 9 * n) iniDists();
     kOmega& K = kOmegaClass;
     if (ko && (K.Kappa_array.size() != n || K.Omega_array.size() != n))
         throw Error("clVariablesLB::ini: k-omega initial values missing", KOFM_ERR_INITIALIZING_KOMEGA);

@@ -129,6 +129,14 @@ class clVariablesLB {
     std::vector<int32_t> ibbArr;
     std::vector<double> ibbDistArr;
 
+    // Walls as heights per column (the polylines of clVariablesLS, through
+    // (x, y_w[x])): when yBot / yTop are set, ini() builds the geometry above
+    // on the device (kofm_set_walls) and copies it back; yBot0 / yTop0 are the
+    // unfouled walls (empty: the same).  "Min dX Dist", "Wall D Search Rad".
+    std::vector<double> yBot, yTop, yBot0, yTop0;
+    double minDxDist = 0.001;
+    int wallDSearchRad = 50;
+
     // Populations FA (9 planes) on the host
     std::vector<double> FA;
 
@@ -156,6 +164,11 @@ class clVariablesLB {
     bool loadRestartFiles(const std::string& dir);
     // device -> host copies of the state (FA, k, omega, nu_t)
     void downloadState();
+    // clVariablesLS::update + clVariablesLB::update (clVariablesLS.cpp:
+    // 1020-1033, clVariablesLB.cpp:905-913): after the walls moved (yBot ...
+    // changed), rebuilds flags, link fractions, interpolated links and wall
+    // distance on the live context; nodes turned solid lose k, omega, nu_t
+    void update();
 
     size_t fullSize() const { return (size_t)p.XsizeFull * (size_t)p.nY; }
 };

@@ -12,6 +12,12 @@
 // <dir>/temp.bin     FP64 temperature (thermal only; Tinitial when absent)
 // <dir>/ibbArr.bin, ibbDistArr.bin   interpolated bounce-back links (int32
 //                    link index, FP64 wall fraction; optional)
+// <dir>/walls.bin    instead of the geometry files above: FP64 wall heights
+//                    per column, [2][nX] (bottom, top) or [4][nX] (+ the
+//                    unfouled walls); the geometry is built on the device
+// <dir>/walls_moved.bin  (with walls.bin, same layout) the walls after they
+//                    moved: applied by clVariablesLB::update after `moveAt`
+//                    steps (params.txt)
 //
 // Loads the restart files, advances nsteps of clProblem::step (Solve_no_TR),
 // writes the restart files of the final state to <dir>/out/ and prints one
@@ -66,6 +72,26 @@ int main(int argc, char** argv) {
 
         clVariablesLB vlb(p);
         const size_t n = vlb.fullSize();
+        const size_t nx = (size_t)p.nX;
+        // wall heights [2][nX] or [4][nX]
+        auto load_walls = [&](const std::string& path, std::vector<double>* w[4]) -> bool {
+            std::ifstream s(path, std::ios::binary | std::ios::ate);
+            if (!s) return false;
+            const size_t nd = (size_t)s.tellg() / sizeof(double);
+            if (nd != 2 * nx && nd != 4 * nx) throw Error(path + ": size", KOFM_ERR_LOADING_PARAMS);
+            s.seekg(0);
+            for (size_t k = 0; k < 4; ++k) {
+                w[k]->clear();
+                if (k * nx >= nd) continue;
+                w[k]->resize(nx);
+                s.read(reinterpret_cast<char*>(w[k]->data()), (std::streamsize)(nx * sizeof(double)));
+            }
+            return true;
+        };
+        std::vector<double>* wv[4] = {&vlb.yBot, &vlb.yTop, &vlb.yBot0, &vlb.yTop0};
+        const bool walls = load_walls(dir + "/walls.bin", wv);
+        const int moveAt = std::stoi(get("moveAt", "-1"));
+        if (!walls) {
         vlb.nType.resize(n);
         {
             std::ifstream s(dir + "/ntype.bin", std::ios::binary);
@@ -93,6 +119,7 @@ int main(int argc, char** argv) {
                     throw Error("ibbDistArr.bin", KOFM_ERR_LOADING_PARAMS);
             }
         }
+        }
         if (!vlb.loadRestartFiles(dir)) throw Error("restart files in " + dir, KOFM_ERR_LOADING_PARAMS);
         vlb.ini();
         clVariablesFD vfd(vlb);
@@ -101,7 +128,13 @@ int main(int argc, char** argv) {
             vfd.ini();
         }
         clProblem prob(vlb, &vfd);
-        for (int t = 0; t < nsteps; ++t) prob.step();
+        for (int t = 0; t < nsteps; ++t) {
+            if (walls && t == moveAt) {
+                if (!load_walls(dir + "/walls_moved.bin", wv)) throw Error("walls_moved.bin", KOFM_ERR_LOADING_PARAMS);
+                vlb.update();
+            }
+            prob.step();
+        }
         const std::string out = dir + "/out";
         mkdir(out.c_str(), 0755);
         vlb.saveRestartFiles(out);

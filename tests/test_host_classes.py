@@ -115,3 +115,40 @@ def test_host_thermal_step_loop_matches_python_path(tmp_path, kofm_lib):
     To = np.fromfile(os.path.join(d, "out", "temp.bin"))
     assert np.array_equal(To, T)
     assert res["sum_temp"] == tsum
+
+
+@pytest.mark.gpu
+def test_host_walls_and_update_match_python_path(tmp_path, kofm_lib):
+    """clVariablesLB with wall heights (geometry built on the device at ini)
+    and clVariablesLB::update after the walls moved, driven by kofm_host_run,
+    against Lattice.set_walls on the same live context path."""
+    from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+    from tests.cases import fp32_state
+    nx, ny = 128, 34
+    x = np.arange(nx)
+    h1 = 0.5 + 2.0 * (1 - np.cos(2 * np.pi * x / 64)) / 2
+    h2 = 0.5 + 3.5 * (1 - np.cos(2 * np.pi * x / 64)) / 2
+    ch = G.channel_from_walls(nx, ny, h1, ny - 1 - h1)
+    (f,) = fp32_state(G.equilibrium_state(ch, ux=0.01))
+    d = str(tmp_path)
+    write_case(d, ch, f, rate=1.25, g=1e-6, nu=0.1)
+    with open(os.path.join(d, "params.txt"), "a") as fh:
+        fh.write("moveAt 10\n")
+    np.concatenate([h1, ny - 1 - h1]).tofile(os.path.join(d, "walls.bin"))
+    np.concatenate([h2, ny - 1 - h2, h1, ny - 1 - h1]).tofile(os.path.join(d, "walls_moved.bin"))
+    r = subprocess.run([RUN, d, "20"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    dd = desc_default()
+    dd.nx, dd.nx_full, dd.ny, dd.tau, dd.fterm, dd.mu = nx, nx, ny, 1.25, 1e-6, 0.1
+    with Lattice(dd) as L:
+        L.set_walls(h1, ny - 1 - h1)
+        L.set_state(f)
+        L.step(10)
+        L.set_walls(h2, ny - 1 - h2, h1, ny - 1 - h1)
+        L.step(10)
+        f2 = L.get_state()[0]
+        sum_rho = L.reduce(_abi.FIELD_RHO)
+    fo = np.fromfile(os.path.join(d, "out", "lbf.bin"))
+    assert np.array_equal(fo, f2.ravel())
+    assert res["sum_rho"] == sum_rho
