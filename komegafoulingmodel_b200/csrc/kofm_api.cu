@@ -713,6 +713,15 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
                 }
             }
     }
+    // from here on the context's tables change: a failure leaves it without
+    // a geometry (and state), so that it cannot step on half-written tables
+    auto fail = [&](int code) {
+        c->have_geometry = false;
+        c->have_state = false;
+        c->n_ibb_rec = 0;
+        c->ibb_links.clear();
+        return code;
+    };
     if (c->ibb) { cudaFree(c->ibb); c->ibb = nullptr; }
     if (c->dxrec) { cudaFree(c->dxrec); c->dxrec = nullptr; }
     c->n_ibb_rec = (int)recs.size();
@@ -722,18 +731,18 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     c->n_dxrec = (d.use_komega || d.use_thermal) ? (int)dxr.size() : -1;
     c->ibb_links.swap(links);
     if (!recs.empty()) {
-        if (dalloc_t(&c->ibb, recs.size())) return KOFM_ERR_BUFFER_ALLOCATION;
-        KOFM_CUDA_TRY(cudaMemcpy(c->ibb, recs.data(), recs.size() * sizeof(IbbRecord), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+        if (dalloc_t(&c->ibb, recs.size())) return fail(KOFM_ERR_BUFFER_ALLOCATION);
+        if (cudaMemcpy(c->ibb, recs.data(), recs.size() * sizeof(IbbRecord), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     }
     if (!dxr.empty()) {
-        if (dalloc_t(&c->dxrec, dxr.size())) return KOFM_ERR_BUFFER_ALLOCATION;
-        KOFM_CUDA_TRY(cudaMemcpy(c->dxrec, dxr.data(), dxr.size() * sizeof(DxRecord), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+        if (dalloc_t(&c->dxrec, dxr.size())) return fail(KOFM_ERR_BUFFER_ALLOCATION);
+        if (cudaMemcpy(c->dxrec, dxr.data(), dxr.size() * sizeof(DxRecord), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     }
-    KOFM_CUDA_TRY(cudaMemcpy(c->ntype, nt.data(), nt.size() * sizeof(int16_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
-    KOFM_CUDA_TRY(cudaMemcpy(c->rec, rec.data(), rec.size() * sizeof(int32_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
-    KOFM_CUDA_TRY(cudaMemcpy(c->dxrec_idx, dxi.data(), dxi.size() * sizeof(int32_t), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+    if (cudaMemcpy(c->ntype, nt.data(), nt.size() * sizeof(int16_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
+    if (cudaMemcpy(c->rec, rec.data(), rec.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
+    if (cudaMemcpy(c->dxrec_idx, dxi.data(), dxi.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     if (d.use_komega)
-        KOFM_CUDA_TRY(cudaMemcpy(c->wallD, wd.data(), wd.size() * sizeof(float), cudaMemcpyHostToDevice), KOFM_ERR_MEMORY_COPY);
+        if (cudaMemcpy(c->wallD, wd.data(), wd.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     c->have_geometry = true;
     return KOFM_OK;
 }
