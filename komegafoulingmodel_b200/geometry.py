@@ -345,13 +345,192 @@ def read_reference_walls(directory: str):
     return nx, ny, y_bot, y_top
 
 
-def channel_from_reference_files(directory: str, nx_full: int | None = None) -> Channel:
-    """channel_from_walls on the wall polylines of a reference run directory
-    (read_reference_walls).  The polylines are sampled at the integer
-    columns, so walls whose vertices lie between columns are represented by
-    the straight segments between those samples."""
+_CXY = ((1.0, 0.0), (-1.0, 0.0), (0.0, 1.0), (0.0, -1.0), (1.0, 1.0), (-1.0, -1.0), (1.0, -1.0), (-1.0, 1.0))
+_REV8 = (1, 0, 3, 2, 5, 4, 7, 6)
+
+
+def _ls_links(pts, nx, ny, nxf, ntype, xlo, xhi):
+    """The reference's list builder updateIBBOnly (lsKernels.cl:428-492, with
+    bcFindIntersectionLS, 172-228) on the polyline pts (bottom wall left to
+    right, then top wall right to left; segment i joins points i and i + 1,
+    except the one from the last bottom point to the first top point), in
+    its order and floating-point operations: (population index, fraction)
+    pairs, a link listed once per segment that finds it.  Columns xlo .. xhi
+    are searched (the reference: 1 .. nx - 2)."""
+    import math
+    n_pts = len(pts)
+    skip = n_pts // 2 - 1
+    D = nxf * ny
+    t = ntype.astype(np.int32) & 0xFFFF
+    out = []
+    for i in range(n_pts - 1):
+        if i == skip:
+            continue
+        c0x, c0y = float(pts[i, 0]), float(pts[i, 1])
+        c1x, c1y = float(pts[i + 1, 0]), float(pts[i + 1, 1])
+        tx, ty = c1x - c0x, c1y - c0y
+        bl = math.sqrt(tx * tx + ty * ty)
+        tx, ty = tx / bl, ty / bl
+        nvx, nvy = -ty, tx
+        xmin, ymin = int(min(c0x, c1x)), int(min(c0y, c1y))           # convert_int2: toward zero
+        xmax, ymax = int(math.ceil(max(c0x, c1x))), int(math.ceil(max(c0y, c1y)))
+        if xmin < xlo:
+            xmin = xlo
+        if xmin > xhi or xmax < 0:
+            continue
+        if xmax > xhi:
+            xmax = xhi
+        if ymin < 0:
+            ymin = 0
+        if ymin >= ny or ymax < 0:
+            continue
+        if ymax >= ny:
+            ymax = ny - 1
+        for ii in range(xmin, xmax + 1):
+            for jj in range(ymin, ymax + 1):
+                gid = ii + nxf * jj
+                if t.flat[gid] & M_SOLID:
+                    continue
+                lx, ly = float(ii), float(jj)
+                for k in range(4):
+                    d = 2 * k
+                    cx, cy = _CXY[d]
+                    den = nvx * cx + nvy * cy
+                    if den == 0.0:
+                        continue
+                    if den > 0.0:
+                        d = _REV8[d]
+                        cx, cy = cx * -1.0, cy * -1.0
+                        den *= -1.0
+                    dist = (nvx * (c0x - lx) + nvy * (c0y - ly)) / den
+                    if dist < 0.0 or dist > 1.0:
+                        continue
+                    ccx, ccy = lx + cx * dist, ly + cy * dist
+                    a0x, a0y = ccx - c0x, ccy - c0y
+                    a1x, a1y = ccx - c1x, ccy - c1y
+                    if abs(bl - math.sqrt(a0x * a0x + a0y * a0y) - math.sqrt(a1x * a1x + a1y * a1y)) >= 1.0e-5:
+                        continue
+                    out.append((gid + D * (d + 1), dist))
+    return out
+
+
+def _ls_map(pts, nx):
+    """The segment each column starts its wall-distance search from
+    (iniLSMap, clVariablesLS.cpp:895-918): per wall, the segment whose left
+    end rounds up to the column, as an index among the wall segments (top
+    segments counted after the bottom ones)."""
+    import math
+    n_pts = len(pts)
+    nb = n_pts // 2 - 1                      # segments per wall
+    lsmap = np.zeros((2, nx), np.int64)
+    for ib in range(nb):
+        cx1, cx2 = pts[ib, 0], pts[ib + 1, 0]
+        if not (cx2 < 0.0 or cx1 >= nx - 1.0):
+            loc = int(math.ceil(cx1))
+            if 0 <= loc < nx:
+                lsmap[0, loc] = ib
+        it = n_pts // 2 + ib                 # top segment: points it, it + 1 (right to left)
+        cx2, cx1 = pts[it, 0], pts[it + 1, 0]
+        if not (cx2 < 0.0 or cx1 >= nx - 1.0):
+            loc = int(math.ceil(cx1))
+            if 0 <= loc < nx:
+                lsmap[1, loc] = ib + nb
+    return lsmap
+
+
+def _ls_wall_distance(pts, lsmap, nx, ny, nxf, fluid, radius=50):
+    """updateWallD / findMinDist (kOmegaKernels.cl:751-840) on the polyline
+    pts with the column map lsmap, in the reference's operations: the window
+    of radius segments around lsmap's entry, used as point indices into pts
+    as the kernel does (bottom: [max(m - r, 0), min(m + r, n/2 - 1)), top:
+    [max(m - r, n/2), min(m + r, n - 1)))."""
+    wall = np.zeros((ny, nxf))
+    jj, ii = np.nonzero(fluid)
+    if len(jj) == 0:
+        return wall
+    n_pts = len(pts)
+    px, py = ii.astype(float), jj.astype(float)
+    dmin = np.full(len(jj), 1000.0)
+    Cx, Cy = pts[:, 0].astype(float), pts[:, 1].astype(float)
+    for top in (False, True):
+        m = lsmap[1 if top else 0][ii]
+        lo = np.maximum(m - radius, n_pts // 2 if top else 0)
+        hi = np.minimum(m + radius, n_pts - 1 if top else n_pts // 2 - 1)
+        for o in range(-radius, radius):
+            k = m + o
+            sel = (k >= lo) & (k < hi)
+            if not sel.any():
+                continue
+            k = k[sel]
+            x, y = px[sel], py[sel]
+            P0x, P0y, P1x, P1y = Cx[k], Cy[k], Cx[k + 1], Cy[k + 1]
+            vTx = P1x - P0x
+            vTy = P1y - P0y
+            vTmag = np.sqrt(vTx * vTx + vTy * vTy)
+            d = np.abs(vTy * x - vTx * y + P1x * P0y - P1y * P0x) / vTmag
+            pcx = x - d * (-(vTy / vTmag))
+            if top:
+                c0 = pcx > P0x
+                c1 = ~c0 & (pcx < P1x)
+            else:
+                c0 = pcx < P0x
+                c1 = ~c0 & (pcx > P1x)
+            e0x, e0y = x - P0x, y - P0y
+            e1x, e1y = x - P1x, y - P1y
+            d = np.where(c0, np.sqrt(e0x * e0x + e0y * e0y), d)
+            d = np.where(c1, np.sqrt(e1x * e1x + e1y * e1y), d)
+            cur = dmin[sel]
+            dmin[sel] = np.where(d < cur, d, cur)
+    wall[jj, ii] = dmin
+    return wall
+
+
+def read_reference_polyline(directory: str):
+    """lsc0.txt points in the order the reference's kernels walk them
+    (bottom wall left to right, then top wall right to left) and lbsize."""
+    import os
+    size = np.loadtxt(os.path.join(directory, "lbsize.txt")).ravel()
+    pts = np.loadtxt(os.path.join(directory, "lsc0.txt"), ndmin=2)
+    return int(size[0]), int(size[1]), pts
+
+
+def channel_from_reference_files(directory: str, nx_full: int | None = None, ibb_all: bool = False,
+                                 min_dx: float = 0.001, wall_radius: int = 50) -> Channel:
+    """The geometry of a reference run directory on its own polylines: node
+    types from the walls' heights at the columns (read_reference_walls, the
+    fill of clVariablesLS), the interpolated links and their fractions from
+    the reference's list builder on the actual segments (_ls_links; columns
+    1 .. nx-2, a link found by two segments kept once, links with q = 1/2
+    left out unless ibb_all), the E/W/N/S link fractions from the same
+    crossings on every column (the smallest, clamped at min_dx; where no
+    segment reaches the crossing, as at the ends of the polylines, the
+    fraction of the walls sampled at the columns), and the wall distance of
+    updateWallD on the actual segments (_ls_wall_distance)."""
     nx, ny, y_bot, y_top = read_reference_walls(directory)
-    return channel_from_walls(nx, ny, y_bot, y_top, nx_full)
+    _, _, pts = read_reference_polyline(directory)
+    ch = channel_from_walls(nx, ny, y_bot, y_top, nx_full, wall_distance=False, min_dx=min_dx)
+    nxf, D = ch.nx_full, ch.n
+    fl = ch.fluid_mask()
+    first = {}
+    for idx, dist in _ls_links(pts, nx, ny, nxf, ch.ntype, 1, nx - 2):
+        first.setdefault(idx, dist)
+    keep = sorted(k for k, v in first.items() if ibb_all or abs(v - 0.5) > 1e-12)
+    ch.ibb_idx = np.asarray(keep, np.int32)
+    ch.ibb_q = np.asarray([first[k] for k in keep], float)
+    dX = ch.dX.reshape(4, D).copy()
+    best = {}
+    for idx, dist in _ls_links(pts, nx, ny, nxf, ch.ntype, 0, nx - 1):
+        q = idx // D
+        if 1 <= q <= 4:
+            best[idx] = min(dist, best.get(idx, np.inf))
+    t = ch.ntype.astype(np.int32) & 0xFFFF
+    for idx, dist in best.items():
+        q, node = idx // D, idx % D
+        if t[node] & BOUND[q]:
+            dX[q - 1, node] = max(dist, min_dx)
+    ch.dX = dX.ravel()
+    ch.wallD = _ls_wall_distance(pts, _ls_map(pts, nx), nx, ny, nxf, fl, wall_radius).ravel()
+    return ch
 
 
 def wavy_channel(nx: int, ny: int, amplitude: float, wavelength: int,

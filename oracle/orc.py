@@ -238,24 +238,30 @@ class RefKernels:
         return np.ascontiguousarray(np.vstack([bot, top]), np.float64)
 
     def wall_distance(self, cfg, ntype, y_bot, y_top, radius=50):
-        """The reference's updateWallD on walls laid out as wall_points; lsMap
-        per iniLSMap (the segment starting at each column)."""
-        nx, nxf, ny = cfg.nx, cfg.nxf, cfg.ny
+        """The reference's updateWallD on walls laid out as wall_points, each
+        column mapped to the segment that starts at it."""
+        nx, nxf = cfg.nx, cfg.nxf
         pts = self.wall_points(nx, y_bot, y_top)
         n2 = len(pts) // 2
         lsmap = np.zeros((2, nxf), np.uint16)
         lsmap[0, :nx] = np.arange(nx) + 1                 # bottom segment from x = i
         lsmap[1, :nx] = n2 + (nx - 1 - np.arange(nx))     # top segment from x = i + 1 to x = i
+        return self.wall_distance_pts(cfg, ntype, pts, lsmap, radius)
+
+    def wall_distance_pts(self, cfg, ntype, pts, lsmap, radius=50):
+        """updateWallD on the polyline pts (the reference's point order) with
+        the column map lsmap [2][nx] (entries as the kernel uses them)."""
+        nx, nxf, ny = cfg.nx, cfg.nxf, cfg.ny
+        lm = np.zeros((2, nxf), np.uint16)
+        lm[:, :nx] = np.asarray(lsmap)[:, :nx]
         wd = np.zeros(nxf * ny)
-        self.L.ref_update_walld(C.byref(cfg), pts.ravel(), len(pts), lsmap.ravel(),
+        self.L.ref_update_walld(C.byref(cfg), np.ascontiguousarray(pts, np.float64).ravel(), len(pts), lm.ravel(),
                                 np.ascontiguousarray(ntype, np.int16), wd, radius)
         return wd
 
-    def ibb_list(self, cfg, ntype, y_bot, y_top, cap=1 << 20):
-        """The reference's interpolated-link list (updateIBBOnly) for walls
-        through (x, y_w[x]), x = -1 .. nx (periodic heights): (population
-        index, wall fraction) in the builder's order, duplicates kept."""
-        pts = self.wall_points(cfg.nx, y_bot, y_top)
+    def ibb_list_pts(self, cfg, ntype, pts, cap=1 << 20):
+        """updateIBBOnly on the polyline pts (the reference's point order)."""
+        pts = np.ascontiguousarray(pts, np.float64)
         ibb = np.zeros(cap, np.int32)
         dist = np.zeros(cap)
         n = C.c_int()
@@ -264,6 +270,12 @@ class RefKernels:
         if n.value > cap:
             raise RuntimeError("reference link list larger than cap")
         return ibb[:n.value], dist[:n.value]
+
+    def ibb_list(self, cfg, ntype, y_bot, y_top, cap=1 << 20):
+        """The reference's interpolated-link list (updateIBBOnly) for walls
+        through (x, y_w[x]), x = -1 .. nx (periodic heights): (population
+        index, wall fraction) in the builder's order, duplicates kept."""
+        return self.ibb_list_pts(cfg, ntype, self.wall_points(cfg.nx, y_bot, y_top), cap)
 
     @staticmethod
     def available(path: str = LIB_REF) -> bool:

@@ -259,5 +259,27 @@ def test_reference_wall_files(tmp_path):
     ch = G.channel_from_reference_files(str(tmp_path / "w"))
     x = np.arange(nx)
     ref = G.channel_from_walls(nx, ny, 0.5 + h(x), ny - 1.5 - h(x))
-    assert np.array_equal(ch.ntype, ref.ntype)
-    assert np.allclose(ch.dX, ref.dX, atol=1e-12) and np.allclose(ch.ibb_q, ref.ibb_q, atol=1e-12)
+    # the same nodes and links; the fractions follow the file's own segments
+    # (points every quarter column) instead of chords between the columns
+    assert np.array_equal(ch.ntype, ref.ntype) and np.array_equal(ch.ibb_idx, ref.ibb_idx)
+    assert np.allclose(ch.ibb_q, ref.ibb_q, atol=2e-2) and not np.allclose(ch.ibb_q, ref.ibb_q, atol=1e-6)
+
+
+@pytest.mark.parametrize("dx", [1.0, 0.25])
+def test_reference_wall_files_match_reference_kernels(tmp_path, refk, dx):
+    """channel_from_reference_files on a reference-style run directory
+    (points from x = -0.75 every dx) against the reference's own
+    updateIBBOnly and updateWallD on the same points: the same links, the
+    same fractions and wall distances bit for bit."""
+    from oracle.orc import make_cfg
+    nx, ny = 128, 40
+    h = lambda x: 3.0 * 0.5 * (1 - np.cos(2 * np.pi * x / 64))  # noqa: E731
+    _write_reference_walls(str(tmp_path), nx, ny, lambda x: 0.5 + h(x), lambda x: ny - 1.5 - h(x), dx=dx)
+    ch = G.channel_from_reference_files(str(tmp_path), ibb_all=True)
+    _, _, pts = G.read_reference_polyline(str(tmp_path))
+    cfg = make_cfg(nx, ny, 1.0, 0.0, 0.1)
+    idx, dist = refk.ibb_list_pts(cfg, ch.ntype, pts)
+    u, first = np.unique(idx, return_index=True)
+    assert np.array_equal(u, ch.ibb_idx) and np.array_equal(dist[first], ch.ibb_q)
+    wd = refk.wall_distance_pts(cfg, ch.ntype, pts, G._ls_map(pts, nx))
+    assert np.array_equal(wd, ch.wallD)
