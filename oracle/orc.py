@@ -219,6 +219,9 @@ class RefKernels:
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
         if hasattr(L, "ref_update_node_boundary_info"):
             L.ref_update_node_boundary_info.argtypes = [cp, _i16]
+        if hasattr(L, "ref_ini_lsmap"):
+            L.ref_ini_lsmap.argtypes = [_dp, _i32, C.c_int, C.c_int, C.c_int,
+                                        np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS")]
         if hasattr(L, "ref_update_walld"):
             L.ref_update_walld.argtypes = [cp, _dp, C.c_int,
                                            np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS"),
@@ -258,6 +261,14 @@ class RefKernels:
         self.L.ref_update_walld(C.byref(cfg), np.ascontiguousarray(pts, np.float64).ravel(), len(pts), lm.ravel(),
                                 np.ascontiguousarray(ntype, np.int16), wd, radius)
         return wd
+
+    def ls_map(self, pts, segs, nx, nxf):
+        """clVariablesLS::iniLSMap on points pts and segments segs (the
+        lsc0 / lsbl tables): [2][nxf] segment index per column and wall."""
+        m = np.zeros((2, nxf), np.uint16)
+        self.L.ref_ini_lsmap(np.ascontiguousarray(pts, np.float64).ravel(),
+                             np.ascontiguousarray(segs, np.int32).ravel(), len(segs), nx, nxf, m)
+        return m
 
     def ibb_list_pts(self, cfg, ntype, pts, cap=1 << 20):
         """updateIBBOnly on the polyline pts (the reference's point order)."""

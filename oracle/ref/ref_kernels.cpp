@@ -291,6 +291,35 @@ int ref_update_walld(const RefCfg* c, const double* C2, int npts, unsigned short
     return 0;
 }
 
+}  // extern "C"
+
+// clVariablesLS::iniLSMap (clVariablesLS.cpp:893-918, host code) over the
+// arrays it reads: the points C0, the segment table BL (point pairs) and the
+// map lsMap(column, wall); writes outside the map go to a sink.
+struct LsMapShim {
+    typedef unsigned short cl_ushort;
+    struct Params { int nX; } p;
+    int nBL = 0, nxf = 0;
+    const double* pts = nullptr;
+    const int* bl = nullptr;
+    unsigned short* map = nullptr;
+    unsigned short sink = 0;
+    struct Pt { double x, y; };
+    Pt C0(int i) const { return Pt{pts[2 * i], pts[2 * i + 1]}; }
+    int BL(int i, int k) const { return bl[2 * i + k]; }
+    unsigned short& lsMap(int i, int j) { return (i >= 0 && i < nxf && j >= 0 && j < 2) ? map[j * nxf + i] : sink; }
+#include "../_ref/gen/lsmap.inc"
+};
+
+extern "C" {
+
+int ref_ini_lsmap(const double* pts, const int* bl, int nbl, int nx, int nxf, unsigned short* map) {
+    LsMapShim s;
+    s.p.nX = nx; s.nBL = nbl; s.nxf = nxf; s.pts = pts; s.bl = bl; s.map = map;
+    s.iniLSMap();
+    return 0;
+}
+
 int ref_abi_version(void) { return 1; }
 
 }  // extern "C"

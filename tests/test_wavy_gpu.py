@@ -281,5 +281,8 @@ def test_reference_wall_files_match_reference_kernels(tmp_path, refk, dx):
     idx, dist = refk.ibb_list_pts(cfg, ch.ntype, pts)
     u, first = np.unique(idx, return_index=True)
     assert np.array_equal(u, ch.ibb_idx) and np.array_equal(dist[first], ch.ibb_q)
-    wd = refk.wall_distance_pts(cfg, ch.ntype, pts, G._ls_map(pts, nx))
+    lsmap = G._ls_map(pts, nx)
+    segs = np.loadtxt(str(tmp_path / "lsbl.txt"), ndmin=2).astype(np.int32)
+    assert np.array_equal(lsmap, refk.ls_map(pts, segs, nx, nx).astype(np.int64))   # iniLSMap
+    wd = refk.wall_distance_pts(cfg, ch.ntype, pts, lsmap)
     assert np.array_equal(wd, ch.wallD)
