@@ -414,6 +414,101 @@ def _ls_links(pts, nx, ny, nxf, ntype, xlo, xhi):
     return out
 
 
+def _ls_dx(pts, segs, nx, ny, nxf, ntype, min_dx=0.001, eps=1.0e-5):
+    """dXArr as the reference's host set-up computes it (iniFillMap's 1 on
+    fluid nodes, then bcFindNodes over every segment with bcFindDirection,
+    bcFindIntersection, bcFindIntersectionLinePlane, testInside and bcSetdXArr,
+    clVariablesLS.cpp:92-290, 330-356, 1195-1208) in its floating-point
+    operations: [4][nxf*ny] (planes E, W, N, S).  A wall link whose crossing
+    no segment reaches keeps 1, as there."""
+    import math
+    t = ntype.astype(np.int32).reshape(ny, nxf) & 0xFFFF
+    dX = np.zeros((4, ny, nxf))
+    dX[:, (t & M_FLUID) != 0] = 1.0
+    dX[:, :, nx:] = 0.0
+    cxy = ((0.0, 0.0), (1.0, 0.0), (-1.0, 0.0), (0.0, 1.0), (0.0, -1.0))
+    rev = (0, 2, 1, 4, 3)
+
+    def intersect(lx, ly, dx_, dy_, c0, c1):
+        p10x, p10y = c1[0] - c0[0], c1[1] - c0[1]
+        nvx, nvy = -p10y, p10x
+        den = nvx * dx_ + nvy * dy_
+        if den == 0.0:
+            return None
+        plx, ply = c0[0] - lx, c0[1] - ly
+        distf = (nvx * plx + nvy * ply) / den
+        cx_, cy_ = lx + dx_ * distf, ly + dy_ * distf
+        d0x, d0y = cx_ - c0[0], cy_ - c0[1]
+        d1x, d1y = cx_ - c1[0], cy_ - c1[1]
+        if not abs(math.sqrt(p10x * p10x + p10y * p10y) - math.sqrt(d0x * d0x + d0y * d0y)
+                   - math.sqrt(d1x * d1x + d1y * d1y)) < eps:
+            return None
+        n_cut = int(math.ceil(distf))
+        dist = 1.0 - (n_cut - distf)
+        c1x, c1y = int(lx + dx_ * n_cut), int(ly + dy_ * n_cut)
+        c0x, c0y = c1x - int(dx_), c1y - int(dy_)
+        if c0x % nx != c0x or c0y % ny != c0y:
+            return None
+        if t[c0y, c0x] & M_SOLID:
+            if dist < eps:
+                dist = 1.0
+                n_cut -= 1
+                c1x, c1y = int(lx + dx_ * n_cut), int(ly + dy_ * n_cut)
+                c0x, c0y = c1x - int(dx_), c1y - int(dy_)
+                if c0x % nx != c0x or c0y % ny != c0y:
+                    return None
+            else:
+                return None
+        return c0x, c0y, c1x, c1y, dist
+
+    for a, b in segs:
+        if a < 0:
+            continue
+        c0, c1 = (float(pts[a, 0]), float(pts[a, 1])), (float(pts[b, 0]), float(pts[b, 1]))
+        cnx, cny = c0[1] - c1[1], c1[0] - c0[0]
+        xmin, ymin = math.floor(min(c0[0], c1[0])), math.floor(min(c0[1], c1[1]))
+        xmax, ymax = math.ceil(max(c0[0], c1[0])), math.ceil(max(c0[1], c1[1]))
+        xmin = max(xmin, 0)
+        if xmin > nx - 1 or xmax < 0:
+            continue
+        xmax = min(xmax, nx - 1)
+        ymin = max(ymin, 0)
+        if ymin > ny - 1 or ymax < 0:
+            continue
+        ymax = min(ymax, ny - 1)
+        for d in (1, 3):
+            dx_, dy_ = cxy[d]
+            cn = cnx * dx_ + cny * dy_
+            if cn == 0.0:
+                continue
+            if cn > 0.0:
+                d = rev[d]
+                dx_, dy_ = cxy[d]
+            starts = []
+            if dx_ != 0.0:
+                i = xmin if dx_ == 1.0 else xmax
+                starts += [(i, j) for j in range(ymin, ymax + 1)]
+            if dy_ != 0.0:
+                j = ymin if dy_ == 1.0 else ymax
+                starts += [(i, j) for i in range(xmin, xmax + 1)]
+            for i, j in starts:
+                r = intersect(float(i), float(j), dx_, dy_, c0, c1)
+                if r is None:
+                    continue
+                x0, y0, x1, y1, dist = r
+                if not (0 <= x0 < nx and 0 <= y0 < ny):
+                    continue
+                x1 %= nx
+                if not (0 <= y1 < ny):
+                    continue
+                if t[y0, x0] & M_SOLID or not (t[y1, x1] & M_SOLID):
+                    continue
+                v = dX[d - 1, y0, x0]
+                v = dist if dist < v else v
+                dX[d - 1, y0, x0] = v if v > min_dx else min_dx
+    return dX.reshape(4, -1)
+
+
 def _ls_map(pts, nx):
     """The segment each column starts its wall-distance search from
     (iniLSMap, clVariablesLS.cpp:895-918): per wall, the segment whose left
@@ -494,6 +589,12 @@ def read_reference_polyline(directory: str):
     return int(size[0]), int(size[1]), pts
 
 
+def read_reference_segments(directory: str):
+    """lsbl.txt: the wall segments as point-index pairs."""
+    import os
+    return np.loadtxt(os.path.join(directory, "lsbl.txt"), ndmin=2).astype(np.int64)
+
+
 def channel_from_reference_files(directory: str, nx_full: int | None = None, ibb_all: bool = False,
                                  min_dx: float = 0.001, wall_radius: int = 50) -> Channel:
     """The geometry of a reference run directory on its own polylines: node
@@ -501,11 +602,10 @@ def channel_from_reference_files(directory: str, nx_full: int | None = None, ibb
     fill of clVariablesLS), the interpolated links and their fractions from
     the reference's list builder on the actual segments (_ls_links; columns
     1 .. nx-2, a link found by two segments kept once, links with q = 1/2
-    left out unless ibb_all), the E/W/N/S link fractions from the same
-    crossings on every column (the smallest, clamped at min_dx; where no
-    segment reaches the crossing, as at the ends of the polylines, the
-    fraction of the walls sampled at the columns), and the wall distance of
-    updateWallD on the actual segments (_ls_wall_distance)."""
+    left out unless ibb_all), the E/W/N/S link fractions of the reference's
+    host set-up on the same segments (_ls_dx: clamped at min_dx, 1 where no
+    segment reaches the crossing, as at the ends of the polylines), and the
+    wall distance of updateWallD on the actual segments (_ls_wall_distance)."""
     nx, ny, y_bot, y_top = read_reference_walls(directory)
     _, _, pts = read_reference_polyline(directory)
     ch = channel_from_walls(nx, ny, y_bot, y_top, nx_full, wall_distance=False, min_dx=min_dx)
@@ -517,18 +617,8 @@ def channel_from_reference_files(directory: str, nx_full: int | None = None, ibb
     keep = sorted(k for k, v in first.items() if ibb_all or abs(v - 0.5) > 1e-12)
     ch.ibb_idx = np.asarray(keep, np.int32)
     ch.ibb_q = np.asarray([first[k] for k in keep], float)
-    dX = ch.dX.reshape(4, D).copy()
-    best = {}
-    for idx, dist in _ls_links(pts, nx, ny, nxf, ch.ntype, 0, nx - 1):
-        q = idx // D
-        if 1 <= q <= 4:
-            best[idx] = min(dist, best.get(idx, np.inf))
-    t = ch.ntype.astype(np.int32) & 0xFFFF
-    for idx, dist in best.items():
-        q, node = idx // D, idx % D
-        if t[node] & BOUND[q]:
-            dX[q - 1, node] = max(dist, min_dx)
-    ch.dX = dX.ravel()
+    segs = read_reference_segments(directory)
+    ch.dX = _ls_dx(pts, segs, nx, ny, nxf, ch.ntype, min_dx).ravel()
     ch.wallD = _ls_wall_distance(pts, _ls_map(pts, nx), nx, ny, nxf, fl, wall_radius).ravel()
     return ch
 

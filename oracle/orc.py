@@ -219,6 +219,9 @@ class RefKernels:
             L.ref_shear_coeffs1.argtypes = [cp, _i32, _i16, _dp, C.c_int, C.c_double]
         if hasattr(L, "ref_update_node_boundary_info"):
             L.ref_update_node_boundary_info.argtypes = [cp, _i16]
+        if hasattr(L, "ref_ini_dx"):
+            L.ref_ini_dx.argtypes = [_dp, C.c_int, _i32, C.c_int, _i16, C.c_int, C.c_int, C.c_int,
+                                     C.c_double, _dp, _dp]
         if hasattr(L, "ref_ini_lsmap"):
             L.ref_ini_lsmap.argtypes = [_dp, _i32, C.c_int, C.c_int, C.c_int,
                                         np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS")]
@@ -269,6 +272,16 @@ class RefKernels:
         self.L.ref_ini_lsmap(np.ascontiguousarray(pts, np.float64).ravel(),
                              np.ascontiguousarray(segs, np.int32).ravel(), len(segs), nx, nxf, m)
         return m
+
+    def link_fractions(self, cfg, ntype, pts, segs, min_dx=0.001):
+        """The reference's host set-up of dXArr and dXArr0 (bcFindNodes over
+        every segment) for points pts and segments segs: two [4][nxf*ny]."""
+        n = cfg.nxf * cfg.ny
+        dx, dx0 = np.zeros(4 * n), np.zeros(4 * n)
+        self.L.ref_ini_dx(np.ascontiguousarray(pts, np.float64).ravel(), len(pts),
+                          np.ascontiguousarray(segs, np.int32).ravel(), len(segs),
+                          np.ascontiguousarray(ntype, np.int16), cfg.nx, cfg.nxf, cfg.ny, min_dx, dx, dx0)
+        return dx, dx0
 
     def ibb_list_pts(self, cfg, ntype, pts, cap=1 << 20):
         """updateIBBOnly on the polyline pts (the reference's point order)."""

@@ -311,7 +311,85 @@ struct LsMapShim {
 #include "../_ref/gen/lsmap.inc"
 };
 
+// The host set-up of the E/W/N/S link fractions (inidXArrays /
+// iniFillMap's dXArr part: 1 on fluid nodes, then bcFindNodes over every
+// wall segment, clVariablesLS.cpp:650-667, 1195-1208) over the arrays it
+// reads: points C (= C0), segments BL, nType, dXArr / dXArr0 [4][XsizeFull nY].
+union cl_double2 {
+    struct { double x, y; };
+    double s[2];
+};
+union cl_int2 {
+    struct { int x, y; };
+    int s[2];
+};
+#undef MAX
+#undef MIN
+struct LsDxShim {
+    enum { find_ibb, find_dx, find_dx0 };
+    struct Params { int nX, nY; double eps; } p;
+    struct Lb { cl_double2 Cxy_double[9]; int rev[9]; int Cx[9]; int Cy[9]; } vlb;
+    struct Fl { double mindXDist; } vfl;
+    LsDxShim& vls;  // read through the reference's global instance
+    int nxf = 0;
+    const cl_double2* C = nullptr;
+    const cl_double2* C0 = nullptr;
+    const int* bl = nullptr;
+    const short* map = nullptr;
+    double* dx = nullptr;
+    double* dx0 = nullptr;
+    LsDxShim() : vls(*this) {}
+    int BL(int i, int k) const { return bl[2 * i + k]; }
+    int nType(int i, int j) const { return (unsigned short)map[(size_t)j * nxf + i]; }
+    double& dXArr(int i, int j, int k) { return dx[((size_t)k * p.nY + j) * nxf + i]; }
+    double& dXArr0(int i, int j, int k) { return dx0[((size_t)k * p.nY + j) * nxf + i]; }
+#include "../_ref/gen/lsdx.inc"
+};
+#undef Subtract2
+#undef GETLEN
+#undef DOT_PROD
+#undef MOD
+#undef MAX
+#undef MIN
+
 extern "C" {
+
+// dx, dx0 [4][nxf*ny]: the fractions of the fouled (M_SOLID) and unfouled
+// (M0_SOLID) walls the reference's host set-up computes for polyline pts and
+// segments bl (nbl), with "Min dX Dist" mindx.
+int ref_ini_dx(const double* pts, int npts, const int* bl, int nbl, const short* map, int nx, int nxf, int ny,
+               double mindx, double* dx, double* dx0) {
+    LsDxShim s;
+    s.p.nX = nx; s.p.nY = ny; s.p.eps = 1.e-5;
+    static const double cxy[9][2] = {{0., 0.}, {1., 0.}, {-1., 0.}, {0., 1.}, {0., -1.},
+                                     {1., 1.}, {-1., -1.}, {1., -1.}, {-1., 1.}};
+    static const int rev[9] = {0, 2, 1, 4, 3, 6, 5, 8, 7};
+    for (int q = 0; q < 9; ++q) {
+        s.vlb.Cxy_double[q].x = cxy[q][0]; s.vlb.Cxy_double[q].y = cxy[q][1];
+        s.vlb.rev[q] = rev[q]; s.vlb.Cx[q] = (int)cxy[q][0]; s.vlb.Cy[q] = (int)cxy[q][1];
+    }
+    s.vfl.mindXDist = mindx;
+    s.nxf = nxf;
+    std::vector<cl_double2> C((size_t)npts);
+    for (int i = 0; i < npts; ++i) { C[(size_t)i].x = pts[2 * i]; C[(size_t)i].y = pts[2 * i + 1]; }
+    s.C = s.C0 = C.data();
+    s.bl = bl; s.map = map; s.dx = dx; s.dx0 = dx0;
+    const size_t plane = (size_t)nxf * ny;
+    for (size_t k = 0; k < 4 * plane; ++k) { dx[k] = 0.0; dx0[k] = 0.0; }
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i)
+            if (s.nType(i, j) & 0x2)                     // M_FLUID_NODE
+                for (int k = 0; k < 4; ++k) { s.dXArr(i, j, k) = 1.0; s.dXArr0(i, j, k) = 1.0; }
+    // the unfouled fractions follow M0_FLUID_NODE (0x8) nodes
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const bool f0 = (s.nType(i, j) & 0x8) != 0;
+            for (int k = 0; k < 4; ++k) s.dXArr0(i, j, k) = f0 ? 1.0 : 0.0;
+        }
+    for (int i = 0; i < nbl; ++i) s.bcFindNodes(i, LsDxShim::find_dx0);
+    for (int i = 0; i < nbl; ++i) s.bcFindNodes(i, LsDxShim::find_dx);
+    return 0;
+}
 
 int ref_ini_lsmap(const double* pts, const int* bl, int nbl, int nx, int nxf, unsigned short* map) {
     LsMapShim s;

@@ -269,8 +269,9 @@ def test_reference_wall_files(tmp_path):
 def test_reference_wall_files_match_reference_kernels(tmp_path, refk, dx):
     """channel_from_reference_files on a reference-style run directory
     (points from x = -0.75 every dx) against the reference's own
-    updateIBBOnly and updateWallD on the same points: the same links, the
-    same fractions and wall distances bit for bit."""
+    updateIBBOnly, updateWallD, iniLSMap and dXArr set-up on the same points:
+    the same links, fractions, link fractions and wall distances bit for
+    bit."""
     from oracle.orc import make_cfg
     nx, ny = 128, 40
     h = lambda x: 3.0 * 0.5 * (1 - np.cos(2 * np.pi * x / 64))  # noqa: E731
@@ -286,3 +287,5 @@ def test_reference_wall_files_match_reference_kernels(tmp_path, refk, dx):
     assert np.array_equal(lsmap, refk.ls_map(pts, segs, nx, nx).astype(np.int64))   # iniLSMap
     wd = refk.wall_distance_pts(cfg, ch.ntype, pts, lsmap)
     assert np.array_equal(wd, ch.wallD)
+    dx, _ = refk.link_fractions(cfg, ch.ntype, pts, segs)   # bcFindNodes .. bcSetdXArr (host code)
+    assert np.array_equal(dx, ch.dX)
