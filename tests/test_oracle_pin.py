@@ -265,3 +265,26 @@ def test_wall_distance_matches_reference_kernel(refk, name):
     ch = G.channel_from_walls(nx, ny, yb, yt)
     wd = refk.wall_distance(make_cfg(nx, ny, 1.0, 0.0, 0.1), ch.ntype, yb, yt)
     assert np.array_equal(ch.wallD, wd)
+
+
+@pytest.mark.parametrize("name", ["wavy", "sine", "random"])
+def test_link_fractions_match_reference_host_setup(refk, name):
+    """channel_from_walls' dXArr against the reference's host set-up
+    (bcFindNodes .. bcSetdXArr, clVariablesLS.cpp:92-290, compiled as C++) on
+    the same walls through the columns: the same links, the same fractions
+    up to the rounding of its 1 - (ceil(d) - d)."""
+    from komegafoulingmodel_b200 import adjoint as A
+    import tests.golden.make_golden_ibb as mk
+    if name == "random":
+        nx, ny = 1024, 256
+        yb, yt = A.walls(A.coefficients(), nx, ny)
+    else:
+        nx, ny = mk.NX, mk.NY
+        yb, yt = mk.walls(name)
+    ch = G.channel_from_walls(nx, ny, yb, yt, wall_distance=False)
+    pts = refk.wall_points(nx, yb, yt)
+    n = len(pts) // 2
+    segs = np.array([(i, i + 1) for i in range(n - 1)] + [(n + i, n + i + 1) for i in range(n - 1)])
+    dx, _ = refk.link_fractions(make_cfg(nx, ny, 1.0, 0.0, 0.1), ch.ntype, pts, segs)
+    assert np.array_equal(dx == 1.0, ch.dX == 1.0) and np.array_equal(dx == 0.0, ch.dX == 0.0)
+    assert np.abs(dx - ch.dX).max() <= 1e-15
