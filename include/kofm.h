@@ -227,7 +227,8 @@ int kofm_get_geometry(kofm_ctx* ctx, int16_t* ntype, double* wallD, double* dX4,
  * planes Sxx,Sxy,Syy).  The k-omega arrays may be NULL when use_komega = 0;
  * nut may be NULL (it is recomputed by the next step).  Replaces the
  * allocate_buffer_w_copy uploads of ini() and the lbf/lbkappa/lbomega bin
- * loads (clVariablesLB.cpp:883-902, kOmega.cpp:685-710). */
+ * loads (clVariablesLB.cpp:883-902, kOmega.cpp:685-710); as there, the
+ * k-omega sub-stepping starts again from the descriptor's komega_dt. */
 int kofm_set_state(kofm_ctx* ctx, const double* f, const double* k,
                    const double* omega, const double* nut, const double* sxy);
 
@@ -267,7 +268,12 @@ int kofm_komega_solve(kofm_ctx* ctx, int32_t* iters, double* rel_res);
 
 /* kOmega::Solve (kOmega.cpp:31-73): adaptive sub-stepping (halve dt on a
  * NaN residual, double it after 20 calm steps; kOmega.cpp:387-414) around
- * assemble + solve. */
+ * assemble + solve.  A field whose solve met a NaN keeps its value from
+ * before that solve.  Where the reference would halve for ever (a NaN that
+ * no smaller dt removes), this returns KOFM_ERR_NAN once more than 2^20
+ * sub-steps per LB step would be needed; kofm_get_stats then shows the
+ * halved dt, and kofm_set_state (a repaired state) starts the sub-stepping
+ * again. */
 int kofm_komega_update(kofm_ctx* ctx);
 
 /* nsteps x Solve_no_TR (LBLS.cpp:185-205): kofm_lb_step with
@@ -330,6 +336,15 @@ int kofm_get_stats(kofm_ctx* ctx, kofm_stats* out);
  * the fields unchanged.  No counterpart in the reference. */
 int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
 
+/* Test hook for the k-omega sub-stepping (kOmega::halveTimeStep,
+ * kOmega.cpp:387-399): the next n k-omega solves report a NaN residual for
+ * the systems in mask (1: omega, 2: k) at their first convergence check and
+ * leave those fields as they were -- what a solve whose right-hand side holds
+ * a NaN does -- so that kofm_komega_update halves dt.  The failure is made on
+ * the host side of the call; nothing faults on the device.  No counterpart in
+ * the reference. */
+int kofm_debug_fail_solves(kofm_ctx* ctx, int32_t n, int32_t mask);
+
 /* ---- discrete adjoint of the laminar step -----------------------------------
  * No counterpart in the reference.  From the current state (a stepped FP32
  * laminar context without thermal update), takes T steps and returns
@@ -367,9 +382,12 @@ int kofm_set_adjoint_memory(kofm_ctx* ctx, int64_t bytes);
  * device that loads it until the process exits: one partial per
  * KOFM_NOALLOC_CHUNK nodes, so pitch*ny may not exceed KOFM_NOALLOC_MAX_NODES
  * (KOFM_ERR_TOO_LARGE otherwise).  All calls share that array: calls that
- * overlap on the GPU race.  Each call overwrites the partials it uses.  The
- * first call on a device resolves the array's address (cudaGetSymbolAddress)
- * with that device current; make that first call before any stream capture. */
+ * overlap on the GPU race.  Each call overwrites the partials it uses.  A
+ * call made outside stream capture looks the array's address up
+ * (cudaGetSymbolAddress) in the calling thread's current CUDA context and
+ * remembers it for that context; a call made while `stream` is being captured
+ * uses the remembered address, so make the first call in each context before
+ * any capture (KOFM_ERR_STATE otherwise). */
 #define KOFM_NOALLOC_MAX_PARTIALS 4096
 #define KOFM_NOALLOC_CHUNK 65536
 #define KOFM_NOALLOC_MAX_NODES (4096LL * 65536LL)

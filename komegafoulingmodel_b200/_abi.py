@@ -105,6 +105,7 @@ SIGNATURES = {
     "kofm_wall_shear": (C.c_int, [_vp, _dp, _dp]),
     "kofm_get_stats": (C.c_int, [_vp, C.POINTER(KofmStats)]),
     "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
+    "kofm_debug_fail_solves": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "kofm_stream": (_vp, [_vp]),
     "kofm_reduce_field_noalloc": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             _vp, _vp]),

@@ -103,6 +103,8 @@ struct kofm_ctx {
     int steps_per_lb = 1;
     int time_since_change = 0;
     double dt = 1.0;
+    int fail_solves = 0;              // kofm_debug_fail_solves
+    int fail_mask = 0;
     kofm_stats stats{};
 
     // wall shear (kofm_set_shear / kofm_wall_shear)
@@ -808,6 +810,11 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
     c->phase = 0;
     c->have_state = true;
     c->stats.phase = 0;
+    // a loaded state starts the k-omega sub-stepping again (kOmega::ini)
+    c->dt = d.komega_dt;
+    c->steps_per_lb = (int)(1.0 / d.komega_dt);
+    if (c->steps_per_lb < 1) c->steps_per_lb = 1;
+    c->time_since_change = 0;
     return KOFM_OK;
 }
 

@@ -57,7 +57,7 @@ struct GmresSys {
     int vecs;       // Krylov vectors built (all cycles)
     int vec_index_sum;  // sum over built vectors of their index k in the cycle
     int update_terms;   // sum over cycles of the update's coefficient count kk
-    int pad;
+    int inject;         // test hook: report a NaN residual at the first check
     double rho0, norm_rhs, rinv, rho, prev_err;
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||
     double h[KOFM_MAX_KRYLOV];   // Gram-Schmidt coefficients for the next vector
@@ -252,7 +252,7 @@ __device__ void serial_section(const GmresArgs& a, int kind, int kcur, int resta
                 S.rho = 1.0;
                 S.restarts += 1;
                 const double resid = S.rho0 / S.norm_rhs;
-                if (isnan(resid)) { S.nan = 1; S.active = 0; }
+                if (isnan(resid) || (restart == 0 && S.inject)) { S.nan = 1; S.active = 0; }
                 else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
                 else { S.cycles += 1; S.done = 0; }
             } else if (kind == SER_KRYLOV) {
@@ -722,10 +722,13 @@ gmres_kernel(const GmresArgs a) {
     }
 
     // ---- x_new = x0 + d on fluid nodes; solid-boundary rows -> 0 -----------------
+    // A solve that met a NaN residual leaves its field as it was before the
+    // solve (the reference adds the correction of the cycles before the NaN,
+    // GMRESSolver.cpp:350-353, and its copyFromPrevSolution restores nothing).
     for (int s = 0; s < 2; ++s) {
         const KoSystem& S = a.sys[s];
         float* f = a.field[s];
-        const bool has_x = ldc(&ctl->sys[s].cycles) > 0;
+        const bool has_x = ldc(&ctl->sys[s].cycles) > 0 && !ldc(&ctl->sys[s].nan);
         for (long long pr = t0; pr < npairs; pr += stride) {
             const long long g = pr * 2;
             const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);

@@ -19,22 +19,81 @@
 //   * every call overwrites the partials it uses (nothing needs to start at
 //     zero), and all calls share the one array: calls that overlap on the GPU
 //     (different streams, or several host threads) race on it;
-//   * the first call on each device resolves the array's device address with
-//     cudaGetSymbolAddress, with that device current; make that first call
-//     before any stream capture.
+//   * host code cannot use the array's name as a device address: every call
+//     made outside stream capture resolves the address with
+//     cudaGetSymbolAddress in the calling thread's current CUDA context and
+//     remembers it for that context; a call made while `stream` is being
+//     captured uses the remembered address of the current context, so the
+//     first call in each context must come before any capture
+//     (KOFM_ERR_STATE otherwise).  Resolving afresh outside capture keeps the
+//     address right after cudaDeviceReset and for callers that drive their
+//     own driver-API contexts, where the array lives at a different address
+//     in each context.
 #include "kofm.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 namespace {
 
 static __device__ __align__(256) double g_noalloc_partials[KOFM_NOALLOC_MAX_PARTIALS];
 
-// Device address of g_noalloc_partials per device ordinal (host code may not
-// use the symbol itself as an address).
-constexpr int MAX_DEVICES = 64;
-double* g_partials_addr[MAX_DEVICES] = {};
+// The array's device address per CUDA context, guarded by a mutex (several
+// host threads may make their first calls at once).
+std::mutex g_addr_mutex;
+std::vector<std::pair<CUcontext, double*>> g_addr;
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link-time
+// dependency on the driver library).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+bool current_context(CUcontext* out) {
+    static CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (CtxGetCurrentFn) nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    *out = nullptr;
+    return fn && fn(out) == CUDA_SUCCESS && *out;
+}
+
+// Device address of g_noalloc_partials in the current context; 0 on success.
+int partials_address(cudaStream_t st, double** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return KOFM_ERR_NO_DEVICE;
+    // outside capture, cudaGetSymbolAddress also makes the device's primary
+    // context current if the calling thread has none yet
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return KOFM_ERR_INVALID_ARG;
+    CUcontext ctx = nullptr;
+    if (cs == cudaStreamCaptureStatusNone) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "kofm: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return KOFM_ERR_NO_DEVICE;
+        }
+        if (!current_context(&ctx)) return KOFM_ERR_NO_DEVICE;
+        std::lock_guard<std::mutex> lock(g_addr_mutex);
+        for (auto& a : g_addr)
+            if (a.first == ctx) { a.second = static_cast<double*>(p); *out = a.second; return KOFM_OK; }
+        g_addr.emplace_back(ctx, static_cast<double*>(p));
+        *out = static_cast<double*>(p);
+        return KOFM_OK;
+    }
+    if (!current_context(&ctx)) return KOFM_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(g_addr_mutex);
+    for (const auto& a : g_addr)
+        if (a.first == ctx) { *out = a.second; return KOFM_OK; }
+    return KOFM_ERR_STATE;  // first call in this context made under capture
+}
 
 template <int OP>
 __device__ __forceinline__ double op2(double a, double b) {
@@ -101,24 +160,16 @@ extern "C" int kofm_reduce_field_noalloc(const float* field, int32_t ncols, int3
     if (op < KOFM_OP_SUM || op > KOFM_OP_MAX) return KOFM_ERR_INVALID_ARG;
     const long long n = (long long)pitch * ny;
     if (n > (long long)KOFM_NOALLOC_MAX_NODES) return KOFM_ERR_TOO_LARGE;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return KOFM_ERR_NO_DEVICE;
-    if (!g_partials_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess || !p) {
-            fprintf(stderr, "kofm: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
-            return KOFM_ERR_NO_DEVICE;
-        }
-        g_partials_addr[dev] = static_cast<double*>(p);
-    }
-    const int np = (int)((n + KOFM_NOALLOC_CHUNK - 1) / KOFM_NOALLOC_CHUNK);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* partials = nullptr;
+    const int sa = partials_address(st, &partials);
+    if (sa != KOFM_OK) return sa;
+    const int np = (int)((n + KOFM_NOALLOC_CHUNK - 1) / KOFM_NOALLOC_CHUNK);
     cudaError_t e;
     switch (op) {
-        case KOFM_OP_SUM: e = launch<KOFM_OP_SUM>(field, n, pitch, ncols, g_partials_addr[dev], np, out, st); break;
-        case KOFM_OP_MIN: e = launch<KOFM_OP_MIN>(field, n, pitch, ncols, g_partials_addr[dev], np, out, st); break;
-        default: e = launch<KOFM_OP_MAX>(field, n, pitch, ncols, g_partials_addr[dev], np, out, st); break;
+        case KOFM_OP_SUM: e = launch<KOFM_OP_SUM>(field, n, pitch, ncols, partials, np, out, st); break;
+        case KOFM_OP_MIN: e = launch<KOFM_OP_MIN>(field, n, pitch, ncols, partials, np, out, st); break;
+        default: e = launch<KOFM_OP_MAX>(field, n, pitch, ncols, partials, np, out, st); break;
     }
     if (e != cudaSuccess) {
         fprintf(stderr, "kofm: no-alloc reduction launch failed: %s\n", cudaGetErrorString(e));

@@ -214,6 +214,15 @@ class Lattice:
     def debug_barrier_timeout(self, spin_limit: int) -> int:
         return self.lib.kofm_debug_barrier_timeout(self._ctx, spin_limit)
 
+    def debug_fail_solves(self, n: int, mask: int = 1):
+        """The next n k-omega solves report a NaN residual for the systems in
+        mask (1: omega, 2: k), host-made (kofm_debug_fail_solves)."""
+        check("kofm_debug_fail_solves", self.lib.kofm_debug_fail_solves(self._ctx, n, mask))
+
+    def komega_update_status(self) -> int:
+        """kofm_komega_update's status without raising."""
+        return self.lib.kofm_komega_update(self._ctx)
+
     @property
     def stream(self) -> int:
         return self.lib.kofm_stream(self._ctx) or 0

@@ -550,6 +550,14 @@ void orc_gmres_solve(int n, const int32_t* IA, const int32_t* JA,
  * (387-414).  The reference's "previous solution" copies act on solver
  * objects that are never created (kOmega.cpp:37-38, 395-396), so a halving
  * restores nothing; that is restated as is. */
+/* A solve stopped by a NaN residual at its first convergence check: one
+ * restart entered, no iteration, the field untouched (test hook). */
+static void orc_fail_stats(orc_gmres_stats* st) {
+    memset(st, 0, sizeof(*st));
+    st->restarts = 1;
+    st->nan = 1;
+}
+
 static void orc_halve(orc_komega_state* s, int* cur) {
     s->steps_per_lb *= 2;
     s->dt /= 2.0;
@@ -577,11 +585,15 @@ void orc_komega_solve(const orc_cfg* c, orc_komega_state* s,
                                  rho, dX);
         orc_komega_coeffs(c, ind, K, O, nut, Dk, Do, F1, dkdo, Sxy, rho, ux,
                           uy, kA, oA, kb, ob, dX, wallD, map, s->dt);
-        orc_gmres_solve(n, IA, JA, oA, ob, O, 10, s->max_iters, s->rel_tol,
-                        s->abs_tol, &s->last_o);
+        const int fail = s->fail_solves > 0 ? s->fail_mask : 0;
+        if (s->fail_solves > 0) s->fail_solves--;
+        if (fail & 1) orc_fail_stats(&s->last_o);
+        else orc_gmres_solve(n, IA, JA, oA, ob, O, 10, s->max_iters, s->rel_tol,
+                             s->abs_tol, &s->last_o);
         if (s->last_o.nan) orc_halve(s, &cur);
-        orc_gmres_solve(n, IA, JA, kA, kb, K, 10, s->max_iters, s->rel_tol,
-                        s->abs_tol, &s->last_k);
+        if (fail & 2) orc_fail_stats(&s->last_k);
+        else orc_gmres_solve(n, IA, JA, kA, kb, K, 10, s->max_iters, s->rel_tol,
+                             s->abs_tol, &s->last_k);
         if (s->last_k.nan) orc_halve(s, &cur);
         /* A NaN that persists halves dt without end in the reference (the
          * state is not restored); stop at 2^20 sub-steps, as the product does. */

@@ -104,6 +104,11 @@ typedef struct orc_komega_state {
     int max_iters;
     double rel_tol, abs_tol;
     orc_gmres_stats last_k, last_o;
+    /* test hook (no counterpart in the reference): the next fail_solves
+     * solves of the systems in fail_mask (1: omega, 2: k) report a NaN
+     * residual at their first convergence check and leave their field as it
+     * was, which is what a solve whose right-hand side holds a NaN does */
+    int fail_solves, fail_mask;
 } orc_komega_state;
 
 /* Runs kOmega::Solve on the given fields.  Work buffers: Dk, Do, F1 [n],

@@ -58,6 +58,7 @@ class KOmegaState(C.Structure):
         ("dt", C.c_double), ("max_iters", C.c_int),
         ("rel_tol", C.c_double), ("abs_tol", C.c_double),
         ("last_k", GmresStats), ("last_o", GmresStats),
+        ("fail_solves", C.c_int), ("fail_mask", C.c_int),
     ]
 
 

@@ -17,9 +17,11 @@ def pytest_configure(config):
 def oracle():
     """The FP64 CPU restatement (built on demand; test infrastructure only)."""
     from oracle.orc import LIB_ORACLE, Oracle
-    if not os.path.exists(LIB_ORACLE):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True)
-    return Oracle()
+    # make rebuilds it when a source is newer than the library
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=False)
+    if r.returncode != 0 and not os.path.exists(LIB_ORACLE):
+        raise RuntimeError("oracle/liboracle.so could not be built")
+    return Oracle(LIB_ORACLE)
 
 
 @pytest.fixture(scope="session")
@@ -27,7 +29,10 @@ def refk():
     """The reference's own kernels compiled for the CPU (oracle/_ref)."""
     from oracle.orc import LIB_REF, RefKernels
     if not os.path.exists(LIB_REF):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False)
+        from __graft_entry__ import REFERENCE_MOUNT
+        ref = os.environ.get("KOFM_REFERENCE") or REFERENCE_MOUNT
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
+                        "REF=" + (ref if os.path.isdir(ref) else "")], check=False)
     if not os.path.exists(LIB_REF):
         pytest.skip("oracle/_ref not built (reference tree absent); golden fixtures cover the pin")
     return RefKernels()

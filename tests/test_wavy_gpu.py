@@ -220,6 +220,44 @@ def test_wavy_komega_2048x256_matches_oracle(kofm_lib, oracle):
         assert err < 5 * spread + 1e-6, (name, err, spread)
 
 
+@pytest.mark.gpu
+def test_wavy_komega_2048x256_at_the_reference_tolerance(kofm_lib, oracle):
+    """The same 2048 x 256 wavy channel with the reference's GMRES tolerances
+    (relTol 1e-4, absTol 1e-7).  Measured against the FP64 oracle: rho, u, k,
+    omega stay below 1e-5 for the first 6 steps (3.1e-6 at step 6); at step 7
+    one discrete switch moves omega by 3.7e-5, and from there the difference
+    grows as the flow's own sensitivity does -- the oracle started from
+    k (1 + 1e-7) spreads from itself by 1e-4 in k by step 18 and 4e-3 by step
+    60, where the GPU stands at 1.3x that spread in u and 1.5x in k.  Held
+    here: 1e-5 after 6 steps, and u, k within 3x the oracle's spread after
+    60."""
+    ch, f, k, o, nut, rate, g, nu = _wavy_komega_case(2048, 256, 32.0, 512)
+    cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
+    mk = lambda kk: OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, kk, o, nut,  # noqa: E731
+                              komega=True, ibb_idx=ch.ibb_idx, ibb_q=ch.ibb_q)
+    sim, pert = mk(k), mk(k * (1 + 1e-7))
+    fl = ch.fluid_mask().ravel()
+    with _lattice(ch, rate, g, nu, True) as L:
+        L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
+        sim.step(6)
+        L.step(6)
+        rho, ux, k2, o2 = _fields(L)
+        errs = dict(rho=rel_l2(rho, sim.rho, fl), ux=rel_l2(ux, sim.ux, fl),
+                    k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
+        print("6 steps", errs)
+        for key in ("rho", "ux", "k", "omega"):
+            assert errs[key] < 1e-5, errs
+        sim.step(54)
+        pert.step(60)
+        L.step(54)
+        rho, ux, k2, o2 = _fields(L)
+    for name, gpu, ref, alt in (("ux", ux, sim.ux, pert.ux), ("k", k2, sim.K, pert.K)):
+        spread = rel_l2(alt, ref, fl)
+        err = rel_l2(gpu, ref, fl)
+        print("60 steps", name, err, spread)
+        assert err < 3 * spread + 1e-6, (name, err, spread)
+
+
 def _write_reference_walls(d, nx, ny, bottom, top, dx=1.0):
     """Wall files in the layout of a reference run directory: points every dx
     from x = -0.75 along the lower wall to past nx - 0.5, then back along the

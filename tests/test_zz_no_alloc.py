@@ -59,3 +59,38 @@ def test_matches_kofm_reduce_on_two_calls_in_a_row(kofm_lib):
                     assert got == pytest.approx(ref, rel=1e-12)
                 else:
                     assert got == ref
+
+
+def _numpy_reduce(a, op):
+    return {_abi.OP_SUM: np.sum, _abi.OP_MIN: np.min, _abi.OP_MAX: np.max}[op](a.astype(np.float64))
+
+
+@pytest.mark.gpu
+def test_padded_rows_and_fields_of_several_chunks(kofm_lib):
+    """Rows with padding columns (ncols 200 in a pitch of 256, the padding
+    filled with +-1e30 so that counting it would show in every operation),
+    and a first field of 1024 x 200 nodes -- four 65,536-node chunks, so
+    several partials and the final combine's per-thread ranges are used --
+    followed by a smaller one (one chunk): the second call reads only the
+    partials it wrote itself."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for (ncols, pitch, ny) in ((200, 256, 1024), (200, 256, 66)):
+        a = rng.uniform(-2.0, 3.0, (ny, pitch)).astype(np.float32)
+        a[:, ncols:] = np.where(rng.random((ny, pitch - ncols)) < 0.5, 1e30, -1e30)
+        ad = torch.from_numpy(a.ravel()).cuda()
+        for op in (_abi.OP_SUM, _abi.OP_MIN, _abi.OP_MAX):
+            st = kofm_lib.kofm_reduce_field_noalloc(
+                C.c_void_p(ad.data_ptr()), ncols, pitch, ny, op, C.c_void_p(out.data_ptr()),
+                C.c_void_p(stream))
+            assert st == 0
+            torch.cuda.synchronize()
+            got = float(out.item())
+            ref = _numpy_reduce(a[:, :ncols], op)
+            if op == _abi.OP_SUM:
+                assert got == pytest.approx(ref, rel=1e-12, abs=1e-9)
+            else:
+                assert got == ref
