@@ -123,7 +123,14 @@ typedef struct kofm_desc {
     double t_in;              /* TFD_X_IN_VAL (TFD_X_IN 2.0): inlet temperature
                                  and upper clamp of T in the source term */
     int32_t thermal_max_iters;/* THERMAL_MAX_ITERS (1000) */
-    int32_t thermal_pad;
+    int32_t komega_classic;   /* k-omega solver form: 0 (default) builds all
+                                 Krylov directions of a cycle in one sweep
+                                 (powers of the off-diagonal operator, Gram
+                                 matrix, the simpler-GMRES steps in that
+                                 basis); 1 builds one vector per sweep as
+                                 GMRESSolver::solve does.  komega_full_cycle = 1
+                                 implies 1.  Both follow the reference's
+                                 restart loop and truncation tests. */
     double thermal_rel_tol;   /* THERMAL_MAX_REL_TOL (1e-4) */
     double thermal_abs_tol;   /* THERMAL_MAX_ABS_TOL (1e-7) */
     double thermal_dt;        /* dTtfd (= tfdSteps, 1); sub-steps per update
@@ -344,6 +351,12 @@ int kofm_debug_barrier_timeout(kofm_ctx* ctx, int64_t spin_limit);
  * the host side of the call; nothing faults on the device.  No counterpart in
  * the reference. */
 int kofm_debug_fail_solves(kofm_ctx* ctx, int32_t n, int32_t mask);
+
+/* Diagnostic: device times (ns after the launch started) at which the last
+ * k-omega solve's grid barriers released -- the ends of its sweeps -- into
+ * ns[0 .. min(*n, cap) - 1]; *n gets the number of barriers (at most 32 are
+ * timed).  Synchronises.  No counterpart in the reference. */
+int kofm_debug_solver_trace(kofm_ctx* ctx, int64_t* ns, int32_t cap, int32_t* n);
 
 /* ---- discrete adjoint of the laminar step -----------------------------------
  * No counterpart in the reference.  From the current state (a stepped FP32

@@ -52,7 +52,7 @@ class KofmDesc(C.Structure):
         ("use_thermal", C.c_int32), ("thermal_every", C.c_int32),
         ("pr_number", C.c_double), ("pr_turb_number", C.c_double),
         ("alpha_foul", C.c_double), ("t_in", C.c_double),
-        ("thermal_max_iters", C.c_int32), ("thermal_pad", C.c_int32),
+        ("thermal_max_iters", C.c_int32), ("komega_classic", C.c_int32),
         ("thermal_rel_tol", C.c_double), ("thermal_abs_tol", C.c_double),
         ("thermal_dt", C.c_double),
     ]
@@ -106,6 +106,7 @@ SIGNATURES = {
     "kofm_get_stats": (C.c_int, [_vp, C.POINTER(KofmStats)]),
     "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
     "kofm_debug_fail_solves": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "kofm_debug_solver_trace": (C.c_int, [_vp, C.POINTER(C.c_int64), C.c_int32, _i32p]),
     "kofm_stream": (_vp, [_vp]),
     "kofm_reduce_field_noalloc": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             _vp, _vp]),

@@ -20,8 +20,14 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libkofm.so")
 SOURCES = ["kofm_api.cu", "kofm_noalloc.cu"]
 DEPS = ["kofm_api.cu", "kofm_noalloc.cu", "kofm_common.cuh", "kofm_lb.cuh",
-        "kofm_komega.cuh", "kofm_gmres.cuh", "kofm_komega_api.inc", "kofm_batch.inc",
-        "kofm_thermal.cuh", "kofm_thermal_api.inc", "kofm_adjoint.inc", "kofm_geometry.inc"]
+        "kofm_komega.cuh", "kofm_gmres.cuh", "kofm_sstep.cuh", "kofm_komega_api.inc",
+        "kofm_batch.inc", "kofm_thermal.cuh", "kofm_thermal_api.inc", "kofm_adjoint.inc",
+        "kofm_geometry.inc"]
+
+
+def _all_sources() -> list[str]:
+    """Every file of csrc/ (a new header can never be missed)."""
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
@@ -42,7 +48,7 @@ def needs_build() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    paths = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(ROOT, "include", "kofm.h")]
+    paths = _all_sources() + [os.path.join(ROOT, "include", "kofm.h")]
     return any(os.path.getmtime(p) > t for p in paths if os.path.exists(p))
 
 

@@ -8,6 +8,7 @@
 #include "kofm_lb.cuh"
 #include "kofm_komega.cuh"
 #include "kofm_gmres.cuh"
+#include "kofm_sstep.cuh"
 #include "kofm_thermal.cuh"
 
 #include <cuda_runtime.h>
@@ -27,6 +28,8 @@ namespace kofm {
 int th_solver_alloc(kofm_ctx* c);
 int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned int** bar,
                     int* nblocks, int P, int ny, int K, int dev, int max_blocks);
+int ss_solver_alloc(double** part, int** lhint, int* nblocks, int* pstrips, int* prows, int nx,
+                    int ny, int K, int dev, int max_blocks);
 void ko_system_free(KoSystem* s);
 }  // namespace kofm
 
@@ -100,6 +103,11 @@ struct kofm_ctx {
     double* gpart = nullptr;          // solver partial sums
     unsigned int* bar = nullptr;      // grid barrier words
     int solver_blocks = 0;
+    // one-sweep-per-cycle solver (kofm_sstep.cuh): partial sums, grid and
+    // the strips of its powers and update sweeps
+    double* spart = nullptr;
+    int* ss_lhint = nullptr;          // powers of a cycle's first round, per system
+    int ss_blocks = 0, ss_pstrips = 0, ss_prows = 0;
     int steps_per_lb = 1;
     int time_since_change = 0;
     double dt = 1.0;
@@ -534,7 +542,7 @@ int kofm_destroy(kofm_ctx* c) {
     void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
-                    c->gpart, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
+                    c->gpart, c->spart, c->ss_lhint, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
                     c->shear_bl_nodes, c->shear_bl_w, c->shear_bl_tau, c->T, c->Tprev, c->tb,
                     c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
                     c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar, c->shear_idx,
@@ -610,6 +618,9 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         ALLOC(c->nut, D);
         int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks,
                                  c->P, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
+        if (s2) { kofm_destroy(c); return s2; }
+        s2 = ss_solver_alloc(&c->spart, &c->ss_lhint, &c->ss_blocks, &c->ss_pstrips, &c->ss_prows,
+                             d->nx, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
         if (s2) { kofm_destroy(c); return s2; }
         if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {
             kofm_destroy(c);

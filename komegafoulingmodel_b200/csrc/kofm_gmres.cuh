@@ -58,6 +58,8 @@ struct GmresSys {
     int vec_index_sum;  // sum over built vectors of their index k in the cycle
     int update_terms;   // sum over cycles of the update's coefficient count kk
     int inject;         // test hook: report a NaN residual at the first check
+    int lev;            // one-sweep cycle: powers computed so far in this cycle
+    int ext;            // one-sweep cycle: 1 = more powers needed before the cut
     double rho0, norm_rhs, rinv, rho, prev_err;
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||
     double h[KOFM_MAX_KRYLOV];   // Gram-Schmidt coefficients for the next vector
@@ -66,13 +68,31 @@ struct GmresSys {
     double R[KOFM_MAX_KRYLOV * KOFM_MAX_KRYLOV];
 };
 
+constexpr int GM_TRACE = 32;
 struct GmresControl {
     GmresSys sys[2];
     int error;        // 0 ok, 1 barrier timeout
     int passes;       // grid sweeps performed
     int any_active;
+    int ntrace;       // grid barriers recorded in trace
+    int any_ext;      // one-sweep cycle: a system asks for more powers
     int pad;
+    unsigned long long t_start;           // %globaltimer at the first block's start (ns)
+    unsigned long long trace[GM_TRACE];   // %globaltimer at each grid barrier's release
 };
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Records the release time of a grid barrier (called by the last block).
+__device__ __forceinline__ void trace_barrier(GmresControl* ctl) {
+    const int n = __ldcg(&ctl->ntrace);
+    if (n < GM_TRACE) __stcg(&ctl->trace[n], globaltimer_ns());
+    __stcg(&ctl->ntrace, n + 1);
+}
 
 struct GridBarrier {
     unsigned int count;
@@ -317,6 +337,7 @@ __device__ bool grid_sync(const GmresArgs& a, int kind, int kcur, int restart) {
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
+            trace_barrier(a.ctl);
             atomicExch(&a.bar->count, 0u);
             __threadfence();
             atomicAdd(&a.bar->gen, 1u);
@@ -571,6 +592,7 @@ __device__ void krylov_strip(const GmresArgs& a, const KoSystem& S, const double
 __global__ void __launch_bounds__(GM_THREADS, KOFM_GM_MINBLOCKS)
 gmres_kernel(const GmresArgs a) {
     GmresControl* ctl = a.ctl;
+    if (blockIdx.x == 0 && threadIdx.x == 0) __stcg(&ctl->t_start, globaltimer_ns());
     extern __shared__ __align__(16) unsigned char gm_smem[];
     SolverSmem& T = *reinterpret_cast<SolverSmem*>(gm_smem);  // dynamic: larger than 48 KiB
     double* ring = T.ring[threadIdx.x >> 5];

@@ -45,7 +45,10 @@ struct KoSystem {
     double* rhs = nullptr;    // [D] b' = b - A x0 (also the residual of restart 0)
     double* r = nullptr;      // [D] residual of restarts >= 1
     double* x = nullptr;     // [D] correction
-    double* V = nullptr;      // [K x D] Krylov basis (orthogonalised, unscaled; interleaved)
+    double* V = nullptr;      // [K x D] Krylov basis (orthogonalised, unscaled; interleaved),
+                              // or the powers p_1 .. p_K of the one-sweep cycle
+    double* x2 = nullptr;     // [D] correction and residual of alternate restarts
+    double* r2 = nullptr;     //     (the one-sweep cycle's update reads one, writes the other)
 };
 
 struct AsmParams {

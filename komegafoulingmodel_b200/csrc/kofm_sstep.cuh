@@ -1,0 +1,716 @@
+// kofm_sstep.cuh - the k-omega solve with all Krylov directions of a cycle
+// built in one sweep (sm_100a).
+//
+// Algorithm: the reference's restarted "simpler GMRES" (GMRESSolver::solve,
+// GMRESSolver.cpp:227-355; Walker & Zhou 1994) on the correction system
+// A d = b' with the same restart loop, convergence test, truncation tests
+// (diag(R) against relTol R(0,0), then |xi_k| >= rho), residual estimator
+// rho *= sin(acos(xi/rho)), back-substitution with the reference's R
+// indexing, and x = x0 + d.  What changes is how the Krylov basis is formed.
+//
+// The rows are normalised by their diagonal, so A = I + N with N the four
+// off-diagonals.  The Krylov space of A on r equals that of N, spanned by the
+// powers p_0 = r, p_{j+1} = N p_j.  One grid sweep (the "powers" phase)
+// computes p_1 .. p_L of a cycle at once: every thread owns one column of a
+// 256-column strip and marches down the rows, level j working one row behind
+// level j-1 (a skewed wavefront), so each coefficient row is read from HBM
+// once for all L levels; the row's coefficients and level-0 value are staged
+// ahead in a per-thread shared-memory ring by cp.async; x neighbours come from
+// warp shuffles, across warps from a shared-memory edge buffer written the
+// step before (one block barrier per row).  A pointwise sweep then forms the
+// Gram matrix G = P^T P of [p_0 .. p_L], and the serial section runs the
+// simpler GMRES steps in the (L+1)-dimensional coefficient space with the
+// inner product a^T G b: with A p_j = p_j + p_{j+1}, every vector of the
+// method (r/||r||, A z, the orthonormal v_k, the update) is a combination of
+// the p_j, and R, xi, rho and the tests are the reference's quantities.  Two
+// pointwise sweeps apply d += sum c_j p_j and form the next residual
+// b' - A d with its norm, so the next restart's test needs no extra sweep.
+//
+// L follows the cycle lengths seen so far (two more powers than the last
+// cycle used, kept per system across solves); a cycle whose tests have not
+// fired by then gets the remaining powers up to the Krylov dimension in a
+// second powers + Gram round and is re-run from its first vector.
+//
+// Per cycle: 4 sweeps (powers, Gram, update, residual) instead of one per
+// Krylov vector plus residual and update sweeps, and the orthogonalisation
+// reads no basis vector.  In exact arithmetic the iterates are those of the
+// reference's classical Gram-Schmidt; in FP64 the truncation tests see
+// rounding of the size the reference's own classical Gram-Schmidt has (both
+// lose orthogonality like eps cond^2), so the cut of a converged cycle moves
+// by a vector or two while restart counts and the solution agree to far below
+// the tolerance.
+#pragma once
+#include "kofm_gmres.cuh"
+
+namespace kofm {
+
+constexpr int SS_THREADS = 256;
+constexpr int SS_WARPS = SS_THREADS / 32;
+constexpr int SS_MAXL = KOFM_MAX_KRYLOV;                  // levels of one sweep
+constexpr int SS_NG = (SS_MAXL + 1) * (SS_MAXL + 2) / 2;  // Gram entries per system
+constexpr int SS_SLOTS = 2 * SS_NG;                       // partial sums per block
+constexpr int SS_PF = 6;                                  // rows staged ahead by the powers sweep
+constexpr int SS_RING = 8;                                // ring rows (power of two > SS_PF + 1)
+static_assert(SS_RING > SS_PF + 1 && (SS_RING & (SS_RING - 1)) == 0, "ring");
+constexpr int SS_RF = 5;                                  // ring fields: level 0, cE, cW, cN, cS
+constexpr int SS_MINL = 4;                                // fewest powers of a first round
+
+struct SsArgs {
+    KoSystem sys[2];          // x / x2 and r / r2 alternate between restarts
+    float* field[2];          // omega, k (FP32 fields, updated in place at the end)
+    const int16_t* ntype;
+    GmresControl* ctl;
+    double* part;             // [SS_SLOTS][gridDim.x] (slot-major)
+    GridBarrier* bar;
+    int* lhint;               // [2] powers of a first round, kept across solves (0: K)
+    int nx, ny, P;
+    long long D;
+    int K;                    // Krylov dimension
+    int max_restarts;
+    double rel_tol, abs_tol;
+    long long spin_limit;
+    int pstrips;              // powers strips of SS_THREADS - 2K own columns
+    int prows;                // row ranges per powers strip
+};
+
+// Gram entry (i, j), i <= j, of one system: slot j (j + 1) / 2 + i.
+__host__ __device__ constexpr int ss_gslot(int i, int j) { return j * (j + 1) / 2 + i; }
+
+struct SsSmem {
+    double edge[2][SS_WARPS][2][SS_MAXL];  // [step parity][warp][left/right lane][level]
+    double red[SS_WARPS][SS_NG];           // block reduction of the Gram partials
+    double c[2][SS_MAXL + 1];              // update coefficients on p_0 .. p_K
+    int act[2];
+    int kk[2];
+    int lfrom[2], lto[2];                  // powers of this round: levels lfrom+1 .. lto
+};
+
+// Dynamic shared memory of the powers phase: per thread (column) a ring of
+// SS_RING rows of SS_RF doubles, [row][field][thread] (conflict-free).
+constexpr size_t SS_DSMEM = sizeof(double) * SS_RING * SS_RF * SS_THREADS;
+
+__device__ __forceinline__ int ss_first_levels(const SsArgs& a, int s) {
+    int l = __ldcg(a.lhint + s);
+    if (l <= 0 || l > a.K) l = a.K;
+    return l < SS_MINL ? (a.K < SS_MINL ? a.K : SS_MINL) : l;
+}
+
+// ---- coefficient-space simpler GMRES (serial section, one thread per system) --
+// G: (L+1) x (L+1) Gram of p_0 .. p_L (full, symmetric).  Builds the cycle's
+// vectors in order and applies the reference's tests after each (the same
+// cycle_step as the one-vector-per-sweep solver).  Returns the vectors built;
+// S.done = 0 when L < K vectors passed every test (more powers needed).  On a
+// finished cycle, cP gets the update y_0 r/rho0 + sum_{j>=1} y_j v_{j-1} on
+// p_0 .. p_L.
+__device__ int ss_cycle(GmresSys& S, const double* G, int L, int K, double rel_tol, double* cP) {
+    const int n = L + 1;
+    double V[SS_MAXL][SS_MAXL + 1];
+    double GV[SS_MAXL][SS_MAXL + 1];
+    double z0[SS_MAXL + 1], w[SS_MAXL + 1], Gw[SS_MAXL + 1];
+    for (int i = 0; i < n; ++i) z0[i] = 0.0;
+    z0[0] = S.rinv;
+    for (int i = 0; i < K * K; ++i) S.R[i] = 0.0;
+    S.rho = 1.0;
+    S.done = 0;
+    const int iters0 = S.iters;
+    int k = 0;
+    for (; k < L && k < K; ++k) {
+        // w = A z, z = r / rho0 (k = 0) or v_{k-1}; A p_j = p_j + p_{j+1}
+        const double* z = k == 0 ? z0 : V[k - 1];
+        w[0] = z[0];
+        for (int i = 1; i < n; ++i) w[i] = z[i] + z[i - 1];
+        for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int j = 0; j < n; ++j) s += G[i * n + j] * w[j];
+            Gw[i] = s;
+        }
+        // classical Gram-Schmidt: R(j, k) = <w, v_j> with the unmodified w
+        double h[SS_MAXL];
+        for (int j = 0; j < k; ++j) {
+            double s = 0.0;
+            for (int i = 0; i < n; ++i) s += w[i] * GV[j][i];
+            h[j] = s;
+        }
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < n; ++i) {
+                w[i] -= h[j] * V[j][i];
+                Gw[i] -= h[j] * GV[j][i];
+            }
+        double nk2 = 0.0;
+        for (int i = 0; i < n; ++i) nk2 += w[i] * Gw[i];
+        const double nk = nk2 > 0.0 ? sqrt(nk2) : 0.0;  // a vanishing direction cuts (diag test)
+        for (int j = 0; j < k; ++j) S.R[j + k * K] = h[j];
+        S.R[k + k * K] = nk;
+        const double inv = nk > 0.0 ? 1.0 / nk : 0.0;
+        double xi = 0.0;
+        for (int i = 0; i < n; ++i) {
+            V[k][i] = w[i] * inv;
+            GV[k][i] = Gw[i] * inv;
+            xi += z0[i] * GV[k][i];
+        }
+        S.xi[k] = xi;
+        cycle_step(S, K, k, rel_tol);
+        if (S.done) break;
+    }
+    const int built = S.done ? k + 1 : k;
+    if (!S.done) {
+        S.iters = iters0;  // the cycle is re-run with more powers
+        return built;
+    }
+    // coefficient 0 is applied even when the cycle is cut at k = 0, as the
+    // reference's update does (its xi(0) then unscaled)
+    const int kk = S.kk;
+    for (int i = 0; i < n; ++i) cP[i] = S.c[0] * z0[i];
+    for (int j = 1; j < kk; ++j)
+        for (int i = 0; i < n; ++i) cP[i] += S.c[j] * V[j - 1][i];
+    return built;
+}
+
+enum SsSerial : int { SS_SER_NONE = 0, SS_SER_GRAM, SS_SER_RESID };
+
+// Serial section (last block to reach a barrier).  SS_SER_GRAM: the Gram of
+// this round's powers is complete (restart 0, round 0 also takes its
+// convergence test from G(0,0) = ||b'||^2); SS_SER_RESID: the residual sweep
+// left ||r||^2 of the next restart in slot 0.
+__device__ void ss_serial(const SsArgs& a, int kind, int restart, int round, int nblocks) {
+    GmresControl* ctl = a.ctl;
+    __shared__ double tot[SS_SLOTS];
+    __shared__ GmresSys sS[2];
+    __shared__ int s_any, s_ext;
+    __shared__ int s_L[2];
+    const int warp = threadIdx.x >> 5;
+    constexpr int NW = (int)(sizeof(GmresSys) / 8);
+    for (int s = 0; s < 2; ++s) {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&ctl->sys[s]);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sS[s]);
+        for (int i = threadIdx.x; i < NW; i += SS_THREADS) dst[i] = __ldcg(src + i);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        // the levels of this round, as every block chose them
+        const int s = threadIdx.x;
+        const GmresSys& S = sS[s];
+        int L = 0;
+        if (S.active && kind == SS_SER_GRAM) {
+            if (round == 0) L = ss_first_levels(a, s);
+            else L = S.ext ? a.K : 0;
+        }
+        s_L[s] = L;
+    }
+    if (threadIdx.x == 0) { s_any = 0; s_ext = 0; }
+    __syncthreads();
+    int used[2];
+    for (int s = 0; s < 2; ++s)
+        used[s] = kind == SS_SER_GRAM ? (s_L[s] + 1) * (s_L[s] + 2) / 2 : 1;
+    for (int i = warp; i < used[0] + used[1]; i += SS_WARPS) {
+        const int s = i < used[0] ? 0 : 1;
+        const int slot = s * SS_NG + (i - s * used[0]);
+        const double v = sum_slot_warp(a.part, nblocks, slot);
+        if ((threadIdx.x & 31) == 0) tot[slot] = v;
+    }
+    __syncthreads();
+    // one thread per system (threads 0 and 32: different warps)
+    if ((threadIdx.x & 31) == 0 && warp < 2) {
+        const int s = warp;
+        GmresSys& S = sS[s];
+        const double* t = tot + SS_NG * s;
+        if (S.active) {
+            if (kind == SS_SER_GRAM && s_L[s] > 0) {
+                const int L = s_L[s];
+                const double rho0 = sqrt(t[0]);
+                if (restart == 0 && round == 0) {
+                    // the restart-0 test (GMRESSolver::solve's checkConvergence)
+                    S.rho0 = rho0;
+                    S.norm_rhs = rho0;
+                    S.restarts += 1;
+                    const double resid = S.rho0 / S.norm_rhs;
+                    if (isnan(resid) || S.inject) { S.nan = 1; S.active = 0; }
+                    else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+                    else S.cycles += 1;
+                }
+                if (S.active) {
+                    S.rho0 = rho0;
+                    S.rinv = 1.0 / rho0;
+                    double G[(SS_MAXL + 1) * (SS_MAXL + 1)];
+                    const int n = L + 1;
+                    for (int j = 0; j < n; ++j)
+                        for (int i = 0; i <= j; ++i) {
+                            const double v = t[ss_gslot(i, j)];
+                            G[i * n + j] = v;
+                            G[j * n + i] = v;
+                        }
+                    double cP[SS_MAXL + 1];
+                    const int built = ss_cycle(S, G, L, a.K, a.rel_tol, cP);
+                    S.lev = L;
+                    if (!S.done) {
+                        S.ext = 1;  // more powers, then the cycle again
+                    } else {
+                        S.ext = 0;
+                        S.vecs += built;
+                        S.vec_index_sum += built * (built - 1) / 2;
+                        // the update sweep reads c on p_0 .. p_{kk-1}
+                        for (int i = 0; i < a.K; ++i) S.h[i] = i < n ? cP[i] : 0.0;
+                        int nl = built + 2;
+                        nl = nl > a.K ? a.K : nl;
+                        __stcg(a.lhint + s, nl);
+                    }
+                }
+            } else if (kind == SS_SER_RESID) {
+                // residual of the next restart (GMRESSolver.cpp:248-256)
+                const int next = restart + 1;
+                if (next < a.max_restarts) {
+                    S.rho0 = sqrt(t[0]);
+                    S.restarts += 1;
+                    const double resid = S.rho0 / S.norm_rhs;
+                    if (isnan(resid)) { S.nan = 1; S.active = 0; }
+                    else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+                    else S.cycles += 1;
+                } else {
+                    S.active = 0;  // iteration cap: the loop ends without a test
+                }
+            }
+        }
+        atomicOr(&s_any, S.active);
+        atomicOr(&s_ext, S.active && S.ext);
+    }
+    __syncthreads();
+    for (int s = 0; s < 2; ++s) {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&sS[s]);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&ctl->sys[s]);
+        for (int i = threadIdx.x; i < NW; i += SS_THREADS) __stcg(dst + i, src[i]);
+    }
+    if (threadIdx.x == 0) {
+        __stcg(&ctl->any_active, s_any);
+        __stcg(&ctl->any_ext, s_ext);
+        __stcg(&ctl->passes, ldc(&ctl->passes) + 1);
+    }
+}
+
+// Bounded grid barrier with the serial section run by the last block to
+// arrive (the same protocol as the one-vector-per-sweep solver's).
+__device__ bool ss_sync(const SsArgs& a, int kind, int restart, int round) {
+    __shared__ int s_last;
+    __shared__ unsigned int s_gen;
+    const int nblocks = gridDim.x;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_gen = ld_acquire_u32(&a.bar->gen);
+        const unsigned int ticket = atomicAdd(&a.bar->count, 1u);
+        s_last = (ticket == (unsigned int)nblocks - 1u);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (kind != SS_SER_NONE) ss_serial(a, kind, restart, round, nblocks);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            trace_barrier(a.ctl);
+            atomicExch(&a.bar->count, 0u);
+            __threadfence();
+            atomicAdd(&a.bar->gen, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire_u32(&a.bar->gen) == s_gen) {
+            if (++it > a.spin_limit || ldc(&a.ctl->error)) {
+                atomicExch(&a.ctl->error, 1);
+                break;
+            }
+            __nanosleep(100);
+        }
+    }
+    __syncthreads();
+    return ldc(&a.ctl->error) == 0;
+}
+
+__device__ __forceinline__ void ss_cp8(unsigned saddr, const double* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(gmem) : "memory");
+}
+
+// ---- powers phase ----------------------------------------------------------------
+// One block: levels lfrom+1 .. lfrom+L of the rows [ya, yb) of the strip
+// whose own columns start at x0, from level lfrom (p0 plain, or basis slot
+// lfrom - 1).  Thread t holds column x0 - L + t (periodic); level j is valid
+// on threads j .. 255 - j.  Step tau takes level 0 at row tau and computes
+// level j at row tau - j from level j-1 at rows tau-j-1 (two steps back),
+// tau-j (one step back; x neighbours) and tau-j+1 (this step, this thread).
+// The thread's level-0 value and four coefficients of row tau + SS_PF are
+// copied into its ring slot (cp.async) while row tau computes; level 1 takes
+// the coefficients of its row from the ring and hands them on to the next
+// level one step later in registers (level j uses the row level j-1 used the
+// step before).  Rows outside the lattice are zero.  Level j is stored in
+// basis slot lfrom + j - 1 (interleaved layout).
+template <int L>
+__device__ void ss_powers(const SsArgs& a, const KoSystem& S, const double* p0, bool p0_basis,
+                          int lfrom, int x0, int own_w, int ya, int yb, SsSmem& sm, double* ring) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int xs = x0 - L + t;
+    const int xc = ((xs % a.nx) + a.nx) % a.nx;
+    const bool own = t >= L && t < L + own_w && xs < a.nx;
+    const long long cbase = (long long)(xc >> 5) * 128 + (xc & 31);
+    const long long cstride = 4LL * a.P;
+    const long long vbase = (long long)(xc >> 5) * (a.K * 32) + (xc & 31);
+    const long long vstride = (long long)a.K * a.P;
+    // level-0 source: plain layout (stride P) or a basis slot (interleaved)
+    const double* src0 = p0_basis ? S.V + vbase + (long long)(lfrom - 1) * 32 : p0 + xc;
+    const long long s0 = p0_basis ? vstride : (long long)a.P;
+    double* myring = ring + t;  // [slot][field][thread]
+    const unsigned ring_s = (unsigned)__cvta_generic_to_shared(myring);
+    auto issue = [&](int row) {
+        const int r = row & (SS_RING - 1);
+        if (row >= 0 && row < a.ny) {
+            ss_cp8(ring_s + 8u * (unsigned)(r * SS_RF * SS_THREADS), src0 + (long long)row * s0);
+            const double* c = S.coef + (long long)row * cstride + cbase;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                ss_cp8(ring_s + 8u * (unsigned)((r * SS_RF + 1 + q) * SS_THREADS), c + 32 * q);
+        } else {
+#pragma unroll
+            for (int f = 0; f < SS_RF; ++f) myring[(r * SS_RF + f) * SS_THREADS] = 0.0;
+        }
+    };
+    double cur[L], prv[L], pr2[L];
+    double cE[L], cW[L], cN[L], cS[L];  // level j's row coefficients (rotated down a level per step)
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        cur[j] = 0.0; prv[j] = 0.0; pr2[j] = 0.0;
+        cE[j] = 0.0; cW[j] = 0.0; cN[j] = 0.0; cS[j] = 0.0;
+    }
+    const int t0 = ya - L, t1 = yb + L;
+#pragma unroll 1
+    for (int i = 0; i < SS_PF; ++i) {
+        issue(t0 + i);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    // store address of level 1 at row tau - 1; level j is (j - 1) rows and slots further
+    double* vrow = S.V + (long long)(t0 - 1) * vstride + vbase + (long long)lfrom * 32;
+    for (int tau = t0; tau < t1; ++tau, vrow += vstride) {
+        issue(tau + SS_PF);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(SS_PF) : "memory");  // rows <= tau landed
+        // coefficients: level j takes level j-1's row of the previous step;
+        // level 1 the ring's row tau - 1
+#pragma unroll
+        for (int j = L - 1; j > 0; --j) { cE[j] = cE[j - 1]; cW[j] = cW[j - 1]; cN[j] = cN[j - 1]; cS[j] = cS[j - 1]; }
+        {
+            const int r1 = (tau - 1) & (SS_RING - 1);
+            const double* q = myring + r1 * SS_RF * SS_THREADS;
+            cE[0] = q[1 * SS_THREADS]; cW[0] = q[2 * SS_THREADS];
+            cN[0] = q[3 * SS_THREADS]; cS[0] = q[4 * SS_THREADS];
+        }
+        pr2[0] = prv[0]; prv[0] = cur[0];
+        cur[0] = myring[(tau & (SS_RING - 1)) * SS_RF * SS_THREADS];
+        __syncthreads();  // the edge values of step tau - 1 are visible
+        const int par = tau & 1;
+        // x neighbours of every level from the previous step (level 0 is
+        // already shifted: its previous value is prv[0]; the others not yet:
+        // cur[j]), then the levels
+        double lft[L], rgt[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            const double mine = j == 0 ? prv[0] : cur[j];
+            lft[j] = __shfl_up_sync(0xffffffffu, mine, 1);
+            rgt[j] = __shfl_down_sync(0xffffffffu, mine, 1);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) lft[j] = w > 0 ? sm.edge[par ^ 1][w - 1][1][j] : 0.0;
+        }
+        if (lane == 31) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) rgt[j] = w < SS_WARPS - 1 ? sm.edge[par ^ 1][w + 1][0][j] : 0.0;
+        }
+        const int yl = tau - L;  // the last level's row
+        const bool st_row = own && tau - 1 >= ya && yl < yb;
+#pragma unroll
+        for (int j = 1; j <= L; ++j) {
+            const int y = tau - j;
+            // N p in the CSR order of an interior row without its centre: S, W, E, N
+            const double v = cS[j - 1] * pr2[j - 1] + cW[j - 1] * lft[j - 1] + cE[j - 1] * rgt[j - 1] +
+                             cN[j - 1] * cur[j - 1];
+            if (j < L) { pr2[j] = prv[j]; prv[j] = cur[j]; cur[j] = v; }
+            if (st_row && y >= ya && y < yb) __stcg(vrow - (long long)(j - 1) * vstride + (j - 1) * 32, v);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) sm.edge[par][w][0][j] = cur[j];
+        }
+        if (lane == 31) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) sm.edge[par][w][1][j] = cur[j];
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();  // the edge buffer and the ring are reused by the next unit
+}
+
+// ---- Gram phase -------------------------------------------------------------------
+// Nodes [g0, g1) of one system, two per thread and iteration (the 2 (L+1)
+// loads of both in flight together): the (L+1)(L+2)/2 products of
+// p_0 .. p_L summed per thread.
+template <int L>
+__device__ void ss_gram(const SsArgs& a, const KoSystem& S, const double* p0, long long g0,
+                        long long g1, double* acc) {
+    constexpr int NGL = (L + 1) * (L + 2) / 2;
+    double s[NGL];
+#pragma unroll
+    for (int i = 0; i < NGL; ++i) s[i] = 0.0;
+    long long g = g0 + threadIdx.x;
+    for (; g + SS_THREADS < g1; g += 2 * SS_THREADS) {
+        double p[L + 1], q[L + 1];
+        const long long g2 = g + SS_THREADS;
+        p[0] = __ldcg(p0 + g);
+        q[0] = __ldcg(p0 + g2);
+        const long long vb = (g >> 5) * (a.K * 32) + (g & 31);
+        const long long vb2 = (g2 >> 5) * (a.K * 32) + (g2 & 31);
+#pragma unroll
+        for (int j = 1; j <= L; ++j) {
+            p[j] = __ldcg(S.V + vb + (j - 1) * 32);
+            q[j] = __ldcg(S.V + vb2 + (j - 1) * 32);
+        }
+#pragma unroll
+        for (int j = 0; j <= L; ++j)
+#pragma unroll
+            for (int i = 0; i <= j; ++i) s[ss_gslot(i, j)] += p[i] * p[j] + q[i] * q[j];
+    }
+    if (g < g1) {
+        double p[L + 1];
+        p[0] = __ldcg(p0 + g);
+        const long long vb = (g >> 5) * (a.K * 32) + (g & 31);
+#pragma unroll
+        for (int j = 1; j <= L; ++j) p[j] = __ldcg(S.V + vb + (j - 1) * 32);
+#pragma unroll
+        for (int j = 0; j <= L; ++j)
+#pragma unroll
+            for (int i = 0; i <= j; ++i) s[ss_gslot(i, j)] += p[i] * p[j];
+    }
+#pragma unroll
+    for (int i = 0; i < NGL; ++i) acc[i] = s[i];
+}
+
+__device__ void ss_block_reduce(const double* v, int n, double* part, int base, SsSmem& sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int s = 0; s < n; ++s) {
+        double x = v[s];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) sm.red[warp][s] = x;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < n; s += SS_THREADS) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < SS_WARPS; ++w) x += sm.red[w][s];
+        part[(long long)(base + s) * gridDim.x + blockIdx.x] = x;
+    }
+    __syncthreads();
+}
+
+// ---- the solver kernel ------------------------------------------------------------------
+__global__ void __launch_bounds__(SS_THREADS, 1)
+sstep_kernel(const SsArgs a) {
+    GmresControl* ctl = a.ctl;
+    __shared__ SsSmem sm;
+    extern __shared__ __align__(16) double ss_ring[];
+    double* ring = ss_ring;
+    if (blockIdx.x == 0 && threadIdx.x == 0) __stcg(&ctl->t_start, globaltimer_ns());
+    const long long stride = (long long)gridDim.x * SS_THREADS;
+    const long long t0 = (long long)blockIdx.x * SS_THREADS + threadIdx.x;
+    for (int restart = 0; restart < a.max_restarts; ++restart) {
+        for (int round = 0;; ++round) {
+            // ---- levels of this round ----------------------------------------------------
+            if (threadIdx.x < 2) {
+                const int s = threadIdx.x;
+                const int act = ldc(&ctl->sys[s].active);
+                int lf = 0, lt = 0;
+                if (act) {
+                    if (round == 0) lt = ss_first_levels(a, s);
+                    else if (ldc(&ctl->sys[s].ext)) { lf = ldc(&ctl->sys[s].lev); lt = a.K; }
+                }
+                sm.act[s] = act;
+                sm.lfrom[s] = lf;
+                sm.lto[s] = lt;
+            }
+            __syncthreads();
+            // ---- powers ---------------------------------------------------------------
+            {
+                const int units = a.pstrips * a.prows;
+                for (int u = blockIdx.x; u < 2 * units; u += gridDim.x) {
+                    const int s = u / units, r = u % units;
+                    const int lf = sm.lfrom[s], L = sm.lto[s] - lf;
+                    if (L <= 0) continue;  // block-uniform
+                    const int strip = r % a.pstrips, rr = r / a.pstrips;
+                    const int ya = (int)((long long)rr * a.ny / a.prows);
+                    const int yb = (int)((long long)(rr + 1) * a.ny / a.prows);
+                    const KoSystem& S = a.sys[s];
+                    const double* p0 = restart == 0 ? S.rhs : ((restart & 1) ? S.r2 : S.r);
+                    // strips are laid out for K levels of halo: own columns x0 .. x0 + 255 - 2K
+                    const int ow = SS_THREADS - 2 * a.K;
+                    const int x0 = strip * ow;
+                    switch (L) {
+#define KOFM_SSP(n) \
+    case n: ss_powers<n>(a, S, p0, lf > 0, lf, x0, ow, ya, yb, sm, ring); break;
+                        KOFM_SSP(1) KOFM_SSP(2) KOFM_SSP(3) KOFM_SSP(4) KOFM_SSP(5)
+                        KOFM_SSP(6) KOFM_SSP(7) KOFM_SSP(8) KOFM_SSP(9) KOFM_SSP(10)
+#undef KOFM_SSP
+                        default: break;
+                    }
+                }
+            }
+            if (!ss_sync(a, SS_SER_NONE, restart, round)) return;
+            // ---- Gram of p_0 .. p_lto ----------------------------------------------------
+            for (int s = 0; s < 2; ++s) {
+                double acc[SS_NG];
+                const int L = sm.lto[s];
+                const int ng = (L + 1) * (L + 2) / 2;
+                if (L > 0) {
+                    const KoSystem& S = a.sys[s];
+                    const double* p0 = restart == 0 ? S.rhs : ((restart & 1) ? S.r2 : S.r);
+                    // a fixed contiguous node range per block (deterministic sums)
+                    const long long n32 = a.D / 32;
+                    const long long g0 = n32 * blockIdx.x / gridDim.x * 32;
+                    const long long g1 = n32 * (blockIdx.x + 1) / gridDim.x * 32;
+                    switch (L) {
+#define KOFM_SSG(n) \
+    case n: ss_gram<n>(a, S, p0, g0, g1, acc); break;
+                        KOFM_SSG(1) KOFM_SSG(2) KOFM_SSG(3) KOFM_SSG(4) KOFM_SSG(5)
+                        KOFM_SSG(6) KOFM_SSG(7) KOFM_SSG(8) KOFM_SSG(9) KOFM_SSG(10)
+#undef KOFM_SSG
+                        default: break;
+                    }
+                }
+                ss_block_reduce(acc, L > 0 ? ng : 0, a.part, SS_NG * s, sm);
+            }
+            if (!ss_sync(a, SS_SER_GRAM, restart, round)) return;
+            if (!ldc(&ctl->any_ext)) break;
+        }
+        if (!ldc(&ctl->any_active)) break;
+        // ---- d = d_prev + sum c_j p_j (pointwise) -------------------------------------
+        if (threadIdx.x < 2) {
+            const int s = threadIdx.x;
+            sm.act[s] = ldc(&ctl->sys[s].active);
+            sm.kk[s] = ldc(&ctl->sys[s].kk);
+        }
+        if (threadIdx.x < 2 * (SS_MAXL + 1)) {
+            const int s = threadIdx.x / (SS_MAXL + 1), i = threadIdx.x % (SS_MAXL + 1);
+            sm.c[s][i] = i < a.K ? ldc(&ctl->sys[s].h[i]) : 0.0;
+        }
+        __syncthreads();
+        // restart n reads the residual and correction of parity n and writes
+        // those of parity n + 1 (restart 0: b' and d = 0)
+        for (int s = 0; s < 2; ++s) {
+            if (!sm.act[s]) continue;
+            const KoSystem& S = a.sys[s];
+            const double* p0 = restart == 0 ? S.rhs : ((restart & 1) ? S.r2 : S.r);
+            const double* xin = restart == 0 ? nullptr : ((restart & 1) ? S.x2 : S.x);
+            double* xout = (restart & 1) ? S.x : S.x2;
+            double cr[SS_MAXL];
+#pragma unroll
+            for (int j = 0; j < SS_MAXL; ++j) cr[j] = sm.c[s][j];
+            const int kk = sm.kk[s];
+            const long long npairs = a.D / 2;
+            // two node pairs per thread and iteration: their loads in flight together
+            for (long long pr = t0; pr < npairs; pr += 2 * stride) {
+                const long long pb = pr + stride < npairs ? pr + stride : pr;
+                const long long g[2] = {pr * 2, pb * 2};  // g, g + 1 share a 32-node group
+                double2 d[2], r[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    d[u] = xin ? __ldcg(reinterpret_cast<const double2*>(xin + g[u])) : make_double2(0.0, 0.0);
+                    r[u] = __ldcg(reinterpret_cast<const double2*>(p0 + g[u]));
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    d[u].x += cr[0] * r[u].x;
+                    d[u].y += cr[0] * r[u].y;
+                }
+#pragma unroll
+                for (int j = 1; j < SS_MAXL; ++j) {
+                    if (j >= kk) break;
+                    double2 p[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        p[u] = __ldcg(reinterpret_cast<const double2*>(
+                            S.V + (g[u] >> 5) * (a.K * 32) + (g[u] & 31) + (j - 1) * 32));
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        d[u].x += cr[j] * p[u].x;
+                        d[u].y += cr[j] * p[u].y;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) __stcg(reinterpret_cast<double2*>(xout + g[u]), d[u]);
+            }
+        }
+        if (!ss_sync(a, SS_SER_NONE, restart, 0)) return;
+        // ---- r = b' - A d, ||r||^2 -------------------------------------------------------
+        for (int s = 0; s < 2; ++s) {
+            double acc = 0.0;
+            if (sm.act[s]) {
+                const KoSystem& S = a.sys[s];
+                const double* xd = (restart & 1) ? S.x : S.x2;
+                double* rout = (restart & 1) ? S.r : S.r2;
+                const long long npairs = a.D / 2;
+                for (long long pr = t0; pr < npairs; pr += stride) {
+                    const long long g = pr * 2;
+                    const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+                    double rr[2] = {0.0, 0.0};
+                    const long long row = (long long)y * a.P;
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const int xj = x + j;
+                        if (xj >= a.nx) continue;
+                        const long long gj = g + j;
+                        const int xw = xj > 0 ? xj - 1 : a.nx - 1;
+                        const int xe = xj + 1 < a.nx ? xj + 1 : 0;
+                        const double* cf = S.coef + ilv(4, 0, gj);
+                        // rows 0 and ny-1 are solid: their off-diagonals are 0
+                        const double dS = y > 0 ? __ldcg(xd + gj - a.P) : 0.0;
+                        const double dN = y + 1 < a.ny ? __ldcg(xd + gj + a.P) : 0.0;
+                        // CSR order of an interior row: S, W, C, E, N
+                        const double Ad = __ldg(cf + 96) * dS + __ldg(cf + 32) * __ldcg(xd + row + xw) +
+                                          __ldcg(xd + gj) + __ldg(cf) * __ldcg(xd + row + xe) +
+                                          __ldg(cf + 64) * dN;
+                        rr[j] = __ldg(S.rhs + gj) - Ad;
+                    }
+                    __stcg(reinterpret_cast<double2*>(rout + g), make_double2(rr[0], rr[1]));
+                    acc += rr[0] * rr[0] + rr[1] * rr[1];
+                }
+            }
+            ss_block_reduce(&acc, sm.act[s] ? 1 : 0, a.part, SS_NG * s, sm);
+        }
+        if (!ss_sync(a, SS_SER_RESID, restart, 0)) return;
+        if (!ldc(&ctl->any_active)) break;
+    }
+
+    // ---- x_new = x0 + d on fluid nodes; solid-boundary rows -> 0 -----------------
+    // A solve that met a NaN residual leaves its field as it was.
+    const long long npairs = a.D / 2;
+    for (int s = 0; s < 2; ++s) {
+        const KoSystem& S = a.sys[s];
+        float* f = a.field[s];
+        // the correction of the last of `cycles` updates is in parity `cycles`
+        const int cyc = ldc(&ctl->sys[s].cycles);
+        const bool has_x = cyc > 0 && !ldc(&ctl->sys[s].nan);
+        const double* xf = (cyc & 1) ? S.x2 : S.x;
+        for (long long pr = t0; pr < npairs; pr += stride) {
+            const long long g = pr * 2;
+            const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+            if (x >= a.nx) continue;
+            const unsigned int t2 = *reinterpret_cast<const unsigned int*>(a.ntype + g);
+            const int tt[2] = {(int)(t2 & 0xffff), (int)(t2 >> 16)};
+            const double2 xv = has_x ? __ldcg(reinterpret_cast<const double2*>(xf + g)) : make_double2(0.0, 0.0);
+            const double dv[2] = {xv.x, xv.y};
+            for (int j = 0; j < 2; ++j) {
+                if (x + j >= a.nx) continue;
+                if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
+                else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+            }
+        }
+    }
+}
+
+}  // namespace kofm

@@ -219,6 +219,14 @@ class Lattice:
         mask (1: omega, 2: k), host-made (kofm_debug_fail_solves)."""
         check("kofm_debug_fail_solves", self.lib.kofm_debug_fail_solves(self._ctx, n, mask))
 
+    def solver_trace(self):
+        """Device times (ns from the launch's start) at which the last
+        k-omega solve's grid barriers released (kofm_debug_solver_trace)."""
+        buf = (C.c_int64 * 32)()
+        n = C.c_int32()
+        check("kofm_debug_solver_trace", self.lib.kofm_debug_solver_trace(self._ctx, buf, 32, C.byref(n)))
+        return [buf[i] for i in range(min(n.value, 32))]
+
     def komega_update_status(self) -> int:
         """kofm_komega_update's status without raising."""
         return self.lib.kofm_komega_update(self._ctx)
