@@ -99,33 +99,6 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def solver_bytes_per_node(stats, K):
-    """Algorithmic bytes per lattice node of one solver launch (both systems),
-    from the launch's own counts of the passes it made; every array is FP64.
-
-    * residual pass: restart 0 reads b' (8); a later restart forms
-      r = b' - A x from b', x, the four coefficients and stores r (56);
-    * Krylov vector k of a cycle: u_{k-1} (or r) and the older basis vectors
-      u_j (j < k-1), the four coefficients, r for <r, u_k>, and the store of
-      u_k: 48 + 8 k;
-    * cycle update: r, the kk - 1 basis vectors with a non-zero coefficient,
-      x (after the first cycle) and the store of x;
-    * write-back: x, the field (FP32 read + write) and the node flag.
-    Halo rows and columns re-read from L2 or shared memory are not counted."""
-    total = 0
-    for sysname in ("omega", "k"):
-        restarts = getattr(stats, sysname + "_restarts")
-        cycles = getattr(stats, sysname + "_cycles")
-        vecs = getattr(stats, sysname + "_vectors")
-        vsum = getattr(stats, sysname + "_vec_index_sum")
-        terms = getattr(stats, sysname + "_update_terms")
-        res = 8 + 56 * max(restarts - 1, 0)
-        kry = 48 * vecs + 8 * vsum
-        upd = 16 * cycles + 8 * max(terms - cycles, 0) + 8 * max(cycles - 1, 0)
-        total += res + kry + upd + 18
-    return total
-
-
 STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
                  "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)"}
 
@@ -176,11 +149,13 @@ def replica_value(nodes: int, steps: int, world: int, ms: float) -> float:
 
 
 # DRAM traffic over algorithmic bytes of one solver launch, from an ncu capture
-# of the 8192x512 case (profiles/gmres_kernel_komega_straight_8192x512.md):
-# 4.797 GB read + written for a launch of 1076 algorithmic B/node x 4,194,304
-# nodes.  Traffic grows with the nodes and the passes of a launch, so the
-# bench's traffic figure is this ratio times its average launch's bytes.
-GMRES_TRAFFIC_RATIO = 4.7967e9 / (1076 * 4194304)
+# of the 8192x512 case (profiles/<kernel>_komega_straight_8192x512.md); the
+# bench's traffic figure is this ratio times its average launch's algorithmic
+# bytes (traffic grows with the nodes and the sweeps of a launch).
+SOLVER_TRAFFIC_RATIO = {
+    "gmres_kernel": 4.7967e9 / (1076 * 4194304),   # one vector per sweep
+    "sstep_kernel": None,                          # one sweep per cycle's powers
+}
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
             "fp16neq": 114}                   # + reference moments read and written
@@ -205,6 +180,8 @@ def run_ours(args, rank, world, local_rank):
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
+    d.komega_classic = 1 if args.solver == "classic" else 0
+    solver_kernel = "gmres_kernel" if args.solver == "classic" else "sstep_kernel"
     d.use_thermal = 1 if args.thermal else 0
     L = Lattice(d)
     W.apply(L, w)
@@ -258,7 +235,7 @@ def run_ours(args, rank, world, local_rank):
         ev[i][3].record(stream)
         s = L.stats()
         passes.append(s.solver_passes)
-        bytes_solver.append(solver_bytes_per_node(s, d.krylov_dim))
+        bytes_solver.append(s.solver_bytes_per_node)
     torch.cuda.synchronize()
     t_lb = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(nb)) / nb
     t_as = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(nb)) / nb
@@ -287,15 +264,16 @@ def run_ours(args, rank, world, local_rank):
                            "gbs": LB_BYTES[args.storage] * nodes / (t_lb * 1e-3) / 1e9},
         "komega_assemble_kernel": {"ms": t_as, "bytes_per_node": ASM_BYTES,
                                    "gbs": ASM_BYTES * nodes / (t_as * 1e-3) / 1e9},
-        "gmres_kernel": {"ms": t_sv, "bytes_per_node": b_sv,
-                         "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
-                         "passes": sum(passes) / nb,
-                         "bytes_per_node_by_launch": bytes_solver},
+        solver_kernel: {"ms": t_sv, "bytes_per_node": b_sv,
+                        "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
+                        "passes": sum(passes) / nb,
+                        "bytes_per_node_by_launch": bytes_solver},
     }
     dom = max(kern, key=lambda k: kern[k]["ms"])
+    ratio = SOLVER_TRAFFIC_RATIO.get(dom)
     roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak,
             "unit": "GB/s", "frac": kern[dom]["gbs"] / peak, "peak_kind": peak_kind,
-            "traffic": (GMRES_TRAFFIC_RATIO * b_sv * nodes if dom == "gmres_kernel" else None),
+            "traffic": (ratio * kern[dom]["bytes_per_node"] * nodes if ratio else None),
             "traffic_source": "ncu dram bytes / algorithmic bytes of one launch on "
                               "komega_straight_8192x512, times this run's average launch",
             "bytes_per_node": kern[dom]["bytes_per_node"]}
@@ -347,12 +325,19 @@ def run_ours(args, rank, world, local_rank):
             "step_roofline": {"bytes_per_node": step_bytes,
                               "achieved": step_bytes * nodes / (step_ms * 1e-3) / 1e9,
                               "frac": step_bytes * nodes / (step_ms * 1e-3) / 1e9 / peak},
+            # the whole timed step against the compulsory per-step traffic of
+            # the FP32 k-omega form (130 B/node: populations, flags, k, omega,
+            # strain rates, wall distance, moments; no solver sweep credited)
+            "step_roofline_130": {"bytes_per_node": 130,
+                                  "achieved": 130 * nodes / (ms / args.steps * 1e-3) / 1e9,
+                                  "frac": 130 * nodes / (ms / args.steps * 1e-3) / 1e9 / peak},
             "kernels": kern,
             **({"thermal": thermal} if thermal else {}),
             "solver": {"omega_iters": st.omega_iters, "k_iters": st.k_iters,
                        "omega_restarts": st.omega_restarts, "k_restarts": st.k_restarts,
                        "omega_vectors": st.omega_vectors, "k_vectors": st.k_vectors,
-                       "passes": st.solver_passes},
+                       "omega_powers": st.omega_powers, "k_powers": st.k_powers,
+                       "passes": st.solver_passes, "form": args.solver},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
         }
@@ -451,6 +436,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq"])
+    ap.add_argument("--solver", default="sstep", choices=["sstep", "classic"],
+                    help="k-omega solve: a cycle's Krylov directions in one sweep (default) "
+                         "or one vector per sweep")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -162,6 +162,10 @@ typedef struct kofm_stats {
     int32_t thermal_time_since_change;  /* clVariablesFD::timeSinceTimeStepChange */
     double thermal_dt;                  /* clVariablesFD::timeStep */
     double thermal_residual;            /* last ||r||_1 / ||b||_1 */
+    double solver_bytes_per_node;       /* algorithmic HBM bytes per lattice node of the
+                                           last k-omega solve (both systems): every
+                                           array its sweeps stream, counted once per sweep */
+    int32_t omega_powers, k_powers;     /* one-sweep cycles: powers computed (all rounds) */
 } kofm_stats;
 
 int kofm_abi_version(void);

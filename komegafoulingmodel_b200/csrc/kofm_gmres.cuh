@@ -60,7 +60,10 @@ struct GmresSys {
     int inject;         // test hook: report a NaN residual at the first check
     int lev;            // one-sweep cycle: powers computed so far in this cycle
     int ext;            // one-sweep cycle: 1 = more powers needed before the cut
+    int powers;         // one-sweep cycle: powers computed (all rounds and cycles)
+    int pad2;
     double rho0, norm_rhs, rinv, rho, prev_err;
+    double abytes;      // one-sweep cycle: algorithmic bytes per node of the sweeps so far
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||
     double h[KOFM_MAX_KRYLOV];   // Gram-Schmidt coefficients for the next vector
     double xi[KOFM_MAX_KRYLOV];

@@ -217,6 +217,11 @@ __device__ void ss_serial(const SsArgs& a, int kind, int restart, int round, int
         if (S.active) {
             if (kind == SS_SER_GRAM && s_L[s] > 0) {
                 const int L = s_L[s];
+                // this round's powers (level 0 and coefficients in, levels
+                // lfrom+1 .. L out) and Gram (levels 0 .. L in), per node
+                const int lfrom = round == 0 ? 0 : S.lev;
+                S.abytes += 8.0 + 32.0 + 8.0 * (L - lfrom) + 8.0 * (L + 1);
+                S.powers += L - lfrom;
                 const double rho0 = sqrt(t[0]);
                 if (restart == 0 && round == 0) {
                     // the restart-0 test (GMRESSolver::solve's checkConvergence)
@@ -256,6 +261,10 @@ __device__ void ss_serial(const SsArgs& a, int kind, int restart, int round, int
                     }
                 }
             } else if (kind == SS_SER_RESID) {
+                // the update (p_0 .. p_{kk-1} and the previous correction in,
+                // the correction out) and the residual (correction, four
+                // coefficients and b' in, r out), per node
+                S.abytes += 8.0 * (S.kk > 1 ? S.kk : 1) + (restart > 0 ? 8.0 : 0.0) + 8.0 + 56.0;
                 // residual of the next restart (GMRESSolver.cpp:248-256)
                 const int next = restart + 1;
                 if (next < a.max_restarts) {
