@@ -100,7 +100,8 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------
 STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
-                 "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)"}
+                 "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)",
+                 "fp64": "fp64 f-w deviation, fp64 fields"}
 
 
 def workload_config(w, args, world: int) -> dict:
@@ -158,8 +159,10 @@ SOLVER_TRAFFIC_RATIO = {
 }
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
-            "fp16neq": 114}                   # + reference moments read and written
-ASM_BYTES = 122                                     # fused assembly, per node
+            "fp16neq": 114,                   # + reference moments read and written
+            "fp64": 250}                      # FP64 populations and fields
+ASM_BYTES = {"fp64": 162}                           # fused assembly, per node (FP64 fields)
+ASM_BYTES_FP32 = 122                                # ... FP32 fields
 
 
 def run_ours(args, rank, world, local_rank):
@@ -176,7 +179,8 @@ def run_ours(args, rank, world, local_rank):
     lib = _abi.load()
     torch.cuda.set_device(local_rank)
     storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV,
-               "fp16neq": _abi.STORE_FP16_NEQ}[args.storage]
+               "fp16neq": _abi.STORE_FP16_NEQ, "fp64": _abi.STORE_FP64}[args.storage]
+    asm_bytes = ASM_BYTES.get(args.storage, ASM_BYTES_FP32)
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
@@ -262,8 +266,8 @@ def run_ours(args, rank, world, local_rank):
     kern = {
         "lb_step_kernel": {"ms": t_lb, "bytes_per_node": LB_BYTES[args.storage],
                            "gbs": LB_BYTES[args.storage] * nodes / (t_lb * 1e-3) / 1e9},
-        "komega_assemble_kernel": {"ms": t_as, "bytes_per_node": ASM_BYTES,
-                                   "gbs": ASM_BYTES * nodes / (t_as * 1e-3) / 1e9},
+        "komega_assemble_kernel": {"ms": t_as, "bytes_per_node": asm_bytes,
+                                   "gbs": asm_bytes * nodes / (t_as * 1e-3) / 1e9},
         solver_kernel: {"ms": t_sv, "bytes_per_node": b_sv,
                         "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
                         "passes": sum(passes) / nb,
@@ -277,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
             "traffic_source": "ncu dram bytes / algorithmic bytes of one launch on "
                               "komega_straight_8192x512, times this run's average launch",
             "bytes_per_node": kern[dom]["bytes_per_node"]}
-    step_bytes = LB_BYTES[args.storage] + ASM_BYTES + b_sv
+    step_bytes = LB_BYTES[args.storage] + asm_bytes + b_sv
     step_ms = t_lb + t_as + t_sv
 
     # ---- end to end through the public API with host buffers ---------------------
@@ -319,7 +323,7 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.storage == "fp32" else "f32", "data": "synthetic",
+            "dtype": "f64" if args.storage in ("fp32", "fp64") else "f32", "data": "synthetic",
             "config": workload_config(w, args, world),
             "roofline": roof,
             "step_roofline": {"bytes_per_node": step_bytes,
@@ -435,7 +439,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq"])
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp64"])
     ap.add_argument("--solver", default="sstep", choices=["sstep", "classic"],
                     help="k-omega solve: a cycle's Krylov directions in one sweep (default) "
                          "or one vector per sweep")

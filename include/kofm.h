@@ -67,6 +67,13 @@ extern "C" {
                                  with the writer's FP32 rho, u as reference;
                                  FP64 collide arithmetic.  No counterpart in
                                  the reference (its arrays are FP64). */
+#define KOFM_STORE_FP64 4     /* f_i - w_i in FP64 and every node field (k,
+                                 omega, nu_t, strain rates, wall distance,
+                                 moments) in FP64, FP64 arithmetic throughout:
+                                 the reference's precision (Heading.cl:7,
+                                 FTYPE double), the truth of the precision
+                                 study.  Not with the thermal update, the
+                                 device geometry builder or the adjoint. */
 
 /* ---- fields for kofm_reduce ---------------------------------------------- */
 #define KOFM_FIELD_RHO 0   /* Ro_array   (clVariablesLB.cpp:343-345 sumRo) */

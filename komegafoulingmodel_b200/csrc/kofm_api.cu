@@ -78,14 +78,17 @@ struct kofm_ctx {
     std::vector<std::pair<long long, int>> ibb_links;  // input order: (device node, direction)
     int32_t* dxrec_idx = nullptr;     // per-node dX record index
     DxRecord* dxrec = nullptr;
-    float* wallD = nullptr;
-    float* K = nullptr;
-    float* O = nullptr;
-    float* S = nullptr;
-    float* nut = nullptr;
-    float* rho = nullptr;
-    float* ux = nullptr;
-    float* uy = nullptr;
+    // node fields: FP32, or FP64 in the FP64 storage form (f64; fbytes = 8)
+    bool f64 = false;
+    size_t fbytes = 4;
+    void* wallD = nullptr;
+    void* K = nullptr;
+    void* O = nullptr;
+    void* S = nullptr;                // 3 planes
+    void* nut = nullptr;
+    void* rho = nullptr;
+    void* ux = nullptr;
+    void* uy = nullptr;
     double* lb_partials = nullptr;
     long long n_lb_partials = 0;
     double* red_partials = nullptr;   // RED_BLOCKS
@@ -316,13 +319,13 @@ __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ n
 // f_neq = FA - feq(rho, u) of the node's populations 1..8 (rho, u the moments
 // the last step wrote), tau = |(f_neq . cx_row, f_neq . cy_row)| (nu + nu_t)
 // / (3 (nu + nu_t) + 1/2) / rho, with the sign of its x component.
-template <typename ST>
+template <typename ST, typename FT = float>
 __global__ void k_shear_nodes(const ST* __restrict__ g, const int16_t* __restrict__ nt,
                               const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
                               int has_ibb, int nx, int ny, int P, long long D, int phase,
-                              const float* __restrict__ ref, const float* __restrict__ rho,
-                              const float* __restrict__ ux, const float* __restrict__ uy,
-                              const float* __restrict__ nut, double mu, const int32_t* __restrict__ nodes,
+                              const float* __restrict__ ref, const FT* __restrict__ rho,
+                              const FT* __restrict__ ux, const FT* __restrict__ uy,
+                              const FT* __restrict__ nut, double mu, const int32_t* __restrict__ nodes,
                               const double* __restrict__ cfss, int n, int nxf, double* __restrict__ tau) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -362,15 +365,17 @@ __global__ void k_shear_links(const double* __restrict__ tau_nodes, const int32_
     out[b] = acc;
 }
 
-// FP64 host-layout scalar field <-> FP32 device field
-__global__ void k_field_in(const double* __restrict__ h, float* __restrict__ dv, int nxf,
+// FP64 host-layout scalar field <-> device field (FP32, or FP64 in the FP64 form)
+template <typename FT>
+__global__ void k_field_in(const double* __restrict__ h, FT* __restrict__ dv, int nxf,
                            int ny, int P) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= P) return;
-    dv[(long long)y * P + x] = x < nxf ? (float)h[(long long)y * nxf + x] : 0.f;
+    dv[(long long)y * P + x] = x < nxf ? (FT)h[(long long)y * nxf + x] : FT(0);
 }
-__global__ void k_field_out(const float* __restrict__ dv, double* __restrict__ h, int nxf,
+template <typename FT>
+__global__ void k_field_out(const FT* __restrict__ dv, double* __restrict__ h, int nxf,
                             int ny, int P) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -422,8 +427,9 @@ __global__ void k_reduce_final(const double* __restrict__ part, int n, double* _
 
 // wall-shear integrand: rho (mu + nu_t) 2 |Sxy| on fluid nodes with an N or S
 // wall link, summed per block.
-__global__ void k_wall_shear(const int16_t* __restrict__ nt, const float* __restrict__ rho,
-                             const float* __restrict__ nut, const float* __restrict__ S,
+template <typename FT>
+__global__ void k_wall_shear(const int16_t* __restrict__ nt, const FT* __restrict__ rho,
+                             const FT* __restrict__ nut, const FT* __restrict__ S,
                              long long nnodes, long long D, int P, int nx, double mu,
                              double* __restrict__ part) {
     __shared__ double sh[32];
@@ -446,16 +452,16 @@ __global__ void k_wall_shear(const int16_t* __restrict__ nt, const float* __rest
 }
 
 // ---- LB step dispatch ------------------------------------------------------------
-template <typename ST, typename AT, bool NEQ = false>
+template <typename ST, typename AT, bool NEQ = false, typename FT = float>
 cudaError_t launch_lb(kofm_ctx* c, const LbParams& p, bool komega, bool phase0) {
     dim3 block(32, 4);
     dim3 grid(c->P / 128, (c->desc.ny + 3) / 4);
     if (komega) {
-        if (phase0) lb_step_kernel<ST, AT, true, true, NEQ><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, true, false, NEQ><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, true, true, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, true, false, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
     } else {
-        if (phase0) lb_step_kernel<ST, AT, false, true, NEQ><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, false, false, NEQ><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, false, true, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, false, false, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
     }
     return cudaGetLastError();
 }
@@ -464,7 +470,9 @@ int validate_desc(const kofm_desc* d) {
     if (!d) return KOFM_ERR_INVALID_ARG;
     if (d->nx < 4 || d->ny < 3 || d->nx_full < d->nx) return KOFM_ERR_LOADING_PARAMS;
     if ((long long)d->nx_full * d->ny > (1LL << 31) - 1) return KOFM_ERR_LOADING_PARAMS;
-    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP16_NEQ) return KOFM_ERR_LOADING_PARAMS;
+    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP64) return KOFM_ERR_LOADING_PARAMS;
+    // the FP64 form is the precision study's reference form: no thermal update
+    if (d->storage == KOFM_STORE_FP64 && d->use_thermal) return KOFM_ERR_LOADING_PARAMS;
     if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
@@ -577,7 +585,9 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
     c->num_sms = prop.multiProcessorCount;
     c->P = ((d->nx_full + 127) / 128) * 128;
     c->D = (long long)c->P * d->ny;
-    c->store_bytes = d->storage == KOFM_STORE_FP32 ? 4 : 2;
+    c->store_bytes = d->storage == KOFM_STORE_FP64 ? 8 : (d->storage == KOFM_STORE_FP32 ? 4 : 2);
+    c->f64 = d->storage == KOFM_STORE_FP64;
+    c->fbytes = c->f64 ? 8 : 4;
     c->dt = d->komega_dt;
     c->steps_per_lb = (int)(1.0 / d->komega_dt);
     if (c->steps_per_lb < 1) c->steps_per_lb = 1;
@@ -600,22 +610,27 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         ALLOC(c->ref[0], 3 * D);
         ALLOC(c->ref[1], 3 * D);
     }
+#define ALLOC_FIELD(ptr, n)                                         \
+    do {                                                            \
+        int _s = dalloc(&(ptr), (size_t)(n) * c->fbytes);           \
+        if (_s) { kofm_destroy(c); return _s; }                     \
+    } while (0)
     ALLOC(c->ntype, D);
     ALLOC(c->rec, D);
     ALLOC(c->dxrec_idx, D);
-    ALLOC(c->rho, D);
-    ALLOC(c->ux, D);
-    ALLOC(c->uy, D);
+    ALLOC_FIELD(c->rho, D);
+    ALLOC_FIELD(c->ux, D);
+    ALLOC_FIELD(c->uy, D);
     c->n_lb_partials = (long long)(c->P / 128) * ((d->ny + 3) / 4) * 4 * 3;
     ALLOC(c->lb_partials, c->n_lb_partials);
     ALLOC(c->red_partials, RED_BLOCKS);
     ALLOC(c->red_out, 8);
     if (d->use_komega) {
-        ALLOC(c->wallD, D);
-        ALLOC(c->K, D);
-        ALLOC(c->O, D);
-        ALLOC(c->S, 3 * D);
-        ALLOC(c->nut, D);
+        ALLOC_FIELD(c->wallD, D);
+        ALLOC_FIELD(c->K, D);
+        ALLOC_FIELD(c->O, D);
+        ALLOC_FIELD(c->S, 3 * D);
+        ALLOC_FIELD(c->nut, D);
         int s2 = ko_solver_alloc(c->sys, &c->ctl, &c->gpart, &c->bar, &c->solver_blocks,
                                  c->P, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
         if (s2) { kofm_destroy(c); return s2; }
@@ -644,6 +659,7 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         cudaMemset(c->dxrec0_idx, 0xff, D * sizeof(int32_t));
     }
 #undef ALLOC
+#undef ALLOC_FIELD
     if (cudaMallocHost(&c->h_red, 64 * sizeof(double)) != cudaSuccess) {
         kofm_destroy(c);
         return KOFM_ERR_BUFFER_ALLOCATION;
@@ -702,14 +718,14 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     // FD link-fraction records for nodes whose dX differs from 1
     std::vector<int32_t> dxi((size_t)c->D, -1);
     std::vector<DxRecord> dxr;
-    std::vector<float> wd;
+    std::vector<double> wd;   // FP64 wall distance, stored in the fields' type
     if (d.use_komega || d.use_thermal) {
-        if (d.use_komega) wd.assign((size_t)c->D, 0.f);
+        if (d.use_komega) wd.assign((size_t)c->D, 0.0);
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
                 const long long h = (long long)y * nxf + x;
                 const size_t node = (size_t)y * P + x;
-                if (d.use_komega) wd[node] = (float)wallD[h];
+                if (d.use_komega) wd[node] = wallD[h];
                 // records for the LB-fluid nodes (k-omega rows) and, with the
                 // thermal update, for the fouling-layer nodes of its rows
                 const int tt = (uint16_t)ntype[h];
@@ -754,27 +770,43 @@ int kofm_set_geometry(kofm_ctx* c, const int16_t* ntype, const double* wallD,
     if (cudaMemcpy(c->ntype, nt.data(), nt.size() * sizeof(int16_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     if (cudaMemcpy(c->rec, rec.data(), rec.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
     if (cudaMemcpy(c->dxrec_idx, dxi.data(), dxi.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
-    if (d.use_komega)
-        if (cudaMemcpy(c->wallD, wd.data(), wd.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
+    if (d.use_komega) {
+        cudaError_t e;
+        if (c->f64) {
+            e = cudaMemcpy(c->wallD, wd.data(), wd.size() * sizeof(double), cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> wf(wd.size());
+            for (size_t i = 0; i < wd.size(); ++i) wf[i] = (float)wd[i];
+            e = cudaMemcpy(c->wallD, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return fail(KOFM_ERR_MEMORY_COPY);
+    }
     c->have_geometry = true;
     return KOFM_OK;
 }
 
-static int upload_field(kofm_ctx* c, const double* h, float* dv) {
+// Plane `plane` of a device field (of the context's field type).
+static inline void* field_plane(kofm_ctx* c, void* f, int plane) {
+    return static_cast<char*>(f) + (size_t)plane * c->D * c->fbytes;
+}
+
+static int upload_field(kofm_ctx* c, const double* h, void* dv) {
     const kofm_desc& d = c->desc;
     const size_t n = (size_t)d.nx_full * d.ny;
     KOFM_CUDA_TRY(cudaMemcpyAsync(c->staging, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream), KOFM_ERR_MEMORY_COPY);
     dim3 grid((c->P + 255) / 256, d.ny);
-    k_field_in<<<grid, 256, 0, c->stream>>>(c->staging, dv, d.nx_full, d.ny, c->P);
+    if (c->f64) k_field_in<double><<<grid, 256, 0, c->stream>>>(c->staging, (double*)dv, d.nx_full, d.ny, c->P);
+    else k_field_in<float><<<grid, 256, 0, c->stream>>>(c->staging, (float*)dv, d.nx_full, d.ny, c->P);
     KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
     return KOFM_OK;
 }
 
-static int download_field(kofm_ctx* c, const float* dv, double* h) {
+static int download_field(kofm_ctx* c, const void* dv, double* h) {
     const kofm_desc& d = c->desc;
     const size_t n = (size_t)d.nx_full * d.ny;
     dim3 grid((d.nx_full + 255) / 256, d.ny);
-    k_field_out<<<grid, 256, 0, c->stream>>>(dv, c->staging, d.nx_full, d.ny, c->P);
+    if (c->f64) k_field_out<double><<<grid, 256, 0, c->stream>>>((const double*)dv, c->staging, d.nx_full, d.ny, c->P);
+    else k_field_out<float><<<grid, 256, 0, c->stream>>>((const float*)dv, c->staging, d.nx_full, d.ny, c->P);
     KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
     KOFM_CUDA_TRY(cudaMemcpyAsync(h, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
     KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_MEMORY_COPY);
@@ -804,6 +836,9 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
         case KOFM_STORE_FP16_NEQ:
             k_fa_in_neq<<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ref[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
+        case KOFM_STORE_FP64:
+            k_fa_in<double><<<grid, 128, 0, c->stream>>>(c->staging, (double*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+            break;
         default:
             k_fa_in<__nv_bfloat16><<<grid, 128, 0, c->stream>>>(c->staging, (__nv_bfloat16*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
     }
@@ -815,7 +850,7 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
             if ((st = upload_field(c, nut, c->nut))) return st;
         }
         for (int s = 0; s < 3; ++s)
-            if ((st = upload_field(c, sxy + s * Dh, c->S + s * c->D))) return st;
+            if ((st = upload_field(c, sxy + s * Dh, field_plane(c, c->S, s)))) return st;
     }
     KOFM_CUDA_TRY(cudaStreamSynchronize(c->stream), KOFM_ERR_MEMORY_COPY);
     c->phase = 0;
@@ -850,6 +885,9 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
             case KOFM_STORE_FP16_NEQ:
                 k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, c->ref[c->cur]);
                 break;
+            case KOFM_STORE_FP64:
+                k_fa_out<double><<<grid, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                break;
             default:
                 k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
         }
@@ -863,7 +901,7 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
         if (nut && (st = download_field(c, c->nut, nut))) return st;
         if (sxy)
             for (int s = 0; s < 3; ++s)
-                if ((st = download_field(c, c->S + s * c->D, sxy + s * Dh))) return st;
+                if ((st = download_field(c, field_plane(c, c->S, s), sxy + s * Dh))) return st;
     }
     return KOFM_OK;
 }
@@ -927,15 +965,22 @@ int kofm_wall_shear(kofm_ctx* c, double* node_tau, double* bl_tau) {
     const int has_ibb = c->n_ibb_rec > 0;
     const float* ref = d.storage == KOFM_STORE_FP16_NEQ ? c->ref[c->cur] : nullptr;
     const int nb = (n + 127) / 128;
+    const float* frho = (const float*)c->rho;
+    const float* fux = (const float*)c->ux;
+    const float* fuy = (const float*)c->uy;
+    const float* fnut = (const float*)c->nut;
     switch (d.storage) {
         case KOFM_STORE_FP32:
-            k_shear_nodes<float><<<nb, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<float><<<nb, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
             break;
         case KOFM_STORE_BF16_DEV:
-            k_shear_nodes<__nv_bfloat16><<<nb, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<__nv_bfloat16><<<nb, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            break;
+        case KOFM_STORE_FP64:
+            k_shear_nodes<double, double><<<nb, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, (const double*)c->rho, (const double*)c->ux, (const double*)c->uy, (const double*)c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
             break;
         default:  // FP16 forms
-            k_shear_nodes<__half><<<nb, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, ref, c->rho, c->ux, c->uy, c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<__half><<<nb, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, ref, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
     }
     KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
     if (c->shear_nbl > 0) {
@@ -988,6 +1033,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
         case KOFM_STORE_FP32: e = launch_lb<float, double>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_DEV: e = launch_lb<__half, float>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, double, true>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP64: e = launch_lb<double, double, false, double>(c, p, ko, ph0); break;
         default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
     }
     if (e != cudaSuccess) {
@@ -1004,7 +1050,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
 int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
     if (!c || !out) return KOFM_ERR_INVALID_ARG;
     const kofm_desc& d = c->desc;
-    const float* v = nullptr;
+    const void* v = nullptr;
     switch (field) {
         case KOFM_FIELD_RHO: v = c->rho; break;
         case KOFM_FIELD_UX: v = c->ux; break;
@@ -1023,7 +1069,10 @@ int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
     const long long n = c->D;
     if (field == KOFM_FIELD_WALL_SHEAR) {
         if (!d.use_komega || op != KOFM_OP_SUM) return KOFM_ERR_INVALID_ARG;
-        k_wall_shear<<<RED_BLOCKS, 256, 0, c->stream>>>(c->ntype, c->rho, c->nut, c->S, n, c->D, c->P, d.nx, d.mu, c->red_partials);
+        if (c->f64)
+            k_wall_shear<double><<<RED_BLOCKS, 256, 0, c->stream>>>(c->ntype, (const double*)c->rho, (const double*)c->nut, (const double*)c->S, n, c->D, c->P, d.nx, d.mu, c->red_partials);
+        else
+            k_wall_shear<float><<<RED_BLOCKS, 256, 0, c->stream>>>(c->ntype, (const float*)c->rho, (const float*)c->nut, (const float*)c->S, n, c->D, c->P, d.nx, d.mu, c->red_partials);
         k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     } else if (field == KOFM_FIELD_TEMP) {
         if (op == KOFM_OP_SUM) k_reduce_field<KOFM_OP_SUM, double><<<RED_BLOCKS, 256, 0, c->stream>>>(c->T, n, c->P, d.nx_full, c->red_partials);
@@ -1032,14 +1081,22 @@ int kofm_reduce(kofm_ctx* c, int32_t field, int32_t op, double* out) {
         if (op == KOFM_OP_SUM) k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
         else if (op == KOFM_OP_MIN) k_reduce_final<KOFM_OP_MIN><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
         else k_reduce_final<KOFM_OP_MAX><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+    } else if (c->f64) {
+        const double* fv = (const double*)v;
+        if (op == KOFM_OP_SUM) k_reduce_field<KOFM_OP_SUM, double><<<RED_BLOCKS, 256, 0, c->stream>>>(fv, n, c->P, d.nx_full, c->red_partials);
+        else if (op == KOFM_OP_MIN) k_reduce_field<KOFM_OP_MIN, double><<<RED_BLOCKS, 256, 0, c->stream>>>(fv, n, c->P, d.nx_full, c->red_partials);
+        else k_reduce_field<KOFM_OP_MAX, double><<<RED_BLOCKS, 256, 0, c->stream>>>(fv, n, c->P, d.nx_full, c->red_partials);
+        if (op == KOFM_OP_SUM) k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+        else if (op == KOFM_OP_MIN) k_reduce_final<KOFM_OP_MIN><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
+        else k_reduce_final<KOFM_OP_MAX><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     } else if (op == KOFM_OP_SUM) {
-        k_reduce_field<KOFM_OP_SUM><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_field<KOFM_OP_SUM><<<RED_BLOCKS, 256, 0, c->stream>>>((const float*)v, n, c->P, d.nx_full, c->red_partials);
         k_reduce_final<KOFM_OP_SUM><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     } else if (op == KOFM_OP_MIN) {
-        k_reduce_field<KOFM_OP_MIN><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_field<KOFM_OP_MIN><<<RED_BLOCKS, 256, 0, c->stream>>>((const float*)v, n, c->P, d.nx_full, c->red_partials);
         k_reduce_final<KOFM_OP_MIN><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     } else {
-        k_reduce_field<KOFM_OP_MAX><<<RED_BLOCKS, 256, 0, c->stream>>>(v, n, c->P, d.nx_full, c->red_partials);
+        k_reduce_field<KOFM_OP_MAX><<<RED_BLOCKS, 256, 0, c->stream>>>((const float*)v, n, c->P, d.nx_full, c->red_partials);
         k_reduce_final<KOFM_OP_MAX><<<1, 32, 0, c->stream>>>(c->red_partials, RED_BLOCKS, c->red_out);
     }
     KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);

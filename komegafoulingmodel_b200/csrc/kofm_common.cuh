@@ -56,7 +56,25 @@ constexpr double KO_GAMMA1 = 5.0 / 9.0, KO_GAMMA2 = 0.44;
 
 // ---- storage conversions ------------------------------------------------
 template <typename ST> struct Store;
+// vt: the type a population is loaded into and stored from (FP32 for the
+// 32- and 16-bit forms, FP64 for the FP64 form)
+template <> struct Store<double> {
+    using vt = double;
+    __device__ static double to_f32(double v) { return v; }
+    __device__ static double to_f64(double v) { return v; }
+    __device__ static double from_f64(double v) { return v; }
+    __device__ static void load4(const double* p, double o[4]) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+    __device__ static void store4(double* p, const double v[4]) {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+};
 template <> struct Store<float> {
+    using vt = float;
     using vec4 = float4;
     __device__ static float to_f32(float v) { return v; }
     __device__ static float from_f32(float v) { return v; }
@@ -71,6 +89,7 @@ template <> struct Store<float> {
     }
 };
 template <> struct Store<__half> {
+    using vt = float;
     __device__ static float to_f32(__half v) { return __half2float(v); }
     __device__ static double to_f64(__half v) { return (double)__half2float(v); }
     __device__ static __half from_f32(float v) { return __float2half_rn(v); }
@@ -92,6 +111,7 @@ template <> struct Store<__half> {
     }
 };
 template <> struct Store<__nv_bfloat16> {
+    using vt = float;
     __device__ static float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ static double to_f64(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
     __device__ static __nv_bfloat16 from_f32(float v) { return __float2bfloat16_rn(v); }
@@ -112,6 +132,33 @@ template <> struct Store<__nv_bfloat16> {
         *reinterpret_cast<uint2*>(p) = raw;
     }
 };
+
+// ---- 4 consecutive field values (16-byte aligned FP32, 32-byte FP64) ---------
+__device__ __forceinline__ void fld_ld4(const float* p, float o[4]) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void fld_ld4(const double* p, double o[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void fld_ldg4(const float* p, float o[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void fld_ldg4(const double* p, double o[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void fld_st4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void fld_st4(double* p, const double v[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
 
 // ---- non-equilibrium storage form (KOFM_STORE_FP16_NEQ) ----------------------
 // A stored population is e_q = f_q - feq_q(rho_r, u_r): its distance from the

@@ -104,7 +104,8 @@ struct GridBarrier {
 
 struct GmresArgs {
     KoSystem sys[2];
-    float* field[2];          // omega, k (FP32 fields, updated in place)
+    void* field[2];           // omega, k (updated in place): FP32, or FP64 when f64
+    int f64;
     const int16_t* ntype;
     GmresControl* ctl;
     double* part;             // [GM_SLOTS][gridDim.x] (slot-major)
@@ -752,7 +753,8 @@ gmres_kernel(const GmresArgs a) {
     // GMRESSolver.cpp:350-353, and its copyFromPrevSolution restores nothing).
     for (int s = 0; s < 2; ++s) {
         const KoSystem& S = a.sys[s];
-        float* f = a.field[s];
+        float* f = static_cast<float*>(a.field[s]);
+        double* f8 = static_cast<double*>(a.field[s]);
         const bool has_x = ldc(&ctl->sys[s].cycles) > 0 && !ldc(&ctl->sys[s].nan);
         for (long long pr = t0; pr < npairs; pr += stride) {
             const long long g = pr * 2;
@@ -764,8 +766,13 @@ gmres_kernel(const GmresArgs a) {
             const double dv[2] = {xv.x, xv.y};
             for (int j = 0; j < 2; ++j) {
                 if (x + j >= a.nx) continue;
-                if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
-                else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+                if (a.f64) {
+                    if (!(tt[j] & M_SOLID)) f8[g + j] = f8[g + j] + dv[j];
+                    else if (tt[j] & SOLID_BOUNDARY) f8[g + j] = 0.0;
+                } else {
+                    if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
+                    else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+                }
             }
         }
     }

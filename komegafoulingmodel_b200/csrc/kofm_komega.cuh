@@ -55,14 +55,15 @@ struct AsmParams {
     const int16_t* ntype;
     const int32_t* dxidx;
     const DxRecord* dxrec;
-    const float* wallD;
-    const float* K;
-    const float* O;
-    const float* nut;
-    const float* rho;
-    const float* ux;
-    const float* uy;
-    const float* S;
+    // node fields: FP32, or FP64 for the FP64 storage form (the kernel's FT)
+    const void* wallD;
+    const void* K;
+    const void* O;
+    const void* nut;
+    const void* rho;
+    const void* ux;
+    const void* uy;
+    const void* S;
     double* coef_o;
     double* rhs_o;
     double* coef_k;
@@ -140,14 +141,16 @@ constexpr int KO_THREADS = 352;  // 11 warps >= KO_RX * KO_RY
 constexpr int KO_HX = KO_TX + 4, KO_HY = KO_TY + 4;  // 2-ring halo
 constexpr int KO_NF = 8;  // node fields: wallD, rho, nut, ux, uy, Sxx, Sxy, Syy
 
+template <typename FT>
 struct AsmStage {
-    float K[KO_HY][KO_HX];
-    float O[KO_HY][KO_HX];
-    float fld[KO_NF][KO_THREADS];
+    FT K[KO_HY][KO_HX];
+    FT O[KO_HY][KO_HX];
+    FT fld[KO_NF][KO_THREADS];
 };
 
+template <typename FT>
 struct AsmSmem {
-    AsmStage st[2];
+    AsmStage<FT> st[2];
     double Dk[KO_RY][KO_RX];
     double Do[KO_RY][KO_RX];
 };
@@ -155,6 +158,10 @@ struct AsmSmem {
 __device__ __forceinline__ void ko_cp4(float* smem, const float* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void ko_cp4(double* smem, const double* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
 // Geometry of this thread's ring node in tile (x0, y0).
@@ -179,35 +186,62 @@ __device__ __forceinline__ KoNode ko_node(const AsmParams& p, int tid, int x0, i
 }
 
 // Issue the copies of tile (x0, y0) into stage S; returns the node flag.
-__device__ __forceinline__ int ko_issue(const AsmParams& p, int tid, int x0, int y0, AsmStage& S) {
+template <typename FT>
+__device__ __forceinline__ int ko_issue(const AsmParams& p, int tid, int x0, int y0, AsmStage<FT>& S) {
+    const FT* pK = static_cast<const FT*>(p.K);
+    const FT* pO = static_cast<const FT*>(p.O);
     for (int i = tid; i < KO_HX * KO_HY; i += KO_THREADS) {
         const int sy = i / KO_HX, sx = i % KO_HX;
         const int hx = wrapx(x0 - 2 + sx, p.nx);
         int hy = y0 - 2 + sy;
         hy = hy < 0 ? 0 : (hy >= p.ny ? p.ny - 1 : hy);
         const long long h = (long long)hy * p.P + hx;
-        ko_cp4(&S.K[sy][sx], p.K + h);
-        ko_cp4(&S.O[sy][sx], p.O + h);
+        ko_cp4(&S.K[sy][sx], pK + h);
+        ko_cp4(&S.O[sy][sx], pO + h);
     }
     const KoNode n = ko_node(p, tid, x0, y0);
     if (!n.inrow) return M_SOLID;
     const long long g = n.g, D = p.D;
-    ko_cp4(&S.fld[0][tid], p.wallD + g);
-    ko_cp4(&S.fld[1][tid], p.rho + g);
-    ko_cp4(&S.fld[2][tid], p.nut + g);
+    ko_cp4(&S.fld[0][tid], static_cast<const FT*>(p.wallD) + g);
+    ko_cp4(&S.fld[1][tid], static_cast<const FT*>(p.rho) + g);
+    ko_cp4(&S.fld[2][tid], static_cast<const FT*>(p.nut) + g);
     if (n.interior) {
-        ko_cp4(&S.fld[3][tid], p.ux + g);
-        ko_cp4(&S.fld[4][tid], p.uy + g);
-        ko_cp4(&S.fld[5][tid], p.S + g);
-        ko_cp4(&S.fld[6][tid], p.S + D + g);
-        ko_cp4(&S.fld[7][tid], p.S + 2 * D + g);
+        const FT* pS = static_cast<const FT*>(p.S);
+        ko_cp4(&S.fld[3][tid], static_cast<const FT*>(p.ux) + g);
+        ko_cp4(&S.fld[4][tid], static_cast<const FT*>(p.uy) + g);
+        ko_cp4(&S.fld[5][tid], pS + g);
+        ko_cp4(&S.fld[6][tid], pS + D + g);
+        ko_cp4(&S.fld[7][tid], pS + 2 * D + g);
     }
     return (uint16_t)__ldg(p.ntype + g);
 }
 
+// Blending function F1 (kOmegaKernels.cl:68-87).  With FP32 fields in FP32:
+// its inputs k, omega, rho, y are FP32 fields; F1 in [0, 1] enters D_k, D_w
+// with an error ~1e-7, the size of the FP32 rounding of nu_t beside it.  With
+// FP64 fields in FP64.
+__device__ __forceinline__ double ko_f1(float, double kv, double om, double yv, double rho, double cdx,
+                                        double mu) {
+    const float CDkw = fmaxf((float)(rho * cdx), 1.0e-10f);
+    const float kf = (float)kv, of = (float)om, yf = (float)yv;
+    float a = fmaxf(sqrtf(kf) / ((float)KO_BETA_STAR * of * yf), 500.f * (float)mu / (yf * yf * of));
+    a = fminf(a, 4.f * kf * (float)KO_SIGMA_O2 / (CDkw * yf * yf));
+    const float a2 = a * a;
+    return (double)tanhf(a2 * a2);
+}
+__device__ __forceinline__ double ko_f1(double, double kv, double om, double yv, double rho, double cdx,
+                                        double mu) {
+    const double CDkw = fmax(rho * cdx, 1.0e-10);
+    double a = fmax(sqrt(kv) / (KO_BETA_STAR * om * yv), 500. * mu / (yv * yv * om));
+    a = fmin(a, 4. * kv * KO_SIGMA_O2 / (CDkw * yv * yv));
+    const double a2 = a * a;
+    return tanh(a2 * a2);
+}
+
 // Phases 2 and 3 of one tile from stage S (all of S visible to the block).
+template <typename FT>
 __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int y0, int t,
-                                        const AsmStage& S, AsmSmem& M) {
+                                        const AsmStage<FT>& S, AsmSmem<FT>& M) {
     const KoNode n = ko_node(p, tid, x0, y0);
     const int rx = n.rx, ry = n.ry;
     const long long g = n.g;
@@ -233,15 +267,7 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
         const double m = 2. * KO_SIGMA_O2 / om;
         mxv = m * dKdx;
         myv = m * dKdy;
-        // blending function F1 (kOmegaKernels.cl:68-87) in FP32: its inputs k,
-        // omega, rho, y are FP32 fields; F1 in [0, 1] enters D_k, D_w with an
-        // error ~1e-7, the size of the FP32 rounding of nu_t beside it
-        const float CDkw = fmaxf((float)(rho * (mxv * dOdx + myv * dOdy)), 1.0e-10f);
-        const float kf = (float)kv, of = (float)om, yf = (float)yv;
-        float a = fmaxf(sqrtf(kf) / ((float)KO_BETA_STAR * of * yf), 500.f * (float)p.mu / (yf * yf * of));
-        a = fminf(a, 4.f * kf * (float)KO_SIGMA_O2 / (CDkw * yf * yf));
-        const float a2 = a * a;
-        F1 = (double)tanhf(a2 * a2);
+        F1 = ko_f1(FT(0), kv, om, yv, rho, mxv * dOdx + myv * dOdy, p.mu);
         Dk = p.mu + (KO_SIGMA_K1 * F1 + KO_SIGMA_K2 * (1. - F1)) * nt;
         Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
     }
@@ -319,10 +345,11 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
 #ifndef KOFM_ASM_MINBLOCKS
 #define KOFM_ASM_MINBLOCKS 2  // resident blocks per SM (registers and the persistent grid)
 #endif
+template <typename FT = float>
 __global__ void __launch_bounds__(KO_THREADS, KOFM_ASM_MINBLOCKS)
 komega_assemble_kernel(const AsmParams p) {
     extern __shared__ __align__(16) unsigned char ko_smem[];
-    AsmSmem& M = *reinterpret_cast<AsmSmem*>(ko_smem);
+    AsmSmem<FT>& M = *reinterpret_cast<AsmSmem<FT>*>(ko_smem);
     const int tid = threadIdx.x;
     const int tiles_x = (p.nx + KO_TX - 1) / KO_TX;
     const int ntiles = tiles_x * ((p.ny + KO_TY - 1) / KO_TY);

@@ -50,14 +50,15 @@ struct LbParams {
     const int16_t* ntype;
     const int32_t* rec;     // per-node IBB record index (-1: none)
     const IbbRecord* ibb;   // IBB records
-    const float* wallD;
-    float* K;
-    float* O;
-    float* S;               // 3 planes Sxx, Sxy, Syy
-    float* nut;
-    float* rho;
-    float* ux;
-    float* uy;
+    // node fields: FP32, or FP64 for the FP64 storage form (the kernel's FT)
+    const void* wallD;
+    void* K;
+    void* O;
+    void* S;                // 3 planes Sxx, Sxy, Syy
+    void* nut;
+    void* rho;
+    void* ux;
+    void* uy;
     double* partials;       // per block: sum rho, sum ux, sum uy (FP64)
     const float* ref_in;    // non-equilibrium form: reference rho, ux, uy of
     float* ref_out;         //   the populations read / written (3 planes)
@@ -85,7 +86,7 @@ template <typename AT>
 __device__ __forceinline__ AT amin(AT a, AT b) { return b < a ? b : a; }
 
 template <typename ST>
-__device__ __forceinline__ float ld1(const ST* base, long long idx) {
+__device__ __forceinline__ typename Store<ST>::vt ld1(const ST* base, long long idx) {
     return Store<ST>::to_f32(base[idx]);
 }
 
@@ -113,10 +114,16 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 
 // ---------------------------------------------------------------------------
 // NEQ: populations stored as f - feq(reference moments of the writing node),
-// FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false>
-__global__ void __launch_bounds__(128, NEQ ? 1 : KOFM_LB_MINBLOCKS)
+// FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.  FT: type of the node fields
+// (k, omega, strain rates, wall distance, nu_t, moments) -- FP32, or FP64 for
+// the FP64 storage form, whose eddy viscosity is then evaluated in FP64 too.
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float>
+__global__ void __launch_bounds__(128, (NEQ || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
 lb_step_kernel(const LbParams p) {
+    using VT = typename Store<ST>::vt;  // type a population is loaded into
+    FT* const fK = static_cast<FT*>(p.K);
+    FT* const fO = static_cast<FT*>(p.O);
+    FT* const fS = static_cast<FT*>(p.S);
     const int lane = threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     // Each warp owns one partial-sum slot; warps that leave early clear it.
@@ -152,7 +159,7 @@ lb_step_kernel(const LbParams p) {
     float own_r[4] = {}, own_u[4] = {}, own_v[4] = {};  // NEQ: this node's reference moments
     // own stored population of direction q, decoded
     auto own_pop = [&](int q, int j) -> AT {
-        const float raw = ld1(gin, q * D + rowoff + x0 + j);
+        const VT raw = ld1(gin, q * D + rowoff + x0 + j);
         if (!NEQ) return AT(raw);
         return AT(feq_dev_f32(q, own_r[j], own_u[j], own_v[j])) + AT(raw) * AT(NEQ_INV_SCALE);
     };
@@ -160,26 +167,26 @@ lb_step_kernel(const LbParams p) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         const int cx = cx_of(q), cy = cy_of(q);
-        float v[4];
+        VT v[4];
         if (PHASE0) {
             Store<ST>::load4(gin + q * D + rowoff + x0, v);
         } else {
             int ys = y - cy;
             ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);  // only solid rows clamp
             const ST* src = gin + q * D + (long long)ys * p.P;
-            float c[4];
+            VT c[4];
             Store<ST>::load4(src + x0, c);
             if (cx == 0) {
                 v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = c[3];
             } else if (cx == 1) {
-                float left = __shfl_up_sync(0xffffffffu, c[3], 1);
+                VT left = __shfl_up_sync(0xffffffffu, c[3], 1);
                 if (lane == 0) {
                     const int xs = x0 > 0 ? x0 - 1 : p.nx - 1;
                     left = ld1(src, xs);
                 }
                 v[0] = left; v[1] = c[0]; v[2] = c[1]; v[3] = c[2];
             } else {
-                float right = __shfl_down_sync(0xffffffffu, c[0], 1);
+                VT right = __shfl_down_sync(0xffffffffu, c[0], 1);
                 if (lane == 31) {
                     const int xs = (x0 + 4 < p.nx) ? x0 + 4 : 0;
                     right = ld1(src, xs);
@@ -247,27 +254,21 @@ lb_step_kernel(const LbParams p) {
 
     // ---- collision ----------------------------------------------------------
     const AT tau0 = AT(p.tau), fterm = AT(p.fterm), mu = AT(p.mu);
-    float o_rho[4], o_ux[4], o_uy[4], o_nut[4], o_s[3][4];
-    float kin[4], oin[4], win[4], sin3[3][4];
+    FT o_rho[4], o_ux[4], o_uy[4], o_nut[4], o_s[3][4];
+    FT kin[4], oin[4], win[4], sin3[3][4];
     if (KOMEGA) {
-        const float4 k4 = *reinterpret_cast<const float4*>(p.K + rowoff + x0);
-        const float4 o4 = *reinterpret_cast<const float4*>(p.O + rowoff + x0);
-        const float4 w4 = __ldg(reinterpret_cast<const float4*>(p.wallD + rowoff + x0));
-        kin[0] = k4.x; kin[1] = k4.y; kin[2] = k4.z; kin[3] = k4.w;
-        oin[0] = o4.x; oin[1] = o4.y; oin[2] = o4.z; oin[3] = o4.w;
-        win[0] = w4.x; win[1] = w4.y; win[2] = w4.z; win[3] = w4.w;
+        fld_ld4(fK + rowoff + x0, kin);
+        fld_ld4(fO + rowoff + x0, oin);
+        fld_ldg4(static_cast<const FT*>(p.wallD) + rowoff + x0, win);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float4 s4 = *reinterpret_cast<const float4*>(p.S + c * D + rowoff + x0);
-            sin3[c][0] = s4.x; sin3[c][1] = s4.y; sin3[c][2] = s4.z; sin3[c][3] = s4.w;
-        }
+        for (int c = 0; c < 3; ++c) fld_ld4(fS + c * D + rowoff + x0, sin3[c]);
     }
     double bsum_rho = 0.0, bsum_ux = 0.0, bsum_uy = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (!fl[j]) {
-            o_rho[j] = 0.f; o_ux[j] = 0.f; o_uy[j] = 0.f; o_nut[j] = 0.f;
-            o_s[0][j] = 0.f; o_s[1][j] = 0.f; o_s[2][j] = 0.f;
+            o_rho[j] = FT(0); o_ux[j] = FT(0); o_uy[j] = FT(0); o_nut[j] = FT(0);
+            o_s[0][j] = FT(0); o_s[1][j] = FT(0); o_s[2][j] = FT(0);
 #pragma unroll
             for (int q = 0; q < 9; ++q) d[q][j] = AT(0);
             continue;
@@ -283,24 +284,25 @@ lb_step_kernel(const LbParams p) {
 
         AT w = tau0;
         if (KOMEGA) {
-            // SST eddy viscosity (lbKernels.cl:400-451) in FP32: k, omega,
-            // S and wall distance are FP32 fields and nu_t is stored in FP32;
-            // the relaxation rate it sets changes the populations by ~1e-7
-            // of their non-equilibrium part, below the FP32 storage rounding.
-            float om = oin[j], kv = kin[j];
-            const float yv = win[j];
+            // SST eddy viscosity (lbKernels.cl:400-451) in the fields' type:
+            // FP32 for the FP32 fields (nu_t is stored in FP32; the relaxation
+            // rate it sets changes the populations by ~1e-7 of their
+            // non-equilibrium part, below the FP32 storage rounding), FP64 in
+            // the FP64 form.
+            FT om = oin[j], kv = kin[j];
+            const FT yv = win[j];
             const long long node = rowoff + x0 + j;
-            if (om < 0.f) { om = fabsf(om); p.O[node] = om; }
-            if (kv < 0.f) { kv = 1e-16f; p.K[node] = 1e-16f; }
-            const float mu_f = (float)p.mu;
-            const float a = 2.f * sqrtf(kv) / ((float)KO_BETA_STAR * om * yv);
-            const float b = 500.f * mu_f / (yv * yv * om);
-            const float arg = fmaxf(a, b);
-            float F2 = tanhf(arg * arg);
-            const float sxx = sin3[0][j], sxy = sin3[1][j], syy = sin3[2][j];
-            F2 *= sqrtf(2.f * (sxx * sxx + 2.f * sxy * sxy + syy * syy));
-            const float a1 = (float)KO_A1;
-            const float nut = fmaxf(fminf((float)p.maxnut, a1 * kv / fmaxf(a1 * om, F2)), 1e-16f);
+            if (om < FT(0)) { om = fabs(om); fO[node] = om; }
+            if (kv < FT(0)) { kv = FT(1e-16); fK[node] = FT(1e-16); }
+            const FT mu_f = (FT)p.mu;
+            const FT a = FT(2) * sqrt(kv) / ((FT)KO_BETA_STAR * om * yv);
+            const FT b = FT(500) * mu_f / (yv * yv * om);
+            const FT arg = fmax(a, b);
+            FT F2 = tanh(arg * arg);
+            const FT sxx = sin3[0][j], sxy = sin3[1][j], syy = sin3[2][j];
+            F2 *= sqrt(FT(2) * (sxx * sxx + FT(2) * sxy * sxy + syy * syy));
+            const FT a1 = (FT)KO_A1;
+            const FT nut = fmax(fmin((FT)p.maxnut, a1 * kv / fmax(a1 * om, F2)), FT(1e-16));
             o_nut[j] = nut;
             w = AT(1) / (AT(3) * (AT(nut) + mu) + AT(0.5));
         }
@@ -323,13 +325,13 @@ lb_step_kernel(const LbParams p) {
         }
         if (KOMEGA) {
             const AT s = AT(-1.5) * tau0 / rho;
-            o_s[0][j] = (float)(s * sxx_n);
-            o_s[1][j] = (float)(s * sxy_n);
-            o_s[2][j] = (float)(s * syy_n);
+            o_s[0][j] = (FT)(s * sxx_n);
+            o_s[1][j] = (FT)(s * sxy_n);
+            o_s[2][j] = (FT)(s * syy_n);
         }
-        o_rho[j] = (float)rho;
-        o_ux[j] = (float)(ux + fterm / AT(2));
-        o_uy[j] = (float)uy;
+        o_rho[j] = (FT)rho;
+        o_ux[j] = (FT)(ux + fterm / AT(2));
+        o_uy[j] = (FT)uy;
         bsum_rho += (double)rho;
         bsum_ux += (double)(ux + fterm / AT(2));
         bsum_uy += (double)uy;
@@ -338,14 +340,14 @@ lb_step_kernel(const LbParams p) {
     // ---- stores -----------------------------------------------------------------
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        float v[4];
+        VT v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (NEQ)
-                v[j] = fl[j] ? (float)((d[q][j] - AT(feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j]))) * AT(NEQ_SCALE))
-                             : 0.f;
+                v[j] = fl[j] ? (VT)((d[q][j] - AT(feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j]))) * AT(NEQ_SCALE))
+                             : VT(0);
             else
-                v[j] = (float)d[q][j];
+                v[j] = (VT)d[q][j];
         }
         Store<ST>::store4(gout + q * D + rowoff + x0, v);
     }
@@ -355,16 +357,14 @@ lb_step_kernel(const LbParams p) {
         *reinterpret_cast<float4*>(p.ref_out + 2 * D + rowoff + x0) = make_float4(o_uy[0], o_uy[1], o_uy[2], o_uy[3]);
     }
     if (p.options & OPTION_SAVE_MACRO_FIELDS) {
-        *reinterpret_cast<float4*>(p.rho + rowoff + x0) = make_float4(o_rho[0], o_rho[1], o_rho[2], o_rho[3]);
-        *reinterpret_cast<float4*>(p.ux + rowoff + x0) = make_float4(o_ux[0], o_ux[1], o_ux[2], o_ux[3]);
-        *reinterpret_cast<float4*>(p.uy + rowoff + x0) = make_float4(o_uy[0], o_uy[1], o_uy[2], o_uy[3]);
+        fld_st4(static_cast<FT*>(p.rho) + rowoff + x0, o_rho);
+        fld_st4(static_cast<FT*>(p.ux) + rowoff + x0, o_ux);
+        fld_st4(static_cast<FT*>(p.uy) + rowoff + x0, o_uy);
     }
     if (KOMEGA) {
-        *reinterpret_cast<float4*>(p.nut + rowoff + x0) = make_float4(o_nut[0], o_nut[1], o_nut[2], o_nut[3]);
+        fld_st4(static_cast<FT*>(p.nut) + rowoff + x0, o_nut);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            *reinterpret_cast<float4*>(p.S + c * D + rowoff + x0) =
-                make_float4(o_s[c][0], o_s[c][1], o_s[c][2], o_s[c][3]);
+        for (int c = 0; c < 3; ++c) fld_st4(fS + c * D + rowoff + x0, o_s[c]);
     }
 
     // ---- per-block FP64 partial sums of rho, ux, uy ----------------------------

@@ -57,7 +57,8 @@ constexpr int SS_MINL = 4;                                // fewest powers of a 
 
 struct SsArgs {
     KoSystem sys[2];          // x / x2 and r / r2 alternate between restarts
-    float* field[2];          // omega, k (FP32 fields, updated in place at the end)
+    void* field[2];           // omega, k (updated in place at the end): FP32, or FP64 when f64
+    int f64;
     const int16_t* ntype;
     GmresControl* ctl;
     double* part;             // [SS_SLOTS][gridDim.x] (slot-major)
@@ -700,7 +701,8 @@ sstep_kernel(const SsArgs a) {
     const long long npairs = a.D / 2;
     for (int s = 0; s < 2; ++s) {
         const KoSystem& S = a.sys[s];
-        float* f = a.field[s];
+        float* f = static_cast<float*>(a.field[s]);
+        double* f8 = static_cast<double*>(a.field[s]);
         // the correction of the last of `cycles` updates is in parity `cycles`
         const int cyc = ldc(&ctl->sys[s].cycles);
         const bool has_x = cyc > 0 && !ldc(&ctl->sys[s].nan);
@@ -715,8 +717,13 @@ sstep_kernel(const SsArgs a) {
             const double dv[2] = {xv.x, xv.y};
             for (int j = 0; j < 2; ++j) {
                 if (x + j >= a.nx) continue;
-                if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
-                else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+                if (a.f64) {
+                    if (!(tt[j] & M_SOLID)) f8[g + j] = f8[g + j] + dv[j];
+                    else if (tt[j] & SOLID_BOUNDARY) f8[g + j] = 0.0;
+                } else {
+                    if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
+                    else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+                }
             }
         }
     }
