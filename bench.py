@@ -101,7 +101,8 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
                  "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)",
-                 "fp64": "fp64 f-w deviation, fp64 fields"}
+                 "fp64": "fp64 f-w deviation, fp64 fields",
+                 "fp16neq32": "fp16 f-feq (FP32 reference moments), fp32 collide"}
 
 
 def workload_config(w, args, world: int) -> dict:
@@ -159,7 +160,7 @@ SOLVER_TRAFFIC_RATIO = {
 }
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
-            "fp16neq": 114,                   # + reference moments read and written
+            "fp16neq": 114, "fp16neq32": 114,  # + reference moments read and written
             "fp64": 250}                      # FP64 populations and fields
 ASM_BYTES = {"fp64": 162}                           # fused assembly, per node (FP64 fields)
 ASM_BYTES_FP32 = 122                                # ... FP32 fields
@@ -179,7 +180,8 @@ def run_ours(args, rank, world, local_rank):
     lib = _abi.load()
     torch.cuda.set_device(local_rank)
     storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV,
-               "fp16neq": _abi.STORE_FP16_NEQ, "fp64": _abi.STORE_FP64}[args.storage]
+               "fp16neq": _abi.STORE_FP16_NEQ, "fp64": _abi.STORE_FP64,
+               "fp16neq32": _abi.STORE_FP16_NEQ32}[args.storage]
     asm_bytes = ASM_BYTES.get(args.storage, ASM_BYTES_FP32)
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
@@ -439,7 +441,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp64"])
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp16neq32", "fp64"])
     ap.add_argument("--solver", default="sstep", choices=["sstep", "classic"],
                     help="k-omega solve: a cycle's Krylov directions in one sweep (default) "
                          "or one vector per sweep")

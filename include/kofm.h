@@ -67,6 +67,11 @@ extern "C" {
                                  with the writer's FP32 rho, u as reference;
                                  FP64 collide arithmetic.  No counterpart in
                                  the reference (its arrays are FP64). */
+#define KOFM_STORE_FP16_NEQ32 5 /* as KOFM_STORE_FP16_NEQ with FP32 collide
+                                   arithmetic; the reference moments of a stored
+                                   value are the writer's unforced rho, u, and the
+                                   value carries the force increment.  No
+                                   counterpart in the reference. */
 #define KOFM_STORE_FP64 4     /* f_i - w_i in FP64 and every node field (k,
                                  omega, nu_t, strain rates, wall distance,
                                  moments) in FP64, FP64 arithmetic throughout:

@@ -470,7 +470,7 @@ int validate_desc(const kofm_desc* d) {
     if (!d) return KOFM_ERR_INVALID_ARG;
     if (d->nx < 4 || d->ny < 3 || d->nx_full < d->nx) return KOFM_ERR_LOADING_PARAMS;
     if ((long long)d->nx_full * d->ny > (1LL << 31) - 1) return KOFM_ERR_LOADING_PARAMS;
-    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP64) return KOFM_ERR_LOADING_PARAMS;
+    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP16_NEQ32) return KOFM_ERR_LOADING_PARAMS;
     // the FP64 form is the precision study's reference form: no thermal update
     if (d->storage == KOFM_STORE_FP64 && d->use_thermal) return KOFM_ERR_LOADING_PARAMS;
     if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
@@ -606,7 +606,7 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         int _s = dalloc(&c->g[b], (size_t)(9 * D) * c->store_bytes);
         if (_s) { kofm_destroy(c); return _s; }
     }
-    if (d->storage == KOFM_STORE_FP16_NEQ) {
+    if (d->storage == KOFM_STORE_FP16_NEQ || d->storage == KOFM_STORE_FP16_NEQ32) {
         ALLOC(c->ref[0], 3 * D);
         ALLOC(c->ref[1], 3 * D);
     }
@@ -834,6 +834,7 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
             k_fa_in<__half><<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
         case KOFM_STORE_FP16_NEQ:
+        case KOFM_STORE_FP16_NEQ32:
             k_fa_in_neq<<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ref[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
         case KOFM_STORE_FP64:
@@ -883,6 +884,7 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
                 k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
                 break;
             case KOFM_STORE_FP16_NEQ:
+            case KOFM_STORE_FP16_NEQ32:
                 k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, c->ref[c->cur]);
                 break;
             case KOFM_STORE_FP64:
@@ -963,7 +965,7 @@ int kofm_wall_shear(kofm_ctx* c, double* node_tau, double* bl_tau) {
     cudaSetDevice(c->dev);
     const int n = c->shear_n;
     const int has_ibb = c->n_ibb_rec > 0;
-    const float* ref = d.storage == KOFM_STORE_FP16_NEQ ? c->ref[c->cur] : nullptr;
+    const float* ref = (d.storage == KOFM_STORE_FP16_NEQ || d.storage == KOFM_STORE_FP16_NEQ32) ? c->ref[c->cur] : nullptr;
     const int nb = (n + 127) / 128;
     const float* frho = (const float*)c->rho;
     const float* fux = (const float*)c->ux;
@@ -1034,6 +1036,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
         case KOFM_STORE_FP16_DEV: e = launch_lb<__half, float>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, double, true>(c, p, ko, ph0); break;
         case KOFM_STORE_FP64: e = launch_lb<double, double, false, double>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP16_NEQ32: e = launch_lb<__half, float, true>(c, p, ko, ph0); break;
         default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
     }
     if (e != cudaSuccess) {

@@ -117,10 +117,19 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 // FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.  FT: type of the node fields
 // (k, omega, strain rates, wall distance, nu_t, moments) -- FP32, or FP64 for
 // the FP64 storage form, whose eddy viscosity is then evaluated in FP64 too.
+//
+// With NEQ and FP32 arithmetic (KOFM_STORE_FP16_NEQ32) the stored value is
+// formed without the full population: relative to the node's own unforced
+// moments (rho, u) it is (1 - w) neq + rho phi_y [phi_x(u + F) - phi_x(u)], both
+// terms small and computed with relative precision, so the exact-difference
+// force increment (~1e-7 of a population of ~0.1, a few FP32 ulps of it) is
+// not rounded away; the equilibrium both sides subtract and add back is the
+// same FP32 function feq_dev_f32 of the same FP32 moments.
 template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float>
-__global__ void __launch_bounds__(128, (NEQ || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
+__global__ void __launch_bounds__(128, ((NEQ && sizeof(AT) == 8) || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
 lb_step_kernel(const LbParams p) {
     using VT = typename Store<ST>::vt;  // type a population is loaded into
+    constexpr bool NEQ32 = NEQ && sizeof(AT) == 4;
     FT* const fK = static_cast<FT*>(p.K);
     FT* const fO = static_cast<FT*>(p.O);
     FT* const fS = static_cast<FT*>(p.S);
@@ -255,6 +264,7 @@ lb_step_kernel(const LbParams p) {
     // ---- collision ----------------------------------------------------------
     const AT tau0 = AT(p.tau), fterm = AT(p.fterm), mu = AT(p.mu);
     FT o_rho[4], o_ux[4], o_uy[4], o_nut[4], o_s[3][4];
+    float o_u0[4];  // NEQ32: the unforced u_x, the reference of the stored values
     FT kin[4], oin[4], win[4], sin3[3][4];
     if (KOMEGA) {
         fld_ld4(fK + rowoff + x0, kin);
@@ -267,7 +277,7 @@ lb_step_kernel(const LbParams p) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (!fl[j]) {
-            o_rho[j] = FT(0); o_ux[j] = FT(0); o_uy[j] = FT(0); o_nut[j] = FT(0);
+            o_rho[j] = FT(0); o_ux[j] = FT(0); o_uy[j] = FT(0); o_nut[j] = FT(0); o_u0[j] = 0.f;
             o_s[0][j] = FT(0); o_s[1][j] = FT(0); o_s[2][j] = FT(0);
 #pragma unroll
             for (int q = 0; q < 9; ++q) d[q][j] = AT(0);
@@ -313,7 +323,8 @@ lb_step_kernel(const LbParams p) {
             const AT px0 = phi0<AT>(cx), py0 = phi0<AT>(cy);
             const AT dpx = dphi<AT>(cx, ux), dpy = dphi<AT>(cy, uy);
             const AT phy = py0 + dpy;
-            const AT feqdev = drho * (px0 + dpx) * phy + (dpx * py0 + px0 * dpy + dpx * dpy);
+            const AT feqdev = NEQ32 ? AT(feq_dev_f32(q, (float)rho, (float)ux, (float)uy))
+                                    : drho * (px0 + dpx) * phy + (dpx * py0 + px0 * dpy + dpx * dpy);
             const AT neq = d[q][j] - feqdev;
             if (KOMEGA) {
                 if (cx != 0) sxx_n += neq;
@@ -321,8 +332,12 @@ lb_step_kernel(const LbParams p) {
                 if (cx * cy == 1) sxy_n += neq;
                 if (cx * cy == -1) sxy_n -= neq;
             }
-            d[q][j] = d[q][j] - w * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
+            if (NEQ32)  // the post-collision value minus feq(rho, u) (stored as is)
+                d[q][j] = (AT(1) - w) * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
+            else
+                d[q][j] = d[q][j] - w * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
         }
+        o_u0[j] = (float)ux;
         if (KOMEGA) {
             const AT s = AT(-1.5) * tau0 / rho;
             o_s[0][j] = (FT)(s * sxx_n);
@@ -343,7 +358,9 @@ lb_step_kernel(const LbParams p) {
         VT v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            if (NEQ)
+            if (NEQ32)
+                v[j] = fl[j] ? (VT)(d[q][j] * AT(NEQ_SCALE)) : VT(0);
+            else if (NEQ)
                 v[j] = fl[j] ? (VT)((d[q][j] - AT(feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j]))) * AT(NEQ_SCALE))
                              : VT(0);
             else
@@ -353,7 +370,10 @@ lb_step_kernel(const LbParams p) {
     }
     if (NEQ) {
         *reinterpret_cast<float4*>(p.ref_out + rowoff + x0) = make_float4(o_rho[0], o_rho[1], o_rho[2], o_rho[3]);
-        *reinterpret_cast<float4*>(p.ref_out + D + rowoff + x0) = make_float4(o_ux[0], o_ux[1], o_ux[2], o_ux[3]);
+        if (NEQ32)
+            *reinterpret_cast<float4*>(p.ref_out + D + rowoff + x0) = make_float4(o_u0[0], o_u0[1], o_u0[2], o_u0[3]);
+        else
+            *reinterpret_cast<float4*>(p.ref_out + D + rowoff + x0) = make_float4(o_ux[0], o_ux[1], o_ux[2], o_ux[3]);
         *reinterpret_cast<float4*>(p.ref_out + 2 * D + rowoff + x0) = make_float4(o_uy[0], o_uy[1], o_uy[2], o_uy[3]);
     }
     if (p.options & OPTION_SAVE_MACRO_FIELDS) {

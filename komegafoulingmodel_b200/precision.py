@@ -4,7 +4,8 @@
         --steps 20000 [--forms fp32,fp16,bf16,fp16neq]
 
 Runs the same seeded channel once per storage form (FP64 throughout; FP32 /
-FP16 / BF16 deviations f - w_i; FP16 non-equilibrium parts f - feq) and
+FP16 / BF16 deviations f - w_i; FP16 non-equilibrium parts f - feq with
+FP64 or FP32 collide arithmetic) and
 reports, for every other form, the rel-L2 of u_x, k and omega over the fluid
 nodes against the reference form -- the FP64 form when it is among the forms
 (the reference's own precision, held to the FP64 oracle by the test suite),
@@ -25,7 +26,8 @@ from . import workloads as W
 from .lattice import Lattice
 
 FORMS = {"fp64": _abi.STORE_FP64, "fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV,
-         "bf16": _abi.STORE_BF16_DEV, "fp16neq": _abi.STORE_FP16_NEQ}
+         "bf16": _abi.STORE_BF16_DEV, "fp16neq": _abi.STORE_FP16_NEQ,
+         "fp16neq32": _abi.STORE_FP16_NEQ32}
 
 
 def rel_l2(a, b, mask):
@@ -56,7 +58,7 @@ def run_form(w, form: str, steps: int, chunk: int = 500):
             "mlups": w.nodes * max(steps - 1, 1) / secs / 1e6}
 
 
-def study(workload: str, steps: int, forms=("fp64", "fp32", "fp16", "bf16", "fp16neq")) -> dict:
+def study(workload: str, steps: int, forms=("fp64", "fp32", "fp16", "bf16", "fp16neq", "fp16neq32")) -> dict:
     w = W.by_name(workload)
     fl = w.channel.fluid_mask().ravel()
     ref_form = "fp64" if "fp64" in forms else "fp32"
@@ -80,7 +82,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="komega_straight_16384x1024")
     ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--forms", default="fp64,fp32,fp16,bf16,fp16neq")
+    ap.add_argument("--forms", default="fp64,fp32,fp16,bf16,fp16neq,fp16neq32")
     args = ap.parse_args()
     print(json.dumps(study(args.workload, args.steps, tuple(args.forms.split(",")))), flush=True)
 
