@@ -317,13 +317,59 @@ lb_step_kernel(const LbParams p) {
             w = AT(1) / (AT(3) * (AT(nut) + mu) + AT(0.5));
         }
         AT sxx_n = AT(0), sxy_n = AT(0), syy_n = AT(0);
+        // NEQ32: the mass and momentum that the FP32 moments leave out -- rho
+        // = 1 + drho rounded on the FP32 grid near 1 (up to 6e-8), u = j / rho
+        // rounded -- kept apart and carried by the stored values unrelaxed, as
+        // the collision conserves them
+        AT cdr = AT(0), cdjx = AT(0), cdjy = AT(0);
+        if (NEQ32) {
+            // the rounding of the moment sums themselves (the same sums in the
+            // same order, error-free transformation of each addition)
+            auto lo = [](AT a, AT b, AT s) -> AT { const AT bp = s - a; return (a - (s - bp)) + (b - bp); };
+            AT lr = AT(0), lx = AT(0), ly = AT(0);
+            {
+                AT sr = d[0][j];
+#pragma unroll
+                for (int q = 1; q < 9; ++q) { const AT t = sr + d[q][j]; lr += lo(sr, d[q][j], t); sr = t; }
+                const int sx[6] = {1, 2, 5, 6, 7, 8}, gx[6] = {1, -1, 1, -1, 1, -1};
+                const int sy[6] = {3, 4, 5, 6, 7, 8}, gy[6] = {1, -1, 1, -1, -1, 1};
+                AT tx = d[1][j], ty = d[3][j];
+#pragma unroll
+                for (int i = 1; i < 6; ++i) {
+                    const AT bx = gx[i] > 0 ? d[sx[i]][j] : -d[sx[i]][j];
+                    const AT by = gy[i] > 0 ? d[sy[i]][j] : -d[sy[i]][j];
+                    const AT nx_ = tx + bx, ny_ = ty + by;
+                    lx += lo(tx, bx, nx_);
+                    ly += lo(ty, by, ny_);
+                    tx = nx_;
+                    ty = ny_;
+                }
+            }
+            cdr = (drho - (rho - AT(1))) + lr;
+            cdjx = fma(-rho, ux, jx) + lx;
+            cdjy = fma(-rho, uy, jy) + ly;
+            // non-equilibrium parts against the FP32 equilibrium of the FP32
+            // moments, with their mass and momentum (rounding) projected out
+            // along w_q (1, 3 c_q): the non-conserved part the collision relaxes
+            AT m0 = AT(0), mx = AT(0), my = AT(0);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                d[q][j] -= AT(feq_dev_f32(q, (float)rho, (float)ux, (float)uy));
+                m0 += d[q][j];
+                mx += AT(cx_of(q)) * d[q][j];
+                my += AT(cy_of(q)) * d[q][j];
+            }
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                d[q][j] -= AT(weight_of(q)) * (m0 + AT(3 * cx_of(q)) * mx + AT(3 * cy_of(q)) * my);
+        }
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
             const int cx = cx_of(q), cy = cy_of(q);
             const AT px0 = phi0<AT>(cx), py0 = phi0<AT>(cy);
             const AT dpx = dphi<AT>(cx, ux), dpy = dphi<AT>(cy, uy);
             const AT phy = py0 + dpy;
-            const AT feqdev = NEQ32 ? AT(feq_dev_f32(q, (float)rho, (float)ux, (float)uy))
+            const AT feqdev = NEQ32 ? AT(0)  // d already holds the non-equilibrium part
                                     : drho * (px0 + dpx) * phy + (dpx * py0 + px0 * dpy + dpx * dpy);
             const AT neq = d[q][j] - feqdev;
             if (KOMEGA) {
@@ -333,7 +379,8 @@ lb_step_kernel(const LbParams p) {
                 if (cx * cy == -1) sxy_n -= neq;
             }
             if (NEQ32)  // the post-collision value minus feq(rho, u) (stored as is)
-                d[q][j] = (AT(1) - w) * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
+                d[q][j] = (AT(1) - w) * neq + AT(weight_of(q)) * (cdr + AT(3 * cx) * cdjx + AT(3 * cy) * cdjy) +
+                          rho * phy * dphiF<AT>(cx, ux, fterm);
             else
                 d[q][j] = d[q][j] - w * neq + rho * phy * dphiF<AT>(cx, ux, fterm);
         }
