@@ -157,6 +157,7 @@ def replica_value(nodes: int, steps: int, world: int, ms: float) -> float:
 SOLVER_TRAFFIC_RATIO = {
     "gmres_kernel": 4.7967e9 / (1076 * 4194304),   # one vector per sweep
     "sstep_kernel": None,                          # one sweep per cycle's powers
+    "sstep_phases": None,                          # the same, one launch per sweep
 }
 
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
@@ -186,8 +187,8 @@ def run_ours(args, rank, world, local_rank):
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
-    d.komega_classic = 1 if args.solver == "classic" else 0
-    solver_kernel = "gmres_kernel" if args.solver == "classic" else "sstep_kernel"
+    d.komega_classic = {"sstep": 0, "classic": 1, "sstep_coop": 2}[args.solver]
+    solver_kernel = {"sstep": "sstep_phases", "classic": "gmres_kernel", "sstep_coop": "sstep_kernel"}[args.solver]
     d.use_thermal = 1 if args.thermal else 0
     L = Lattice(d)
     W.apply(L, w)
@@ -210,9 +211,12 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    solver_launches = 0
     e0.record(stream)
     for _ in range(args.steps):
         L.step(1)
+        if w.komega:  # host-side counters of the step just enqueued and finished
+            solver_launches += L.stats().solver_launches
     e1.record(stream)
     L.sync()
     torch.cuda.synchronize()
@@ -221,9 +225,9 @@ def run_ours(args, rank, world, local_rank):
     ms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local_rank}")
     st = L.stats()
     value = replica_value(nodes, args.steps, world, ms)
-    # kernels of one kofm_step: collide, assembly, solver control-block init,
-    # solver (one k-omega sub-step per LB step here: steps_per_lb stays 1)
-    launches_per_step = 4 if w.komega else 1
+    # kernels of one kofm_step: collide, assembly and the solver's launches
+    # (counted per step: the phase-launch solver enqueues one round per pass)
+    launches_per_step = (2 + solver_launches / args.steps) if w.komega else 1
     if args.thermal:  # assembly, control-block init and BiCGStab per solve
         launches_per_step += 3 * max(1, st.thermal_solves)
 
@@ -345,7 +349,7 @@ def run_ours(args, rank, world, local_rank):
                        "omega_powers": st.omega_powers, "k_powers": st.k_powers,
                        "passes": st.solver_passes, "form": args.solver},
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": int(round(launches_per_step * args.steps)),
         }
         print(json.dumps(line), flush=True)
 
@@ -442,9 +446,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp16neq32", "fp64"])
-    ap.add_argument("--solver", default="sstep", choices=["sstep", "classic"],
-                    help="k-omega solve: a cycle's Krylov directions in one sweep (default) "
-                         "or one vector per sweep")
+    ap.add_argument("--solver", default="sstep", choices=["sstep", "sstep_coop", "classic"],
+                    help="k-omega solve: a cycle's Krylov directions in one sweep, each sweep "
+                         "its own launch (default) or all in one cooperative launch "
+                         "(sstep_coop), or one vector per sweep (classic)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define KOFM_ABI_VERSION 2
+#define KOFM_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 #define KOFM_OK 0
@@ -139,9 +139,13 @@ typedef struct kofm_desc {
                                  Krylov directions of a cycle in one sweep
                                  (powers of the off-diagonal operator, Gram
                                  matrix, the simpler-GMRES steps in that
-                                 basis); 1 builds one vector per sweep as
+                                 basis), each sweep its own kernel launch and
+                                 the host enqueueing one round at a time;
+                                 2 is the same solve in one cooperative
+                                 launch (the form kofm_batch graphs capture);
+                                 1 builds one vector per sweep as
                                  GMRESSolver::solve does.  komega_full_cycle = 1
-                                 implies 1.  Both follow the reference's
+                                 implies 1.  All follow the reference's
                                  restart loop and truncation tests. */
     double thermal_rel_tol;   /* THERMAL_MAX_REL_TOL (1e-4) */
     double thermal_abs_tol;   /* THERMAL_MAX_ABS_TOL (1e-7) */
@@ -178,6 +182,9 @@ typedef struct kofm_stats {
                                            last k-omega solve (both systems): every
                                            array its sweeps stream, counted once per sweep */
     int32_t omega_powers, k_powers;     /* one-sweep cycles: powers computed (all rounds) */
+    int32_t solver_launches;            /* kernel launches of the last k-omega solve */
+    int32_t solver_rounds;              /* host round trips of the last solve (phase
+                                           launches: rounds enqueued; 1 otherwise) */
 } kofm_stats;
 
 int kofm_abi_version(void);

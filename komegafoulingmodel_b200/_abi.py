@@ -75,6 +75,7 @@ class KofmStats(C.Structure):
         ("thermal_steps_per_lb", C.c_int32), ("thermal_time_since_change", C.c_int32),
         ("thermal_dt", C.c_double), ("thermal_residual", C.c_double),
         ("solver_bytes_per_node", C.c_double), ("omega_powers", C.c_int32), ("k_powers", C.c_int32),
+        ("solver_launches", C.c_int32), ("solver_rounds", C.c_int32),
     ]
 
 

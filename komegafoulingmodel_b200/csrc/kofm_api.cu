@@ -30,6 +30,7 @@ int ko_solver_alloc(KoSystem* sys, GmresControl** ctl, double** part, unsigned i
                     int* nblocks, int P, int ny, int K, int dev, int max_blocks);
 int ss_solver_alloc(double** part, int** lhint, int* nblocks, int* pstrips, int* prows, int nx,
                     int ny, int K, int dev, int max_blocks);
+int sp_solver_alloc(kofm_ctx* c);
 void ko_system_free(KoSystem* s);
 }  // namespace kofm
 
@@ -111,6 +112,8 @@ struct kofm_ctx {
     double* spart = nullptr;
     int* ss_lhint = nullptr;          // powers of a cycle's first round, per system
     int ss_blocks = 0, ss_pstrips = 0, ss_prows = 0;
+    SsLaunch sp{};                    // the same solver as separate phase launches
+    int ss_hint[2] = {0, 0};          // host copy of ss_lhint (first-round powers)
     int steps_per_lb = 1;
     int time_since_change = 0;
     double dt = 1.0;
@@ -477,6 +480,7 @@ int validate_desc(const kofm_desc* d) {
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
     if (d->solver_max_blocks < 0) return KOFM_ERR_LOADING_PARAMS;
+    if (d->komega_classic < 0 || d->komega_classic > 2) return KOFM_ERR_LOADING_PARAMS;
     if (d->use_thermal) {
         if (d->thermal_every < 1 || d->thermal_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
         if (!(d->pr_number > 0.0) || !(d->pr_turb_number > 0.0) || !(d->thermal_dt > 0.0))
@@ -636,6 +640,7 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
         if (s2) { kofm_destroy(c); return s2; }
         s2 = ss_solver_alloc(&c->spart, &c->ss_lhint, &c->ss_blocks, &c->ss_pstrips, &c->ss_prows,
                              d->nx, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
+        if (!s2) s2 = sp_solver_alloc(c);
         if (s2) { kofm_destroy(c); return s2; }
         if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {
             kofm_destroy(c);

@@ -61,7 +61,12 @@ struct GmresSys {
     int lev;            // one-sweep cycle: powers computed so far in this cycle
     int ext;            // one-sweep cycle: 1 = more powers needed before the cut
     int powers;         // one-sweep cycle: powers computed (all rounds and cycles)
-    int pad2;
+    int lnext;          // one-sweep cycle: first-round powers chosen for the next cycle (0: none yet)
+    // one-sweep cycle run as separate phase launches: the restart whose
+    // vectors are in use (buffer parity), the levels of the pending powers
+    // round (lfrom + 1 .. lto), a finished cycle waiting for its update and
+    // residual sweeps, and the field write-back done
+    int rst, lfrom, lto, ready, written;
     double rho0, norm_rhs, rinv, rho, prev_err;
     double abytes;      // one-sweep cycle: algorithmic bytes per node of the sweeps so far
     double s[KOFM_MAX_KRYLOV];   // 1 / ||u_j||

@@ -167,6 +167,88 @@ __device__ int ss_cycle(GmresSys& S, const double* G, int L, int K, double rel_t
     return built;
 }
 
+// One system's serial step after a Gram round: t holds G(i, j) of p_0 .. p_L
+// (slots ss_gslot), the round computed powers lfrom + 1 .. L; `first` marks
+// restart 0's first round, which also takes the restart-0 convergence test
+// from G(0, 0) = ||b'||^2 (GMRESSolver::solve's checkConvergence).  A cycle
+// whose tests have not fired asks for the remaining powers (ext); a finished
+// one leaves its update coefficients on p_0 .. p_L in S.h.
+__device__ __noinline__ void ss_gram_step(const SsArgs& a, GmresSys& S, int s, const double* t, int L,
+                                          int lfrom, bool first) {
+    // this round's powers (level 0 and coefficients in, levels lfrom+1 .. L
+    // out) and Gram (levels 0 .. L in), per node
+    S.abytes += 8.0 + 32.0 + 8.0 * (L - lfrom) + 8.0 * (L + 1);
+    S.powers += L - lfrom;
+    const double rho0 = sqrt(t[0]);
+    if (first) {
+        S.rho0 = rho0;
+        S.norm_rhs = rho0;
+        S.restarts += 1;
+        const double resid = S.rho0 / S.norm_rhs;
+        if (isnan(resid) || S.inject) { S.nan = 1; S.active = 0; }
+        else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+        else S.cycles += 1;
+    }
+    if (!S.active) {
+        S.lfrom = S.lto = 0;
+        return;
+    }
+    S.rho0 = rho0;
+    S.rinv = 1.0 / rho0;
+    double G[(SS_MAXL + 1) * (SS_MAXL + 1)];
+    const int n = L + 1;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            const double v = t[ss_gslot(i, j)];
+            G[i * n + j] = v;
+            G[j * n + i] = v;
+        }
+    double cP[SS_MAXL + 1];
+    const int built = ss_cycle(S, G, L, a.K, a.rel_tol, cP);
+    S.lev = L;
+    if (!S.done) {
+        S.ext = 1;  // more powers, then the cycle again
+        S.lfrom = L;
+        S.lto = a.K;
+    } else {
+        S.ext = 0;
+        S.vecs += built;
+        S.vec_index_sum += built * (built - 1) / 2;
+        // the update sweep reads c on p_0 .. p_{kk-1}
+        for (int i = 0; i < a.K; ++i) S.h[i] = i < n ? cP[i] : 0.0;
+        int nl = built + 2;
+        nl = nl > a.K ? a.K : nl;
+        __stcg(a.lhint + s, nl);
+        S.lnext = nl;
+        S.ready = 1;
+        S.lfrom = S.lto = 0;
+    }
+}
+
+// One system's serial step after the residual sweep of restart `restart`:
+// rr = ||b' - A d||^2, the residual of the next restart (GMRESSolver.cpp:248-256).
+__device__ __noinline__ void ss_resid_step(const SsArgs& a, GmresSys& S, int s, double rr, int restart) {
+    // the update (p_0 .. p_{kk-1} and the previous correction in, the
+    // correction out) and the residual (correction, four coefficients and b'
+    // in, r out), per node
+    S.abytes += 8.0 * (S.kk > 1 ? S.kk : 1) + (restart > 0 ? 8.0 : 0.0) + 8.0 + 56.0;
+    const int next = restart + 1;
+    if (next < a.max_restarts) {
+        S.rho0 = sqrt(rr);
+        S.restarts += 1;
+        const double resid = S.rho0 / S.norm_rhs;
+        if (isnan(resid)) { S.nan = 1; S.active = 0; }
+        else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+        else S.cycles += 1;
+    } else {
+        S.active = 0;  // iteration cap: the loop ends without a test
+    }
+    S.rst = next;
+    S.ready = 0;
+    S.lfrom = 0;
+    S.lto = S.active ? ss_first_levels(a, s) : 0;
+}
+
 enum SsSerial : int { SS_SER_NONE = 0, SS_SER_GRAM, SS_SER_RESID };
 
 // Serial section (last block to reach a barrier).  SS_SER_GRAM: the Gram of
@@ -216,69 +298,10 @@ __device__ void ss_serial(const SsArgs& a, int kind, int restart, int round, int
         GmresSys& S = sS[s];
         const double* t = tot + SS_NG * s;
         if (S.active) {
-            if (kind == SS_SER_GRAM && s_L[s] > 0) {
-                const int L = s_L[s];
-                // this round's powers (level 0 and coefficients in, levels
-                // lfrom+1 .. L out) and Gram (levels 0 .. L in), per node
-                const int lfrom = round == 0 ? 0 : S.lev;
-                S.abytes += 8.0 + 32.0 + 8.0 * (L - lfrom) + 8.0 * (L + 1);
-                S.powers += L - lfrom;
-                const double rho0 = sqrt(t[0]);
-                if (restart == 0 && round == 0) {
-                    // the restart-0 test (GMRESSolver::solve's checkConvergence)
-                    S.rho0 = rho0;
-                    S.norm_rhs = rho0;
-                    S.restarts += 1;
-                    const double resid = S.rho0 / S.norm_rhs;
-                    if (isnan(resid) || S.inject) { S.nan = 1; S.active = 0; }
-                    else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
-                    else S.cycles += 1;
-                }
-                if (S.active) {
-                    S.rho0 = rho0;
-                    S.rinv = 1.0 / rho0;
-                    double G[(SS_MAXL + 1) * (SS_MAXL + 1)];
-                    const int n = L + 1;
-                    for (int j = 0; j < n; ++j)
-                        for (int i = 0; i <= j; ++i) {
-                            const double v = t[ss_gslot(i, j)];
-                            G[i * n + j] = v;
-                            G[j * n + i] = v;
-                        }
-                    double cP[SS_MAXL + 1];
-                    const int built = ss_cycle(S, G, L, a.K, a.rel_tol, cP);
-                    S.lev = L;
-                    if (!S.done) {
-                        S.ext = 1;  // more powers, then the cycle again
-                    } else {
-                        S.ext = 0;
-                        S.vecs += built;
-                        S.vec_index_sum += built * (built - 1) / 2;
-                        // the update sweep reads c on p_0 .. p_{kk-1}
-                        for (int i = 0; i < a.K; ++i) S.h[i] = i < n ? cP[i] : 0.0;
-                        int nl = built + 2;
-                        nl = nl > a.K ? a.K : nl;
-                        __stcg(a.lhint + s, nl);
-                    }
-                }
-            } else if (kind == SS_SER_RESID) {
-                // the update (p_0 .. p_{kk-1} and the previous correction in,
-                // the correction out) and the residual (correction, four
-                // coefficients and b' in, r out), per node
-                S.abytes += 8.0 * (S.kk > 1 ? S.kk : 1) + (restart > 0 ? 8.0 : 0.0) + 8.0 + 56.0;
-                // residual of the next restart (GMRESSolver.cpp:248-256)
-                const int next = restart + 1;
-                if (next < a.max_restarts) {
-                    S.rho0 = sqrt(t[0]);
-                    S.restarts += 1;
-                    const double resid = S.rho0 / S.norm_rhs;
-                    if (isnan(resid)) { S.nan = 1; S.active = 0; }
-                    else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
-                    else S.cycles += 1;
-                } else {
-                    S.active = 0;  // iteration cap: the loop ends without a test
-                }
-            }
+            if (kind == SS_SER_GRAM && s_L[s] > 0)
+                ss_gram_step(a, S, s, t, s_L[s], round == 0 ? 0 : S.lev, restart == 0 && round == 0);
+            else if (kind == SS_SER_RESID)
+                ss_resid_step(a, S, s, t[0], restart);
         }
         atomicOr(&s_any, S.active);
         atomicOr(&s_ext, S.active && S.ext);
@@ -458,35 +481,38 @@ __device__ void ss_powers(const SsArgs& a, const KoSystem& S, const double* p0, 
 }
 
 // ---- Gram phase -------------------------------------------------------------------
-// Nodes [g0, g1) of one system, two per thread and iteration (the 2 (L+1)
-// loads of both in flight together): the (L+1)(L+2)/2 products of
-// p_0 .. p_L summed per thread.
-template <int L>
-__device__ void ss_gram(const SsArgs& a, const KoSystem& S, const double* p0, long long g0,
-                        long long g1, double* acc) {
+// Nodes [g0, g1) of one system, U per thread and iteration (the U (L+1)
+// loads in flight together): the (L+1)(L+2)/2 products of p_0 .. p_L summed
+// per thread.
+template <int L, int U = 2>
+__device__ __forceinline__ void ss_gram(const SsArgs& a, const KoSystem& S, const double* p0, long long g0,
+                                        long long g1, double* acc) {
     constexpr int NGL = (L + 1) * (L + 2) / 2;
     double s[NGL];
 #pragma unroll
     for (int i = 0; i < NGL; ++i) s[i] = 0.0;
     long long g = g0 + threadIdx.x;
-    for (; g + SS_THREADS < g1; g += 2 * SS_THREADS) {
-        double p[L + 1], q[L + 1];
-        const long long g2 = g + SS_THREADS;
-        p[0] = __ldcg(p0 + g);
-        q[0] = __ldcg(p0 + g2);
-        const long long vb = (g >> 5) * (a.K * 32) + (g & 31);
-        const long long vb2 = (g2 >> 5) * (a.K * 32) + (g2 & 31);
+    for (; g + (U - 1) * SS_THREADS < g1; g += U * SS_THREADS) {
+        double p[U][L + 1];
 #pragma unroll
-        for (int j = 1; j <= L; ++j) {
-            p[j] = __ldcg(S.V + vb + (j - 1) * 32);
-            q[j] = __ldcg(S.V + vb2 + (j - 1) * 32);
+        for (int u = 0; u < U; ++u) {
+            const long long gu = g + u * SS_THREADS;
+            p[u][0] = __ldcg(p0 + gu);
+            const long long vb = (gu >> 5) * (a.K * 32) + (gu & 31);
+#pragma unroll
+            for (int j = 1; j <= L; ++j) p[u][j] = __ldcg(S.V + vb + (j - 1) * 32);
         }
 #pragma unroll
         for (int j = 0; j <= L; ++j)
 #pragma unroll
-            for (int i = 0; i <= j; ++i) s[ss_gslot(i, j)] += p[i] * p[j] + q[i] * q[j];
+            for (int i = 0; i <= j; ++i) {
+                double t = p[0][i] * p[0][j];
+#pragma unroll
+                for (int u = 1; u < U; ++u) t += p[u][i] * p[u][j];
+                s[ss_gslot(i, j)] += t;
+            }
     }
-    if (g < g1) {
+    if (U > 1 && g < g1) {
         double p[L + 1];
         p[0] = __ldcg(p0 + g);
         const long long vb = (g >> 5) * (a.K * 32) + (g & 31);
@@ -727,6 +753,358 @@ sstep_kernel(const SsArgs a) {
             }
         }
     }
+}
+
+// ---- the same solver as separate phase launches -----------------------------------------
+// sstep_kernel's sweeps and serial steps, each sweep its own launch with its
+// own grid and register budget (the pointwise sweeps run at full occupancy,
+// the powers and Gram sweeps are compiled per level count).  The host
+// enqueues one round at a time: per system its powers and Gram sweeps, then
+// the update, residual and write-back sweeps of both systems; each sweep
+// reads what it has to do from the control block (a system whose cycle asks
+// for more powers skips the update; a finished one is written back once), and
+// the host reads the control block after the round to enqueue the next (an
+// extension round, or the next restart) while a system is still iterating.
+// The serial steps run in the last block to finish a sweep (ticket counter,
+// no grid barrier and no spin-wait).
+
+// Launch shapes of the phase sweeps (host side, per level count).
+struct SsLaunch {
+    int pow_grid[SS_MAXL + 1];   // powers sweep of L levels: blocks
+    int pow_prows[SS_MAXL + 1];  // and row ranges per strip
+    int gram_grid[SS_MAXL + 1];  // Gram sweep of p_0 .. p_L: blocks
+    int pt_grid;                 // update / residual / write-back sweeps: blocks
+};
+
+// blocks per SM the powers sweep of L levels is compiled for (its per-thread
+// state is 9 L doubles)
+__host__ __device__ constexpr int sp_pow_minb(int L) { return L <= 5 ? 2 : 1; }
+
+// True in every thread of the block that finishes a sweep last; that block
+// then sees every other block's partial sums.  Resets the ticket counter for
+// the next sweep on the stream.
+__device__ __forceinline__ bool sp_last_block(GridBarrier* bar) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int ticket = atomicAdd(&bar->count, 1u);
+        s_last = ticket == gridDim.x - 1u;
+        if (s_last) atomicExch(&bar->count, 0u);
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+__device__ __forceinline__ void sp_sys_load(const GmresControl* ctl, int s, GmresSys& dst) {
+    constexpr int NW = (int)(sizeof(GmresSys) / 8);
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&ctl->sys[s]);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+    for (int i = threadIdx.x; i < NW; i += blockDim.x) d[i] = __ldcg(src + i);
+}
+
+__device__ __forceinline__ void sp_sys_store(GmresControl* ctl, int s, const GmresSys& src) {
+    constexpr int NW = (int)(sizeof(GmresSys) / 8);
+    const unsigned long long* sp = reinterpret_cast<const unsigned long long*>(&src);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(&ctl->sys[s]);
+    for (int i = threadIdx.x; i < NW; i += blockDim.x) __stcg(d + i, sp[i]);
+}
+
+// Block reduction of N per-thread sums into part[base + i][blockIdx.x].
+template <int N>
+__device__ __forceinline__ void sp_block_reduce(const double (&v)[N], double* part, int base, SsSmem& sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < N; ++s) {
+        double x = v[s];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) sm.red[warp][s] = x;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < N; s += SS_THREADS) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < SS_WARPS; ++w) x += sm.red[w][s];
+        part[(long long)(base + s) * gridDim.x + blockIdx.x] = x;
+    }
+    __syncthreads();
+}
+
+// Control block of a solve: both systems iterating, restart 0, first round
+// of L0 / L1 powers (chosen by the host from the cycle lengths seen so far).
+__global__ void sp_init_kernel(GmresControl* ctl, GridBarrier* bar, int inject, int L0, int L1) {
+    constexpr int NW = (int)(sizeof(GmresControl) / sizeof(unsigned int));
+    unsigned int* w = reinterpret_cast<unsigned int*>(ctl);
+    for (int i = threadIdx.x; i < NW; i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            ctl->sys[s].active = 1;
+            ctl->sys[s].inject = (inject >> s) & 1;
+            ctl->sys[s].lto = s == 0 ? L0 : L1;
+        }
+        ctl->any_active = 1;
+        ctl->t_start = globaltimer_ns();
+        bar->count = 0u;
+        bar->gen = 0u;
+    }
+}
+
+// The pending round of system s as the host launched it; false (and the
+// error word set to 2) if the control block disagrees.
+__device__ __forceinline__ bool sp_round(const SsArgs& a, int s, int lev, bool powers, int& lf, int& lt,
+                                         int& rst) {
+    const GmresSys* S = &a.ctl->sys[s];
+    const int act = ldc(&S->active);
+    lf = ldc(&S->lfrom);
+    lt = ldc(&S->lto);
+    rst = ldc(&S->rst);
+    if (!act || lt <= lf) return false;
+    if ((powers ? lt - lf : lt) != lev) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(&a.ctl->error, 2);
+        return false;
+    }
+    return true;
+}
+
+// Powers lfrom + 1 .. lto (= lfrom + L) of system s; units (strip, row
+// range) of its lattice over the grid.
+template <int L>
+__global__ void __launch_bounds__(SS_THREADS, sp_pow_minb(L))
+sp_powers_kernel(const SsArgs a, int s) {
+    __shared__ SsSmem sm;
+    extern __shared__ __align__(16) double ss_ring[];
+    int lf, lt, rst;
+    if (!sp_round(a, s, L, true, lf, lt, rst)) return;
+    const KoSystem& S = a.sys[s];
+    const double* p0 = rst == 0 ? S.rhs : ((rst & 1) ? S.r2 : S.r);
+    const int ow = SS_THREADS - 2 * a.K;
+    const int units = a.pstrips * a.prows;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int strip = u % a.pstrips, rr = u / a.pstrips;
+        const int ya = (int)((long long)rr * a.ny / a.prows);
+        const int yb = (int)((long long)(rr + 1) * a.ny / a.prows);
+        ss_powers<L>(a, S, p0, lf > 0, lf, strip * ow, ow, ya, yb, sm, ss_ring);
+    }
+}
+
+// Gram of p_0 .. p_L of system s; the last block runs the system's serial
+// step (the simpler-GMRES cycle in the power basis).
+template <int L>
+__global__ void __launch_bounds__(SS_THREADS)
+sp_gram_kernel(const SsArgs a, int s) {
+    constexpr int NGL = (L + 1) * (L + 2) / 2;
+    __shared__ SsSmem sm;
+    int lf, lt, rst;
+    if (!sp_round(a, s, L, false, lf, lt, rst)) return;
+    const KoSystem& S = a.sys[s];
+    const double* p0 = rst == 0 ? S.rhs : ((rst & 1) ? S.r2 : S.r);
+    {
+        // a fixed contiguous node range per block (deterministic sums)
+        const long long n32 = a.D / 32;
+        const long long g0 = n32 * blockIdx.x / gridDim.x * 32;
+        const long long g1 = n32 * (blockIdx.x + 1) / gridDim.x * 32;
+        double acc[SS_NG];
+        ss_gram<L, (L <= 6 ? 2 : 1)>(a, S, p0, g0, g1, acc);
+        double v[NGL];
+#pragma unroll
+        for (int i = 0; i < NGL; ++i) v[i] = acc[i];
+        sp_block_reduce<NGL>(v, a.part, 0, sm);
+    }
+    if (!sp_last_block(a.bar)) return;
+    __shared__ double tot[SS_NG];
+    __shared__ GmresSys sS;
+    sp_sys_load(a.ctl, s, sS);
+    const int warp = threadIdx.x >> 5;
+    for (int i = warp; i < NGL; i += SS_WARPS) {
+        const double v = sum_slot_warp(a.part, gridDim.x, i);
+        if ((threadIdx.x & 31) == 0) tot[i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ss_gram_step(a, sS, s, tot, L, lf, rst == 0 && lf == 0);
+        trace_barrier(a.ctl);
+        __stcg(&a.ctl->passes, ldc(&a.ctl->passes) + 1);
+    }
+    __syncthreads();
+    sp_sys_store(a.ctl, s, sS);
+}
+
+// d = d_prev + sum_j c_j p_j of every system with a finished cycle
+// (pointwise; restart n reads the correction of parity n and writes parity
+// n + 1, restart 0 starts from d = 0).
+__global__ void __launch_bounds__(SS_THREADS)
+sp_update_kernel(const SsArgs a) {
+    __shared__ double c[2][SS_MAXL];
+    __shared__ int act[2], kk[2], rs[2];
+    if (threadIdx.x < 2) {
+        const int s = threadIdx.x;
+        const GmresSys* S = &a.ctl->sys[s];
+        act[s] = ldc(&S->active) && ldc(&S->ready);
+        kk[s] = ldc(&S->kk);
+        rs[s] = ldc(&S->rst);
+    }
+    if (threadIdx.x < 2 * SS_MAXL) {
+        const int s = threadIdx.x / SS_MAXL, i = threadIdx.x % SS_MAXL;
+        c[s][i] = i < a.K ? ldc(&a.ctl->sys[s].h[i]) : 0.0;
+    }
+    __syncthreads();
+    const long long stride = (long long)gridDim.x * SS_THREADS;
+    const long long npairs = a.D / 2;
+    for (int s = 0; s < 2; ++s) {
+        if (!act[s]) continue;
+        const KoSystem& S = a.sys[s];
+        const int restart = rs[s];
+        const double* p0 = restart == 0 ? S.rhs : ((restart & 1) ? S.r2 : S.r);
+        const double* xin = restart == 0 ? nullptr : ((restart & 1) ? S.x2 : S.x);
+        double* xout = (restart & 1) ? S.x : S.x2;
+        double cr[SS_MAXL];
+#pragma unroll
+        for (int j = 0; j < SS_MAXL; ++j) cr[j] = c[s][j];
+        const int n = kk[s];
+        for (long long pr = (long long)blockIdx.x * SS_THREADS + threadIdx.x; pr < npairs; pr += stride) {
+            const long long g = pr * 2;  // g, g + 1 share a 32-node group
+            double2 d = xin ? __ldcg(reinterpret_cast<const double2*>(xin + g)) : make_double2(0.0, 0.0);
+            const double2 r = __ldcg(reinterpret_cast<const double2*>(p0 + g));
+            double2 p[SS_MAXL - 1];
+            const double* vb = S.V + (g >> 5) * (a.K * 32) + (g & 31);
+            // coefficients past kk are exact zeros: their directions are not read
+#pragma unroll
+            for (int j = 1; j < SS_MAXL; ++j)
+                p[j - 1] = j < n ? __ldcg(reinterpret_cast<const double2*>(vb + (j - 1) * 32)) : make_double2(0.0, 0.0);
+            d.x += cr[0] * r.x;
+            d.y += cr[0] * r.y;
+#pragma unroll
+            for (int j = 1; j < SS_MAXL; ++j) {
+                d.x += cr[j] * p[j - 1].x;
+                d.y += cr[j] * p[j - 1].y;
+            }
+            __stcg(reinterpret_cast<double2*>(xout + g), d);
+        }
+    }
+}
+
+// r = b' - A d and ||r||^2 of every system with a finished cycle; the last
+// block runs their serial steps (the next restart's convergence test).
+__global__ void __launch_bounds__(SS_THREADS)
+sp_resid_kernel(const SsArgs a) {
+    __shared__ SsSmem sm;
+    __shared__ int act[2], rs[2];
+    if (threadIdx.x < 2) {
+        const int s = threadIdx.x;
+        act[s] = ldc(&a.ctl->sys[s].active) && ldc(&a.ctl->sys[s].ready);
+        rs[s] = ldc(&a.ctl->sys[s].rst);
+    }
+    __syncthreads();
+    if (!act[0] && !act[1]) return;
+    const long long stride = (long long)gridDim.x * SS_THREADS;
+    const long long npairs = a.D / 2;
+    for (int s = 0; s < 2; ++s) {
+        double acc[1] = {0.0};
+        if (act[s]) {
+            const KoSystem& S = a.sys[s];
+            const int restart = rs[s];
+            const double* xd = (restart & 1) ? S.x : S.x2;
+            double* rout = (restart & 1) ? S.r : S.r2;
+            for (long long pr = (long long)blockIdx.x * SS_THREADS + threadIdx.x; pr < npairs; pr += stride) {
+                const long long g = pr * 2;
+                const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+                double rr[2] = {0.0, 0.0};
+                const long long row = (long long)y * a.P;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int xj = x + j;
+                    if (xj >= a.nx) continue;
+                    const long long gj = g + j;
+                    const int xw = xj > 0 ? xj - 1 : a.nx - 1;
+                    const int xe = xj + 1 < a.nx ? xj + 1 : 0;
+                    const double* cf = S.coef + ilv(4, 0, gj);
+                    // rows 0 and ny-1 are solid: their off-diagonals are 0
+                    const double dS = y > 0 ? __ldcg(xd + gj - a.P) : 0.0;
+                    const double dN = y + 1 < a.ny ? __ldcg(xd + gj + a.P) : 0.0;
+                    // CSR order of an interior row: S, W, C, E, N
+                    const double Ad = __ldg(cf + 96) * dS + __ldg(cf + 32) * __ldcg(xd + row + xw) +
+                                      __ldcg(xd + gj) + __ldg(cf) * __ldcg(xd + row + xe) +
+                                      __ldg(cf + 64) * dN;
+                    rr[j] = __ldg(S.rhs + gj) - Ad;
+                }
+                __stcg(reinterpret_cast<double2*>(rout + g), make_double2(rr[0], rr[1]));
+                acc[0] += rr[0] * rr[0] + rr[1] * rr[1];
+            }
+        }
+        sp_block_reduce<1>(acc, a.part, SS_NG * s, sm);
+    }
+    if (!sp_last_block(a.bar)) return;
+    __shared__ double tot[2];
+    __shared__ GmresSys sS[2];
+    sp_sys_load(a.ctl, 0, sS[0]);
+    sp_sys_load(a.ctl, 1, sS[1]);
+    const int warp = threadIdx.x >> 5;
+    if (warp < 2) {
+        const double v = sum_slot_warp(a.part, gridDim.x, SS_NG * warp);
+        if ((threadIdx.x & 31) == 0) tot[warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 && act[threadIdx.x])
+        ss_resid_step(a, sS[threadIdx.x], threadIdx.x, tot[threadIdx.x], rs[threadIdx.x]);
+    if (threadIdx.x == 0) {
+        trace_barrier(a.ctl);
+        __stcg(&a.ctl->passes, ldc(&a.ctl->passes) + 1);
+    }
+    __syncthreads();
+    sp_sys_store(a.ctl, 0, sS[0]);
+    sp_sys_store(a.ctl, 1, sS[1]);
+    if (threadIdx.x == 0) __stcg(&a.ctl->any_active, (int)(sS[0].active || sS[1].active));
+}
+
+// x_new = x0 + d on fluid nodes and 0 on solid-boundary rows, once per
+// system, as soon as it has stopped iterating; a solve that met a NaN
+// residual leaves its field as it was.
+__global__ void __launch_bounds__(SS_THREADS)
+sp_write_kernel(const SsArgs a) {
+    __shared__ int wr[2], hx[2], cy[2];
+    if (threadIdx.x < 2) {
+        const int s = threadIdx.x;
+        const GmresSys* S = &a.ctl->sys[s];
+        wr[s] = !ldc(&S->active) && !ldc(&S->written);
+        cy[s] = ldc(&S->cycles);
+        hx[s] = cy[s] > 0 && !ldc(&S->nan);
+    }
+    __syncthreads();
+    if (!wr[0] && !wr[1]) return;
+    const long long stride = (long long)gridDim.x * SS_THREADS;
+    const long long npairs = a.D / 2;
+    for (int s = 0; s < 2; ++s) {
+        if (!wr[s]) continue;
+        const KoSystem& S = a.sys[s];
+        float* f = static_cast<float*>(a.field[s]);
+        double* f8 = static_cast<double*>(a.field[s]);
+        // the correction of the last of `cycles` updates is in parity `cycles`
+        const double* xf = (cy[s] & 1) ? S.x2 : S.x;
+        for (long long pr = (long long)blockIdx.x * SS_THREADS + threadIdx.x; pr < npairs; pr += stride) {
+            const long long g = pr * 2;
+            const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+            if (x >= a.nx) continue;
+            const unsigned int t2 = *reinterpret_cast<const unsigned int*>(a.ntype + g);
+            const int tt[2] = {(int)(t2 & 0xffff), (int)(t2 >> 16)};
+            const double2 xv = hx[s] ? __ldcg(reinterpret_cast<const double2*>(xf + g)) : make_double2(0.0, 0.0);
+            const double dv[2] = {xv.x, xv.y};
+            for (int j = 0; j < 2; ++j) {
+                if (x + j >= a.nx) continue;
+                if (a.f64) {
+                    if (!(tt[j] & M_SOLID)) f8[g + j] = f8[g + j] + dv[j];
+                    else if (tt[j] & SOLID_BOUNDARY) f8[g + j] = 0.0;
+                } else {
+                    if (!(tt[j] & M_SOLID)) f[g + j] = (float)((double)f[g + j] + dv[j]);
+                    else if (tt[j] & SOLID_BOUNDARY) f[g + j] = 0.f;
+                }
+            }
+        }
+    }
+    if (sp_last_block(a.bar) && threadIdx.x < 2 && wr[threadIdx.x])
+        __stcg(&a.ctl->sys[threadIdx.x].written, 1);
 }
 
 }  // namespace kofm

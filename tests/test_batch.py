@@ -35,10 +35,11 @@ def _cases():
     return out
 
 
-def _open(case, storage=_abi.STORE_FP32):
+def _open(case, storage=_abi.STORE_FP32, form=2):
     kind, ch, f, k, o, nut, rate, g, nu = case
     d = desc_default()
     d.storage = storage
+    d.komega_classic = form
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = rate, g, nu
     d.use_komega = 1 if kind == "komega" else 0
@@ -53,6 +54,8 @@ def _open(case, storage=_abi.STORE_FP32):
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage", [_abi.STORE_FP32, _abi.STORE_FP16_NEQ])
 def test_batch_matches_one_by_one(kofm_lib, storage):
+    """A graph replays the one-launch form of the solve (komega_classic = 2):
+    bit-identical to stepping contexts of that form one by one."""
     cases = _cases()
     solo = [_open(c, storage) for c in cases]
     both = [_open(c, storage) for c in cases]
@@ -86,3 +89,28 @@ def test_batch_needs_stepped_contexts(kofm_lib):
             Batch([L])                          # populations still in the set_state form
     finally:
         L.close()
+
+
+@pytest.mark.gpu
+def test_batch_of_phase_form_contexts_agrees_to_rounding(kofm_lib):
+    """Contexts of the default form (phase launches, stepped on their own)
+    batched: the graph runs the same solve in one launch, whose partial sums
+    group differently; fields agree to rounding (rel-L2 1e-6)."""
+    cases = _cases()
+    solo = [_open(c, form=0) for c in cases]
+    both = [_open(c, form=0) for c in cases]
+    try:
+        for L in solo + both:
+            L.step(1)
+        with Batch(both) as B:
+            B.step(4)
+        for L in solo:
+            L.step(4)
+        for a, b in zip(solo, both):
+            for x, y in zip(a.get_state(), b.get_state()):
+                if x is not None:
+                    x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
+                    assert np.linalg.norm(x - y) <= 1e-6 * max(np.linalg.norm(x), 1e-30)
+    finally:
+        for L in solo + both:
+            L.close()

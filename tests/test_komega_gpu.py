@@ -29,8 +29,9 @@ def channel_case(nx=256, ny=66, u_max=0.05, nu=5e-4):
     return ch, f, k, o, nut, rate, g, nu
 
 
-def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0):
+def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0, form=0):
     d = desc_default()
+    d.komega_classic = form
     d.nx, d.nx_full, d.ny = ch.nx, ch.nx_full, ch.ny
     d.tau, d.fterm, d.mu = rate, g, nu
     d.use_komega = 1
@@ -41,16 +42,21 @@ def make_lattice(ch, rate, g, nu, krylov=10, full_cycle=0):
     return L
 
 
-@pytest.mark.parametrize("full_cycle,nx", [(0, 128), (1, 128), (0, 200), (0, 610)])
-def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle, nx):
-    """nx = 200 and 610 are not multiples of the solver's 30-column strips
-    (periodic tail strip) nor of the 128-node padding; at 610 the strips form
-    three groups of eight and the blocks split the rows of a group."""
+@pytest.mark.parametrize("full_cycle,form,nx", [(0, 0, 128), (0, 2, 128), (0, 1, 128), (1, 0, 128),
+                                                (0, 0, 200), (0, 2, 200), (0, 1, 200), (0, 0, 610),
+                                                (0, 1, 610)])
+def test_one_update_matches_oracle(kofm_lib, oracle, full_cycle, form, nx):
+    """Every solver form (0: a cycle's directions in one sweep, one launch per
+    sweep; 2: the same in one cooperative launch; 1 and full cycles: one
+    vector per sweep).  nx = 200 and 610 are not multiples of the one-vector
+    solver's 30-column strips (periodic tail strip), of the powers sweep's
+    236-column strips, nor of the 128-node padding; at 610 the 30-column strips
+    form three groups of eight and the blocks split the rows of a group."""
     ch, f, k, o, nut, rate, g, nu = channel_case(nx=nx, ny=34)
     cfg = make_cfg(ch.nx, ch.ny, rate, g, nu)
     sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f, k, o, nut, komega=True)
     sim.step(2)
-    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle) as L:
+    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle, form=form) as L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
         L.step(2)
         st = L.stats()
@@ -84,14 +90,14 @@ def _oracle_channel_1000(oracle):
     return _ORACLE_1000["sim"]
 
 
-@pytest.mark.parametrize("full_cycle", [0, 1])
-def test_channel_1000_steps_parity(kofm_lib, oracle, full_cycle):
+@pytest.mark.parametrize("full_cycle,form", [(0, 0), (0, 2), (0, 1), (1, 0)])
+def test_channel_1000_steps_parity(kofm_lib, oracle, full_cycle, form):
     """rho, u, k, omega within rel-L2 1e-5 of the FP64 oracle after 1000
-    steps, with cycles ended at their first truncation (default) and with the
-    reference's full cycles."""
+    steps, with cycles ended at their first truncation (each solver form) and
+    with the reference's full cycles."""
     ch, f, k, o, nut, rate, g, nu = channel_case()
     sim = _oracle_channel_1000(oracle)
-    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle) as L:
+    with make_lattice(ch, rate, g, nu, full_cycle=full_cycle, form=form) as L:
         L.set_state(f, k, o, nut, np.zeros(3 * ch.n))
         L.step(1000)
         rho, ux, uy = L.get_macro()
