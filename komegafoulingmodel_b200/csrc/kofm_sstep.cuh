@@ -96,133 +96,161 @@ __device__ __forceinline__ int ss_first_levels(const SsArgs& a, int s) {
     return l < SS_MINL ? (a.K < SS_MINL ? a.K : SS_MINL) : l;
 }
 
-// ---- coefficient-space simpler GMRES (serial section, one thread per system) --
-// G: (L+1) x (L+1) Gram of p_0 .. p_L (full, symmetric).  Builds the cycle's
-// vectors in order and applies the reference's tests after each (the same
-// cycle_step as the one-vector-per-sweep solver).  Returns the vectors built;
+// ---- coefficient-space simpler GMRES (serial step, one warp per system) --------
+// G: (L+1) x (L+1) Gram of p_0 .. p_L (full, symmetric, row-major in shared
+// memory).  Builds the cycle's vectors in order and applies the reference's
+// tests after each (the same cycle_step as the one-vector-per-sweep solver).
+// Lane i holds coefficient i (on p_i) of every vector; the products with G
+// and the inner products a^T G b are formed across the warp, the scalar
+// tests on lane 0 (S lives in shared memory).  Returns the vectors built;
 // S.done = 0 when L < K vectors passed every test (more powers needed).  On a
 // finished cycle, cP gets the update y_0 r/rho0 + sum_{j>=1} y_j v_{j-1} on
 // p_0 .. p_L.
-__device__ int ss_cycle(GmresSys& S, const double* G, int L, int K, double rel_tol, double* cP) {
+__device__ __forceinline__ double ss_warp_sum(double x) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    return __shfl_sync(0xffffffffu, x, 0);
+}
+
+__device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double rel_tol, double* cP) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const int n = L + 1;
-    double V[SS_MAXL][SS_MAXL + 1];
-    double GV[SS_MAXL][SS_MAXL + 1];
-    double z0[SS_MAXL + 1], w[SS_MAXL + 1], Gw[SS_MAXL + 1];
-    for (int i = 0; i < n; ++i) z0[i] = 0.0;
-    z0[0] = S.rinv;
-    for (int i = 0; i < K * K; ++i) S.R[i] = 0.0;
-    S.rho = 1.0;
-    S.done = 0;
+    const double rinv = S.rinv;
+    const double z0 = lane == 0 ? rinv : 0.0;  // r / ||r|| = p_0 / rho0
     const int iters0 = S.iters;
-    int k = 0;
-    for (; k < L && k < K; ++k) {
+    for (int i = lane; i < K * K; i += 32) S.R[i] = 0.0;
+    __syncwarp();
+    if (lane == 0) {
+        S.rho = 1.0;
+        S.done = 0;
+    }
+    __syncwarp();
+    double V[SS_MAXL], GV[SS_MAXL];
+    int built = 0;
+#pragma unroll
+    for (int k = 0; k < SS_MAXL; ++k) {
+        if (k >= L || k >= K) break;
         // w = A z, z = r / rho0 (k = 0) or v_{k-1}; A p_j = p_j + p_{j+1}
-        const double* z = k == 0 ? z0 : V[k - 1];
-        w[0] = z[0];
-        for (int i = 1; i < n; ++i) w[i] = z[i] + z[i - 1];
-        for (int i = 0; i < n; ++i) {
-            double s = 0.0;
-            for (int j = 0; j < n; ++j) s += G[i * n + j] * w[j];
-            Gw[i] = s;
+        const double z = k == 0 ? z0 : V[k - 1];
+        const double zm = __shfl_up_sync(FULL, z, 1);
+        double w = lane < n ? (lane == 0 ? z : z + zm) : 0.0;
+        double Gw = 0.0;
+        for (int j = 0; j < n; ++j) {
+            const double wj = __shfl_sync(FULL, w, j);
+            if (lane < n) Gw += G[lane * n + j] * wj;
         }
         // classical Gram-Schmidt: R(j, k) = <w, v_j> with the unmodified w
         double h[SS_MAXL];
+#pragma unroll
+        for (int j = 0; j < k; ++j) h[j] = ss_warp_sum(w * GV[j]);
+#pragma unroll
         for (int j = 0; j < k; ++j) {
-            double s = 0.0;
-            for (int i = 0; i < n; ++i) s += w[i] * GV[j][i];
-            h[j] = s;
+            w -= h[j] * V[j];
+            Gw -= h[j] * GV[j];
         }
-        for (int j = 0; j < k; ++j)
-            for (int i = 0; i < n; ++i) {
-                w[i] -= h[j] * V[j][i];
-                Gw[i] -= h[j] * GV[j][i];
-            }
-        double nk2 = 0.0;
-        for (int i = 0; i < n; ++i) nk2 += w[i] * Gw[i];
+        const double nk2 = ss_warp_sum(w * Gw);
         const double nk = nk2 > 0.0 ? sqrt(nk2) : 0.0;  // a vanishing direction cuts (diag test)
-        for (int j = 0; j < k; ++j) S.R[j + k * K] = h[j];
-        S.R[k + k * K] = nk;
         const double inv = nk > 0.0 ? 1.0 / nk : 0.0;
-        double xi = 0.0;
-        for (int i = 0; i < n; ++i) {
-            V[k][i] = w[i] * inv;
-            GV[k][i] = Gw[i] * inv;
-            xi += z0[i] * GV[k][i];
+        V[k] = w * inv;
+        GV[k] = Gw * inv;
+        const double xi = rinv * __shfl_sync(FULL, GV[k], 0);  // z0^T G v_k
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < k; ++j) S.R[j + k * K] = h[j];
+            S.R[k + k * K] = nk;
+            S.xi[k] = xi;
+            cycle_step(S, K, k, rel_tol);
         }
-        S.xi[k] = xi;
-        cycle_step(S, K, k, rel_tol);
+        __syncwarp();
+        built = k + 1;
         if (S.done) break;
     }
-    const int built = S.done ? k + 1 : k;
     if (!S.done) {
-        S.iters = iters0;  // the cycle is re-run with more powers
+        __syncwarp();
+        if (lane == 0) S.iters = iters0;  // the cycle is re-run with more powers
+        __syncwarp();
         return built;
     }
     // coefficient 0 is applied even when the cycle is cut at k = 0, as the
     // reference's update does (its xi(0) then unscaled)
     const int kk = S.kk;
-    for (int i = 0; i < n; ++i) cP[i] = S.c[0] * z0[i];
-    for (int j = 1; j < kk; ++j)
-        for (int i = 0; i < n; ++i) cP[i] += S.c[j] * V[j - 1][i];
+    double cp = S.c[0] * z0;
+#pragma unroll
+    for (int j = 1; j < SS_MAXL; ++j)
+        if (j < kk) cp += S.c[j] * V[j - 1];
+    if (lane < n) cP[lane] = cp;
+    __syncwarp();
     return built;
 }
 
-// One system's serial step after a Gram round: t holds G(i, j) of p_0 .. p_L
-// (slots ss_gslot), the round computed powers lfrom + 1 .. L; `first` marks
-// restart 0's first round, which also takes the restart-0 convergence test
-// from G(0, 0) = ||b'||^2 (GMRESSolver::solve's checkConvergence).  A cycle
-// whose tests have not fired asks for the remaining powers (ext); a finished
-// one leaves its update coefficients on p_0 .. p_L in S.h.
-__device__ __noinline__ void ss_gram_step(const SsArgs& a, GmresSys& S, int s, const double* t, int L,
-                                          int lfrom, bool first) {
-    // this round's powers (level 0 and coefficients in, levels lfrom+1 .. L
-    // out) and Gram (levels 0 .. L in), per node
-    S.abytes += 8.0 + 32.0 + 8.0 * (L - lfrom) + 8.0 * (L + 1);
-    S.powers += L - lfrom;
-    const double rho0 = sqrt(t[0]);
-    if (first) {
-        S.rho0 = rho0;
-        S.norm_rhs = rho0;
-        S.restarts += 1;
-        const double resid = S.rho0 / S.norm_rhs;
-        if (isnan(resid) || S.inject) { S.nan = 1; S.active = 0; }
-        else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
-        else S.cycles += 1;
-    }
-    if (!S.active) {
-        S.lfrom = S.lto = 0;
-        return;
-    }
-    S.rho0 = rho0;
-    S.rinv = 1.0 / rho0;
+// Shared scratch of one warp's serial step.
+struct SsCycleSmem {
     double G[(SS_MAXL + 1) * (SS_MAXL + 1)];
-    const int n = L + 1;
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i <= j; ++i) {
-            const double v = t[ss_gslot(i, j)];
-            G[i * n + j] = v;
-            G[j * n + i] = v;
-        }
     double cP[SS_MAXL + 1];
-    const int built = ss_cycle(S, G, L, a.K, a.rel_tol, cP);
-    S.lev = L;
-    if (!S.done) {
-        S.ext = 1;  // more powers, then the cycle again
-        S.lfrom = L;
-        S.lto = a.K;
-    } else {
-        S.ext = 0;
-        S.vecs += built;
-        S.vec_index_sum += built * (built - 1) / 2;
-        // the update sweep reads c on p_0 .. p_{kk-1}
-        for (int i = 0; i < a.K; ++i) S.h[i] = i < n ? cP[i] : 0.0;
-        int nl = built + 2;
-        nl = nl > a.K ? a.K : nl;
-        __stcg(a.lhint + s, nl);
-        S.lnext = nl;
-        S.ready = 1;
-        S.lfrom = S.lto = 0;
+};
+
+// One system's serial step after a Gram round, run by one warp: t holds
+// G(i, j) of p_0 .. p_L (slots ss_gslot), the round computed powers
+// lfrom + 1 .. L; `first` marks restart 0's first round, which also takes the
+// restart-0 convergence test from G(0, 0) = ||b'||^2 (GMRESSolver::solve's
+// checkConvergence).  A cycle whose tests have not fired asks for the
+// remaining powers (ext); a finished one leaves its update coefficients on
+// p_0 .. p_L in S.h.
+__device__ __noinline__ void ss_gram_step(const SsArgs& a, GmresSys& S, int s, const double* t, int L,
+                                          int lfrom, bool first, SsCycleSmem& cs) {
+    const int lane = threadIdx.x & 31;
+    const double rho0 = sqrt(t[0]);
+    if (lane == 0) {
+        // this round's powers (level 0 and coefficients in, levels lfrom+1 .. L
+        // out) and Gram (levels 0 .. L in), per node
+        S.abytes += 8.0 + 32.0 + 8.0 * (L - lfrom) + 8.0 * (L + 1);
+        S.powers += L - lfrom;
+        if (first) {
+            S.rho0 = rho0;
+            S.norm_rhs = rho0;
+            S.restarts += 1;
+            const double resid = S.rho0 / S.norm_rhs;
+            if (isnan(resid) || S.inject) { S.nan = 1; S.active = 0; }
+            else if (resid <= a.rel_tol || S.rho0 <= a.abs_tol) { S.conv = 1; S.active = 0; }
+            else S.cycles += 1;
+        }
+        if (!S.active) S.lfrom = S.lto = 0;
+        else {
+            S.rho0 = rho0;
+            S.rinv = 1.0 / rho0;
+        }
     }
+    __syncwarp();
+    if (!S.active) return;
+    const int n = L + 1;
+    for (int e = lane; e < n * n; e += 32) {
+        const int i = e / n, j = e - i * n;
+        cs.G[e] = t[i <= j ? ss_gslot(i, j) : ss_gslot(j, i)];
+    }
+    __syncwarp();
+    const int built = ss_cycle_warp(S, cs.G, L, a.K, a.rel_tol, cs.cP);
+    if (lane == 0) {
+        S.lev = L;
+        if (!S.done) {
+            S.ext = 1;  // more powers, then the cycle again
+            S.lfrom = L;
+            S.lto = a.K;
+        } else {
+            S.ext = 0;
+            S.vecs += built;
+            S.vec_index_sum += built * (built - 1) / 2;
+            // the update sweep reads c on p_0 .. p_{kk-1}
+            for (int i = 0; i < a.K; ++i) S.h[i] = i < n ? cs.cP[i] : 0.0;
+            int nl = built + 2;
+            nl = nl > a.K ? a.K : nl;
+            __stcg(a.lhint + s, nl);
+            S.lnext = nl;
+            S.ready = 1;
+            S.lfrom = S.lto = 0;
+        }
+    }
+    __syncwarp();
 }
 
 // One system's serial step after the residual sweep of restart `restart`:
@@ -292,19 +320,20 @@ __device__ void ss_serial(const SsArgs& a, int kind, int restart, int round, int
         if ((threadIdx.x & 31) == 0) tot[slot] = v;
     }
     __syncthreads();
-    // one thread per system (threads 0 and 32: different warps)
-    if ((threadIdx.x & 31) == 0 && warp < 2) {
+    // one warp per system (warps 0 and 1)
+    __shared__ SsCycleSmem cs[2];
+    if (warp < 2) {
         const int s = warp;
         GmresSys& S = sS[s];
         const double* t = tot + SS_NG * s;
-        if (S.active) {
-            if (kind == SS_SER_GRAM && s_L[s] > 0)
-                ss_gram_step(a, S, s, t, s_L[s], round == 0 ? 0 : S.lev, restart == 0 && round == 0);
-            else if (kind == SS_SER_RESID)
-                ss_resid_step(a, S, s, t[0], restart);
+        const bool act = S.active;
+        if (act && kind == SS_SER_GRAM && s_L[s] > 0)
+            ss_gram_step(a, S, s, t, s_L[s], round == 0 ? 0 : S.lev, restart == 0 && round == 0, cs[s]);
+        if ((threadIdx.x & 31) == 0) {
+            if (act && kind == SS_SER_RESID) ss_resid_step(a, S, s, t[0], restart);
+            atomicOr(&s_any, S.active);
+            atomicOr(&s_ext, S.active && S.ext);
         }
-        atomicOr(&s_any, S.active);
-        atomicOr(&s_ext, S.active && S.ext);
     }
     __syncthreads();
     for (int s = 0; s < 2; ++s) {
@@ -368,17 +397,25 @@ __device__ __forceinline__ void ss_cp8(unsigned saddr, const double* gmem) {
 // whose own columns start at x0, from level lfrom (p0 plain, or basis slot
 // lfrom - 1).  Thread t holds column x0 - L + t (periodic); level j is valid
 // on threads j .. 255 - j.  Step tau takes level 0 at row tau and computes
-// level j at row tau - j from level j-1 at rows tau-j-1 (two steps back),
-// tau-j (one step back; x neighbours) and tau-j+1 (this step, this thread).
-// The thread's level-0 value and four coefficients of row tau + SS_PF are
-// copied into its ring slot (cp.async) while row tau computes; level 1 takes
-// the coefficients of its row from the ring and hands them on to the next
-// level one step later in registers (level j uses the row level j-1 used the
-// step before).  Rows outside the lattice are zero.  Level j is stored in
-// basis slot lfrom + j - 1 (interleaved layout).
+// level j at row tau - j from level j-1 at rows tau-j-1, tau-j (x
+// neighbours, by warp shuffles and across warps from the edge buffer the
+// step before wrote) and tau-j+1.  The thread's level-0 value and four
+// coefficients of row tau + SS_PF are copied into its ring slot (cp.async)
+// while row tau computes; level 1 takes the coefficients of its row from the
+// ring and later levels reuse them from registers.  Rows outside the lattice
+// are zero.  Level j is stored in basis slot lfrom + j - 1 (interleaved
+// layout).
+//
+// The step loop is unrolled U = 3 ceil(L / 3) times so that both register
+// windows are circular buffers with compile-time slots: level j's last three
+// rows (row y in slot (step - j) mod 3 of H[j]) and the coefficients of the
+// last U rows (row y in slot (y - t0) mod U).  The step count is rounded up
+// to a multiple of U (the extra steps march past the last row: zero input,
+// nothing stored).
 template <int L>
 __device__ void ss_powers(const SsArgs& a, const KoSystem& S, const double* p0, bool p0_basis,
                           int lfrom, int x0, int own_w, int ya, int yb, SsSmem& sm, double* ring) {
+    constexpr int U = (L + 2) / 3 * 3;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int xs = x0 - L + t;
     const int xc = ((xs % a.nx) + a.nx) % a.nx;
@@ -405,14 +442,14 @@ __device__ void ss_powers(const SsArgs& a, const KoSystem& S, const double* p0, 
             for (int f = 0; f < SS_RF; ++f) myring[(r * SS_RF + f) * SS_THREADS] = 0.0;
         }
     };
-    double cur[L], prv[L], pr2[L];
-    double cE[L], cW[L], cN[L], cS[L];  // level j's row coefficients (rotated down a level per step)
+    double H[L][3];
+    double cE[U], cW[U], cN[U], cS[U];
 #pragma unroll
-    for (int j = 0; j < L; ++j) {
-        cur[j] = 0.0; prv[j] = 0.0; pr2[j] = 0.0;
-        cE[j] = 0.0; cW[j] = 0.0; cN[j] = 0.0; cS[j] = 0.0;
-    }
+    for (int j = 0; j < L; ++j) H[j][0] = H[j][1] = H[j][2] = 0.0;
+#pragma unroll
+    for (int j = 0; j < U; ++j) { cE[j] = 0.0; cW[j] = 0.0; cN[j] = 0.0; cS[j] = 0.0; }
     const int t0 = ya - L, t1 = yb + L;
+    const int nsteps = (t1 - t0 + U - 1) / U * U;
 #pragma unroll 1
     for (int i = 0; i < SS_PF; ++i) {
         issue(t0 + i);
@@ -420,60 +457,68 @@ __device__ void ss_powers(const SsArgs& a, const KoSystem& S, const double* p0, 
     }
     // store address of level 1 at row tau - 1; level j is (j - 1) rows and slots further
     double* vrow = S.V + (long long)(t0 - 1) * vstride + vbase + (long long)lfrom * 32;
-    for (int tau = t0; tau < t1; ++tau, vrow += vstride) {
-        issue(tau + SS_PF);
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(SS_PF) : "memory");  // rows <= tau landed
-        // coefficients: level j takes level j-1's row of the previous step;
-        // level 1 the ring's row tau - 1
+#pragma unroll 1
+    for (int b = 0; b < nsteps; b += U) {
 #pragma unroll
-        for (int j = L - 1; j > 0; --j) { cE[j] = cE[j - 1]; cW[j] = cW[j - 1]; cN[j] = cN[j - 1]; cS[j] = cS[j - 1]; }
-        {
-            const int r1 = (tau - 1) & (SS_RING - 1);
-            const double* q = myring + r1 * SS_RF * SS_THREADS;
-            cE[0] = q[1 * SS_THREADS]; cW[0] = q[2 * SS_THREADS];
-            cN[0] = q[3 * SS_THREADS]; cS[0] = q[4 * SS_THREADS];
-        }
-        pr2[0] = prv[0]; prv[0] = cur[0];
-        cur[0] = myring[(tau & (SS_RING - 1)) * SS_RF * SS_THREADS];
-        __syncthreads();  // the edge values of step tau - 1 are visible
-        const int par = tau & 1;
-        // x neighbours of every level from the previous step (level 0 is
-        // already shifted: its previous value is prv[0]; the others not yet:
-        // cur[j]), then the levels
-        double lft[L], rgt[L];
+        for (int u = 0; u < U; ++u) {
+            const int tau = t0 + b + u;
+            issue(tau + SS_PF);
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(SS_PF) : "memory");  // rows <= tau landed
+            {
+                // coefficients of row tau - 1 (level 1's row)
+                const int c1 = (u + U - 1) % U;
+                const double* q = myring + ((tau - 1) & (SS_RING - 1)) * SS_RF * SS_THREADS;
+                cE[c1] = q[1 * SS_THREADS];
+                cW[c1] = q[2 * SS_THREADS];
+                cN[c1] = q[3 * SS_THREADS];
+                cS[c1] = q[4 * SS_THREADS];
+            }
+            H[0][u % 3] = myring[(tau & (SS_RING - 1)) * SS_RF * SS_THREADS];
+            __syncthreads();  // the edge values of step tau - 1 are visible
+            const int par = tau & 1;
+            const int yl = tau - L;  // the last level's row
+            const bool st_row = own && tau - 1 >= ya && yl < yb;
+            // x neighbours of every level at its row of the step before
+            // (level j at row tau - 1 - j)
+            double lft[L], rgt[L];
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            const double mine = j == 0 ? prv[0] : cur[j];
-            lft[j] = __shfl_up_sync(0xffffffffu, mine, 1);
-            rgt[j] = __shfl_down_sync(0xffffffffu, mine, 1);
-        }
-        if (lane == 0) {
+            for (int j = 0; j < L; ++j) {
+                const double mine = H[j][((u - 1 - j) % 3 + 3) % 3];
+                lft[j] = __shfl_up_sync(0xffffffffu, mine, 1);
+                rgt[j] = __shfl_down_sync(0xffffffffu, mine, 1);
+            }
+            if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < L; ++j) lft[j] = w > 0 ? sm.edge[par ^ 1][w - 1][1][j] : 0.0;
-        }
-        if (lane == 31) {
+                for (int j = 0; j < L; ++j) lft[j] = w > 0 ? sm.edge[par ^ 1][w - 1][1][j] : 0.0;
+            }
+            if (lane == 31) {
 #pragma unroll
-            for (int j = 0; j < L; ++j) rgt[j] = w < SS_WARPS - 1 ? sm.edge[par ^ 1][w + 1][0][j] : 0.0;
-        }
-        const int yl = tau - L;  // the last level's row
-        const bool st_row = own && tau - 1 >= ya && yl < yb;
+                for (int j = 0; j < L; ++j) rgt[j] = w < SS_WARPS - 1 ? sm.edge[par ^ 1][w + 1][0][j] : 0.0;
+            }
 #pragma unroll
-        for (int j = 1; j <= L; ++j) {
-            const int y = tau - j;
-            // N p in the CSR order of an interior row without its centre: S, W, E, N
-            const double v = cS[j - 1] * pr2[j - 1] + cW[j - 1] * lft[j - 1] + cE[j - 1] * rgt[j - 1] +
-                             cN[j - 1] * cur[j - 1];
-            if (j < L) { pr2[j] = prv[j]; prv[j] = cur[j]; cur[j] = v; }
-            if (st_row && y >= ya && y < yb) __stcg(vrow - (long long)(j - 1) * vstride + (j - 1) * 32, v);
-        }
-        if (lane == 0) {
+            for (int j = 1; j <= L; ++j) {
+                const int y = tau - j;
+                // level j-1 at rows y + 1 (newest) and y - 1
+                const int sN = ((u - (j - 1)) % 3 + 3) % 3;
+                const int sS = ((u - j - 1) % 3 + 3) % 3;
+                const int cs = ((u - j) % U + U) % U;
+                // N p in the CSR order of an interior row without its centre: S, W, E, N
+                const double v = cS[cs] * H[j - 1][sS] + cW[cs] * lft[j - 1] + cE[cs] * rgt[j - 1] +
+                                 cN[cs] * H[j - 1][sN];
+                if (j < L) H[j][((u - j) % 3 + 3) % 3] = v;
+                if (st_row && y >= ya && y < yb) __stcg(vrow - (long long)(j - 1) * vstride + (j - 1) * 32, v);
+            }
+            // level j's newest row (tau - j) for the neighbours' next step
+            if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < L; ++j) sm.edge[par][w][0][j] = cur[j];
-        }
-        if (lane == 31) {
+                for (int j = 0; j < L; ++j) sm.edge[par][w][0][j] = H[j][((u - j) % 3 + 3) % 3];
+            }
+            if (lane == 31) {
 #pragma unroll
-            for (int j = 0; j < L; ++j) sm.edge[par][w][1][j] = cur[j];
+                for (int j = 0; j < L; ++j) sm.edge[par][w][1][j] = H[j][((u - j) % 3 + 3) % 3];
+            }
+            vrow += vstride;
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -891,7 +936,10 @@ sp_powers_kernel(const SsArgs a, int s) {
 }
 
 // Gram of p_0 .. p_L of system s; the last block runs the system's serial
-// step (the simpler-GMRES cycle in the power basis).
+// step (the simpler-GMRES cycle in the power basis, one warp).  Each block
+// takes a fixed contiguous range of nodes (deterministic sums); a thread
+// takes one node per iteration (two for L <= 6, where the registers allow),
+// its L + 1 loads in flight together.
 template <int L>
 __global__ void __launch_bounds__(SS_THREADS)
 sp_gram_kernel(const SsArgs a, int s) {
@@ -901,8 +949,8 @@ sp_gram_kernel(const SsArgs a, int s) {
     if (!sp_round(a, s, L, false, lf, lt, rst)) return;
     const KoSystem& S = a.sys[s];
     const double* p0 = rst == 0 ? S.rhs : ((rst & 1) ? S.r2 : S.r);
+    const int tid = threadIdx.x;
     {
-        // a fixed contiguous node range per block (deterministic sums)
         const long long n32 = a.D / 32;
         const long long g0 = n32 * blockIdx.x / gridDim.x * 32;
         const long long g1 = n32 * (blockIdx.x + 1) / gridDim.x * 32;
@@ -917,14 +965,15 @@ sp_gram_kernel(const SsArgs a, int s) {
     __shared__ double tot[SS_NG];
     __shared__ GmresSys sS;
     sp_sys_load(a.ctl, s, sS);
-    const int warp = threadIdx.x >> 5;
+    const int warp = tid >> 5;
     for (int i = warp; i < NGL; i += SS_WARPS) {
         const double v = sum_slot_warp(a.part, gridDim.x, i);
-        if ((threadIdx.x & 31) == 0) tot[i] = v;
+        if ((tid & 31) == 0) tot[i] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        ss_gram_step(a, sS, s, tot, L, lf, rst == 0 && lf == 0);
+    __shared__ SsCycleSmem cs;
+    if (warp == 0) ss_gram_step(a, sS, s, tot, L, lf, rst == 0 && lf == 0, cs);
+    if (tid == 0) {
         trace_barrier(a.ctl);
         __stcg(&a.ctl->passes, ldc(&a.ctl->passes) + 1);
     }
@@ -999,8 +1048,9 @@ sp_resid_kernel(const SsArgs a) {
     }
     __syncthreads();
     if (!act[0] && !act[1]) return;
-    const long long stride = (long long)gridDim.x * SS_THREADS;
-    const long long npairs = a.D / 2;
+    // units of (row, chunk of 2 x 256 columns): one 32-bit division per unit
+    const int cpr = (a.P / 2 + SS_THREADS - 1) / SS_THREADS;
+    const int units = a.ny * cpr;
     for (int s = 0; s < 2; ++s) {
         double acc[1] = {0.0};
         if (act[s]) {
@@ -1008,9 +1058,11 @@ sp_resid_kernel(const SsArgs a) {
             const int restart = rs[s];
             const double* xd = (restart & 1) ? S.x : S.x2;
             double* rout = (restart & 1) ? S.r : S.r2;
-            for (long long pr = (long long)blockIdx.x * SS_THREADS + threadIdx.x; pr < npairs; pr += stride) {
-                const long long g = pr * 2;
-                const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+            for (int u = blockIdx.x; u < units; u += gridDim.x) {
+                const int y = u / cpr;
+                const int x = ((u - y * cpr) * SS_THREADS + threadIdx.x) * 2;
+                if (x >= a.P) continue;
+                const long long g = (long long)y * a.P + x;
                 double rr[2] = {0.0, 0.0};
                 const long long row = (long long)y * a.P;
 #pragma unroll
@@ -1074,8 +1126,8 @@ sp_write_kernel(const SsArgs a) {
     }
     __syncthreads();
     if (!wr[0] && !wr[1]) return;
-    const long long stride = (long long)gridDim.x * SS_THREADS;
-    const long long npairs = a.D / 2;
+    const int cpr = (a.P / 2 + SS_THREADS - 1) / SS_THREADS;
+    const int units = a.ny * cpr;
     for (int s = 0; s < 2; ++s) {
         if (!wr[s]) continue;
         const KoSystem& S = a.sys[s];
@@ -1083,10 +1135,11 @@ sp_write_kernel(const SsArgs a) {
         double* f8 = static_cast<double*>(a.field[s]);
         // the correction of the last of `cycles` updates is in parity `cycles`
         const double* xf = (cy[s] & 1) ? S.x2 : S.x;
-        for (long long pr = (long long)blockIdx.x * SS_THREADS + threadIdx.x; pr < npairs; pr += stride) {
-            const long long g = pr * 2;
-            const int y = (int)(g / a.P), x = (int)(g - (long long)y * a.P);
+        for (int u = blockIdx.x; u < units; u += gridDim.x) {
+            const int y = u / cpr;
+            const int x = ((u - y * cpr) * SS_THREADS + threadIdx.x) * 2;
             if (x >= a.nx) continue;
+            const long long g = (long long)y * a.P + x;
             const unsigned int t2 = *reinterpret_cast<const unsigned int*>(a.ntype + g);
             const int tt[2] = {(int)(t2 & 0xffff), (int)(t2 >> 16)};
             const double2 xv = hx[s] ? __ldcg(reinterpret_cast<const double2*>(xf + g)) : make_double2(0.0, 0.0);
