@@ -211,12 +211,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    solver_launches = 0
+    launches0 = L.stats().solver_launches_total if w.komega else 0
     e0.record(stream)
     for _ in range(args.steps):
         L.step(1)
-        if w.komega:  # host-side counters of the step just enqueued and finished
-            solver_launches += L.stats().solver_launches
     e1.record(stream)
     L.sync()
     torch.cuda.synchronize()
@@ -224,10 +222,12 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local_rank}")
     st = L.stats()
+    solver_launches = (st.solver_launches_total - launches0) if w.komega else 0
     value = replica_value(nodes, args.steps, world, ms)
-    # kernels of one kofm_step: collide, assembly and the solver's launches
-    # (counted per step: the phase-launch solver enqueues one round per pass)
-    launches_per_step = (2 + solver_launches / args.steps) if w.komega else 1
+    # kernels of the timed steps: one collide per step plus the k-omega
+    # updates' kernels (assembly, solver, the graph's control kernels), which
+    # the library counts on the device
+    launches_per_step = (1 + solver_launches / args.steps) if w.komega else 1
     if args.thermal:  # assembly, control-block init and BiCGStab per solve
         launches_per_step += 3 * max(1, st.thermal_solves)
 

@@ -183,8 +183,10 @@ typedef struct kofm_stats {
                                            array its sweeps stream, counted once per sweep */
     int32_t omega_powers, k_powers;     /* one-sweep cycles: powers computed (all rounds) */
     int32_t solver_launches;            /* kernel launches of the last k-omega solve */
-    int32_t solver_rounds;              /* host round trips of the last solve (phase
-                                           launches: rounds enqueued; 1 otherwise) */
+    int32_t solver_rounds;              /* rounds of the last solve (phase launches:
+                                           powers + Gram + update sweeps; 1 otherwise) */
+    int64_t solver_launches_total;      /* kernel launches of all k-omega updates
+                                           since the state was loaded */
 } kofm_stats;
 
 int kofm_abi_version(void);

@@ -76,6 +76,7 @@ class KofmStats(C.Structure):
         ("thermal_dt", C.c_double), ("thermal_residual", C.c_double),
         ("solver_bytes_per_node", C.c_double), ("omega_powers", C.c_int32), ("k_powers", C.c_int32),
         ("solver_launches", C.c_int32), ("solver_rounds", C.c_int32),
+        ("solver_launches_total", C.c_int64),
     ]
 
 

@@ -32,6 +32,8 @@ int ss_solver_alloc(double** part, int** lhint, int* nblocks, int* pstrips, int*
                     int ny, int K, int dev, int max_blocks);
 int sp_solver_alloc(kofm_ctx* c);
 void ko_system_free(KoSystem* s);
+static int ug_pull(kofm_ctx* c);
+static void ug_reset(kofm_ctx* c);
 }  // namespace kofm
 
 namespace {
@@ -114,6 +116,13 @@ struct kofm_ctx {
     int ss_blocks = 0, ss_pstrips = 0, ss_prows = 0;
     SsLaunch sp{};                    // the same solver as separate phase launches
     int ss_hint[2] = {0, 0};          // host copy of ss_lhint (first-round powers)
+    // the k-omega update as a device-driven CUDA graph (kofm_stepgraph.inc)
+    KoStepState* kst = nullptr;       // sub-stepping state (device)
+    KoStepState* h_kst = nullptr;     // pinned copy
+    cudaGraph_t ug = nullptr;
+    cudaGraphExec_t ugx = nullptr;
+    bool ug_pending = false;          // updates launched since the state was last read back
+    long long launches_host = 0;      // k-omega kernel launches the host loop made since set_state
     int steps_per_lb = 1;
     int time_since_change = 0;
     double dt = 1.0;
@@ -559,12 +568,15 @@ int kofm_destroy(kofm_ctx* c) {
                     c->tr0, c->tp[0], c->tp[1], c->tv[0], c->tv[1], c->ts, c->tcoef,
                     c->dxrec0_idx, c->dxrec0, c->tctl, c->tpart, c->tbar, c->shear_idx,
                     c->adj.cps, c->adj.seg, c->adj.lam, c->adj.nu, c->adj.jpart, c->adj.dq, c->adj.sgrad, c->adj.cls,
-                    c->ibb_node, c->geo_walls, c->geo_rows};
+                    c->ibb_node, c->geo_walls, c->geo_rows, c->kst};
+    if (c->ugx) cudaGraphExecDestroy(c->ugx);
+    if (c->ug) cudaGraphDestroy(c->ug);
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int s = 0; s < 2; ++s) ko_system_free(&c->sys[s]);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_ctl) cudaFreeHost(c->h_ctl);
+    if (c->h_kst) cudaFreeHost(c->h_kst);
     if (c->h_tctl) cudaFreeHost(c->h_tctl);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -642,10 +654,13 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
                              d->nx, d->ny, d->krylov_dim, c->dev, d->solver_max_blocks);
         if (!s2) s2 = sp_solver_alloc(c);
         if (s2) { kofm_destroy(c); return s2; }
-        if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess) {
+        if (cudaMallocHost(&c->h_ctl, sizeof(GmresControl)) != cudaSuccess ||
+            cudaMallocHost(&c->h_kst, sizeof(KoStepState)) != cudaSuccess) {
             kofm_destroy(c);
             return KOFM_ERR_BUFFER_ALLOCATION;
         }
+        memset(c->h_kst, 0, sizeof(KoStepState));
+        ALLOC(c->kst, 1);
     }
     if (d->use_thermal) {
         ALLOC(c->T, D);
@@ -867,6 +882,12 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
     c->steps_per_lb = (int)(1.0 / d.komega_dt);
     if (c->steps_per_lb < 1) c->steps_per_lb = 1;
     c->time_since_change = 0;
+    if (d.use_komega) {
+        ug_pull(c);  // updates still in flight finish first
+        ug_reset(c);
+        c->launches_host = 0;
+        c->stats.solver_launches_total = 0;
+    }
     return KOFM_OK;
 }
 
@@ -1122,11 +1143,17 @@ int kofm_sync(kofm_ctx* c) {
         fprintf(stderr, "kofm: stream error: %s\n", cudaGetErrorString(e));
         return KOFM_ERR_CALLING_KERNEL;
     }
+    // the status the device-driven k-omega updates stopped with, if any
+    if (c->desc.use_komega) return ug_pull(c);
     return KOFM_OK;
 }
 
 int kofm_get_stats(kofm_ctx* c, kofm_stats* out) {
     if (!c || !out) return KOFM_ERR_INVALID_ARG;
+    if (c->desc.use_komega) {
+        cudaSetDevice(c->dev);
+        ug_pull(c);
+    }
     c->stats.steps_per_lb = c->steps_per_lb;
     c->stats.time_since_change = c->time_since_change;
     c->stats.dt = c->dt;

@@ -84,6 +84,8 @@ struct GmresControl {
     int any_active;
     int ntrace;       // grid barriers recorded in trace
     int any_ext;      // one-sweep cycle: a system asks for more powers
+    int rounds;       // phase-launch solve: rounds run
+    int launches;     // phase-launch solve: kernel launches of the solve
     int pad;
     unsigned long long t_start;           // %globaltimer at the first block's start (ns)
     unsigned long long trace[GM_TRACE];   // %globaltimer at each grid barrier's release

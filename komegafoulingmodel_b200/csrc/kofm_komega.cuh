@@ -71,6 +71,7 @@ struct AsmParams {
     int nx, ny, P;
     long long D;
     double mu, dt;
+    const double* dt_dev;  // when set, the time step is read here (device-driven updates)
 };
 
 struct Fd3 {
@@ -303,7 +304,7 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     Pk = dmaxr(dminr(Pk, 10. * KO_BETA_STAR * kv * om), 0.0);
     const double gam = (f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2) / nt;
     double Sc = -KO_BETA_STAR * om;
-    double dt = p.dt;
+    double dt = p.dt_dev ? __ldg(p.dt_dev) : p.dt;
 
     double Kc = 1. + dt * (Jxk * X.c + Jyk * Y.c - dk * (X2.c + Y2.c)) - Sc;
     double Ke = dt * (Jxk * X.e - dk * X2.e);

@@ -877,14 +877,36 @@ __device__ __forceinline__ void sp_block_reduce(const double (&v)[N], double* pa
     __syncthreads();
 }
 
+// Sub-stepping state of one context (device memory; the host pushes a reset
+// when a state is loaded and reads it back when it synchronises).
+struct KoStepState {
+    double dt;             // kOmega::timeStep (first member: the assembly reads it by address)
+    int steps_per_lb;      // kOmega::stepsPerLB
+    int time_since_change; // kOmega::timeSinceTimeStepChange
+    int cur;               // sub-step of the running update
+    int status;            // KOFM_OK, or the error that stopped updates (sticky until a reset)
+    int fail_solves;       // kofm_debug_fail_solves: solves still to report a NaN
+    int fail_mask;
+    int substeps;          // solves of the last update
+    int launches;          // kernel launches of the last update
+    long long updates;     // updates run since the last reset
+    long long launches_total;  // kernel launches of all updates since the last reset
+};
+
 // Control block of a solve: both systems iterating, restart 0, first round
-// of L0 / L1 powers (chosen by the host from the cycle lengths seen so far).
-__global__ void sp_init_kernel(GmresControl* ctl, GridBarrier* bar, int inject, int L0, int L1) {
+// of L0 / L1 powers (chosen by the host from the cycle lengths seen so far);
+// a pending failure injection (kofm_debug_fail_solves) is taken from st.
+__global__ void sp_init_kernel(GmresControl* ctl, GridBarrier* bar, KoStepState* st, int L0, int L1) {
     constexpr int NW = (int)(sizeof(GmresControl) / sizeof(unsigned int));
     unsigned int* w = reinterpret_cast<unsigned int*>(ctl);
     for (int i = threadIdx.x; i < NW; i += blockDim.x) w[i] = 0u;
     __syncthreads();
     if (threadIdx.x == 0) {
+        int inject = 0;
+        if (st->fail_solves > 0) {
+            inject = st->fail_mask;
+            st->fail_solves--;
+        }
         for (int s = 0; s < 2; ++s) {
             ctl->sys[s].active = 1;
             ctl->sys[s].inject = (inject >> s) & 1;
@@ -1158,6 +1180,160 @@ sp_write_kernel(const SsArgs a) {
     }
     if (sp_last_block(a.bar) && threadIdx.x < 2 && wr[threadIdx.x])
         __stcg(&a.ctl->sys[threadIdx.x].written, 1);
+}
+
+// ---- the update as a device-driven graph -------------------------------------------------
+// kOmega::Solve (kOmega.cpp:31-73: the doubling test, then sub-steps of
+// assembly + both solves, halving dt on a NaN residual) with every decision
+// taken on the device: these kernels set the conditions of the graph's WHILE
+// and SWITCH nodes (cudaGraphSetConditional), so a time step needs no host
+// round trip.  The loops are bounded by counters the kernels keep: a solve by
+// its round cap, an update by the halving cap (steps_per_lb <= 2^20) and a
+// total of KU_MAX_SUBSTEPS solves.
+
+constexpr int KU_MAX_SUBSTEPS = (1 << 21) + 64;  // above any sequence the halving cap allows
+
+__global__ void ku_reset_kernel(KoStepState* st, double dt, int steps_per_lb) {
+    if (threadIdx.x) return;
+    st->dt = dt;
+    st->steps_per_lb = steps_per_lb;
+    st->time_since_change = 0;
+    st->cur = 0;
+    st->status = 0;
+    st->substeps = 0;
+    st->launches = 0;
+    st->updates = 0;
+    st->launches_total = 0;
+}
+
+__global__ void ku_fail_kernel(KoStepState* st, int n, int mask) {
+    if (threadIdx.x) return;
+    st->fail_solves = n;
+    st->fail_mask = mask;
+}
+
+// Start of an update: the doubling test (doubleTimeStep, kOmega.cpp:401-414)
+// and the sub-step loop's condition.
+__global__ void ku_begin_kernel(KoStepState* st, cudaGraphConditionalHandle sub) {
+    if (threadIdx.x) return;
+    if (st->status) {
+        cudaGraphSetConditional(sub, 0);
+        return;
+    }
+    st->time_since_change++;
+    if (st->time_since_change >= 20) {
+        st->time_since_change = 0;
+        if (st->steps_per_lb != 1) {
+            st->steps_per_lb /= 2;
+            st->dt *= 2.0;
+        }
+    }
+    st->cur = 0;
+    st->substeps = 0;
+    st->launches = 1;  // this kernel
+    st->launches_total++;
+    st->updates++;
+    cudaGraphSetConditional(sub, st->cur < st->steps_per_lb ? 1u : 0u);
+}
+
+// Control block of one solve (as sp_init_kernel), the first round's levels
+// from the cycle lengths kept per system, a pending failure injection, and
+// the round loop's condition.
+__global__ void ku_init_kernel(GmresControl* ctl, GridBarrier* bar, KoStepState* st, const int* lhint, int K,
+                               cudaGraphConditionalHandle round) {
+    constexpr int NW = (int)(sizeof(GmresControl) / sizeof(unsigned int));
+    unsigned int* w = reinterpret_cast<unsigned int*>(ctl);
+    for (int i = threadIdx.x; i < NW; i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int inject = 0;
+        if (st->fail_solves > 0) {
+            inject = st->fail_mask;
+            st->fail_solves--;
+        }
+        for (int s = 0; s < 2; ++s) {
+            int l = lhint[s];
+            l = l <= 0 || l > K ? K : l;
+            l = l < SS_MINL ? (K < SS_MINL ? K : SS_MINL) : l;
+            ctl->sys[s].active = 1;
+            ctl->sys[s].inject = (inject >> s) & 1;
+            ctl->sys[s].lto = l;
+        }
+        ctl->any_active = 1;
+        ctl->t_start = globaltimer_ns();
+        bar->count = 0u;
+        bar->gen = 0u;
+        cudaGraphSetConditional(round, 1u);
+    }
+}
+
+// The kernels of this round: SWITCH values L - 1 for the powers sweep of L
+// levels and the Gram sweep of p_0 .. p_L of each system (SS_MAXL: none).
+__global__ void ku_select_kernel(GmresControl* ctl, cudaGraphConditionalHandle p0, cudaGraphConditionalHandle p1,
+                                 cudaGraphConditionalHandle g0, cudaGraphConditionalHandle g1) {
+    if (threadIdx.x) return;
+    int n = 5;  // select, update, residual, write-back, end
+    unsigned pv[2], gv[2];
+    for (int s = 0; s < 2; ++s) {
+        const GmresSys& S = ctl->sys[s];
+        const bool run = S.active && S.lto > S.lfrom;
+        pv[s] = run ? (unsigned)(S.lto - S.lfrom - 1) : (unsigned)SS_MAXL;
+        gv[s] = run ? (unsigned)(S.lto - 1) : (unsigned)SS_MAXL;
+        n += run ? 2 : 0;
+    }
+    ctl->launches += n;
+    cudaGraphSetConditional(p0, pv[0]);
+    cudaGraphSetConditional(p1, pv[1]);
+    cudaGraphSetConditional(g0, gv[0]);
+    cudaGraphSetConditional(g1, gv[1]);
+}
+
+// End of a round: the round loop goes on while a system iterates, up to
+// max_rounds (a solve past that cap, or a failed sweep, stops the update).
+__global__ void ku_round_end_kernel(GmresControl* ctl, KoStepState* st, int max_rounds,
+                                    cudaGraphConditionalHandle round) {
+    if (threadIdx.x) return;
+    const int r = ++ctl->rounds;
+    const bool any = ctl->sys[0].active || ctl->sys[1].active;
+    unsigned go = any ? 1u : 0u;
+    if (ctl->error) {
+        st->status = ctl->error == 2 ? KOFM_ERR_STATE : KOFM_ERR_TIMEOUT;
+        go = 0u;
+    } else if (any && r >= max_rounds) {
+        st->status = KOFM_ERR_STATE;
+        go = 0u;
+    }
+    cudaGraphSetConditional(round, go);
+}
+
+// End of a sub-step: halveTimeStep on a NaN residual (omega first, then k;
+// kOmega.cpp:68-70, 387-399), the halving cap, and the sub-step loop's
+// condition.
+__global__ void ku_substep_kernel(const GmresControl* ctl, KoStepState* st, cudaGraphConditionalHandle sub) {
+    if (threadIdx.x) return;
+    const int n = ctl->launches + 3;  // the rounds' kernels + assembly, control-block init, this kernel
+    st->launches += n;
+    st->launches_total += n;
+    st->substeps++;
+    if (st->status) {
+        cudaGraphSetConditional(sub, 0u);
+        return;
+    }
+    for (int s = 0; s < 2; ++s) {
+        if (ctl->sys[s].nan) {
+            st->steps_per_lb *= 2;
+            st->dt /= 2.0;
+            st->cur = 0;
+            st->time_since_change = 0;
+        }
+    }
+    if (st->steps_per_lb > (1 << 20) || st->substeps >= KU_MAX_SUBSTEPS) {
+        st->status = KOFM_ERR_NAN;  // runaway halving
+        cudaGraphSetConditional(sub, 0u);
+        return;
+    }
+    st->cur++;
+    cudaGraphSetConditional(sub, st->cur < st->steps_per_lb ? 1u : 0u);
 }
 
 }  // namespace kofm

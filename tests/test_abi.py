@@ -42,7 +42,7 @@ def test_host_only_calls(kofm_lib):
     assert (d.pr_number, d.pr_turb_number, d.t_in, d.thermal_dt) == (0.708, 0.9, 2.0, 1.0)
     assert abs(d.thermal_rel_tol - 1e-4) < 1e-18 and abs(d.thermal_abs_tol - 1e-7) < 1e-20
     # the Python mirror of the structs has the C sizes
-    assert C.sizeof(_abi.KofmDesc) == 168 and C.sizeof(_abi.KofmStats) == 168
+    assert C.sizeof(_abi.KofmDesc) == 168 and C.sizeof(_abi.KofmStats) == 176
     assert abs(d.komega_rel_tol - 1e-4) < 1e-18 and abs(d.komega_abs_tol - 1e-7) < 1e-20
     assert d.max_turb_visc == 10.0
     assert kofm_lib.kofm_error_string(-204) == b"bounded device wait expired"
