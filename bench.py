@@ -107,10 +107,15 @@ STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
 
 def workload_config(w, args, world: int) -> dict:
     """The `config` object of both arms' JSON lines."""
+    # resident bytes per node: populations (two buffers), node fields and, for
+    # k-omega, both systems' solver vectors (coefficients, b', r, x twice, basis)
+    per_node = 2 * 9 * STORE_BYTES.get(args.storage, 4) + 60 + (2 * 8 * (4 + 5 + 10) if w.komega else 0)
+    big = per_node * w.nodes > 126e6
     cfg = {"workload": w.name, "nx": w.channel.nx, "ny": w.channel.ny, "nodes": w.nodes,
            "storage": STORAGE_NAMES[args.storage], "krylov_dim": 10, "rel_tol": 1.0e-4,
            "abs_tol": 1.0e-7, "parallelism": f"replicas x{world}",
-           "l2": "inputs larger than L2 (populations and solver vectors), no flush"}
+           "l2": ("inputs larger than L2 (populations and solver vectors), no flush" if big else
+                  "working set within the 126 MB L2, no flush: steps of an L2-resident lattice")}
     if getattr(args, "thermal", False):
         cfg["thermal"] = "implicit FD temperature update every step (BiCGStab to 1e-4)"
     return cfg
@@ -160,6 +165,9 @@ SOLVER_TRAFFIC_RATIO = {
     "sstep_phases": None,                          # the same, one launch per sweep
 }
 
+STORE_BYTES = {"fp32": 4, "fp16": 2, "bf16": 2, "fp16neq": 2, "fp16neq32": 2, "fp64": 8}
+# laminar collide (no macro fields saved by the plain step): f read + write, flags
+LB_BYTES_LAMINAR = {"fp32": 74, "fp16": 38, "bf16": 38, "fp16neq": 62, "fp16neq32": 62, "fp64": 146}
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
             "fp16neq": 114, "fp16neq32": 114,  # + reference moments read and written
             "fp64": 250}                      # FP64 populations and fields
@@ -187,8 +195,9 @@ def run_ours(args, rank, world, local_rank):
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
     d.device = local_rank
-    d.komega_classic = {"sstep": 0, "classic": 1, "sstep_coop": 2}[args.solver]
-    solver_kernel = {"sstep": "sstep_phases", "classic": "gmres_kernel", "sstep_coop": "sstep_kernel"}[args.solver]
+    d.komega_classic = {"sstep": 0, "classic": 1, "sstep_coop": 2, "sstep_host": 3}[args.solver]
+    solver_kernel = {"sstep": "sstep_phases", "classic": "gmres_kernel", "sstep_coop": "sstep_kernel",
+                     "sstep_host": "sstep_phases"}[args.solver]
     d.use_thermal = 1 if args.thermal else 0
     L = Lattice(d)
     W.apply(L, w)
@@ -237,20 +246,23 @@ def run_ours(args, rank, world, local_rank):
     passes, bytes_solver = [], []
     for i in range(nb):
         ev[i][0].record(stream)
-        L.lb_step(_abi.OPTION_SAVE_MACRO_FIELDS)
+        L.lb_step(_abi.OPTION_SAVE_MACRO_FIELDS if w.komega else 0)
         ev[i][1].record(stream)
-        L.komega_assemble(1.0)
+        if w.komega:
+            L.komega_assemble(1.0)
         ev[i][2].record(stream)
-        L.komega_solve(raise_on_error=False)
+        if w.komega:
+            L.komega_solve(raise_on_error=False)
         ev[i][3].record(stream)
-        s = L.stats()
-        passes.append(s.solver_passes)
-        bytes_solver.append(s.solver_bytes_per_node)
+        if w.komega:
+            s = L.stats()
+            passes.append(s.solver_passes)
+            bytes_solver.append(s.solver_bytes_per_node)
     torch.cuda.synchronize()
     t_lb = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(nb)) / nb
     t_as = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(nb)) / nb
     t_sv = sum(ev[i][2].elapsed_time(ev[i][3]) for i in range(nb)) / nb
-    b_sv = sum(bytes_solver) / nb
+    b_sv = sum(bytes_solver) / nb if bytes_solver else 0.0
     thermal = None
     if args.thermal:
         tev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(nb)]
@@ -269,16 +281,16 @@ def run_ours(args, rank, world, local_rank):
                    "checks_by_update": tchecks,
                    "kernels": "thermal_assemble_kernel + bicgstab_kernel (+ T copy, control init)"}
     peak, peak_kind = measured_peaks()
-    kern = {
-        "lb_step_kernel": {"ms": t_lb, "bytes_per_node": LB_BYTES[args.storage],
-                           "gbs": LB_BYTES[args.storage] * nodes / (t_lb * 1e-3) / 1e9},
-        "komega_assemble_kernel": {"ms": t_as, "bytes_per_node": asm_bytes,
-                                   "gbs": asm_bytes * nodes / (t_as * 1e-3) / 1e9},
-        solver_kernel: {"ms": t_sv, "bytes_per_node": b_sv,
-                        "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
-                        "passes": sum(passes) / nb,
-                        "bytes_per_node_by_launch": bytes_solver},
-    }
+    lb_bytes = LB_BYTES[args.storage] if w.komega else LB_BYTES_LAMINAR[args.storage]
+    kern = {"lb_step_kernel": {"ms": t_lb, "bytes_per_node": lb_bytes,
+                               "gbs": lb_bytes * nodes / (t_lb * 1e-3) / 1e9}}
+    if w.komega:
+        kern["komega_assemble_kernel"] = {"ms": t_as, "bytes_per_node": asm_bytes,
+                                          "gbs": asm_bytes * nodes / (t_as * 1e-3) / 1e9}
+        kern[solver_kernel] = {"ms": t_sv, "bytes_per_node": b_sv,
+                               "gbs": b_sv * nodes / (t_sv * 1e-3) / 1e9,
+                               "passes": sum(passes) / nb,
+                               "bytes_per_node_by_launch": bytes_solver}
     dom = max(kern, key=lambda k: kern[k]["ms"])
     ratio = SOLVER_TRAFFIC_RATIO.get(dom)
     roof = {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak,
@@ -287,17 +299,17 @@ def run_ours(args, rank, world, local_rank):
             "traffic_source": "ncu dram bytes / algorithmic bytes of one launch on "
                               "komega_straight_8192x512, times this run's average launch",
             "bytes_per_node": kern[dom]["bytes_per_node"]}
-    step_bytes = LB_BYTES[args.storage] + asm_bytes + b_sv
+    step_bytes = lb_bytes + (asm_bytes + b_sv if w.komega else 0.0)
     step_ms = t_lb + t_as + t_sv
 
     # ---- end to end through the public API with host buffers ---------------------
     e2e = None
     if not args.no_e2e:
         n = w.channel.n
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        pin = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
         hf, hk, ho, hn, hs = pin(w.f), pin(w.k), pin(w.omega), pin(w.nut), pin(w.sxy)
         hr, hu = torch.empty(n, dtype=torch.float64).pin_memory(), torch.empty(n, dtype=torch.float64).pin_memory()
-        dp = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_double))  # noqa: E731
+        dp = lambda t: None if t is None else C.cast(t.data_ptr(), C.POINTER(C.c_double))  # noqa: E731
         out = C.c_double()
         ctx = L._ctx
         barrier()
@@ -311,7 +323,7 @@ def run_ours(args, rank, world, local_rank):
         _abi.check("get_macro", lib.kofm_get_macro(ctx, dp(hr), dp(hu), None))
         t1 = time.perf_counter()
         secs = max_over_ranks(t1 - t0, world, f"cuda:{local_rank}")
-        h2d = 8 * (9 * n + 3 * n + 3 * n)
+        h2d = 8 * (9 * n + (6 * n if w.komega else 0))
         d2h = 8 * 2 * args.steps + 8 * 2 * n
         e2e = {"value": nodes * args.steps * world / secs / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
@@ -368,8 +380,9 @@ def cpu_reference_sample(w, steps=2, warmup=0, budget_s=None):
     orc = Oracle()
     ch = w.channel
     cfg = make_cfg(ch.nx, ch.ny, w.tau, w.fterm, w.mu, nxf=ch.nx_full)
+    ibb = (ch.ibb_idx, ch.ibb_q) if len(ch.ibb_idx) else (None, None)
     sim = OracleSim(orc, cfg, ch.ntype, ch.dX, ch.wallD, w.f, w.k, w.omega, w.nut, w.sxy,
-                    komega=w.komega)
+                    komega=w.komega, ibb_idx=ibb[0], ibb_q=ibb[1])
     kind = "port"
     ref = RefKernels() if os.path.exists(LIB_REF) else None
     if ref is not None:
@@ -387,6 +400,8 @@ def cpu_reference_sample(w, steps=2, warmup=0, budget_s=None):
                                      sim.wallD, sim.nut, sim.K, sim.O, sim.S, 2)
         else:
             ref.L.ref_collide_laminar(cp, sim.rho, sim.ux, sim.uy, sim.FA, sim.FB, sim.m, 2)
+        if len(sim.ibb_idx):  # lbIBB on the post-stream populations
+            ref.L.ref_ibb(cp, sim.ibb_idx, sim.ibb_q, sim.FB, len(sim.ibb_idx))
         sim.FA, sim.FB = sim.FB, sim.FA
         if w.komega:
             ref.L.ref_komega_diffusivities(cp, sim.m, sim.K, sim.O, sim.nut, sim.wallD, sim.Dk,
@@ -412,8 +427,9 @@ def cpu_reference_sample(w, steps=2, warmup=0, budget_s=None):
     cores = len(os.sched_getaffinity(0))
     return {"value": w.nodes * done / secs / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"{done} of {steps} full steps of {w.name} ({w.nodes} nodes), "
-                      f"after {warmup} untimed: reference kernels (oracle/_ref) for collide + "
-                      "k-omega assembly, C restatement of its GMRES(10); OpenMP over rows",
+                      f"after {warmup} untimed: reference kernels (oracle/_ref) for collide"
+                      f"{' + lbIBB' if len(sim.ibb_idx) else ''} + k-omega assembly, C restatement "
+                      "of its GMRES(10); OpenMP over rows",
             "seconds": secs, "steps_timed": done}
 
 
@@ -446,10 +462,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp16neq32", "fp64"])
-    ap.add_argument("--solver", default="sstep", choices=["sstep", "sstep_coop", "classic"],
+    ap.add_argument("--solver", default="sstep", choices=["sstep", "sstep_host", "sstep_coop", "classic"],
                     help="k-omega solve: a cycle's Krylov directions in one sweep, each sweep "
-                         "its own launch (default) or all in one cooperative launch "
-                         "(sstep_coop), or one vector per sweep (classic)")
+                         "its own launch in a device-driven update graph (default) or enqueued "
+                         "round by round by the host (sstep_host), or all in one cooperative "
+                         "launch (sstep_coop); or one vector per sweep (classic)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -143,6 +143,9 @@ typedef struct kofm_desc {
                                  the host enqueueing one round at a time;
                                  2 is the same solve in one cooperative
                                  launch (the form kofm_batch graphs capture);
+                                 3 is form 0 with the host enqueueing each
+                                 round and synchronising per solve (status
+                                 codes at once, no update graph);
                                  1 builds one vector per sweep as
                                  GMRESSolver::solve does.  komega_full_cycle = 1
                                  implies 1.  All follow the reference's

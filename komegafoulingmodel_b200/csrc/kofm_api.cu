@@ -122,6 +122,7 @@ struct kofm_ctx {
     cudaGraph_t ug = nullptr;
     cudaGraphExec_t ugx = nullptr;
     bool ug_pending = false;          // updates launched since the state was last read back
+    bool ug_devupd = false;           // the graph's assembly node takes dt as a device-updated parameter
     long long launches_host = 0;      // k-omega kernel launches the host loop made since set_state
     int steps_per_lb = 1;
     int time_since_change = 0;
@@ -489,7 +490,7 @@ int validate_desc(const kofm_desc* d) {
     if (d->krylov_dim < 1 || d->krylov_dim > KOFM_MAX_KRYLOV) return KOFM_ERR_LOADING_PARAMS;
     if (d->komega_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
     if (d->solver_max_blocks < 0) return KOFM_ERR_LOADING_PARAMS;
-    if (d->komega_classic < 0 || d->komega_classic > 2) return KOFM_ERR_LOADING_PARAMS;
+    if (d->komega_classic < 0 || d->komega_classic > 3) return KOFM_ERR_LOADING_PARAMS;
     if (d->use_thermal) {
         if (d->thermal_every < 1 || d->thermal_max_iters < 1) return KOFM_ERR_LOADING_PARAMS;
         if (!(d->pr_number > 0.0) || !(d->pr_turb_number > 0.0) || !(d->thermal_dt > 0.0))

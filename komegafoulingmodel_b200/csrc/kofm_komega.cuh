@@ -71,7 +71,6 @@ struct AsmParams {
     int nx, ny, P;
     long long D;
     double mu, dt;
-    const double* dt_dev;  // when set, the time step is read here (device-driven updates)
 };
 
 struct Fd3 {
@@ -154,6 +153,7 @@ struct AsmSmem {
     AsmStage<FT> st[2];
     double Dk[KO_RY][KO_RX];
     double Do[KO_RY][KO_RX];
+    double dt;  // the time step of this launch (p.dt, or read from p.dt_dev)
 };
 
 __device__ __forceinline__ void ko_cp4(float* smem, const float* gmem) {
@@ -240,7 +240,7 @@ __device__ __forceinline__ double ko_f1(double, double kv, double om, double yv,
 }
 
 // Phases 2 and 3 of one tile from stage S (all of S visible to the block).
-template <typename FT>
+template <typename FT, bool DEVDT>
 __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int y0, int t,
                                         const AsmStage<FT>& S, AsmSmem<FT>& M) {
     const KoNode n = ko_node(p, tid, x0, y0);
@@ -304,7 +304,14 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
     Pk = dmaxr(dminr(Pk, 10. * KO_BETA_STAR * kv * om), 0.0);
     const double gam = (f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2) / nt;
     double Sc = -KO_BETA_STAR * om;
-    double dt = p.dt_dev ? __ldg(p.dt_dev) : p.dt;
+    // the launch's time step: a kernel parameter (constant bank), or the value
+    // the device-driven update keeps in device memory (staged in M.dt; loaded
+    // here, where it is first used, so it holds no register through the tile)
+    double dt = p.dt;
+    if (DEVDT) {
+        const unsigned a = (unsigned)__cvta_generic_to_shared(&M.dt);
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(dt) : "r"(a));
+    }
 
     double Kc = 1. + dt * (Jxk * X.c + Jyk * Y.c - dk * (X2.c + Y2.c)) - Sc;
     double Ke = dt * (Jxk * X.e - dk * X2.e);
@@ -346,9 +353,9 @@ __device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int
 #ifndef KOFM_ASM_MINBLOCKS
 #define KOFM_ASM_MINBLOCKS 2  // resident blocks per SM (registers and the persistent grid)
 #endif
-template <typename FT = float>
+template <typename FT = float, bool DEVDT = false>
 __global__ void __launch_bounds__(KO_THREADS, KOFM_ASM_MINBLOCKS)
-komega_assemble_kernel(const AsmParams p) {
+komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     extern __shared__ __align__(16) unsigned char ko_smem[];
     AsmSmem<FT>& M = *reinterpret_cast<AsmSmem<FT>*>(ko_smem);
     const int tid = threadIdx.x;
@@ -356,6 +363,9 @@ komega_assemble_kernel(const AsmParams p) {
     const int ntiles = tiles_x * ((p.ny + KO_TY - 1) / KO_TY);
     int tile = blockIdx.x;
     if (tile >= ntiles) return;  // block-uniform
+    // DEVDT: the time step is read from dt_dev (device-driven updates);
+    // visible after the loop's first barrier
+    if (DEVDT && tid == 0) M.dt = *dt_dev;
     int buf = 0;
     int t_cur = ko_issue(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, M.st[0]);
     cp_async_commit();
@@ -367,7 +377,7 @@ komega_assemble_kernel(const AsmParams p) {
         if (next < ntiles)
             t_next = ko_issue(p, tid, (next % tiles_x) * KO_TX, (next / tiles_x) * KO_TY, M.st[buf ^ 1]);
         cp_async_commit();
-        ko_tile(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, t_cur, M.st[buf], M);
+        ko_tile<FT, DEVDT>(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, t_cur, M.st[buf], M);
         t_cur = t_next;
         buf ^= 1;
     }

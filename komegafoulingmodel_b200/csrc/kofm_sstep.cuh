@@ -112,7 +112,7 @@ __device__ __forceinline__ double ss_warp_sum(double x) {
     return __shfl_sync(0xffffffffu, x, 0);
 }
 
-__device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double rel_tol, double* cP) {
+__device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double rel_tol, double* cP, int cap) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n = L + 1;
@@ -130,7 +130,7 @@ __device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double 
     int built = 0;
 #pragma unroll
     for (int k = 0; k < SS_MAXL; ++k) {
-        if (k >= L || k >= K) break;
+        if (k >= L || k >= K || k >= cap) break;
         // w = A z, z = r / rho0 (k = 0) or v_{k-1}; A p_j = p_j + p_{j+1}
         const double z = k == 0 ? z0 : V[k - 1];
         const double zm = __shfl_up_sync(FULL, z, 1);
@@ -166,6 +166,13 @@ __device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double 
         built = k + 1;
         if (S.done) break;
     }
+    if (!S.done && built >= cap && cap < L && cap < K) {
+        // the powers past level cap are numerically dependent on the earlier
+        // ones: the cycle ends with the vectors built (back-substitution as
+        // for a xi cut), and the next restart goes on from its residual
+        if (lane == 0) cycle_finish(S, K, built, K);
+        __syncwarp();
+    }
     if (!S.done) {
         __syncwarp();
         if (lane == 0) S.iters = iters0;  // the cycle is re-run with more powers
@@ -188,7 +195,11 @@ __device__ int ss_cycle_warp(GmresSys& S, const double* G, int L, int K, double 
 struct SsCycleSmem {
     double G[(SS_MAXL + 1) * (SS_MAXL + 1)];
     double cP[SS_MAXL + 1];
+    int cap;  // vectors the cycle may build (numerical rank of the power basis)
 };
+
+// Smallest pivot of the unit-diagonal Gram Cholesky accepted for a level.
+constexpr double SS_PIVOT_MIN = 1.0e-9;
 
 // One system's serial step after a Gram round, run by one warp: t holds
 // G(i, j) of p_0 .. p_L (slots ss_gslot), the round computed powers
@@ -229,7 +240,31 @@ __device__ __noinline__ void ss_gram_step(const SsArgs& a, GmresSys& S, int s, c
         cs.G[e] = t[i <= j ? ss_gslot(i, j) : ss_gslot(j, i)];
     }
     __syncwarp();
-    const int built = ss_cycle_warp(S, cs.G, L, a.K, a.rel_tol, cs.cP);
+    // Numerical rank of the power basis: Cholesky of the Gram matrix scaled
+    // to a unit diagonal, whose j-th pivot is sin^2 of the angle between p_j
+    // and span(p_0 .. p_{j-1}).  Levels from the first pivot below
+    // SS_PIVOT_MIN on carry too few correct digits for the coefficient-space
+    // orthogonalisation (the monomial basis turns towards the dominant
+    // eigenvector as the operator's convective part grows), so the cycle
+    // uses at most that many levels.
+    if (lane == 0) {
+        double Lc[(SS_MAXL + 1) * (SS_MAXL + 1)];
+        int m = n;
+        for (int j = 0; j < n && m == n; ++j) {
+            const double gjj = cs.G[j * n + j];
+            for (int i = 0; i <= j && m == n; ++i) {
+                const double gii = cs.G[i * n + i];
+                double v = (gii > 0.0 && gjj > 0.0) ? cs.G[i * n + j] / sqrt(gii * gjj) : 0.0;
+                for (int q = 0; q < i; ++q) v -= Lc[j * n + q] * Lc[i * n + q];
+                if (i < j) Lc[j * n + i] = v / Lc[i * n + i];
+                else if (v > SS_PIVOT_MIN) Lc[j * n + j] = sqrt(v);
+                else m = j;  // levels 0 .. j-1 usable
+            }
+        }
+        cs.cap = m - 1 < 1 ? 1 : m - 1;  // vector k uses levels up to k + 1
+    }
+    __syncwarp();
+    const int built = ss_cycle_warp(S, cs.G, L, a.K, a.rel_tol, cs.cP, cs.cap);
     if (lane == 0) {
         S.lev = L;
         if (!S.done) {
@@ -1214,7 +1249,15 @@ __global__ void ku_fail_kernel(KoStepState* st, int n, int mask) {
 
 // Start of an update: the doubling test (doubleTimeStep, kOmega.cpp:401-414)
 // and the sub-step loop's condition.
-__global__ void ku_begin_kernel(KoStepState* st, cudaGraphConditionalHandle sub) {
+// The assembly node of the update graph takes its time step as a kernel
+// parameter (constant bank) that these kernels rewrite whenever dt changes
+// (asm_node non-null); else the assembly reads dt from st.
+__device__ __forceinline__ void ku_set_dt(cudaGraphDeviceNode_t asm_node, size_t dt_offset, double dt) {
+    if (asm_node) cudaGraphKernelNodeSetParam(asm_node, dt_offset, &dt, sizeof(double));
+}
+
+__global__ void ku_begin_kernel(KoStepState* st, cudaGraphConditionalHandle sub, cudaGraphDeviceNode_t asm_node,
+                                unsigned long long dt_offset) {
     if (threadIdx.x) return;
     if (st->status) {
         cudaGraphSetConditional(sub, 0);
@@ -1228,6 +1271,7 @@ __global__ void ku_begin_kernel(KoStepState* st, cudaGraphConditionalHandle sub)
             st->dt *= 2.0;
         }
     }
+    ku_set_dt(asm_node, dt_offset, st->dt);
     st->cur = 0;
     st->substeps = 0;
     st->launches = 1;  // this kernel
@@ -1309,7 +1353,8 @@ __global__ void ku_round_end_kernel(GmresControl* ctl, KoStepState* st, int max_
 // End of a sub-step: halveTimeStep on a NaN residual (omega first, then k;
 // kOmega.cpp:68-70, 387-399), the halving cap, and the sub-step loop's
 // condition.
-__global__ void ku_substep_kernel(const GmresControl* ctl, KoStepState* st, cudaGraphConditionalHandle sub) {
+__global__ void ku_substep_kernel(const GmresControl* ctl, KoStepState* st, cudaGraphConditionalHandle sub,
+                                  cudaGraphDeviceNode_t asm_node, unsigned long long dt_offset) {
     if (threadIdx.x) return;
     const int n = ctl->launches + 3;  // the rounds' kernels + assembly, control-block init, this kernel
     st->launches += n;
@@ -1333,6 +1378,7 @@ __global__ void ku_substep_kernel(const GmresControl* ctl, KoStepState* st, cuda
         return;
     }
     st->cur++;
+    ku_set_dt(asm_node, dt_offset, st->dt);
     cudaGraphSetConditional(sub, st->cur < st->steps_per_lb ? 1u : 0u);
 }
 

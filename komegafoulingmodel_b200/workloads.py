@@ -9,6 +9,10 @@ state built on the host.  Names and sizes:
                           Re on the channel height about 5e4 (config 3)
   komega_straight_2048x256    the config-2 size as a straight, periodic,
                           body-forced channel (the variant with a reference)
+  komega_wavy_2048x256    the config-2 shape: walls 0.5 + 16 (1 - cos(2 pi x /
+                          512)) and mirrored (interpolated bounce-back), k-omega,
+                          nu = 5e-4, periodic and body-forced
+  komega_straight_<nx>x<ny>   other sizes of the straight k-omega channel
 """
 from __future__ import annotations
 
@@ -68,11 +72,32 @@ def komega_channel(nx, ny, re_height=5.0e4, nu=5.0e-4, steps=1000, intensity=0.0
                     f, k, o, nut, np.zeros(3 * ch.n), steps=steps)
 
 
+def komega_wavy(nx=2048, ny=256, amplitude=32.0, wavelength=512, nu=5.0e-4, u_max=0.05,
+                intensity=0.05, steps=1000) -> Workload:
+    """Wavy k-omega channel: walls displaced by A (1 - cos(2 pi x / L)) / 2
+    (mirrored, the seam at a crest), parabolic start of peak u_max between the
+    mean walls, body force from the reference's Re -> Fval relation on the
+    half-height, k and omega from the turbulence intensity as komega_channel."""
+    ch = G.wavy_channel(nx, ny, amplitude, wavelength)
+    R = ch.pipe_radius
+    y = np.arange(ny)[:, None] - 0.5
+    ux = np.clip(u_max * (1.0 - ((y - R) / R) ** 2), 0.0, None) * np.ones((1, ch.nx_full))
+    f = G.equilibrium_state(ch, ux=ux)
+    g = G.force_from_re((2.0 / 3.0) * u_max * R / nu, nu, R)
+    k0 = 1.5 * (intensity * u_max) ** 2
+    o0 = np.sqrt(k0) / (0.09 ** 0.25 * 0.07 * 2 * R)
+    k, o, nut = G.komega_fields(ch, k0, o0)
+    return Workload(f"komega_wavy_{nx}x{ny}", ch, 1.0 / (3.0 * nu + 0.5), g, nu, True,
+                    f, k, o, nut, np.zeros(3 * ch.n), steps=steps)
+
+
 def by_name(name: str) -> Workload:
     if name.startswith("poiseuille"):
         return poiseuille()
     if name == "komega_straight_16384x1024":
         return komega_channel(16384, 1024, steps=20000)
+    if name == "komega_wavy_2048x256":
+        return komega_wavy(steps=50000)
     if name == "komega_straight_2048x256":
         return komega_channel(2048, 256, re_height=2.5e4, steps=50000)
     if name.startswith("komega_straight_"):
