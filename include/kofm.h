@@ -442,18 +442,26 @@ void* kofm_stream(kofm_ctx* ctx);
 /* ---- batched lattices ------------------------------------------------------
  * No counterpart in the reference, which runs one channel per process.
  * Advances n independent lattices together: two time steps of every lattice
- * (collide-stream; for k-omega lattices also assembly and solve) are captured
- * once into one CUDA graph whose per-lattice branches run concurrently, and
- * kofm_batch_step replays it (one graph launch per two steps).  Requirements
- * checked by kofm_batch_create: all contexts on one device, each past its
- * first step (kofm_step / kofm_lb_step called at least once), and for k-omega
- * lattices steps_per_lb == 1 (no dt halving in progress).  The captured solves
- * cannot run the host's dt halving: a NaN residual in any of them stops
+ * are captured once into one CUDA graph, and kofm_batch_step replays it (one
+ * graph launch per two steps).  Per step the collide of all lattices runs as
+ * one persistent launch per group of lattices with the same storage form and
+ * model, its blocks walking a table of tiles (tile_rows block rows of 4
+ * lattice rows x 128 columns of one lattice; kofm_batch_create_tiled chooses
+ * tile_rows, 0 or kofm_batch_create: 2; -1 keeps one collide launch per
+ * lattice in the lattice's own branch); then every k-omega lattice's
+ * assembly and solve run as concurrent graph branches (the one-sweep-per-
+ * cycle solver in its one-launch form, komega_classic 2, for contexts of the
+ * phase-launch forms).  Requirements checked by kofm_batch_create: all
+ * contexts on one device, each past its first step (kofm_step /
+ * kofm_lb_step called at least once), and for k-omega lattices
+ * steps_per_lb == 1 (no dt halving in progress).  The captured solves
+ * cannot run the dt halving: a NaN residual in any of them stops
  * kofm_batch_step with KOFM_ERR_NAN, after which the contexts are used on
  * their own (kofm_step).  While the batch exists the contexts may be read
  * (kofm_get_*, kofm_reduce, kofm_get_stats) but not stepped on their own. */
 typedef struct kofm_batch kofm_batch;
 int kofm_batch_create(kofm_ctx* const* ctxs, int32_t n, kofm_batch** out);
+int kofm_batch_create_tiled(kofm_ctx* const* ctxs, int32_t n, int32_t tile_rows, kofm_batch** out);
 /* nsteps must be a multiple of 2; returns after the steps completed. */
 int kofm_batch_step(kofm_batch* b, int32_t nsteps);
 int kofm_batch_destroy(kofm_batch* b);

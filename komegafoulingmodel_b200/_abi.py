@@ -114,6 +114,7 @@ SIGNATURES = {
     "kofm_reduce_field_noalloc": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             _vp, _vp]),
     "kofm_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
+    "kofm_batch_create_tiled": (C.c_int, [C.POINTER(_vp), C.c_int32, C.c_int32, C.POINTER(_vp)]),
     "kofm_batch_step": (C.c_int, [_vp, C.c_int32]),
     "kofm_batch_destroy": (C.c_int, [_vp]),
     "kofm_set_temperature": (C.c_int, [_vp, _dp]),

@@ -1036,13 +1036,16 @@ int kofm_get_macro(kofm_ctx* c, double* rho, double* ux, double* uy) {
     return KOFM_OK;
 }
 
-int kofm_lb_step(kofm_ctx* c, int32_t options) {
-    if (!c) return KOFM_ERR_INVALID_ARG;
-    if (!c->have_state) return KOFM_ERR_STATE;
+}  // extern "C"
+
+namespace {
+
+// Parameters of the collide from buffer parity cur (read g[cur], write g[cur ^ 1]).
+LbParams lb_params(const kofm_ctx* c, int32_t options, int cur) {
     const kofm_desc& d = c->desc;
     LbParams p;
-    p.gin = c->g[c->cur];
-    p.gout = c->g[c->cur ^ 1];
+    p.gin = c->g[cur];
+    p.gout = c->g[cur ^ 1];
     p.ntype = c->ntype;
     p.rec = c->rec;
     p.ibb = c->ibb;
@@ -1050,12 +1053,32 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
     p.K = c->K; p.O = c->O; p.S = c->S; p.nut = c->nut;
     p.rho = c->rho; p.ux = c->ux; p.uy = c->uy;
     p.partials = c->lb_partials;
-    p.ref_in = c->ref[c->cur];
-    p.ref_out = c->ref[c->cur ^ 1];
+    p.ref_in = c->ref[cur];
+    p.ref_out = c->ref[cur ^ 1];
     p.nx = d.nx; p.ny = d.ny; p.P = c->P; p.D = c->D;
     p.tau = d.tau; p.fterm = d.fterm; p.mu = d.mu; p.maxnut = d.max_turb_visc;
     p.options = options;
     p.has_ibb = c->n_ibb_rec > 0;
+    return p;
+}
+
+// Host-side record of a collide enqueued for c.
+void lb_done(kofm_ctx* c) {
+    c->cur ^= 1;
+    c->phase = 1;
+    c->stats.phase = 1;
+    c->stats.steps += 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kofm_lb_step(kofm_ctx* c, int32_t options) {
+    if (!c) return KOFM_ERR_INVALID_ARG;
+    if (!c->have_state) return KOFM_ERR_STATE;
+    const kofm_desc& d = c->desc;
+    const LbParams p = lb_params(c, options, c->cur);
     const bool ko = d.use_komega != 0, ph0 = c->phase == 0;
     cudaError_t e;
     switch (d.storage) {
@@ -1070,10 +1093,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
         fprintf(stderr, "kofm: lb step launch failed: %s\n", cudaGetErrorString(e));
         return KOFM_ERR_CALLING_KERNEL;
     }
-    c->cur ^= 1;
-    c->phase = 1;
-    c->stats.phase = 1;
-    c->stats.steps += 1;
+    lb_done(c);
     return KOFM_OK;
 }
 

@@ -125,25 +125,31 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 // force increment (~1e-7 of a population of ~0.1, a few FP32 ulps of it) is
 // not rounded away; the equilibrium both sides subtract and add back is the
 // same FP32 function feq_dev_f32 of the same FP32 moments.
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float>
-__global__ void __launch_bounds__(128, ((NEQ && sizeof(AT) == 8) || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
-lb_step_kernel(const LbParams p) {
+//
+// One block of 32 x 4 threads covers 128 columns x 4 rows: block (bx, by) of
+// a lattice whose grid has gx = P / 128 block columns.  lb_step_kernel runs
+// one lattice; lb_multi_kernel walks a table of such blocks over several
+// lattices.
+constexpr int LB_BLOCK_ROWS = 4;
+
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ, typename FT>
+__device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int gx) {
     using VT = typename Store<ST>::vt;  // type a population is loaded into
     constexpr bool NEQ32 = NEQ && sizeof(AT) == 4;
     FT* const fK = static_cast<FT*>(p.K);
     FT* const fO = static_cast<FT*>(p.O);
     FT* const fS = static_cast<FT*>(p.S);
     const int lane = threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int y = by * LB_BLOCK_ROWS + threadIdx.y;
     // Each warp owns one partial-sum slot; warps that leave early clear it.
     double* slot = nullptr;
     if (p.partials && (p.options & OPTION_SAVE_MACRO_FIELDS))
-        slot = p.partials + (((long long)blockIdx.y * gridDim.x + blockIdx.x) * 4 + threadIdx.y) * 3;
+        slot = p.partials + (((long long)by * gx + bx) * 4 + threadIdx.y) * 3;
     if (y >= p.ny) {  // warp-uniform
         if (slot && lane == 0) { slot[0] = 0.0; slot[1] = 0.0; slot[2] = 0.0; }
         return;
     }
-    const int x0 = (blockIdx.x * 32 + lane) * 4;
+    const int x0 = (bx * 32 + lane) * 4;
     const ST* gin = static_cast<const ST*>(p.gin);
     ST* gout = static_cast<ST*>(p.gout);
     const long long rowoff = (long long)y * p.P;
@@ -443,6 +449,45 @@ lb_step_kernel(const LbParams p) {
             bsum_uy += __shfl_down_sync(0xffffffffu, bsum_uy, off);
         }
         if (lane == 0) { slot[0] = bsum_rho; slot[1] = bsum_ux; slot[2] = bsum_uy; }
+    }
+}
+
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float>
+__global__ void __launch_bounds__(128, ((NEQ && sizeof(AT) == 8) || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
+lb_step_kernel(const LbParams p) {
+    lb_block<ST, AT, KOMEGA, PHASE0, NEQ, FT>(p, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
+// A tile of the multi-lattice collide: `rows` block rows from `by` of block
+// column `bx` of lattice `lat`.
+struct LbTile {
+    int lat, bx, by, rows;
+};
+
+// The collide of several lattices (same storage form and model) in one
+// persistent launch: the blocks walk a tile table; each tile's lattice
+// parameters are staged in shared memory.  Per node the same arithmetic and
+// the same partial-sum slots as lb_step_kernel.
+template <typename ST, typename AT, bool KOMEGA, bool NEQ = false, typename FT = float>
+__global__ void __launch_bounds__(128, ((NEQ && sizeof(AT) == 8) || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
+lb_multi_kernel(const LbParams* __restrict__ lats, const LbTile* __restrict__ tiles, int ntiles) {
+    __shared__ LbParams sp;
+    constexpr int NW = (int)(sizeof(LbParams) / sizeof(unsigned long long));
+    static_assert(sizeof(LbParams) % sizeof(unsigned long long) == 0, "staged as 8-byte words");
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    int cur = -1;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const LbTile T = tiles[t];
+        if (T.lat != cur) {  // block-uniform
+            __syncthreads();  // every warp is done with the previous lattice's parameters
+            if (tid < NW)
+                reinterpret_cast<unsigned long long*>(&sp)[tid] =
+                    reinterpret_cast<const unsigned long long*>(lats + T.lat)[tid];
+            __syncthreads();
+            cur = T.lat;
+        }
+        for (int r = 0; r < T.rows; ++r)
+            lb_block<ST, AT, KOMEGA, false, NEQ, FT>(sp, T.bx, T.by + r, sp.P / 128);
     }
 }
 

@@ -114,3 +114,30 @@ def test_batch_of_phase_form_contexts_agrees_to_rounding(kofm_lib):
     finally:
         for L in solo + both:
             L.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tile_rows", [1, 3, -1])
+def test_tile_shapes_of_the_multi_lattice_collide_give_identical_steps(kofm_lib, tile_rows):
+    """The persistent multi-lattice collide walks tiles of tile_rows block
+    rows (-1: one collide launch per lattice): every tile shape computes each
+    node as the one-lattice collide does, so the batch stays bit-identical to
+    stepping the contexts one by one."""
+    cases = _cases()
+    solo = [_open(c) for c in cases]
+    both = [_open(c) for c in cases]
+    try:
+        for L in solo + both:
+            L.step(1)
+        with Batch(both, tile_rows) as B:
+            B.step(4)
+        for L in solo:
+            L.step(4)
+        for a, b in zip(solo, both):
+            for x, y in zip(a.get_state(), b.get_state()):
+                if x is not None:
+                    assert np.array_equal(x, y)
+            assert a.get_macro()[0].tobytes() == b.get_macro()[0].tobytes()
+    finally:
+        for L in solo + both:
+            L.close()

@@ -166,3 +166,38 @@ def test_channel_16bit_storage_precision(kofm_lib, oracle, storage, bound):
     errs = dict(ux=rel_l2(ux, sim.ux, fl), k=rel_l2(k2, sim.K, fl), omega=rel_l2(o2, sim.O, fl))
     print(errs)
     assert errs["ux"] < bound, errs
+
+
+def test_high_re_k_solve_caps_the_cycle_at_the_power_basis_rank(kofm_lib):
+    """A 1024 x 256 wavy k-omega channel at Re 1.45e4 (the batched sweep's
+    channel 28): its first k system needs a full 10-vector cycle in the
+    one-vector-per-sweep solver, and its first 10 powers N^j r are
+    numerically dependent (the convective part of the rows dominates).  The
+    one-sweep-per-cycle forms cap the cycle where the unit-diagonal Gram
+    Cholesky pivot falls below 1e-9 and restart from the residual: the solve
+    converges (no NaN, no dt halving) in one more restart, to a k within
+    1e-2 rel-L2 of the one-vector-per-sweep solve (both stop at the 1e-4
+    tolerance of a system whose k grows 200-fold in this first step)."""
+    from komegafoulingmodel_b200 import workloads as W
+    from komegafoulingmodel_b200.batch import sweep_channels
+    w = sweep_channels(29, 0)[28]
+    out = {}
+    for form in (0, 2, 1):
+        d = W.descriptor(w)
+        d.komega_classic = form
+        with Lattice(d) as L:
+            W.apply(L, w)
+            L.lb_step()
+            L.komega_assemble(1.0)
+            st, iters, rel = L.komega_solve(raise_on_error=False)
+            s = L.stats()
+            _, k, o, _, _ = L.get_state()
+        assert st == 0 and s.k_nan == 0 and s.omega_nan == 0, (form, st, rel)
+        assert rel[1] <= 1e-4 and rel[0] <= 1e-4, (form, rel)
+        out[form] = (k, o, s.k_restarts)
+    fl = w.channel.fluid_mask().ravel()
+    for form in (0, 2):
+        e = rel_l2(out[form][0], out[1][0], fl)
+        print(form, out[form][2], out[1][2], e)
+        assert e < 1e-2, (form, e)
+        assert out[form][2] >= out[1][2]
