@@ -386,6 +386,16 @@ int kofm_debug_fail_solves(kofm_ctx* ctx, int32_t n, int32_t mask);
  * timed).  Synchronises.  No counterpart in the reference. */
 int kofm_debug_solver_trace(kofm_ctx* ctx, int64_t* ns, int32_t cap, int32_t* n);
 
+/* Diagnostic: the rows of one k-omega system (0: omega, 1: k) as the last
+ * assembly (kofm_komega_assemble, or the assembly of the last update) left
+ * them.  coef: [4][ny][nx_full] off-diagonals E, W, N, S of each row
+ * normalised by its diagonal (the values Update_kOmega_Coeffs_Implicit,
+ * kOmegaKernels.cl:187-480, scatters into the CSR row); rhs: [ny][nx_full]
+ * b - A x0 with b the normalised right-hand side and x0 the field the
+ * assembly read.  Columns x >= nx are left untouched; either pointer may be
+ * NULL.  Synchronises.  No counterpart in the reference. */
+int kofm_debug_komega_rows(kofm_ctx* ctx, int32_t system, double* coef, double* rhs);
+
 /* ---- discrete adjoint of the laminar step -----------------------------------
  * No counterpart in the reference.  From the current state (a stepped FP32
  * laminar context without thermal update), takes T steps and returns

@@ -110,6 +110,7 @@ SIGNATURES = {
     "kofm_debug_barrier_timeout": (C.c_int, [_vp, C.c_int64]),
     "kofm_debug_fail_solves": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "kofm_debug_solver_trace": (C.c_int, [_vp, C.POINTER(C.c_int64), C.c_int32, _i32p]),
+    "kofm_debug_komega_rows": (C.c_int, [_vp, C.c_int32, _dp, _dp]),
     "kofm_stream": (_vp, [_vp]),
     "kofm_reduce_field_noalloc": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                             _vp, _vp]),

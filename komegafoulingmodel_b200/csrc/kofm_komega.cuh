@@ -3,14 +3,16 @@
 // One kernel replaces the reference's Update_kOmega_Diffusivities and
 // Update_kOmega_Coeffs_Implicit (Kernels/kOmegaKernels.cl:7-95, 187-480) and
 // the GMRES updateRHS step (gmresKernels.cl:353-420, b -= A x0):
-//   * a 32x8 tile of nodes stages k and omega with a 2-node halo in shared
-//     memory;
-//   * the blending function F1, the cross-diffusion multipliers and the
-//     diffusivities D_k, D_w are evaluated on the tile plus a 1-node ring,
-//     one node per thread (D_k, D_w are needed at the neighbours for grad D);
-//   * each fluid node of the tile then builds its backward-Euler rows for k and
-//     omega, normalised by the diagonal (which is therefore 1 and not
-//     stored), with the wall-omega Dirichlet row of kOmegaKernels.cl:389-403;
+//   * a warp owns a strip of 30 columns and marches up a chunk of rows with
+//     no shared memory and no block barrier: lane l holds column x0 - 1 + l,
+//     so lanes 0 and 31 are the 1-node ring the strip's rows need;
+//   * at row r the warp evaluates the blending function F1, the
+//     cross-diffusion multipliers and the diffusivities D_k, D_w of row r
+//     (k, omega neighbours in x by shuffles, in y from a register window);
+//   * it then builds the backward-Euler rows for k and omega of row r - 1
+//     (D neighbours in x by shuffles, in y from registers), normalised by the
+//     diagonal (which is therefore 1 and not stored), with the wall-omega
+//     Dirichlet row of kOmegaKernels.cl:389-403;
 //   * the correction right-hand side b' = b - A x0 (x0 = current k / omega)
 //     is formed in FP64 here, so the solver never re-reads x0 or b.
 // D_k, D_w, F1 and the cross-diffusion terms never reach HBM (the reference
@@ -20,7 +22,6 @@
 
 namespace kofm {
 
-constexpr int KO_TX = 32, KO_TY = 8;
 
 // One implicit system (index 0: omega, 1: k) as the solver sees it.  The
 // matrix stays FP64: an FP32-rounded operator would perturb every implicit
@@ -69,6 +70,7 @@ struct AsmParams {
     double* coef_k;
     double* rhs_k;
     int nx, ny, P;
+    int rows;  // rows per warp strip chunk
     long long D;
     double mu, dt;
 };
@@ -94,143 +96,55 @@ __device__ __forceinline__ void fd_weights(double dpos, double dneg, Fd3& d1, Fd
     d2.c = -2. / (a * b);
 }
 
-// Weights for unit link fractions (every node without an E/W/N/S wall link):
-// d1 = (1/2, -1/2, 0), d2 = (1, 1, -2), exactly what fd_weights(1, 1) gives.
-__device__ __forceinline__ void fd_unit(Fd3& d1, Fd3& d2) {
-    d1.e = 0.5; d1.w = -0.5; d1.c = 0.0;
-    d2.e = 1.0; d2.w = 1.0; d2.c = -2.0;
-}
-
-// Weights of one node: constants unless it has a dX record.
-__device__ __forceinline__ void node_weights(const AsmParams& p, int t, long long g, Fd3& X,
-                                             Fd3& X2, Fd3& Y, Fd3& Y2) {
-    if (t & NESW_BOUNDARY) {
-        const int r = p.dxidx[g];
-        if (r >= 0) {
-            const DxRecord rec = p.dxrec[r];
-            fd_weights(rec.dx[0], rec.dx[1], X, X2);
-            fd_weights(rec.dx[2], rec.dx[3], Y, Y2);
-            return;
-        }
-    }
-    fd_unit(X, X2);
-    fd_unit(Y, Y2);
-}
-
 __device__ __forceinline__ double dmaxr(double a, double b) { return a < b ? b : a; }
 __device__ __forceinline__ double dminr(double a, double b) { return b < a ? b : a; }
 
-__device__ __forceinline__ int wrapx(int x, int nx) {
-    return x < 0 ? x + nx : (x >= nx ? x - nx : x);
-}
+// Warp strips: KM_W interior columns per warp (lanes 1..30; lanes 0 and 31
+// are the ring), KM_WARPS independent warps per block, KOFM_ASM_ROWS rows per
+// warp (each chunk re-evaluates the closure of the ring rows above and below
+// it: 2 of KOFM_ASM_ROWS + 2 rows).
+constexpr int KM_W = 30;
+constexpr int KM_WARPS = 4;
+#ifndef KOFM_ASM_ROWS
+#define KOFM_ASM_ROWS 32
+#endif
+#ifndef KOFM_ASM_MINBLOCKS
+#define KOFM_ASM_MINBLOCKS 4  // resident blocks per SM the register budget is set for
+#endif
+#ifndef KOFM_ASM_CLOSURE_FP32
+#define KOFM_ASM_CLOSURE_FP32 1
+#endif
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// One thread per node of the tile plus its 1-node ring (34 x 10 = 340 of the
-// 352 threads), so the transcendental-heavy diffusivity phase takes one round;
-// the threads of the 32 x 8 interior then build the rows.
-//
-// The kernel is persistent: a block walks the tiles tile += gridDim.x and,
-// while it computes one tile, streams the next tile's k, omega halo and every
-// thread's node fields into the other half of a double-buffered shared-memory
-// stage with 4-byte cp.async (the node flag goes into a register), so the
-// loads of a tile overlap the FP64 work of the previous one.
-constexpr int KO_RX = KO_TX + 2, KO_RY = KO_TY + 2;
-constexpr int KO_THREADS = 352;  // 11 warps >= KO_RX * KO_RY
-constexpr int KO_HX = KO_TX + 4, KO_HY = KO_TY + 4;  // 2-ring halo
-constexpr int KO_NF = 8;  // node fields: wallD, rho, nut, ux, uy, Sxx, Sxy, Syy
-
+// Arithmetic type of the closure (F1, D_k, D_w, the cross-diffusion
+// multipliers, grad D) for a field type.  FP32 fields: FP32 -- its inputs are
+// FP32 fields and its rounding (~1e-7 relative) is the size of the FP32
+// rounding of nu_t and k beside it; the rows, b' and the operator stay FP64.
+// FP64 fields: FP64.
 template <typename FT>
-struct AsmStage {
-    FT K[KO_HY][KO_HX];
-    FT O[KO_HY][KO_HX];
-    FT fld[KO_NF][KO_THREADS];
+struct KoClosure {
+    using type = double;
 };
-
-template <typename FT>
-struct AsmSmem {
-    AsmStage<FT> st[2];
-    double Dk[KO_RY][KO_RX];
-    double Do[KO_RY][KO_RX];
-    double dt;  // the time step of this launch (p.dt, or read from p.dt_dev)
+#if KOFM_ASM_CLOSURE_FP32
+template <>
+struct KoClosure<float> {
+    using type = float;
 };
+#endif
 
-__device__ __forceinline__ void ko_cp4(float* smem, const float* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void ko_cp4(double* smem, const double* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+__host__ __device__ __forceinline__ int km_wrap(int x, int nx) {
+    x %= nx;
+    return x < 0 ? x + nx : x;
 }
 
-// Geometry of this thread's ring node in tile (x0, y0).
-struct KoNode {
-    int rx, ry, gxu, gx, gy;
-    bool inrow, interior;
-    long long g;
-};
-
-__device__ __forceinline__ KoNode ko_node(const AsmParams& p, int tid, int x0, int y0) {
-    KoNode n;
-    const bool ring = tid < KO_RX * KO_RY;
-    n.rx = ring ? tid % KO_RX : 0;
-    n.ry = ring ? tid / KO_RX : 0;
-    n.gxu = x0 - 1 + n.rx;
-    n.gx = wrapx(n.gxu, p.nx);
-    n.gy = y0 - 1 + n.ry;
-    n.inrow = ring && n.gy >= 0 && n.gy < p.ny;
-    n.interior = n.inrow && n.rx >= 1 && n.rx <= KO_TX && n.ry >= 1 && n.ry <= KO_TY && n.gxu < p.nx;
-    n.g = (long long)(n.inrow ? n.gy : 0) * p.P + n.gx;
-    return n;
-}
-
-// Issue the copies of tile (x0, y0) into stage S; returns the node flag.
-template <typename FT>
-__device__ __forceinline__ int ko_issue(const AsmParams& p, int tid, int x0, int y0, AsmStage<FT>& S) {
-    const FT* pK = static_cast<const FT*>(p.K);
-    const FT* pO = static_cast<const FT*>(p.O);
-    for (int i = tid; i < KO_HX * KO_HY; i += KO_THREADS) {
-        const int sy = i / KO_HX, sx = i % KO_HX;
-        const int hx = wrapx(x0 - 2 + sx, p.nx);
-        int hy = y0 - 2 + sy;
-        hy = hy < 0 ? 0 : (hy >= p.ny ? p.ny - 1 : hy);
-        const long long h = (long long)hy * p.P + hx;
-        ko_cp4(&S.K[sy][sx], pK + h);
-        ko_cp4(&S.O[sy][sx], pO + h);
-    }
-    const KoNode n = ko_node(p, tid, x0, y0);
-    if (!n.inrow) return M_SOLID;
-    const long long g = n.g, D = p.D;
-    ko_cp4(&S.fld[0][tid], static_cast<const FT*>(p.wallD) + g);
-    ko_cp4(&S.fld[1][tid], static_cast<const FT*>(p.rho) + g);
-    ko_cp4(&S.fld[2][tid], static_cast<const FT*>(p.nut) + g);
-    if (n.interior) {
-        const FT* pS = static_cast<const FT*>(p.S);
-        ko_cp4(&S.fld[3][tid], static_cast<const FT*>(p.ux) + g);
-        ko_cp4(&S.fld[4][tid], static_cast<const FT*>(p.uy) + g);
-        ko_cp4(&S.fld[5][tid], pS + g);
-        ko_cp4(&S.fld[6][tid], pS + D + g);
-        ko_cp4(&S.fld[7][tid], pS + 2 * D + g);
-    }
-    return (uint16_t)__ldg(p.ntype + g);
-}
-
-// Blending function F1 (kOmegaKernels.cl:68-87).  With FP32 fields in FP32:
-// its inputs k, omega, rho, y are FP32 fields; F1 in [0, 1] enters D_k, D_w
-// with an error ~1e-7, the size of the FP32 rounding of nu_t beside it.  With
-// FP64 fields in FP64.
-__device__ __forceinline__ double ko_f1(float, double kv, double om, double yv, double rho, double cdx,
-                                        double mu) {
-    const float CDkw = fmaxf((float)(rho * cdx), 1.0e-10f);
-    const float kf = (float)kv, of = (float)om, yf = (float)yv;
-    float a = fmaxf(sqrtf(kf) / ((float)KO_BETA_STAR * of * yf), 500.f * (float)mu / (yf * yf * of));
-    a = fminf(a, 4.f * kf * (float)KO_SIGMA_O2 / (CDkw * yf * yf));
+// Blending function F1 (kOmegaKernels.cl:68-87), in the closure's type.
+__device__ __forceinline__ float ko_f1(float kv, float om, float yv, float rho, float cdx, float mu) {
+    const float CDkw = fmaxf(rho * cdx, 1.0e-10f);
+    float a = fmaxf(sqrtf(kv) / ((float)KO_BETA_STAR * om * yv), 500.f * mu / (yv * yv * om));
+    a = fminf(a, 4.f * kv * (float)KO_SIGMA_O2 / (CDkw * yv * yv));
     const float a2 = a * a;
-    return (double)tanhf(a2 * a2);
+    return tanhf(a2 * a2);
 }
-__device__ __forceinline__ double ko_f1(double, double kv, double om, double yv, double rho, double cdx,
+__device__ __forceinline__ double ko_f1(double kv, double om, double yv, double rho, double cdx,
                                         double mu) {
     const double CDkw = fmax(rho * cdx, 1.0e-10);
     double a = fmax(sqrt(kv) / (KO_BETA_STAR * om * yv), 500. * mu / (yv * yv * om));
@@ -239,149 +153,262 @@ __device__ __forceinline__ double ko_f1(double, double kv, double om, double yv,
     return tanh(a2 * a2);
 }
 
-// Phases 2 and 3 of one tile from stage S (all of S visible to the block).
-template <typename FT, bool DEVDT>
-__device__ __forceinline__ void ko_tile(const AsmParams& p, int tid, int x0, int y0, int t,
-                                        const AsmStage<FT>& S, AsmSmem<FT>& M) {
-    const KoNode n = ko_node(p, tid, x0, y0);
-    const int rx = n.rx, ry = n.ry;
-    const long long g = n.g;
-    const bool ring = tid < KO_RX * KO_RY;
+// Weights of a node with a link-fraction record (NESW_BOUNDARY nodes whose
+// dX differs from 1); rec < 0 means the unit weights d1 = (1/2, -1/2, 0),
+// d2 = (1, 1, -2), which the code below applies as constants.
+__device__ __forceinline__ int km_record(const AsmParams& p, int t, int g) {
+    return (t & NESW_BOUNDARY) ? __ldg(p.dxidx + g) : -1;
+}
+__device__ __forceinline__ void km_weights(const AsmParams& p, int rec, Fd3& X, Fd3& X2, Fd3& Y, Fd3& Y2) {
+    const DxRecord r = p.dxrec[rec];
+    fd_weights(r.dx[0], r.dx[1], X, X2);
+    fd_weights(r.dx[2], r.dx[3], Y, Y2);
+}
 
-    // ---- F1, cross-diffusion, diffusivities on the tile + 1 ring -------------
-    // (Update_kOmega_Diffusivities, kOmegaKernels.cl:24-94)
-    const int sy = ry + 1, sx = rx + 1;  // position in the 2-ring tile
-    double Dk = 0.0, Do = 0.0, F1 = 0.0, mxv = 0.0, myv = 0.0;
-    double yv = 1.0, rho = 0.0, nt = 0.0;
-    Fd3 X, Y, X2, Y2;
-    const bool fluid = n.inrow && !(t & M_SOLID);
-    if (fluid) {
-        yv = S.fld[0][tid];
-        rho = S.fld[1][tid];
-        nt = S.fld[2][tid];
-        node_weights(p, t, g, X, X2, Y, Y2);
-        const double om = S.O[sy][sx], kv = S.K[sy][sx];
-        const double dOdx = X.e * S.O[sy][sx + 1] + X.w * S.O[sy][sx - 1] + X.c * om;
-        const double dKdx = X.e * S.K[sy][sx + 1] + X.w * S.K[sy][sx - 1] + X.c * kv;
-        const double dOdy = Y.e * S.O[sy + 1][sx] + Y.w * S.O[sy - 1][sx] + Y.c * om;
-        const double dKdy = Y.e * S.K[sy + 1][sx] + Y.w * S.K[sy - 1][sx] + Y.c * kv;
-        const double m = 2. * KO_SIGMA_O2 / om;
-        mxv = m * dKdx;
-        myv = m * dKdy;
-        F1 = ko_f1(FT(0), kv, om, yv, rho, mxv * dOdx + myv * dOdy, p.mu);
-        Dk = p.mu + (KO_SIGMA_K1 * F1 + KO_SIGMA_K2 * (1. - F1)) * nt;
-        Do = p.mu + (KO_SIGMA_O1 * F1 + KO_SIGMA_O2 * (1. - F1)) * nt;
+// Closure of one fluid node (Update_kOmega_Diffusivities,
+// kOmegaKernels.cl:24-94): neighbours c (centre), e, w, n, s.
+template <typename CT, typename FT>
+__device__ __forceinline__ void km_closure(const AsmParams& p, int rec, FT kc, FT ke, FT kw, FT kn, FT ks,
+                                           FT oc, FT oe, FT ow, FT on, FT os, FT yv, FT rho, FT nt,
+                                           CT& Dk, CT& Do, CT& F1, CT& mx, CT& my) {
+    CT dOdx, dKdx, dOdy, dKdy;
+    if (rec < 0) {
+        // X.e E + X.w W + X.c C with (1/2, -1/2, 0): the same value as the
+        // general form (scaling by 1/2 is exact)
+        dOdx = CT(0.5) * (CT(oe) - CT(ow));
+        dKdx = CT(0.5) * (CT(ke) - CT(kw));
+        dOdy = CT(0.5) * (CT(on) - CT(os));
+        dKdy = CT(0.5) * (CT(kn) - CT(ks));
+    } else {
+        Fd3 X, X2, Y, Y2;
+        km_weights(p, rec, X, X2, Y, Y2);
+        dOdx = CT(X.e) * CT(oe) + CT(X.w) * CT(ow) + CT(X.c) * CT(oc);
+        dKdx = CT(X.e) * CT(ke) + CT(X.w) * CT(kw) + CT(X.c) * CT(kc);
+        dOdy = CT(Y.e) * CT(on) + CT(Y.w) * CT(os) + CT(Y.c) * CT(oc);
+        dKdy = CT(Y.e) * CT(kn) + CT(Y.w) * CT(ks) + CT(Y.c) * CT(kc);
     }
-    if (ring) {
-        M.Dk[ry][rx] = Dk;
-        M.Do[ry][rx] = Do;
-    }
-    __syncthreads();
+    const CT m = CT(2. * KO_SIGMA_O2) / CT(oc);
+    mx = m * dKdx;
+    my = m * dKdy;
+    F1 = ko_f1(CT(kc), CT(oc), CT(yv), CT(rho), mx * dOdx + my * dOdy, CT(p.mu));
+    Dk = CT(p.mu) + (CT(KO_SIGMA_K1) * F1 + CT(KO_SIGMA_K2) * (CT(1) - F1)) * CT(nt);
+    Do = CT(p.mu) + (CT(KO_SIGMA_O1) * F1 + CT(KO_SIGMA_O2) * (CT(1) - F1)) * CT(nt);
+}
 
-    // ---- rows of the tile's nodes (Update_kOmega_Coeffs_Implicit) ------------
-    if (!n.interior) return;
-    if (t & M_SOLID) {
-        for (int c = 0; c < 4; ++c) { p.coef_o[ilv(4, c, g)] = 0.0; p.coef_k[ilv(4, c, g)] = 0.0; }
-        p.rhs_o[g] = 0.0;
-        p.rhs_k[g] = 0.0;
-        return;
-    }
-    const double Ux = S.fld[3][tid], Uy = S.fld[4][tid];
-    const double Sxx = S.fld[5][tid], Sxy = S.fld[6][tid], Syy = S.fld[7][tid];
-    const double dk = Dk, dom = Do;
-    const double dk_dx = X.e * M.Dk[ry][rx + 1] + X.w * M.Dk[ry][rx - 1] + X.c * dk;
-    const double do_dx = X.e * M.Do[ry][rx + 1] + X.w * M.Do[ry][rx - 1] + X.c * dom;
-    const double dk_dy = Y.e * M.Dk[ry + 1][rx] + Y.w * M.Dk[ry - 1][rx] + Y.c * dk;
-    const double do_dy = Y.e * M.Do[ry + 1][rx] + Y.w * M.Do[ry - 1][rx] + Y.c * dom;
-    const double Jxo = Ux - do_dx - mxv;
-    const double Jyo = Uy - do_dy - myv;
-    const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
-    const double Kraw = S.K[sy][sx], Oraw = S.O[sy][sx];
-    double om = dmaxr(0.0, Oraw);
-    const double kv = dmaxr(0.0, Kraw);
+// Rows of one fluid node (Update_kOmega_Coeffs_Implicit,
+// kOmegaKernels.cl:187-480), normalised by their diagonals, and
+// b' = b - A x0 summed in the CSR order of an interior row (S, W, C, E, N).
+// D* are the diffusivities of the node and its neighbours; cb is the
+// interleaved index of coefficient 0 of node g.
+template <typename CT, typename FT>
+__device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, int rec, int g, int cb,
+                                        CT dkc, CT dke, CT dkw, CT dkn, CT dks, CT doc, CT doe, CT dow,
+                                        CT don, CT dos, CT F1, CT mx, CT my, FT kc, FT ke, FT kw, FT kn,
+                                        FT ks, FT oc, FT oe, FT ow, FT on, FT os, FT fux, FT fuy,
+                                        FT fsxx, FT fsxy, FT fsyy, FT fnt, FT frho, FT fyv) {
+    const double dk = dkc, dom = doc;
+    const double Ux = fux, Uy = fuy;
+    const double Sxx = fsxx, Sxy = fsxy, Syy = fsyy;
+    const double nt = fnt, rho = frho;
+    const double om = dmaxr(0.0, (double)oc);
+    const double kv = dmaxr(0.0, (double)kc);
     const double f1 = F1;
     double Pk = 2. * nt * (Sxx * Sxx + Syy * Syy + 2. * Sxy * Sxy) - 2. / 3. * kv * rho * (Sxx + Syy);
     Pk = dmaxr(dminr(Pk, 10. * KO_BETA_STAR * kv * om), 0.0);
     const double gam = (f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2) / nt;
-    double Sc = -KO_BETA_STAR * om;
-    // the launch's time step: a kernel parameter (constant bank), or the value
-    // the device-driven update keeps in device memory (staged in M.dt; loaded
-    // here, where it is first used, so it holds no register through the tile)
-    double dt = p.dt;
-    if (DEVDT) {
-        const unsigned a = (unsigned)__cvta_generic_to_shared(&M.dt);
-        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(dt) : "r"(a));
-    }
-
-    double Kc = 1. + dt * (Jxk * X.c + Jyk * Y.c - dk * (X2.c + Y2.c)) - Sc;
-    double Ke = dt * (Jxk * X.e - dk * X2.e);
-    double Kw = dt * (Jxk * X.w - dk * X2.w);
-    double Kn = dt * (Jyk * Y.e - dk * Y2.e);
-    double Ks = dt * (Jyk * Y.w - dk * Y2.w);
-    double Ksrc = kv + dt * Pk;
-    const double iKc = 1. / Kc;
-    Ke *= iKc; Kw *= iKc; Kn *= iKc; Ks *= iKc; Ksrc *= iKc;
-
+    const double Sc = -KO_BETA_STAR * om;
+    // the omega row of a node beside an E/W/N/S wall holds the wall value
+    // (kOmegaKernels.cl:389-403): no time derivative, no source
+    double dtw = dt, Scw = Sc, omw = om;
     if (t & NESW_BOUNDARY) {
-        dt = 0.;
-        Sc = 0.;
-        const double yp = yv;
+        dtw = 0.;
+        Scw = 0.;
+        const double yp = fyv;
         const double ovis = (6. * p.mu / 0.075) / (yp * yp);
         const double olog = sqrt(kv) / (KO_C_MU_0_25 * KO_KAPPA * yp);
-        om = dminr(1000., sqrt(ovis * ovis + olog * olog));
+        omw = dminr(1000., sqrt(ovis * ovis + olog * olog));
     }
-    double Wc = 1. + dt * (Jxo * X.c + Jyo * Y.c - dom * (X2.c + Y2.c)) - Sc;
-    double We = dt * (Jxo * X.e - dom * X2.e);
-    double Ww = dt * (Jxo * X.w - dom * X2.w);
-    double Wn = dt * (Jyo * Y.e - dom * Y2.e);
-    double Ws = dt * (Jyo * Y.w - dom * Y2.w);
-    double Wsrc = om + dt * (gam * Pk);
+    double Kc, Ke, Kw, Kn, Ks, Wc, We, Ww, Wn, Ws;
+    if (rec < 0) {
+        // unit weights: X.c = Y.c = 0, X2.c + Y2.c = -4, X2.e = X2.w = 1
+        const double dk_dx = (double)(CT(0.5) * (dke - dkw));
+        const double do_dx = (double)(CT(0.5) * (doe - dow));
+        const double dk_dy = (double)(CT(0.5) * (dkn - dks));
+        const double do_dy = (double)(CT(0.5) * (don - dos));
+        const double Jxo = Ux - do_dx - (double)mx;
+        const double Jyo = Uy - do_dy - (double)my;
+        const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
+        Kc = 1. + dt * (4. * dk) - Sc;
+        Ke = dt * (0.5 * Jxk - dk);
+        Kw = dt * (-0.5 * Jxk - dk);
+        Kn = dt * (0.5 * Jyk - dk);
+        Ks = dt * (-0.5 * Jyk - dk);
+        Wc = 1. + dtw * (4. * dom) - Scw;
+        We = dtw * (0.5 * Jxo - dom);
+        Ww = dtw * (-0.5 * Jxo - dom);
+        Wn = dtw * (0.5 * Jyo - dom);
+        Ws = dtw * (-0.5 * Jyo - dom);
+    } else {
+        Fd3 X, X2, Y, Y2;
+        km_weights(p, rec, X, X2, Y, Y2);
+        const double dk_dx = X.e * (double)dke + X.w * (double)dkw + X.c * dk;
+        const double do_dx = X.e * (double)doe + X.w * (double)dow + X.c * dom;
+        const double dk_dy = Y.e * (double)dkn + Y.w * (double)dks + Y.c * dk;
+        const double do_dy = Y.e * (double)don + Y.w * (double)dos + Y.c * dom;
+        const double Jxo = Ux - do_dx - (double)mx;
+        const double Jyo = Uy - do_dy - (double)my;
+        const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
+        Kc = 1. + dt * (Jxk * X.c + Jyk * Y.c - dk * (X2.c + Y2.c)) - Sc;
+        Ke = dt * (Jxk * X.e - dk * X2.e);
+        Kw = dt * (Jxk * X.w - dk * X2.w);
+        Kn = dt * (Jyk * Y.e - dk * Y2.e);
+        Ks = dt * (Jyk * Y.w - dk * Y2.w);
+        Wc = 1. + dtw * (Jxo * X.c + Jyo * Y.c - dom * (X2.c + Y2.c)) - Scw;
+        We = dtw * (Jxo * X.e - dom * X2.e);
+        Ww = dtw * (Jxo * X.w - dom * X2.w);
+        Wn = dtw * (Jyo * Y.e - dom * Y2.e);
+        Ws = dtw * (Jyo * Y.w - dom * Y2.w);
+    }
+    const double iKc = 1. / Kc;
+    Ke *= iKc; Kw *= iKc; Kn *= iKc; Ks *= iKc;
+    const double Ksrc = (kv + dt * Pk) * iKc;
     const double iWc = 1. / Wc;
-    We *= iWc; Ww *= iWc; Wn *= iWc; Ws *= iWc; Wsrc *= iWc;
-
-    // b' = b - A x0, summed in the CSR order of an interior row (S, W, C, E, N)
-    const double kS = S.K[sy - 1][sx], kW = S.K[sy][sx - 1], kE = S.K[sy][sx + 1], kN = S.K[sy + 1][sx];
-    const double oS = S.O[sy - 1][sx], oW = S.O[sy][sx - 1], oE = S.O[sy][sx + 1], oN = S.O[sy + 1][sx];
-    const double Axk = Ks * kS + Kw * kW + Kraw + Ke * kE + Kn * kN;
-    const double Axo = Ws * oS + Ww * oW + Oraw + We * oE + Wn * oN;
-    p.coef_o[ilv(4, 0, g)] = We; p.coef_o[ilv(4, 1, g)] = Ww; p.coef_o[ilv(4, 2, g)] = Wn; p.coef_o[ilv(4, 3, g)] = Ws;
-    p.coef_k[ilv(4, 0, g)] = Ke; p.coef_k[ilv(4, 1, g)] = Kw; p.coef_k[ilv(4, 2, g)] = Kn; p.coef_k[ilv(4, 3, g)] = Ks;
-    p.rhs_o[g] = (Wsrc - Axo);
-    p.rhs_k[g] = (Ksrc - Axk);
+    We *= iWc; Ww *= iWc; Wn *= iWc; Ws *= iWc;
+    const double Wsrc = (omw + dtw * (gam * Pk)) * iWc;
+    const double Axk = Ks * (double)ks + Kw * (double)kw + (double)kc + Ke * (double)ke + Kn * (double)kn;
+    const double Axo = Ws * (double)os + Ww * (double)ow + (double)oc + We * (double)oe + Wn * (double)on;
+    p.coef_o[cb] = We; p.coef_o[cb + 32] = Ww; p.coef_o[cb + 64] = Wn; p.coef_o[cb + 96] = Ws;
+    p.coef_k[cb] = Ke; p.coef_k[cb + 32] = Kw; p.coef_k[cb + 64] = Kn; p.coef_k[cb + 96] = Ks;
+    p.rhs_o[g] = Wsrc - Axo;
+    p.rhs_k[g] = Ksrc - Axk;
 }
 
-#ifndef KOFM_ASM_MINBLOCKS
-#define KOFM_ASM_MINBLOCKS 2  // resident blocks per SM (registers and the persistent grid)
-#endif
+// The assembly: one warp per (strip of KM_W columns, chunk of p.rows rows).
+// At row r the warp holds k, omega of rows r-2 .. r+1 (rows clamped to the
+// lattice, as the halo of the tiles), the diffusivities of rows r-2 .. r and
+// the closure outputs of row r-1, and loads row r+2 (k, omega), row r+1 (the
+// ring fields) and row r (the row fields) for the next step while it works.
 template <typename FT = float, bool DEVDT = false>
-__global__ void __launch_bounds__(KO_THREADS, KOFM_ASM_MINBLOCKS)
+__global__ void __launch_bounds__(KM_WARPS * 32, KOFM_ASM_MINBLOCKS)
 komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
-    extern __shared__ __align__(16) unsigned char ko_smem[];
-    AsmSmem<FT>& M = *reinterpret_cast<AsmSmem<FT>*>(ko_smem);
-    const int tid = threadIdx.x;
-    const int tiles_x = (p.nx + KO_TX - 1) / KO_TX;
-    const int ntiles = tiles_x * ((p.ny + KO_TY - 1) / KO_TY);
-    int tile = blockIdx.x;
-    if (tile >= ntiles) return;  // block-uniform
-    // DEVDT: the time step is read from dt_dev (device-driven updates);
-    // visible after the loop's first barrier
-    if (DEVDT && tid == 0) M.dt = *dt_dev;
-    int buf = 0;
-    int t_cur = ko_issue(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, M.st[0]);
-    cp_async_commit();
-    for (; tile < ntiles; tile += gridDim.x) {
-        cp_async_wait_all();
-        __syncthreads();  // stage `buf` complete for every thread; the previous tile is done
-        const int next = tile + gridDim.x;
-        int t_next = M_SOLID;
-        if (next < ntiles)
-            t_next = ko_issue(p, tid, (next % tiles_x) * KO_TX, (next / tiles_x) * KO_TY, M.st[buf ^ 1]);
-        cp_async_commit();
-        ko_tile<FT, DEVDT>(p, tid, (tile % tiles_x) * KO_TX, (tile / tiles_x) * KO_TY, t_cur, M.st[buf], M);
-        t_cur = t_next;
-        buf ^= 1;
+    using CT = typename KoClosure<FT>::type;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int nx = p.nx, ny = p.ny;
+    const int nstrips = (nx + KM_W - 1) / KM_W;
+    const int nchunks = (ny + p.rows - 1) / p.rows;
+    const int wid = blockIdx.x * KM_WARPS + (threadIdx.x >> 5);
+    if (wid >= nstrips * nchunks) return;  // whole warps
+    const int x0 = (wid % nstrips) * KM_W;
+    const int y0 = (wid / nstrips) * p.rows;
+    const int y1 = min(ny, y0 + p.rows);
+    // 32-bit node offsets: the launch requires 4 D < 2^31
+    const int P = p.P, D = (int)p.D;
+    const int gxu = x0 - 1 + lane;
+    const int cx = km_wrap(gxu, nx);
+    // lanes 0 and 31 also load the column beyond them (their W / E neighbour)
+    const int cxx = km_wrap(lane == 0 ? x0 - 2 : x0 + KM_W + 1, nx);
+    const bool xl = lane == 0 || lane == 31;
+    const bool icol = lane >= 1 && lane <= KM_W && gxu < nx;
+    const int colb = ((cx >> 5) << 7) + (cx & 31);
+    double dt = p.dt;
+    if (DEVDT) dt = __ldg(dt_dev);
+    const FT* pK = static_cast<const FT*>(p.K);
+    const FT* pO = static_cast<const FT*>(p.O);
+    const FT* pY = static_cast<const FT*>(p.wallD);
+    const FT* pR = static_cast<const FT*>(p.rho);
+    const FT* pN = static_cast<const FT*>(p.nut);
+    const FT* pU = static_cast<const FT*>(p.ux);
+    const FT* pV = static_cast<const FT*>(p.uy);
+    const FT* pS = static_cast<const FT*>(p.S);
+    auto crow = [ny](int y) -> int { return y < 0 ? 0 : (y >= ny ? ny - 1 : y); };
+
+    // k, omega of rows r-2 .. r+1 (start r = y0 - 1; row y0 - 3 is never used)
+    FT k0 = FT(0), o0 = FT(0);
+    FT k1 = __ldg(pK + crow(y0 - 2) * P + cx), o1 = __ldg(pO + crow(y0 - 2) * P + cx);
+    FT k2 = __ldg(pK + crow(y0 - 1) * P + cx), o2 = __ldg(pO + crow(y0 - 1) * P + cx);
+    FT k3 = __ldg(pK + crow(y0) * P + cx), o3 = __ldg(pO + crow(y0) * P + cx);
+    FT kx = FT(0), ox = FT(0);  // row r, column beyond (lanes 0 / 31)
+    if (xl) { kx = __ldg(pK + crow(y0 - 1) * P + cxx); ox = __ldg(pO + crow(y0 - 1) * P + cxx); }
+    // ring fields and flag of row r
+    FT yv = FT(0), rh = FT(0), nt = FT(0);
+    int t = M_SOLID;
+    if (y0 - 1 >= 0) {
+        const int g = (y0 - 1) * P + cx;
+        yv = __ldg(pY + g); rh = __ldg(pR + g); nt = __ldg(pN + g);
+        t = (uint16_t)__ldg(p.ntype + g);
     }
-    cp_async_wait_all();
+    // row fields of row r - 1 (never used for r = y0 - 1)
+    FT u1 = FT(0), v1 = FT(0), sa1 = FT(0), sb1 = FT(0), sc1 = FT(0);
+    // carried from row r - 1: flag, ring fields, closure, k / omega x-neighbours
+    int tm = M_SOLID;
+    FT yvm = FT(0), rhm = FT(0), ntm = FT(0);
+    CT f1m = CT(0), mxm = CT(0), mym = CT(0);
+    FT kem = FT(0), kwm = FT(0), oem = FT(0), owm = FT(0);
+    // diffusivities of rows r-2 and r-1
+    CT dk0 = CT(0), do0 = CT(0), dk1 = CT(0), do1 = CT(0);
+
+    for (int r = y0 - 1; r <= y1; ++r) {
+        // ---- loads for row r + 1 -------------------------------------------
+        FT kn = FT(0), on = FT(0), kxn = FT(0), oxn = FT(0);
+        FT yvn = FT(0), rhn = FT(0), ntn = FT(0);
+        FT un = FT(0), vn = FT(0), san = FT(0), sbn = FT(0), scn = FT(0);
+        int tn = M_SOLID;
+        if (r < y1) {
+            kn = __ldg(pK + crow(r + 2) * P + cx);
+            on = __ldg(pO + crow(r + 2) * P + cx);
+            if (xl) { kxn = __ldg(pK + crow(r + 1) * P + cxx); oxn = __ldg(pO + crow(r + 1) * P + cxx); }
+            if (r + 1 < ny) {
+                const int g = (r + 1) * P + cx;
+                yvn = __ldg(pY + g); rhn = __ldg(pR + g); ntn = __ldg(pN + g);
+                tn = (uint16_t)__ldg(p.ntype + g);
+            }
+            if (icol && r >= 0) {
+                const int g = r * P + cx;
+                un = __ldg(pU + g); vn = __ldg(pV + g);
+                san = __ldg(pS + g); sbn = __ldg(pS + D + g); scn = __ldg(pS + 2 * D + g);
+            }
+        }
+        // ---- closure of row r ----------------------------------------------
+        FT ke = __shfl_down_sync(FULL, k2, 1), kw = __shfl_up_sync(FULL, k2, 1);
+        FT oe = __shfl_down_sync(FULL, o2, 1), ow = __shfl_up_sync(FULL, o2, 1);
+        if (lane == 31) { ke = kx; oe = ox; }
+        if (lane == 0) { kw = kx; ow = ox; }
+        CT dk2 = CT(0), do2 = CT(0), f1 = CT(0), mx = CT(0), my = CT(0);
+        if (r >= 0 && r < ny && !(t & M_SOLID)) {
+            const int rec = km_record(p, t, r * P + cx);
+            km_closure<CT, FT>(p, rec, k2, ke, kw, k3, k1, o2, oe, ow, o3, o1, yv, rh, nt, dk2, do2, f1, mx, my);
+        }
+        // ---- rows of row q = r - 1 -----------------------------------------
+        const CT dke = __shfl_down_sync(FULL, dk1, 1), dkw = __shfl_up_sync(FULL, dk1, 1);
+        const CT doe = __shfl_down_sync(FULL, do1, 1), dow = __shfl_up_sync(FULL, do1, 1);
+        const int q = r - 1;
+        if (icol && q >= y0) {
+            const int g = q * P + cx;
+            const int cb = 4 * q * P + colb;
+            if (tm & M_SOLID) {
+                p.coef_o[cb] = 0.0; p.coef_o[cb + 32] = 0.0; p.coef_o[cb + 64] = 0.0; p.coef_o[cb + 96] = 0.0;
+                p.coef_k[cb] = 0.0; p.coef_k[cb + 32] = 0.0; p.coef_k[cb + 64] = 0.0; p.coef_k[cb + 96] = 0.0;
+                p.rhs_o[g] = 0.0;
+                p.rhs_k[g] = 0.0;
+            } else {
+                const int rec = km_record(p, tm, g);
+                km_rows<CT, FT>(p, dt, tm, rec, g, cb, dk1, dke, dkw, dk2, dk0, do1, doe, dow, do2, do0,
+                                f1m, mxm, mym, k1, kem, kwm, k2, k0, o1, oem, owm, o2, o0,
+                                u1, v1, sa1, sb1, sc1, ntm, rhm, yvm);
+            }
+        }
+        // ---- advance one row -------------------------------------------------
+        k0 = k1; k1 = k2; k2 = k3; k3 = kn;
+        o0 = o1; o1 = o2; o2 = o3; o3 = on;
+        kx = kxn; ox = oxn;
+        dk0 = dk1; do0 = do1; dk1 = dk2; do1 = do2;
+        f1m = f1; mxm = mx; mym = my;
+        kem = ke; kwm = kw; oem = oe; owm = ow;
+        tm = t; yvm = yv; rhm = rh; ntm = nt;
+        t = tn; yv = yvn; rh = rhn; nt = ntn;
+        u1 = un; v1 = vn; sa1 = san; sb1 = sbn; sc1 = scn;
+    }
 }
 
 }  // namespace kofm

@@ -227,6 +227,18 @@ class Lattice:
         check("kofm_debug_solver_trace", self.lib.kofm_debug_solver_trace(self._ctx, buf, 32, C.byref(n)))
         return [buf[i] for i in range(min(n.value, 32))]
 
+    def komega_rows(self, system: int):
+        """(coef [4, ny * nx_full] E/W/N/S off-diagonals normalised by the
+        diagonal, rhs [ny * nx_full] = b - A x0) of one k-omega system (0:
+        omega, 1: k) as the last assembly left them (kofm_debug_komega_rows)."""
+        n = self.nxf * self.ny
+        coef = np.zeros((4, n))
+        rhs = np.zeros(n)
+        check("kofm_debug_komega_rows",
+              self.lib.kofm_debug_komega_rows(self._ctx, system, coef.ctypes.data_as(_abi._dp),
+                                              rhs.ctypes.data_as(_abi._dp)))
+        return coef, rhs
+
     def komega_update_status(self) -> int:
         """kofm_komega_update's status without raising."""
         return self.lib.kofm_komega_update(self._ctx)

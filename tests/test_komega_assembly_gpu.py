@@ -1,0 +1,85 @@
+"""The fused k-omega assembly (kofm_komega_assemble) against the oracle's
+restatement of Update_kOmega_Diffusivities + Update_kOmega_Coeffs_Implicit
+(kOmegaKernels.cl:7-95, 187-480) on the state the device holds: the
+normalised E/W/N/S entries of the omega and k rows and b - A x0, node by node.
+
+The wavy channel of nx 200 in rows of 256 (padding columns), 66 rows, has
+nodes with and without link-fraction records, a partial strip of columns at
+the periodic seam and a partial chunk of rows; k and omega are seeded random
+(30% spread), so every gradient of the closure is non-zero."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from komegafoulingmodel_b200 import Lattice, _abi, desc_default
+from komegafoulingmodel_b200 import geometry as G
+from oracle.orc import make_cfg
+from tests.cases import komega_state, perturbed_state, rel_l2
+
+NX, NXF, NY = 200, 256, 66
+
+
+def _case():
+    ch = G.wavy_channel(NX, NY, 8.0, 100, nx_full=NXF)
+    f = perturbed_state(ch, seed=3, u_mean=0.03)
+    k, o, nut, s = komega_state(ch, seed=4, k0=4e-5, o0=2e-3, s_amp=2e-4)
+    return ch, f, k, o, nut, s
+
+
+def _oracle_rows(orc, ch, fields, dt, mu):
+    """[(coef [4, n], b - A x0 [n], b [n])] for systems 0: omega, 1: k."""
+    K, O, nut, S, rho, ux, uy, wallD = (np.ascontiguousarray(a, np.float64) for a in fields)
+    n = ch.n
+    cfg = make_cfg(NX, NY, 1.0, 0.0, mu, nxf=NXF)
+    m = np.ascontiguousarray(ch.ntype, np.int16)
+    dX = np.ascontiguousarray(ch.dX, np.float64)
+    IA, JA, ind = orc.csr(cfg, m)
+    Dk, Do, F1, dkdo = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(2 * n)
+    orc.L.orc_komega_diffusivities(C.byref(cfg), m, K, O, nut, wallD, Dk, Do, F1, dkdo, rho, dX)
+    kA, oA = np.zeros(len(JA)), np.zeros(len(JA))
+    kb, ob = np.zeros(n), np.zeros(n)
+    orc.L.orc_komega_coeffs(C.byref(cfg), ind, K, O, nut, Dk, Do, F1, dkdo, S, rho, ux, uy,
+                            kA, oA, kb, ob, dX, wallD, m, dt)
+    out = []
+    for A, b, x in ((oA, ob, O), (kA, kb, K)):
+        coef = np.stack([A[ind[(1 + j) * n:(2 + j) * n]] for j in range(4)])
+        Ax = sp.csr_matrix((A, JA, IA), shape=(n, n)) @ x
+        out.append((coef, b - Ax, b))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [(_abi.STORE_FP32, 1e-6), (_abi.STORE_FP64, 1e-13)])
+@pytest.mark.parametrize("dt", [1.0, 0.25])
+def test_assembly_rows_match_oracle(kofm_lib, oracle, storage, tol, dt):
+    """FP64 form: the oracle's rows to rounding.  FP32 form: the closure
+    (F1, D_k, D_w, cross-diffusion, grad D) runs in FP32 on the FP32 fields,
+    the rows and b - A x0 in FP64; held to 1e-6."""
+    ch, f, k, o, nut, s = _case()
+    mu = 5e-4
+    d = desc_default()
+    d.nx, d.nx_full, d.ny = NX, NXF, NY
+    d.tau, d.fterm, d.mu = 1.0 / (3 * mu + 0.5), 0.0, mu
+    d.use_komega = 1
+    d.storage = storage
+    fl = ch.fluid_mask().ravel()
+    with Lattice(d) as L:
+        L.set_geometry(ch.ntype, ch.wallD, ch.dX, ch.ibb_idx, ch.ibb_q)
+        L.set_state(f, k, o, nut, s)
+        L.lb_step()  # macro fields, nu_t and S as the assembly reads them
+        L.komega_assemble(dt)
+        rows = [L.komega_rows(0), L.komega_rows(1)]
+        _, K, O, Nut, S = L.get_state()
+        rho, ux, uy = L.get_macro()
+    wallD = ch.wallD if storage == _abi.STORE_FP64 else ch.wallD.astype(np.float32).astype(np.float64)
+    ref = _oracle_rows(oracle, ch, (K, O, Nut, S, rho, ux, uy, wallD), dt, mu)
+    rec = ch.dX.reshape(4, -1)[:, fl]
+    assert np.any(rec != 1.0) and np.any(np.all(rec == 1.0, axis=0))  # both kinds of node
+    for name, (coef, rhs), (rcoef, rrhs, b) in zip(("omega", "k"), rows, ref):
+        e_coef = rel_l2(coef[:, fl], rcoef[:, fl])
+        e_rhs = float(np.linalg.norm((rhs - rrhs)[fl]) / np.linalg.norm(b[fl]))
+        print(name, storage, dt, e_coef, e_rhs)
+        assert e_coef < tol and e_rhs < tol, (name, e_coef, e_rhs)
+        assert np.all(coef[:, ~fl] == 0.0) and np.all(rhs[~fl] == 0.0)
