@@ -104,7 +104,10 @@ __device__ __forceinline__ double dminr(double a, double b) { return b < a ? b :
 // warp (each chunk re-evaluates the closure of the ring rows above and below
 // it: 2 of KOFM_ASM_ROWS + 2 rows).
 constexpr int KM_W = 30;
-constexpr int KM_WARPS = 4;
+#ifndef KOFM_ASM_WARPS
+#define KOFM_ASM_WARPS 4
+#endif
+constexpr int KM_WARPS = KOFM_ASM_WARPS;
 #ifndef KOFM_ASM_ROWS
 #define KOFM_ASM_ROWS 32
 #endif
@@ -195,6 +198,36 @@ __device__ __forceinline__ void km_closure(const AsmParams& p, int rec, FT kc, F
     Do = CT(p.mu) + (CT(KO_SIGMA_O1) * F1 + CT(KO_SIGMA_O2) * (CT(1) - F1)) * CT(nt);
 }
 
+// One normalised row, k or omega: advection velocity J, diffusivity d, time
+// step dtr and sink Scr of the row, numerator src of its right-hand side,
+// the field x at the node and its neighbours; coefficients E, W, N, S at
+// coef[cb + 32 j], b - A x at rhs[g] (the sum in the CSR order S, W, C, E, N).
+template <bool UNIT, typename FT>
+__device__ __forceinline__ void km_row(const Fd3& X, const Fd3& X2, const Fd3& Y, const Fd3& Y2, double Jx,
+                                       double Jy, double d, double dtr, double Scr, double src, FT xc, FT xe,
+                                       FT xw, FT xn, FT xs, double* coef, int cb, double* rhs, int g) {
+    double c, e, w, n, s;
+    if (UNIT) {
+        // X.c = Y.c = 0, X2.c + Y2.c = -4, X2.e = X2.w = 1
+        c = 1. + dtr * (4. * d) - Scr;
+        e = dtr * (0.5 * Jx - d);
+        w = dtr * (-0.5 * Jx - d);
+        n = dtr * (0.5 * Jy - d);
+        s = dtr * (-0.5 * Jy - d);
+    } else {
+        c = 1. + dtr * (Jx * X.c + Jy * Y.c - d * (X2.c + Y2.c)) - Scr;
+        e = dtr * (Jx * X.e - d * X2.e);
+        w = dtr * (Jx * X.w - d * X2.w);
+        n = dtr * (Jy * Y.e - d * Y2.e);
+        s = dtr * (Jy * Y.w - d * Y2.w);
+    }
+    const double ic = 1. / c;
+    e *= ic; w *= ic; n *= ic; s *= ic;
+    const double Ax = s * (double)xs + w * (double)xw + (double)xc + e * (double)xe + n * (double)xn;
+    coef[cb] = e; coef[cb + 32] = w; coef[cb + 64] = n; coef[cb + 96] = s;
+    rhs[g] = src * ic - Ax;
+}
+
 // Rows of one fluid node (Update_kOmega_Coeffs_Implicit,
 // kOmegaKernels.cl:187-480), normalised by their diagonals, and
 // b' = b - A x0 summed in the CSR order of an interior row (S, W, C, E, N).
@@ -228,26 +261,17 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
         const double olog = sqrt(kv) / (KO_C_MU_0_25 * KO_KAPPA * yp);
         omw = dminr(1000., sqrt(ovis * ovis + olog * olog));
     }
-    double Kc, Ke, Kw, Kn, Ks, Wc, We, Ww, Wn, Ws;
+    const double srck = kv + dt * Pk, srcw = omw + dtw * (gam * Pk);
     if (rec < 0) {
-        // unit weights: X.c = Y.c = 0, X2.c + Y2.c = -4, X2.e = X2.w = 1
+        const Fd3 Z = {0., 0., 0.};  // unit weights: constants inside km_row
         const double dk_dx = (double)(CT(0.5) * (dke - dkw));
         const double do_dx = (double)(CT(0.5) * (doe - dow));
         const double dk_dy = (double)(CT(0.5) * (dkn - dks));
         const double do_dy = (double)(CT(0.5) * (don - dos));
-        const double Jxo = Ux - do_dx - (double)mx;
-        const double Jyo = Uy - do_dy - (double)my;
-        const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
-        Kc = 1. + dt * (4. * dk) - Sc;
-        Ke = dt * (0.5 * Jxk - dk);
-        Kw = dt * (-0.5 * Jxk - dk);
-        Kn = dt * (0.5 * Jyk - dk);
-        Ks = dt * (-0.5 * Jyk - dk);
-        Wc = 1. + dtw * (4. * dom) - Scw;
-        We = dtw * (0.5 * Jxo - dom);
-        Ww = dtw * (-0.5 * Jxo - dom);
-        Wn = dtw * (0.5 * Jyo - dom);
-        Ws = dtw * (-0.5 * Jyo - dom);
+        km_row<true>(Z, Z, Z, Z, Ux - dk_dx, Uy - dk_dy, dk, dt, Sc, srck, kc, ke, kw, kn, ks,
+                     p.coef_k, cb, p.rhs_k, g);
+        km_row<true>(Z, Z, Z, Z, Ux - do_dx - (double)mx, Uy - do_dy - (double)my, dom, dtw, Scw, srcw,
+                     oc, oe, ow, on, os, p.coef_o, cb, p.rhs_o, g);
     } else {
         Fd3 X, X2, Y, Y2;
         km_weights(p, rec, X, X2, Y, Y2);
@@ -255,32 +279,11 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
         const double do_dx = X.e * (double)doe + X.w * (double)dow + X.c * dom;
         const double dk_dy = Y.e * (double)dkn + Y.w * (double)dks + Y.c * dk;
         const double do_dy = Y.e * (double)don + Y.w * (double)dos + Y.c * dom;
-        const double Jxo = Ux - do_dx - (double)mx;
-        const double Jyo = Uy - do_dy - (double)my;
-        const double Jxk = Ux - dk_dx, Jyk = Uy - dk_dy;
-        Kc = 1. + dt * (Jxk * X.c + Jyk * Y.c - dk * (X2.c + Y2.c)) - Sc;
-        Ke = dt * (Jxk * X.e - dk * X2.e);
-        Kw = dt * (Jxk * X.w - dk * X2.w);
-        Kn = dt * (Jyk * Y.e - dk * Y2.e);
-        Ks = dt * (Jyk * Y.w - dk * Y2.w);
-        Wc = 1. + dtw * (Jxo * X.c + Jyo * Y.c - dom * (X2.c + Y2.c)) - Scw;
-        We = dtw * (Jxo * X.e - dom * X2.e);
-        Ww = dtw * (Jxo * X.w - dom * X2.w);
-        Wn = dtw * (Jyo * Y.e - dom * Y2.e);
-        Ws = dtw * (Jyo * Y.w - dom * Y2.w);
+        km_row<false>(X, X2, Y, Y2, Ux - dk_dx, Uy - dk_dy, dk, dt, Sc, srck, kc, ke, kw, kn, ks,
+                      p.coef_k, cb, p.rhs_k, g);
+        km_row<false>(X, X2, Y, Y2, Ux - do_dx - (double)mx, Uy - do_dy - (double)my, dom, dtw, Scw, srcw,
+                      oc, oe, ow, on, os, p.coef_o, cb, p.rhs_o, g);
     }
-    const double iKc = 1. / Kc;
-    Ke *= iKc; Kw *= iKc; Kn *= iKc; Ks *= iKc;
-    const double Ksrc = (kv + dt * Pk) * iKc;
-    const double iWc = 1. / Wc;
-    We *= iWc; Ww *= iWc; Wn *= iWc; Ws *= iWc;
-    const double Wsrc = (omw + dtw * (gam * Pk)) * iWc;
-    const double Axk = Ks * (double)ks + Kw * (double)kw + (double)kc + Ke * (double)ke + Kn * (double)kn;
-    const double Axo = Ws * (double)os + Ww * (double)ow + (double)oc + We * (double)oe + Wn * (double)on;
-    p.coef_o[cb] = We; p.coef_o[cb + 32] = Ww; p.coef_o[cb + 64] = Wn; p.coef_o[cb + 96] = Ws;
-    p.coef_k[cb] = Ke; p.coef_k[cb + 32] = Kw; p.coef_k[cb + 64] = Kn; p.coef_k[cb + 96] = Ks;
-    p.rhs_o[g] = Wsrc - Axo;
-    p.rhs_k[g] = Ksrc - Axk;
 }
 
 // The assembly: one warp per (strip of KM_W columns, chunk of p.rows rows).
@@ -340,11 +343,10 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     }
     // row fields of row r - 1 (never used for r = y0 - 1)
     FT u1 = FT(0), v1 = FT(0), sa1 = FT(0), sb1 = FT(0), sc1 = FT(0);
-    // carried from row r - 1: flag, ring fields, closure, k / omega x-neighbours
+    // carried from row r - 1: flag, ring fields, closure
     int tm = M_SOLID;
     FT yvm = FT(0), rhm = FT(0), ntm = FT(0);
     CT f1m = CT(0), mxm = CT(0), mym = CT(0);
-    FT kem = FT(0), kwm = FT(0), oem = FT(0), owm = FT(0);
     // diffusivities of rows r-2 and r-1
     CT dk0 = CT(0), do0 = CT(0), dk1 = CT(0), do1 = CT(0);
 
@@ -382,6 +384,8 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
         // ---- rows of row q = r - 1 -----------------------------------------
         const CT dke = __shfl_down_sync(FULL, dk1, 1), dkw = __shfl_up_sync(FULL, dk1, 1);
         const CT doe = __shfl_down_sync(FULL, do1, 1), dow = __shfl_up_sync(FULL, do1, 1);
+        const FT kem = __shfl_down_sync(FULL, k1, 1), kwm = __shfl_up_sync(FULL, k1, 1);
+        const FT oem = __shfl_down_sync(FULL, o1, 1), owm = __shfl_up_sync(FULL, o1, 1);
         const int q = r - 1;
         if (icol && q >= y0) {
             const int g = q * P + cx;
@@ -404,7 +408,6 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
         kx = kxn; ox = oxn;
         dk0 = dk1; do0 = do1; dk1 = dk2; do1 = do2;
         f1m = f1; mxm = mx; mym = my;
-        kem = ke; kwm = kw; oem = oe; owm = ow;
         tm = t; yvm = yv; rhm = rh; ntm = nt;
         t = tn; yv = yvn; rh = rhn; nt = ntn;
         u1 = un; v1 = vn; sa1 = san; sb1 = sbn; sc1 = scn;

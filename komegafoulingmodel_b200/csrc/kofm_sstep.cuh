@@ -247,21 +247,36 @@ __device__ __noinline__ void ss_gram_step(const SsArgs& a, GmresSys& S, int s, c
     // orthogonalisation (the monomial basis turns towards the dominant
     // eigenvector as the operator's convective part grows), so the cycle
     // uses at most that many levels.
-    if (lane == 0) {
-        double Lc[(SS_MAXL + 1) * (SS_MAXL + 1)];
+    // Right-looking, lane i holding row i of the scaled Gram (its trailing
+    // Schur complement after each step); every lane learns the pivots by
+    // broadcast, so the first one below SS_PIVOT_MIN ends the loop in step.
+    {
+        double row[SS_MAXL + 1];
+        const double gii = lane < n ? cs.G[lane * n + lane] : 0.0;
+#pragma unroll
+        for (int k = 0; k <= SS_MAXL; ++k) {
+            double v = 0.0;
+            if (lane < n && k < n) {
+                const double gkk = cs.G[k * n + k];
+                v = (gii > 0.0 && gkk > 0.0) ? cs.G[lane * n + k] / sqrt(gii * gkk) : 0.0;
+            }
+            row[k] = v;
+        }
         int m = n;
-        for (int j = 0; j < n && m == n; ++j) {
-            const double gjj = cs.G[j * n + j];
-            for (int i = 0; i <= j && m == n; ++i) {
-                const double gii = cs.G[i * n + i];
-                double v = (gii > 0.0 && gjj > 0.0) ? cs.G[i * n + j] / sqrt(gii * gjj) : 0.0;
-                for (int q = 0; q < i; ++q) v -= Lc[j * n + q] * Lc[i * n + q];
-                if (i < j) Lc[j * n + i] = v / Lc[i * n + i];
-                else if (v > SS_PIVOT_MIN) Lc[j * n + j] = sqrt(v);
-                else m = j;  // levels 0 .. j-1 usable
+#pragma unroll
+        for (int j = 0; j <= SS_MAXL; ++j) {
+            if (j >= n) break;
+            const double v = __shfl_sync(0xffffffffu, row[j], j);
+            if (!(v > SS_PIVOT_MIN)) { m = j; break; }  // levels 0 .. j-1 usable
+            const double d = sqrt(v);
+            const double lij = lane > j ? row[j] / d : 0.0;
+#pragma unroll
+            for (int k = j + 1; k <= SS_MAXL; ++k) {
+                const double lkj = __shfl_sync(0xffffffffu, lij, k);
+                if (lane > j) row[k] -= lij * lkj;
             }
         }
-        cs.cap = m - 1 < 1 ? 1 : m - 1;  // vector k uses levels up to k + 1
+        if (lane == 0) cs.cap = m - 1 < 1 ? 1 : m - 1;  // vector k uses levels up to k + 1
     }
     __syncwarp();
     const int built = ss_cycle_warp(S, cs.G, L, a.K, a.rel_tol, cs.cP, cs.cap);
