@@ -286,21 +286,51 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
     }
 }
 
+// Depth of each warp's row ring: the fields of a row are copied
+// KM_RING - 1 rows before the row is used.
+#ifndef KOFM_ASM_RING
+#define KOFM_ASM_RING 4
+#endif
+constexpr int KM_R = KOFM_ASM_RING;
+static_assert((KM_R & (KM_R - 1)) == 0 && KM_R >= 2, "ring depth: a power of two");
+// Fields of one ring slot ([field][lane]): k, omega of row i + 1; k, omega of
+// row i at the column beyond lanes 0 / 31; wall distance, rho, nu_t of row
+// i; u_x, u_y, S_xx, S_xy, S_yy of row i - 1.
+enum { KF_K, KF_O, KF_KX, KF_OX, KF_Y, KF_R, KF_N, KF_U, KF_V, KF_SA, KF_SB, KF_SC, KM_NF };
+
+template <typename FT>
+constexpr size_t km_smem_bytes() { return sizeof(FT) * KM_WARPS * KM_R * KM_NF * 32; }
+
+template <typename FT>
+__device__ __forceinline__ void km_cp(FT* dst, const FT* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(FT) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void km_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void km_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // The assembly: one warp per (strip of KM_W columns, chunk of p.rows rows).
 // At row r the warp holds k, omega of rows r-2 .. r+1 (rows clamped to the
 // lattice, as the halo of the tiles), the diffusivities of rows r-2 .. r and
-// the closure outputs of row r-1, and loads row r+2 (k, omega), row r+1 (the
-// ring fields) and row r (the row fields) for the next step while it works.
+// the closure outputs of row r-1.  The fields each step reads stream through
+// a per-warp ring of KM_R slots in shared memory, copied with cp.async
+// KM_R - 1 steps ahead; each lane reads back only the elements it copied, so
+// the warp needs no barrier.
 template <typename FT = float, bool DEVDT = false>
 __global__ void __launch_bounds__(KM_WARPS * 32, KOFM_ASM_MINBLOCKS)
 komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     using CT = typename KoClosure<FT>::type;
     constexpr unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) unsigned char km_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nx = p.nx, ny = p.ny;
     const int nstrips = (nx + KM_W - 1) / KM_W;
     const int nchunks = (ny + p.rows - 1) / p.rows;
-    const int wid = blockIdx.x * KM_WARPS + (threadIdx.x >> 5);
+    const int wid = blockIdx.x * KM_WARPS + warp;
     if (wid >= nstrips * nchunks) return;  // whole warps
     const int x0 = (wid % nstrips) * KM_W;
     const int y0 = (wid / nstrips) * p.rows;
@@ -309,7 +339,7 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     const int P = p.P, D = (int)p.D;
     const int gxu = x0 - 1 + lane;
     const int cx = km_wrap(gxu, nx);
-    // lanes 0 and 31 also load the column beyond them (their W / E neighbour)
+    // lanes 0 and 31 also read the column beyond them (their W / E neighbour)
     const int cxx = km_wrap(lane == 0 ? x0 - 2 : x0 + KM_W + 1, nx);
     const bool xl = lane == 0 || lane == 31;
     const bool icol = lane >= 1 && lane <= KM_W && gxu < nx;
@@ -325,24 +355,46 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     const FT* pV = static_cast<const FT*>(p.uy);
     const FT* pS = static_cast<const FT*>(p.S);
     auto crow = [ny](int y) -> int { return y < 0 ? 0 : (y >= ny ? ny - 1 : y); };
+    FT* ring = reinterpret_cast<FT*>(km_smem) + warp * (KM_R * KM_NF * 32) + lane;
+    // copies of the fields step i reads (i = y0 - 1 .. y1) into slot i mod KM_R
+    auto stage = [&](int i) {
+        FT* s = ring + ((i - y0 + 1) & (KM_R - 1)) * (KM_NF * 32);
+        const int ga = crow(i + 1) * P;
+        km_cp(s + KF_K * 32, pK + ga + cx);
+        km_cp(s + KF_O * 32, pO + ga + cx);
+        if (xl) {
+            const int gx = crow(i) * P + cxx;
+            km_cp(s + KF_KX * 32, pK + gx);
+            km_cp(s + KF_OX * 32, pO + gx);
+        }
+        if (i >= 0 && i < ny) {
+            const int g = i * P + cx;
+            km_cp(s + KF_Y * 32, pY + g);
+            km_cp(s + KF_R * 32, pR + g);
+            km_cp(s + KF_N * 32, pN + g);
+        }
+        if (icol && i - 1 >= y0) {
+            const int g = (i - 1) * P + cx;
+            km_cp(s + KF_U * 32, pU + g);
+            km_cp(s + KF_V * 32, pV + g);
+            km_cp(s + KF_SA * 32, pS + g);
+            km_cp(s + KF_SB * 32, pS + D + g);
+            km_cp(s + KF_SC * 32, pS + 2 * D + g);
+        }
+    };
+#pragma unroll
+    for (int j = 0; j < KM_R - 1; ++j) {
+        if (y0 - 1 + j <= y1) stage(y0 - 1 + j);
+        km_commit();
+    }
 
-    // k, omega of rows r-2 .. r+1 (start r = y0 - 1; row y0 - 3 is never used)
+    // k, omega of rows r-2 .. r (start r = y0 - 1; row y0 - 3 is never used);
+    // row r + 1 comes from the ring
     FT k0 = FT(0), o0 = FT(0);
     FT k1 = __ldg(pK + crow(y0 - 2) * P + cx), o1 = __ldg(pO + crow(y0 - 2) * P + cx);
     FT k2 = __ldg(pK + crow(y0 - 1) * P + cx), o2 = __ldg(pO + crow(y0 - 1) * P + cx);
-    FT k3 = __ldg(pK + crow(y0) * P + cx), o3 = __ldg(pO + crow(y0) * P + cx);
-    FT kx = FT(0), ox = FT(0);  // row r, column beyond (lanes 0 / 31)
-    if (xl) { kx = __ldg(pK + crow(y0 - 1) * P + cxx); ox = __ldg(pO + crow(y0 - 1) * P + cxx); }
-    // ring fields and flag of row r
-    FT yv = FT(0), rh = FT(0), nt = FT(0);
-    int t = M_SOLID;
-    if (y0 - 1 >= 0) {
-        const int g = (y0 - 1) * P + cx;
-        yv = __ldg(pY + g); rh = __ldg(pR + g); nt = __ldg(pN + g);
-        t = (uint16_t)__ldg(p.ntype + g);
-    }
-    // row fields of row r - 1 (never used for r = y0 - 1)
-    FT u1 = FT(0), v1 = FT(0), sa1 = FT(0), sb1 = FT(0), sc1 = FT(0);
+    // flag of row r (loaded one step ahead)
+    int t = y0 - 1 >= 0 ? (uint16_t)__ldg(p.ntype + (y0 - 1) * P + cx) : M_SOLID;
     // carried from row r - 1: flag, ring fields, closure
     int tm = M_SOLID;
     FT yvm = FT(0), rhm = FT(0), ntm = FT(0);
@@ -351,26 +403,18 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
     CT dk0 = CT(0), do0 = CT(0), dk1 = CT(0), do1 = CT(0);
 
     for (int r = y0 - 1; r <= y1; ++r) {
-        // ---- loads for row r + 1 -------------------------------------------
-        FT kn = FT(0), on = FT(0), kxn = FT(0), oxn = FT(0);
-        FT yvn = FT(0), rhn = FT(0), ntn = FT(0);
-        FT un = FT(0), vn = FT(0), san = FT(0), sbn = FT(0), scn = FT(0);
+        // ---- this step's fields from the ring; the copies of step r + KM_R - 1
+        km_wait<KM_R - 2>();
+        const FT* s = ring + ((r - y0 + 1) & (KM_R - 1)) * (KM_NF * 32);
+        const FT k3 = s[KF_K * 32], o3 = s[KF_O * 32];
+        const FT kx = s[KF_KX * 32], ox = s[KF_OX * 32];
+        const FT yv = s[KF_Y * 32], rh = s[KF_R * 32], nt = s[KF_N * 32];
+        const FT u1 = s[KF_U * 32], v1 = s[KF_V * 32];
+        const FT sa1 = s[KF_SA * 32], sb1 = s[KF_SB * 32], sc1 = s[KF_SC * 32];
+        if (r + KM_R - 1 <= y1) stage(r + KM_R - 1);
+        km_commit();
         int tn = M_SOLID;
-        if (r < y1) {
-            kn = __ldg(pK + crow(r + 2) * P + cx);
-            on = __ldg(pO + crow(r + 2) * P + cx);
-            if (xl) { kxn = __ldg(pK + crow(r + 1) * P + cxx); oxn = __ldg(pO + crow(r + 1) * P + cxx); }
-            if (r + 1 < ny) {
-                const int g = (r + 1) * P + cx;
-                yvn = __ldg(pY + g); rhn = __ldg(pR + g); ntn = __ldg(pN + g);
-                tn = (uint16_t)__ldg(p.ntype + g);
-            }
-            if (icol && r >= 0) {
-                const int g = r * P + cx;
-                un = __ldg(pU + g); vn = __ldg(pV + g);
-                san = __ldg(pS + g); sbn = __ldg(pS + D + g); scn = __ldg(pS + 2 * D + g);
-            }
-        }
+        if (r + 1 < ny && r < y1) tn = (uint16_t)__ldg(p.ntype + (r + 1) * P + cx);
         // ---- closure of row r ----------------------------------------------
         FT ke = __shfl_down_sync(FULL, k2, 1), kw = __shfl_up_sync(FULL, k2, 1);
         FT oe = __shfl_down_sync(FULL, o2, 1), ow = __shfl_up_sync(FULL, o2, 1);
@@ -403,15 +447,14 @@ komega_assemble_kernel(const AsmParams p, const double* dt_dev) {
             }
         }
         // ---- advance one row -------------------------------------------------
-        k0 = k1; k1 = k2; k2 = k3; k3 = kn;
-        o0 = o1; o1 = o2; o2 = o3; o3 = on;
-        kx = kxn; ox = oxn;
+        k0 = k1; k1 = k2; k2 = k3;
+        o0 = o1; o1 = o2; o2 = o3;
         dk0 = dk1; do0 = do1; dk1 = dk2; do1 = do2;
         f1m = f1; mxm = mx; mym = my;
         tm = t; yvm = yv; rhm = rh; ntm = nt;
-        t = tn; yv = yvn; rh = rhn; nt = ntn;
-        u1 = un; v1 = vn; sa1 = san; sb1 = sbn; sc1 = scn;
+        t = tn;
     }
+    km_wait<0>();
 }
 
 }  // namespace kofm
