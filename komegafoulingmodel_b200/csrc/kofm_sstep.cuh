@@ -622,6 +622,60 @@ __device__ __forceinline__ void ss_gram(const SsArgs& a, const KoSystem& S, cons
     for (int i = 0; i < NGL; ++i) acc[i] = s[i];
 }
 
+// The same sums with each thread's node values streamed through a ring of
+// SP_GRAM_RING nodes in dynamic shared memory ([slot][level][thread],
+// cp.async SP_GRAM_RING - 1 nodes ahead): the (L+1)(L+2)/2 sums hold most of
+// a thread's registers, so the loads in flight come from the ring, not from
+// more warps.  Each thread reads back only what it copied: no barrier.
+constexpr int SP_GRAM_RING = 4;
+__host__ __device__ constexpr size_t sp_gram_dsmem(int L) {
+    return sizeof(double) * SP_GRAM_RING * (L + 1) * SS_THREADS;
+}
+__device__ __forceinline__ void ss_cp8(double* dst, const double* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+}
+template <int L>
+__device__ __forceinline__ void ss_gram_ring(const SsArgs& a, const KoSystem& S, const double* p0, long long g0,
+                                             long long g1, double* ring, double* acc) {
+    constexpr int NGL = (L + 1) * (L + 2) / 2;
+    constexpr int R = SP_GRAM_RING;
+    double s[NGL];
+#pragma unroll
+    for (int i = 0; i < NGL; ++i) s[i] = 0.0;
+    double* mine = ring + threadIdx.x;
+    auto issue = [&](long long g, int slot) {
+        if (g < g1) {
+            double* d = mine + slot * (L + 1) * SS_THREADS;
+            ss_cp8(d, p0 + g);
+            const long long vb = (g >> 5) * (a.K * 32) + (g & 31);
+#pragma unroll
+            for (int j = 1; j <= L; ++j) ss_cp8(d + j * SS_THREADS, S.V + vb + (j - 1) * 32);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    long long g = g0 + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < R - 1; ++k) issue(g + k * SS_THREADS, k);
+    for (int slot = 0; g < g1; g += SS_THREADS, slot = (slot + 1) & (R - 1)) {
+        // the copies of node g + (R - 1) threads-strides ahead go into the slot
+        // read in the previous iteration
+        issue(g + (R - 1) * SS_THREADS, (slot + R - 1) & (R - 1));
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(R - 1) : "memory");
+        const double* d = mine + slot * (L + 1) * SS_THREADS;
+        double p[L + 1];
+#pragma unroll
+        for (int j = 0; j <= L; ++j) p[j] = d[j * SS_THREADS];
+#pragma unroll
+        for (int j = 0; j <= L; ++j)
+#pragma unroll
+            for (int i = 0; i <= j; ++i) s[ss_gslot(i, j)] += p[i] * p[j];
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < NGL; ++i) acc[i] = s[i];
+}
+
 __device__ void ss_block_reduce(const double* v, int n, double* part, int base, SsSmem& sm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int s = 0; s < n; ++s) {
@@ -1010,8 +1064,8 @@ sp_powers_kernel(const SsArgs a, int s) {
 // Gram of p_0 .. p_L of system s; the last block runs the system's serial
 // step (the simpler-GMRES cycle in the power basis, one warp).  Each block
 // takes a fixed contiguous range of nodes (deterministic sums); a thread
-// takes one node per iteration (two for L <= 6, where the registers allow),
-// its L + 1 loads in flight together.
+// takes one node per iteration, its L + 1 values copied SP_GRAM_RING - 1
+// iterations ahead (dynamic shared memory: sp_gram_dsmem(L)).
 template <int L>
 __global__ void __launch_bounds__(SS_THREADS)
 sp_gram_kernel(const SsArgs a, int s) {
@@ -1026,8 +1080,9 @@ sp_gram_kernel(const SsArgs a, int s) {
         const long long n32 = a.D / 32;
         const long long g0 = n32 * blockIdx.x / gridDim.x * 32;
         const long long g1 = n32 * (blockIdx.x + 1) / gridDim.x * 32;
+        extern __shared__ __align__(16) double sp_gram_ring_smem[];
         double acc[SS_NG];
-        ss_gram<L, (L <= 6 ? 2 : 1)>(a, S, p0, g0, g1, acc);
+        ss_gram_ring<L>(a, S, p0, g0, g1, sp_gram_ring_smem, acc);
         double v[NGL];
 #pragma unroll
         for (int i = 0; i < NGL; ++i) v[i] = acc[i];
