@@ -198,41 +198,68 @@ __device__ __forceinline__ void km_closure(const AsmParams& p, int rec, FT kc, F
     Do = CT(p.mu) + (CT(KO_SIGMA_O1) * F1 + CT(KO_SIGMA_O2) * (CT(1) - F1)) * CT(nt);
 }
 
-// One normalised row, k or omega: advection velocity J, diffusivity d, time
-// step dtr and sink Scr of the row, numerator src of its right-hand side,
-// the field x at the node and its neighbours; coefficients E, W, N, S at
-// coef[cb + 32 j], b - A x at rhs[g] (the sum in the CSR order S, W, C, E, N).
+// Diagonal of a row, k or omega: advection velocity J, diffusivity d, time
+// step dtr and sink Scr of the row.
+template <bool UNIT>
+__device__ __forceinline__ double km_diag(const Fd3& X, const Fd3& X2, const Fd3& Y, const Fd3& Y2, double Jx,
+                                          double Jy, double d, double dtr, double Scr) {
+    // unit weights: X.c = Y.c = 0, X2.c + Y2.c = -4
+    if (UNIT) return 1. + dtr * (4. * d) - Scr;
+    return 1. + dtr * (Jx * X.c + Jy * Y.c - d * (X2.c + Y2.c)) - Scr;
+}
+
+// One row normalised by the reciprocal ic of its diagonal: coefficients E, W,
+// N, S at coef[cb + 32 j]; b - A x at rhs[g], with b = src ic and the sum in
+// the CSR order S, W, C, E, N over the field x at the node and its
+// neighbours.
 template <bool UNIT, typename FT>
 __device__ __forceinline__ void km_row(const Fd3& X, const Fd3& X2, const Fd3& Y, const Fd3& Y2, double Jx,
-                                       double Jy, double d, double dtr, double Scr, double src, FT xc, FT xe,
+                                       double Jy, double d, double dtr, double ic, double src, FT xc, FT xe,
                                        FT xw, FT xn, FT xs, double* coef, int cb, double* rhs, int g) {
-    double c, e, w, n, s;
+    double e, w, n, s;
     if (UNIT) {
-        // X.c = Y.c = 0, X2.c + Y2.c = -4, X2.e = X2.w = 1
-        c = 1. + dtr * (4. * d) - Scr;
+        // X2.e = X2.w = 1
         e = dtr * (0.5 * Jx - d);
         w = dtr * (-0.5 * Jx - d);
         n = dtr * (0.5 * Jy - d);
         s = dtr * (-0.5 * Jy - d);
     } else {
-        c = 1. + dtr * (Jx * X.c + Jy * Y.c - d * (X2.c + Y2.c)) - Scr;
         e = dtr * (Jx * X.e - d * X2.e);
         w = dtr * (Jx * X.w - d * X2.w);
         n = dtr * (Jy * Y.e - d * Y2.e);
         s = dtr * (Jy * Y.w - d * Y2.w);
     }
-    const double ic = 1. / c;
     e *= ic; w *= ic; n *= ic; s *= ic;
     const double Ax = s * (double)xs + w * (double)xw + (double)xc + e * (double)xe + n * (double)xn;
     coef[cb] = e; coef[cb + 32] = w; coef[cb + 64] = n; coef[cb + 96] = s;
     rhs[g] = src * ic - Ax;
 }
 
+// Both rows of a node.  One FP64 reciprocal serves the three divisions of
+// the node (the two diagonals and gamma / nu_t): r = 1 / (Kc Wc nu_t), then
+// 1/Kc = Wc nu_t r, 1/Wc = Kc nu_t r, 1/nu_t = Kc Wc r (a few ulp from the
+// quotients; a row's coefficients and right-hand side take the same factor).
+template <bool UNIT, typename FT>
+__device__ __forceinline__ void km_pair(const AsmParams& p, const Fd3& X, const Fd3& X2, const Fd3& Y,
+                                        const Fd3& Y2, double Jxk, double Jyk, double Jxo, double Jyo,
+                                        double dk, double dom, double dt, double dtw, double Sc, double Scw,
+                                        double kv, double omw, double Pk, double gnum, double nt, int g, int cb,
+                                        FT kc, FT ke, FT kw, FT kn, FT ks, FT oc, FT oe, FT ow, FT on, FT os) {
+    const double Kc = km_diag<UNIT>(X, X2, Y, Y2, Jxk, Jyk, dk, dt, Sc);
+    const double Wc = km_diag<UNIT>(X, X2, Y, Y2, Jxo, Jyo, dom, dtw, Scw);
+    const double KW = Kc * Wc;
+    const double r = 1. / (KW * nt);
+    const double gam = gnum * (KW * r);
+    km_row<UNIT>(X, X2, Y, Y2, Jxk, Jyk, dk, dt, (Wc * nt) * r, kv + dt * Pk, kc, ke, kw, kn, ks, p.coef_k, cb,
+                 p.rhs_k, g);
+    km_row<UNIT>(X, X2, Y, Y2, Jxo, Jyo, dom, dtw, (Kc * nt) * r, omw + dtw * (gam * Pk), oc, oe, ow, on, os,
+                 p.coef_o, cb, p.rhs_o, g);
+}
+
 // Rows of one fluid node (Update_kOmega_Coeffs_Implicit,
 // kOmegaKernels.cl:187-480), normalised by their diagonals, and
-// b' = b - A x0 summed in the CSR order of an interior row (S, W, C, E, N).
-// D* are the diffusivities of the node and its neighbours; cb is the
-// interleaved index of coefficient 0 of node g.
+// b' = b - A x0.  D* are the diffusivities of the node and its neighbours;
+// cb is the interleaved index of coefficient 0 of node g.
 template <typename CT, typename FT>
 __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, int rec, int g, int cb,
                                         CT dkc, CT dke, CT dkw, CT dkn, CT dks, CT doc, CT doe, CT dow,
@@ -248,7 +275,7 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
     const double f1 = F1;
     double Pk = 2. * nt * (Sxx * Sxx + Syy * Syy + 2. * Sxy * Sxy) - 2. / 3. * kv * rho * (Sxx + Syy);
     Pk = dmaxr(dminr(Pk, 10. * KO_BETA_STAR * kv * om), 0.0);
-    const double gam = (f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2) / nt;
+    const double gnum = f1 * KO_GAMMA1 + (1. - f1) * KO_GAMMA2;  // gamma nu_t
     const double Sc = -KO_BETA_STAR * om;
     // the omega row of a node beside an E/W/N/S wall holds the wall value
     // (kOmegaKernels.cl:389-403): no time derivative, no source
@@ -261,17 +288,15 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
         const double olog = sqrt(kv) / (KO_C_MU_0_25 * KO_KAPPA * yp);
         omw = dminr(1000., sqrt(ovis * ovis + olog * olog));
     }
-    const double srck = kv + dt * Pk, srcw = omw + dtw * (gam * Pk);
     if (rec < 0) {
-        const Fd3 Z = {0., 0., 0.};  // unit weights: constants inside km_row
+        const Fd3 Z = {0., 0., 0.};  // unit weights: constants inside km_pair
         const double dk_dx = (double)(CT(0.5) * (dke - dkw));
         const double do_dx = (double)(CT(0.5) * (doe - dow));
         const double dk_dy = (double)(CT(0.5) * (dkn - dks));
         const double do_dy = (double)(CT(0.5) * (don - dos));
-        km_row<true>(Z, Z, Z, Z, Ux - dk_dx, Uy - dk_dy, dk, dt, Sc, srck, kc, ke, kw, kn, ks,
-                     p.coef_k, cb, p.rhs_k, g);
-        km_row<true>(Z, Z, Z, Z, Ux - do_dx - (double)mx, Uy - do_dy - (double)my, dom, dtw, Scw, srcw,
-                     oc, oe, ow, on, os, p.coef_o, cb, p.rhs_o, g);
+        km_pair<true>(p, Z, Z, Z, Z, Ux - dk_dx, Uy - dk_dy, Ux - do_dx - (double)mx, Uy - do_dy - (double)my,
+                      dk, dom, dt, dtw, Sc, Scw, kv, omw, Pk, gnum, nt, g, cb, kc, ke, kw, kn, ks, oc, oe, ow,
+                      on, os);
     } else {
         Fd3 X, X2, Y, Y2;
         km_weights(p, rec, X, X2, Y, Y2);
@@ -279,10 +304,9 @@ __device__ __forceinline__ void km_rows(const AsmParams& p, double dt, int t, in
         const double do_dx = X.e * (double)doe + X.w * (double)dow + X.c * dom;
         const double dk_dy = Y.e * (double)dkn + Y.w * (double)dks + Y.c * dk;
         const double do_dy = Y.e * (double)don + Y.w * (double)dos + Y.c * dom;
-        km_row<false>(X, X2, Y, Y2, Ux - dk_dx, Uy - dk_dy, dk, dt, Sc, srck, kc, ke, kw, kn, ks,
-                      p.coef_k, cb, p.rhs_k, g);
-        km_row<false>(X, X2, Y, Y2, Ux - do_dx - (double)mx, Uy - do_dy - (double)my, dom, dtw, Scw, srcw,
-                      oc, oe, ow, on, os, p.coef_o, cb, p.rhs_o, g);
+        km_pair<false>(p, X, X2, Y, Y2, Ux - dk_dx, Uy - dk_dy, Ux - do_dx - (double)mx,
+                       Uy - do_dy - (double)my, dk, dom, dt, dtw, Sc, Scw, kv, omw, Pk, gnum, nt, g, cb, kc,
+                       ke, kw, kn, ks, oc, oe, ow, on, os);
     }
 }
 
