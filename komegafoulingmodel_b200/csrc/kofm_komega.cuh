@@ -140,10 +140,12 @@ __host__ __device__ __forceinline__ int km_wrap(int x, int nx) {
 }
 
 // Blending function F1 (kOmegaKernels.cl:68-87), in the closure's type.
+// The FP32 form's quotients are the fast ones (__fdividef, 2 ulp): F1 =
+// tanh(a^4) carries four times the rounding of a either way.
 __device__ __forceinline__ float ko_f1(float kv, float om, float yv, float rho, float cdx, float mu) {
     const float CDkw = fmaxf(rho * cdx, 1.0e-10f);
-    float a = fmaxf(sqrtf(kv) / ((float)KO_BETA_STAR * om * yv), 500.f * mu / (yv * yv * om));
-    a = fminf(a, 4.f * kv * (float)KO_SIGMA_O2 / (CDkw * yv * yv));
+    float a = fmaxf(__fdividef(sqrtf(kv), (float)KO_BETA_STAR * om * yv), __fdividef(500.f * mu, yv * yv * om));
+    a = fminf(a, __fdividef(4.f * kv * (float)KO_SIGMA_O2, CDkw * yv * yv));
     const float a2 = a * a;
     return tanhf(a2 * a2);
 }
@@ -155,6 +157,9 @@ __device__ __forceinline__ double ko_f1(double kv, double om, double yv, double 
     const double a2 = a * a;
     return tanh(a2 * a2);
 }
+
+__device__ __forceinline__ float km_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double km_div(double a, double b) { return a / b; }
 
 // Weights of a node with a link-fraction record (NESW_BOUNDARY nodes whose
 // dX differs from 1); rec < 0 means the unit weights d1 = (1/2, -1/2, 0),
@@ -190,7 +195,7 @@ __device__ __forceinline__ void km_closure(const AsmParams& p, int rec, FT kc, F
         dOdy = CT(Y.e) * CT(on) + CT(Y.w) * CT(os) + CT(Y.c) * CT(oc);
         dKdy = CT(Y.e) * CT(kn) + CT(Y.w) * CT(ks) + CT(Y.c) * CT(kc);
     }
-    const CT m = CT(2. * KO_SIGMA_O2) / CT(oc);
+    const CT m = km_div(CT(2. * KO_SIGMA_O2), CT(oc));
     mx = m * dKdx;
     my = m * dKdy;
     F1 = ko_f1(CT(kc), CT(oc), CT(yv), CT(rho), mx * dOdx + my * dOdy, CT(p.mu));
@@ -216,20 +221,20 @@ template <bool UNIT, typename FT>
 __device__ __forceinline__ void km_row(const Fd3& X, const Fd3& X2, const Fd3& Y, const Fd3& Y2, double Jx,
                                        double Jy, double d, double dtr, double ic, double src, FT xc, FT xe,
                                        FT xw, FT xn, FT xs, double* coef, int cb, double* rhs, int g) {
+    const double f = dtr * ic;  // time step over the diagonal
     double e, w, n, s;
     if (UNIT) {
         // X2.e = X2.w = 1
-        e = dtr * (0.5 * Jx - d);
-        w = dtr * (-0.5 * Jx - d);
-        n = dtr * (0.5 * Jy - d);
-        s = dtr * (-0.5 * Jy - d);
+        e = (0.5 * Jx - d) * f;
+        w = (-0.5 * Jx - d) * f;
+        n = (0.5 * Jy - d) * f;
+        s = (-0.5 * Jy - d) * f;
     } else {
-        e = dtr * (Jx * X.e - d * X2.e);
-        w = dtr * (Jx * X.w - d * X2.w);
-        n = dtr * (Jy * Y.e - d * Y2.e);
-        s = dtr * (Jy * Y.w - d * Y2.w);
+        e = (Jx * X.e - d * X2.e) * f;
+        w = (Jx * X.w - d * X2.w) * f;
+        n = (Jy * Y.e - d * Y2.e) * f;
+        s = (Jy * Y.w - d * Y2.w) * f;
     }
-    e *= ic; w *= ic; n *= ic; s *= ic;
     const double Ax = s * (double)xs + w * (double)xw + (double)xc + e * (double)xe + n * (double)xn;
     coef[cb] = e; coef[cb + 32] = w; coef[cb + 64] = n; coef[cb + 96] = s;
     rhs[g] = src * ic - Ax;
