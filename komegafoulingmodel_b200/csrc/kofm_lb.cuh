@@ -113,6 +113,12 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 }
 
 // ---------------------------------------------------------------------------
+// Quotients of the SST eddy viscosity: the fast FP32 quotient (__fdividef,
+// 2 ulp) for the FP32 fields, whose rounding (~1e-7) already bounds nu_t;
+// the IEEE quotient in FP64.
+__device__ __forceinline__ float lb_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double lb_div(double a, double b) { return a / b; }
+
 // NEQ: populations stored as f - feq(reference moments of the writing node),
 // FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.  FT: type of the node fields
 // (k, omega, strain rates, wall distance, nu_t, moments) -- FP32, or FP64 for
@@ -295,10 +301,8 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
         const AT rho = AT(1) + drho;
         const AT jx = d[1][j] - d[2][j] + d[5][j] - d[6][j] + d[7][j] - d[8][j];
         const AT jy = d[3][j] - d[4][j] + d[5][j] - d[6][j] - d[7][j] + d[8][j];
-        const AT inv = AT(1) / rho;
-        const AT ux = inv * jx, uy = inv * jy;
-
         AT w = tau0;
+        AT inv;  // 1 / rho
         if (KOMEGA) {
             // SST eddy viscosity (lbKernels.cl:400-451) in the fields' type:
             // FP32 for the FP32 fields (nu_t is stored in FP32; the relaxation
@@ -311,17 +315,25 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
             if (om < FT(0)) { om = fabs(om); fO[node] = om; }
             if (kv < FT(0)) { kv = FT(1e-16); fK[node] = FT(1e-16); }
             const FT mu_f = (FT)p.mu;
-            const FT a = FT(2) * sqrt(kv) / ((FT)KO_BETA_STAR * om * yv);
-            const FT b = FT(500) * mu_f / (yv * yv * om);
+            const FT a = lb_div(FT(2) * sqrt(kv), (FT)KO_BETA_STAR * om * yv);
+            const FT b = lb_div(FT(500) * mu_f, yv * yv * om);
             const FT arg = fmax(a, b);
             FT F2 = tanh(arg * arg);
             const FT sxx = sin3[0][j], sxy = sin3[1][j], syy = sin3[2][j];
             F2 *= sqrt(FT(2) * (sxx * sxx + FT(2) * sxy * sxy + syy * syy));
             const FT a1 = (FT)KO_A1;
-            const FT nut = fmax(fmin((FT)p.maxnut, a1 * kv / fmax(a1 * om, F2)), FT(1e-16));
+            const FT nut = fmax(fmin((FT)p.maxnut, lb_div(a1 * kv, fmax(a1 * om, F2))), FT(1e-16));
             o_nut[j] = nut;
-            w = AT(1) / (AT(3) * (AT(nut) + mu) + AT(0.5));
+            // one reciprocal for 1 / rho and the relaxation rate
+            // 1 / (3 (nu_t + mu) + 1/2): r = 1 / (rho den), 1/rho = den r, w = rho r
+            const AT den = AT(3) * (AT(nut) + mu) + AT(0.5);
+            const AT r = AT(1) / (rho * den);
+            inv = den * r;
+            w = rho * r;
+        } else {
+            inv = AT(1) / rho;
         }
+        const AT ux = inv * jx, uy = inv * jy;
         AT sxx_n = AT(0), sxy_n = AT(0), syy_n = AT(0);
         // NEQ32: the mass and momentum that the FP32 moments leave out -- rho
         // = 1 + drho rounded on the FP32 grid near 1 (up to 6e-8), u = j / rho
@@ -392,7 +404,7 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
         }
         o_u0[j] = (float)ux;
         if (KOMEGA) {
-            const AT s = AT(-1.5) * tau0 / rho;
+            const AT s = AT(-1.5) * tau0 * inv;
             o_s[0][j] = (FT)(s * sxx_n);
             o_s[1][j] = (FT)(s * sxy_n);
             o_s[2][j] = (FT)(s * syy_n);
