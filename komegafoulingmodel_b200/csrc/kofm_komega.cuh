@@ -109,7 +109,7 @@ constexpr int KM_W = 30;
 #endif
 constexpr int KM_WARPS = KOFM_ASM_WARPS;
 #ifndef KOFM_ASM_ROWS
-#define KOFM_ASM_ROWS 32
+#define KOFM_ASM_ROWS 16
 #endif
 #ifndef KOFM_ASM_MINBLOCKS
 #define KOFM_ASM_MINBLOCKS 4  // resident blocks per SM the register budget is set for
