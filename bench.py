@@ -102,7 +102,8 @@ class ClockSampler:
 STORAGE_NAMES = {"fp32": "fp32 f-w deviation", "fp16": "fp16 f-w deviation",
                  "bf16": "bf16 f-w deviation", "fp16neq": "fp16 f-feq (FP32 reference moments)",
                  "fp64": "fp64 f-w deviation, fp64 fields",
-                 "fp16neq32": "fp16 f-feq (FP32 reference moments), fp32 collide"}
+                 "fp16neq32": "fp16 f-feq (FP32 reference moments), fp32 collide",
+                 "fp16row": "fp16 f-feq (one reference per row), fp32 collide"}
 
 
 def workload_config(w, args, world: int) -> dict:
@@ -165,11 +166,13 @@ SOLVER_TRAFFIC_RATIO = {
     "sstep_phases": None,                          # the same, one launch per sweep
 }
 
-STORE_BYTES = {"fp32": 4, "fp16": 2, "bf16": 2, "fp16neq": 2, "fp16neq32": 2, "fp64": 8}
+STORE_BYTES = {"fp32": 4, "fp16": 2, "bf16": 2, "fp16neq": 2, "fp16neq32": 2, "fp16row": 2, "fp64": 8}
 # laminar collide (no macro fields saved by the plain step): f read + write, flags
-LB_BYTES_LAMINAR = {"fp32": 74, "fp16": 38, "bf16": 38, "fp16neq": 62, "fp16neq32": 62, "fp64": 146}
+LB_BYTES_LAMINAR = {"fp32": 74, "fp16": 38, "bf16": 38, "fp16neq": 62, "fp16neq32": 62, "fp16row": 38,
+                    "fp64": 146}
 LB_BYTES = {"fp32": 126, "fp16": 90, "bf16": 90,   # k-omega collide, per node
             "fp16neq": 114, "fp16neq32": 114,  # + reference moments read and written
+            "fp16row": 90,                      # row references: a few KB, cached
             "fp64": 250}                      # FP64 populations and fields
 ASM_BYTES = {"fp64": 162}                           # fused assembly, per node (FP64 fields)
 ASM_BYTES_FP32 = 122                                # ... FP32 fields
@@ -190,7 +193,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     storage = {"fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV, "bf16": _abi.STORE_BF16_DEV,
                "fp16neq": _abi.STORE_FP16_NEQ, "fp64": _abi.STORE_FP64,
-               "fp16neq32": _abi.STORE_FP16_NEQ32}[args.storage]
+               "fp16neq32": _abi.STORE_FP16_NEQ32, "fp16row": _abi.STORE_FP16_ROW}[args.storage]
     asm_bytes = ASM_BYTES.get(args.storage, ASM_BYTES_FP32)
     w = W.by_name(args.workload)
     d = W.descriptor(w, storage=storage)
@@ -461,7 +464,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="komega_straight_16384x1024")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp16neq32", "fp64"])
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16", "fp16neq", "fp16neq32", "fp16row", "fp64"])
     ap.add_argument("--solver", default="sstep", choices=["sstep", "sstep_host", "sstep_coop", "classic"],
                     help="k-omega solve: a cycle's Krylov directions in one sweep, each sweep "
                          "its own launch in a device-driven update graph (default) or enqueued "

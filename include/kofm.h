@@ -79,6 +79,15 @@ extern "C" {
                                  FTYPE double), the truth of the precision
                                  study.  Not with the thermal update, the
                                  device geometry builder or the adjoint. */
+#define KOFM_STORE_FP16_ROW 6 /* f_i - feq_i(rho_R(y), u_R(y)) in FP16 (scaled
+                                 by 2^12) with ONE reference per row: the mean
+                                 density and velocity of the row's fluid nodes
+                                 at kofm_set_state, re-centred on the row means
+                                 of the moments every 32 collides that save
+                                 them (the stored values re-encoded).  FP32
+                                 collide arithmetic.  Suited to flows close to
+                                 their row profile (straight channels); not in
+                                 kofm_batch.  No counterpart in the reference. */
 
 /* ---- fields for kofm_reduce ---------------------------------------------- */
 #define KOFM_FIELD_RHO 0   /* Ro_array   (clVariablesLB.cpp:343-345 sumRo) */

@@ -32,6 +32,7 @@ ERR_TIMEOUT = -204
 
 OPTION_SAVE_MACRO_FIELDS = 0x2
 STORE_FP32, STORE_FP16_DEV, STORE_BF16_DEV, STORE_FP16_NEQ, STORE_FP64, STORE_FP16_NEQ32 = 0, 1, 2, 3, 4, 5
+STORE_FP16_ROW = 6
 FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_K, FIELD_OMEGA, FIELD_NUT, FIELD_WALL_SHEAR, FIELD_TEMP = range(8)
 WALLS_IBB_ALL, WALLS_SEAM_IBB = 1, 2
 OP_SUM, OP_MIN, OP_MAX = 0, 1, 2

@@ -72,6 +72,9 @@ struct kofm_ctx {
     // lattice state
     void* g[2] = {nullptr, nullptr};  // population buffers (9 planes each)
     float* ref[2] = {nullptr, nullptr};  // KOFM_STORE_FP16_NEQ: reference rho, ux, uy of g[b]
+    float* rowref = nullptr;             // KOFM_STORE_FP16_ROW: rho, ux, uy of each row ([3][ny])
+    float* rowref_next = nullptr;        //   the next references (re-centring)
+    long long row_steps = 0;             //   collides since the last re-centring
     int cur = 0;                      // buffer holding the current state
     int phase = 0;                    // 0: FA form, 1: post-collision (pull)
     int16_t* ntype = nullptr;
@@ -255,6 +258,133 @@ __global__ void k_fa_in_neq(const double* __restrict__ f, __half* __restrict__ g
     }
 }
 
+// Reference of the stored populations of a non-equilibrium form: per node
+// (KOFM_STORE_FP16_NEQ*: rho, ux, uy planes of D) or per row
+// (KOFM_STORE_FP16_ROW: [3][ny]); neither for the f - w forms.
+struct PopRef {
+    const float* node;
+    const float* row;
+};
+
+// Row references of KOFM_STORE_FP16_ROW from the host-layout FP64 FA: the
+// mean density of the row's fluid nodes and its mean velocity (momentum over
+// mass); 1, 0, 0 for a row without fluid.  One block per row.
+__global__ void k_row_ref(const double* __restrict__ f, float* __restrict__ rowref,
+                          const int16_t* __restrict__ nt, int nx, int nxf, int ny, int P) {
+    const int y = blockIdx.x;
+    const long long Dh = (long long)nxf * ny;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};  // rho, jx, jy, nodes
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        if ((uint16_t)nt[(long long)y * P + x] & M_SOLID) continue;
+        for (int q = 0; q < 9; ++q) {
+            const double fq = f[q * Dh + (long long)y * nxf + x];
+            s[0] += fq;
+            s[1] += cx_of(q) * fq;
+            s[2] += cy_of(q) * fq;
+        }
+        s[3] += 1.0;
+    }
+    __shared__ double red[4][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < 4; ++k) {
+        double v = s[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[k][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < 4; ++k)
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t[k] += red[k][i];
+        const bool any = t[3] > 0.0 && t[0] > 0.0;
+        rowref[y] = any ? (float)(t[0] / t[3]) : 1.f;
+        rowref[ny + y] = any ? (float)(t[1] / t[0]) : 0.f;
+        rowref[2 * ny + y] = any ? (float)(t[2] / t[0]) : 0.f;
+    }
+}
+
+// host-layout FP64 FA -> row-reference form: e = f - feq(reference of the
+// node's row), scaled, in FP16
+__global__ void k_fa_in_row(const double* __restrict__ f, __half* __restrict__ g,
+                            const float* __restrict__ rowref, const int16_t* __restrict__ nt, int nx,
+                            int nxf, int ny, int P, long long D) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= P) return;
+    const long long node = (long long)y * P + x;
+    const bool fluid = x < nx && !((uint16_t)nt[node] & M_SOLID);
+    const long long Dh = (long long)nxf * ny;
+    const float r = rowref[y], u = rowref[ny + y], v = rowref[2 * ny + y];
+    for (int q = 0; q < 9; ++q) {
+        const double fq = fluid ? f[q * Dh + (long long)y * nxf + x] : 0.0;
+        const float e = fluid ? (float)((fq - weight_of(q)) - (double)feq_dev_f32(q, r, u, v)) : 0.f;
+        g[q * D + node] = __float2half_rn(e * NEQ_SCALE);
+    }
+}
+
+// Collide arithmetic of KOFM_STORE_FP16_ROW.
+#ifndef KOFM_ROW_AT
+#define KOFM_ROW_AT float
+#endif
+// Collides between re-centrings of the row references (KOFM_STORE_FP16_ROW).
+#ifndef KOFM_ROW_RECENTRE
+#define KOFM_ROW_RECENTRE 32
+#endif
+
+// Row references from the moments the last collide wrote: the row's mean
+// density and its mean velocity (momentum over mass) over its fluid nodes.
+__global__ void k_row_ref_fields(const float* __restrict__ rho, const float* __restrict__ ux,
+                                 const float* __restrict__ uy, float* __restrict__ rowref,
+                                 const int16_t* __restrict__ nt, int nx, int ny, int P) {
+    const int y = blockIdx.x;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};  // rho, jx, jy, nodes
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        const long long n = (long long)y * P + x;
+        if ((uint16_t)nt[n] & M_SOLID) continue;
+        const double r = rho[n];
+        s[0] += r;
+        s[1] += r * ux[n];
+        s[2] += r * uy[n];
+        s[3] += 1.0;
+    }
+    __shared__ double red[4][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < 4; ++k) {
+        double v = s[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[k][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < 4; ++k)
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t[k] += red[k][i];
+        const bool any = t[3] > 0.0 && t[0] > 0.0;
+        rowref[y] = any ? (float)(t[0] / t[3]) : 1.f;
+        rowref[ny + y] = any ? (float)(t[1] / t[0]) : 0.f;
+        rowref[2 * ny + y] = any ? (float)(t[2] / t[0]) : 0.f;
+    }
+}
+
+// Re-encodes the stored populations of every fluid node against the new
+// references of its row: e' = e + feq(old) - feq(new) (scaled, FP16).
+__global__ void k_row_recentre(__half* __restrict__ g, const float* __restrict__ oldref,
+                               const float* __restrict__ newref, const int16_t* __restrict__ nt, int nx,
+                               int ny, int P, long long D) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= nx) return;
+    const long long node = (long long)y * P + x;
+    if ((uint16_t)nt[node] & M_SOLID) return;
+    const float r0 = oldref[y], u0 = oldref[ny + y], v0 = oldref[2 * ny + y];
+    const float r1 = newref[y], u1 = newref[ny + y], v1 = newref[2 * ny + y];
+    for (int q = 0; q < 9; ++q) {
+        const float e = __half2float(g[q * D + node]) +
+                        (feq_dev_f32(q, r0, u0, v0) - feq_dev_f32(q, r1, u1, v1)) * NEQ_SCALE;
+        g[q * D + node] = __float2half_rn(e);
+    }
+}
+
 // device state -> host-layout FP64 FA.  phase 0: own deviations; phase 1:
 // gather + bounce-back + interpolated bounce-back (the next step's pull).
 // Deviations f - w of the populations FA of fluid node (x, y) -- the
@@ -266,13 +396,19 @@ __global__ void k_fa_in_neq(const double* __restrict__ f, __half* __restrict__ g
 template <typename ST>
 __device__ void fa_node(const ST* __restrict__ g, int type, const int32_t* __restrict__ rec,
                         const IbbRecord* __restrict__ ibb, int has_ibb, int nx, int ny, int P,
-                        long long D, int phase, const float* __restrict__ ref, int x, int y,
-                        double d[9]) {
+                        long long D, int phase, PopRef ref, int x, int y, double d[9]) {
     auto dec = [&](int q, long long n) -> double {
         const double raw = Store<ST>::to_f64(g[q * D + n]);
-        if (!ref) return raw;
-        return (double)(feq_dev_f32(q, ref[n], ref[D + n], ref[2 * D + n]) +
-                        (float)raw * NEQ_INV_SCALE);
+        if (ref.node) {
+            const float* rf = ref.node;
+            return (double)(feq_dev_f32(q, rf[n], rf[D + n], rf[2 * D + n]) + (float)raw * NEQ_INV_SCALE);
+        }
+        if (ref.row) {
+            const int r = (int)(n / P);
+            const float* rr = ref.row;
+            return (double)(feq_dev_f32(q, rr[r], rr[ny + r], rr[2 * ny + r]) + (float)raw * NEQ_INV_SCALE);
+        }
+        return raw;
     };
     const long long node = (long long)y * P + x;
     for (int q = 0; q < 9; ++q) {
@@ -312,7 +448,7 @@ template <typename ST>
 __global__ void k_fa_out(const ST* __restrict__ g, const int16_t* __restrict__ nt,
                          const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
                          int has_ibb, double* __restrict__ f, int nx, int nxf, int ny,
-                         int P, long long D, int phase, const float* __restrict__ ref) {
+                         int P, long long D, int phase, PopRef ref) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= nxf) return;
@@ -336,7 +472,7 @@ template <typename ST, typename FT = float>
 __global__ void k_shear_nodes(const ST* __restrict__ g, const int16_t* __restrict__ nt,
                               const int32_t* __restrict__ rec, const IbbRecord* __restrict__ ibb,
                               int has_ibb, int nx, int ny, int P, long long D, int phase,
-                              const float* __restrict__ ref, const FT* __restrict__ rho,
+                              PopRef ref, const FT* __restrict__ rho,
                               const FT* __restrict__ ux, const FT* __restrict__ uy,
                               const FT* __restrict__ nut, double mu, const int32_t* __restrict__ nodes,
                               const double* __restrict__ cfss, int n, int nxf, double* __restrict__ tau) {
@@ -465,16 +601,16 @@ __global__ void k_wall_shear(const int16_t* __restrict__ nt, const FT* __restric
 }
 
 // ---- LB step dispatch ------------------------------------------------------------
-template <typename ST, typename AT, bool NEQ = false, typename FT = float>
+template <typename ST, typename AT, bool NEQ = false, typename FT = float, bool ROW = false>
 cudaError_t launch_lb(kofm_ctx* c, const LbParams& p, bool komega, bool phase0) {
     dim3 block(32, 4);
     dim3 grid(c->P / 128, (c->desc.ny + 3) / 4);
     if (komega) {
-        if (phase0) lb_step_kernel<ST, AT, true, true, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, true, false, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, true, true, NEQ, FT, ROW><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, true, false, NEQ, FT, ROW><<<grid, block, 0, c->stream>>>(p);
     } else {
-        if (phase0) lb_step_kernel<ST, AT, false, true, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
-        else lb_step_kernel<ST, AT, false, false, NEQ, FT><<<grid, block, 0, c->stream>>>(p);
+        if (phase0) lb_step_kernel<ST, AT, false, true, NEQ, FT, ROW><<<grid, block, 0, c->stream>>>(p);
+        else lb_step_kernel<ST, AT, false, false, NEQ, FT, ROW><<<grid, block, 0, c->stream>>>(p);
     }
     return cudaGetLastError();
 }
@@ -483,7 +619,7 @@ int validate_desc(const kofm_desc* d) {
     if (!d) return KOFM_ERR_INVALID_ARG;
     if (d->nx < 4 || d->ny < 3 || d->nx_full < d->nx) return KOFM_ERR_LOADING_PARAMS;
     if ((long long)d->nx_full * d->ny > (1LL << 31) - 1) return KOFM_ERR_LOADING_PARAMS;
-    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP16_NEQ32) return KOFM_ERR_LOADING_PARAMS;
+    if (d->storage < KOFM_STORE_FP32 || d->storage > KOFM_STORE_FP16_ROW) return KOFM_ERR_LOADING_PARAMS;
     // the FP64 form is the precision study's reference form: no thermal update
     if (d->storage == KOFM_STORE_FP64 && d->use_thermal) return KOFM_ERR_LOADING_PARAMS;
     if (!(d->tau > 0.0 && d->tau < 2.0)) return KOFM_ERR_LOADING_PARAMS;
@@ -561,7 +697,7 @@ int kofm_destroy(kofm_ctx* c) {
     if (!c) return KOFM_ERR_INVALID_ARG;
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
+    void* bufs[] = {c->g[0], c->g[1], c->ref[0], c->ref[1], c->rowref, c->rowref_next, c->ntype, c->rec, c->ibb, c->dxrec_idx, c->dxrec,
                     c->wallD, c->K, c->O, c->S, c->nut, c->rho, c->ux, c->uy,
                     c->lb_partials, c->red_partials, c->red_out, c->staging, c->ctl,
                     c->gpart, c->spart, c->ss_lhint, c->bar, c->shear_nodes, c->shear_cfss, c->shear_tau,
@@ -626,6 +762,10 @@ int kofm_create(const kofm_desc* d, kofm_ctx** out) {
     if (d->storage == KOFM_STORE_FP16_NEQ || d->storage == KOFM_STORE_FP16_NEQ32) {
         ALLOC(c->ref[0], 3 * D);
         ALLOC(c->ref[1], 3 * D);
+    }
+    if (d->storage == KOFM_STORE_FP16_ROW) {
+        ALLOC(c->rowref, 3 * d->ny);
+        ALLOC(c->rowref_next, 3 * d->ny);
     }
 #define ALLOC_FIELD(ptr, n)                                         \
     do {                                                            \
@@ -858,6 +998,11 @@ int kofm_set_state(kofm_ctx* c, const double* f, const double* k, const double* 
         case KOFM_STORE_FP16_NEQ32:
             k_fa_in_neq<<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->ref[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
+        case KOFM_STORE_FP16_ROW:
+            k_row_ref<<<d.ny, 256, 0, c->stream>>>(c->staging, c->rowref, c->ntype, d.nx, d.nx_full, d.ny, c->P);
+            c->row_steps = 0;
+            k_fa_in_row<<<grid, 128, 0, c->stream>>>(c->staging, (__half*)c->g[0], c->rowref, c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
+            break;
         case KOFM_STORE_FP64:
             k_fa_in<double><<<grid, 128, 0, c->stream>>>(c->staging, (double*)c->g[0], c->ntype, d.nx, d.nx_full, d.ny, c->P, c->D);
             break;
@@ -905,20 +1050,23 @@ int kofm_get_state(kofm_ctx* c, double* f, double* k, double* omega, double* nut
         const int has_ibb = c->n_ibb_rec > 0;
         switch (d.storage) {
             case KOFM_STORE_FP32:
-                k_fa_out<float><<<grid, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                k_fa_out<float><<<grid, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr});
                 break;
             case KOFM_STORE_FP16_DEV:
-                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr});
                 break;
             case KOFM_STORE_FP16_NEQ:
             case KOFM_STORE_FP16_NEQ32:
-                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, c->ref[c->cur]);
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{c->ref[c->cur], nullptr});
+                break;
+            case KOFM_STORE_FP16_ROW:
+                k_fa_out<__half><<<grid, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{nullptr, c->rowref});
                 break;
             case KOFM_STORE_FP64:
-                k_fa_out<double><<<grid, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                k_fa_out<double><<<grid, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr});
                 break;
             default:
-                k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, nullptr);
+                k_fa_out<__nv_bfloat16><<<grid, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, c->staging, d.nx, d.nx_full, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr});
         }
         KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
         KOFM_CUDA_TRY(cudaMemcpyAsync(f, c->staging, 9 * Dh * sizeof(double), cudaMemcpyDeviceToHost, c->stream), KOFM_ERR_MEMORY_COPY);
@@ -992,7 +1140,9 @@ int kofm_wall_shear(kofm_ctx* c, double* node_tau, double* bl_tau) {
     cudaSetDevice(c->dev);
     const int n = c->shear_n;
     const int has_ibb = c->n_ibb_rec > 0;
-    const float* ref = (d.storage == KOFM_STORE_FP16_NEQ || d.storage == KOFM_STORE_FP16_NEQ32) ? c->ref[c->cur] : nullptr;
+    const PopRef ref = (d.storage == KOFM_STORE_FP16_NEQ || d.storage == KOFM_STORE_FP16_NEQ32)
+                           ? PopRef{c->ref[c->cur], nullptr}
+                           : PopRef{nullptr, d.storage == KOFM_STORE_FP16_ROW ? c->rowref : nullptr};
     const int nb = (n + 127) / 128;
     const float* frho = (const float*)c->rho;
     const float* fux = (const float*)c->ux;
@@ -1000,13 +1150,13 @@ int kofm_wall_shear(kofm_ctx* c, double* node_tau, double* bl_tau) {
     const float* fnut = (const float*)c->nut;
     switch (d.storage) {
         case KOFM_STORE_FP32:
-            k_shear_nodes<float><<<nb, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<float><<<nb, 128, 0, c->stream>>>((const float*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr}, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
             break;
         case KOFM_STORE_BF16_DEV:
-            k_shear_nodes<__nv_bfloat16><<<nb, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<__nv_bfloat16><<<nb, 128, 0, c->stream>>>((const __nv_bfloat16*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr}, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
             break;
         case KOFM_STORE_FP64:
-            k_shear_nodes<double, double><<<nb, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, nullptr, (const double*)c->rho, (const double*)c->ux, (const double*)c->uy, (const double*)c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
+            k_shear_nodes<double, double><<<nb, 128, 0, c->stream>>>((const double*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, PopRef{nullptr, nullptr}, (const double*)c->rho, (const double*)c->ux, (const double*)c->uy, (const double*)c->nut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
             break;
         default:  // FP16 forms
             k_shear_nodes<__half><<<nb, 128, 0, c->stream>>>((const __half*)c->g[c->cur], c->ntype, c->rec, c->ibb, has_ibb, d.nx, d.ny, c->P, c->D, c->phase, ref, frho, fux, fuy, fnut, d.mu, c->shear_nodes, c->shear_cfss, n, d.nx_full, c->shear_tau);
@@ -1055,6 +1205,7 @@ LbParams lb_params(const kofm_ctx* c, int32_t options, int cur) {
     p.partials = c->lb_partials;
     p.ref_in = c->ref[cur];
     p.ref_out = c->ref[cur ^ 1];
+    p.rowref = c->rowref;
     p.nx = d.nx; p.ny = d.ny; p.P = c->P; p.D = c->D;
     p.tau = d.tau; p.fterm = d.fterm; p.mu = d.mu; p.maxnut = d.max_turb_visc;
     p.options = options;
@@ -1087,6 +1238,7 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
         case KOFM_STORE_FP16_NEQ: e = launch_lb<__half, double, true>(c, p, ko, ph0); break;
         case KOFM_STORE_FP64: e = launch_lb<double, double, false, double>(c, p, ko, ph0); break;
         case KOFM_STORE_FP16_NEQ32: e = launch_lb<__half, float, true>(c, p, ko, ph0); break;
+        case KOFM_STORE_FP16_ROW: e = launch_lb<__half, KOFM_ROW_AT, false, float, true>(c, p, ko, ph0); break;
         default: e = launch_lb<__nv_bfloat16, float>(c, p, ko, ph0); break;
     }
     if (e != cudaSuccess) {
@@ -1094,6 +1246,20 @@ int kofm_lb_step(kofm_ctx* c, int32_t options) {
         return KOFM_ERR_CALLING_KERNEL;
     }
     lb_done(c);
+    if (d.storage == KOFM_STORE_FP16_ROW && (options & KOFM_OPTION_SAVE_MACRO_FIELDS) &&
+        ++c->row_steps >= KOFM_ROW_RECENTRE) {
+        // the row references follow the flow: the row means of the moments
+        // this collide wrote, the stored values re-encoded against them
+        k_row_ref_fields<<<d.ny, 256, 0, c->stream>>>((const float*)c->rho, (const float*)c->ux,
+                                                      (const float*)c->uy, c->rowref_next, c->ntype,
+                                                      d.nx, d.ny, c->P);
+        dim3 grid((c->P + 127) / 128, d.ny);
+        k_row_recentre<<<grid, 128, 0, c->stream>>>((__half*)c->g[c->cur], c->rowref, c->rowref_next,
+                                                    c->ntype, d.nx, d.ny, c->P, c->D);
+        KOFM_CUDA_TRY(cudaGetLastError(), KOFM_ERR_CALLING_KERNEL);
+        std::swap(c->rowref, c->rowref_next);
+        c->row_steps = 0;
+    }
     return KOFM_OK;
 }
 

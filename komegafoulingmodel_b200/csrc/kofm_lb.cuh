@@ -62,6 +62,7 @@ struct LbParams {
     double* partials;       // per block: sum rho, sum ux, sum uy (FP64)
     const float* ref_in;    // non-equilibrium form: reference rho, ux, uy of
     float* ref_out;         //   the populations read / written (3 planes)
+    const float* rowref;    // row-reference form: rho, ux, uy of each row ([3][ny])
     int nx, ny, P;
     long long D;
     double tau, fterm, mu, maxnut;
@@ -119,6 +120,11 @@ __device__ __forceinline__ void pull_row_f32(const float* row, int cx, int lane,
 __device__ __forceinline__ float lb_div(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double lb_div(double a, double b) { return a / b; }
 
+// ROW: populations stored as f - feq(reference moments of their row), FP16
+// scaled as NEQ (KOFM_STORE_FP16_ROW); one reference (rho, u_x, u_y) per row,
+// the same for all the nodes of a row within a collide (the host re-centres
+// them between collides), so a warp decodes the values of one gathered row
+// with one equilibrium per direction and encodes its own row's with another.
 // NEQ: populations stored as f - feq(reference moments of the writing node),
 // FP16 (KOFM_STORE_FP16_NEQ); see feq_dev_f32.  FT: type of the node fields
 // (k, omega, strain rates, wall distance, nu_t, moments) -- FP32, or FP64 for
@@ -138,7 +144,7 @@ __device__ __forceinline__ double lb_div(double a, double b) { return a / b; }
 // lattices.
 constexpr int LB_BLOCK_ROWS = 4;
 
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ, typename FT>
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ, typename FT, bool ROW = false>
 __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int gx) {
     using VT = typename Store<ST>::vt;  // type a population is loaded into
     constexpr bool NEQ32 = NEQ && sizeof(AT) == 4;
@@ -178,9 +184,14 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
 
     AT d[9][4];
     float own_r[4] = {}, own_u[4] = {}, own_v[4] = {};  // NEQ: this node's reference moments
+    // ROW: equilibrium deviation feq - w of the reference moments of row r
+    auto row_feq = [&](int q, int r) -> float {
+        return feq_dev_f32(q, p.rowref[r], p.rowref[p.ny + r], p.rowref[2 * p.ny + r]);
+    };
     // own stored population of direction q, decoded
     auto own_pop = [&](int q, int j) -> AT {
         const VT raw = ld1(gin, q * D + rowoff + x0 + j);
+        if (ROW) return AT(row_feq(q, y)) + AT(raw) * AT(NEQ_INV_SCALE);
         if (!NEQ) return AT(raw);
         return AT(feq_dev_f32(q, own_r[j], own_u[j], own_v[j])) + AT(raw) * AT(NEQ_INV_SCALE);
     };
@@ -233,6 +244,13 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 d[q][j] = AT(feq_dev_f32(q, rr[j], ru[j], rv[j])) + AT(v[j]) * AT(NEQ_INV_SCALE);
+        } else if (ROW) {
+            // the reference of the row the 4 values were read from
+            int ys = y - (PHASE0 ? 0 : cy);
+            ys = ys < 0 ? 0 : (ys >= p.ny ? p.ny - 1 : ys);
+            const AT fe = AT(row_feq(q, ys));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) d[q][j] = fe + AT(v[j]) * AT(NEQ_INV_SCALE);
         } else {
 #pragma unroll
             for (int j = 0; j < 4; ++j) d[q][j] = AT(v[j]);
@@ -421,9 +439,12 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         VT v[4];
+        const AT fe_row = ROW ? AT(row_feq(q, y)) : AT(0);  // this row's reference
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            if (NEQ32)
+            if (ROW)
+                v[j] = fl[j] ? (VT)((d[q][j] - fe_row) * AT(NEQ_SCALE)) : VT(0);
+            else if (NEQ32)
                 v[j] = fl[j] ? (VT)(d[q][j] * AT(NEQ_SCALE)) : VT(0);
             else if (NEQ)
                 v[j] = fl[j] ? (VT)((d[q][j] - AT(feq_dev_f32(q, o_rho[j], o_ux[j], o_uy[j]))) * AT(NEQ_SCALE))
@@ -464,10 +485,10 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
     }
 }
 
-template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float>
+template <typename ST, typename AT, bool KOMEGA, bool PHASE0, bool NEQ = false, typename FT = float, bool ROW = false>
 __global__ void __launch_bounds__(128, ((NEQ && sizeof(AT) == 8) || sizeof(FT) == 8) ? 1 : KOFM_LB_MINBLOCKS)
 lb_step_kernel(const LbParams p) {
-    lb_block<ST, AT, KOMEGA, PHASE0, NEQ, FT>(p, blockIdx.x, blockIdx.y, gridDim.x);
+    lb_block<ST, AT, KOMEGA, PHASE0, NEQ, FT, ROW>(p, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // A tile of the multi-lattice collide: `rows` block rows from `by` of block

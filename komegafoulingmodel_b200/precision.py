@@ -27,7 +27,7 @@ from .lattice import Lattice
 
 FORMS = {"fp64": _abi.STORE_FP64, "fp32": _abi.STORE_FP32, "fp16": _abi.STORE_FP16_DEV,
          "bf16": _abi.STORE_BF16_DEV, "fp16neq": _abi.STORE_FP16_NEQ,
-         "fp16neq32": _abi.STORE_FP16_NEQ32}
+         "fp16neq32": _abi.STORE_FP16_NEQ32, "fp16row": _abi.STORE_FP16_ROW}
 
 
 def rel_l2(a, b, mask):

@@ -144,7 +144,8 @@ def test_wall_shear_and_turbulence_reductions(kofm_lib):
     assert tw == pytest.approx(ref, rel=1e-6)
 
 
-@pytest.mark.parametrize("storage,bound", [(_abi.STORE_FP16_NEQ, 1e-3), (_abi.STORE_FP16_NEQ32, 1e-3)])
+@pytest.mark.parametrize("storage,bound", [(_abi.STORE_FP16_NEQ, 1e-3), (_abi.STORE_FP16_NEQ32, 1e-3),
+                                           (_abi.STORE_FP16_ROW, 1e-3)])
 def test_channel_16bit_storage_precision(kofm_lib, oracle, storage, bound):
     """The metric's precision gate for 16-bit population storage: u within
     rel-L2 1e-3 of the FP64 oracle after 1000 steps of the k-omega channel.

@@ -157,7 +157,8 @@ def test_poiseuille_c1_10000_steps_analytic(kofm_lib):
     assert np.linalg.norm(prof - ua) / np.linalg.norm(ua) < 2e-3
 
 
-@pytest.mark.parametrize("storage", [_abi.STORE_FP16_DEV, _abi.STORE_BF16_DEV, _abi.STORE_FP16_NEQ])
+@pytest.mark.parametrize("storage", [_abi.STORE_FP16_DEV, _abi.STORE_BF16_DEV, _abi.STORE_FP16_NEQ,
+                                     _abi.STORE_FP16_ROW])
 def test_half_storage_forms_run_and_conserve_mass(kofm_lib, oracle, storage):
     nx, ny = 256, 64
     ch = G.straight_channel(nx, ny)
@@ -172,8 +173,10 @@ def test_half_storage_forms_run_and_conserve_mass(kofm_lib, oracle, storage):
         rho, ux, uy = L.get_macro()
     fl = ch.fluid_mask().ravel()
     # 16-bit deviations round to 2^-11 (FP16) / 2^-8 (BF16) of their size
-    # every step; the non-equilibrium form rounds only f - feq
-    bound = {_abi.STORE_FP16_DEV: 2e-2, _abi.STORE_BF16_DEV: 5e-2, _abi.STORE_FP16_NEQ: 1e-3}[storage]
+    # every step; the non-equilibrium forms round only f - feq (of the node's
+    # own moments, or of its row's at the upload)
+    bound = {_abi.STORE_FP16_DEV: 2e-2, _abi.STORE_BF16_DEV: 5e-2, _abi.STORE_FP16_NEQ: 1e-3,
+             _abi.STORE_FP16_ROW: 1e-3}[storage]
     assert rel_l2(ux, sim.ux, fl) < bound
     assert abs(rho[fl].mean() - 1.0) < 1e-2
 
@@ -205,3 +208,39 @@ def test_fp16_neq_round_trip_and_first_step(kofm_lib, oracle):
     err = np.abs(fluid_pops(ch, g1) - fluid_pops(ch, sim.FA))
     # input rounding carried through one collision plus the new rounding
     assert err.max() < 2.0 ** -9 * np.abs(e).max(), (err.max(), np.abs(e).max())
+
+
+def test_fp16_row_round_trip_and_first_step(kofm_lib, oracle):
+    """The row-reference form stores f - feq(rho_R, u_R) with one reference
+    per row, the mean density and velocity of the row's fluid nodes at the
+    upload: a state upload and download reproduces f to FP16 precision of
+    that difference, and one step matches the oracle at that level."""
+    nx, ny = 128, 20
+    ch = G.straight_channel(nx, ny)
+    (f,) = fp32_state(perturbed_state(ch, seed=5, u_mean=0.02))
+    with lattice(nx, ny, 1.25, 1e-5, 0.1, storage=_abi.STORE_FP16_ROW) as L:
+        L.set_geometry(ch.ntype)
+        L.set_state(f)
+        g, *_ = L.get_state()
+        L.lb_step()
+        g1, *_ = L.get_state()
+    a, b = fluid_pops(ch, g), fluid_pops(ch, f)
+    fr = f.reshape(9, ny, ch.nx_full)
+    fl = ch.fluid_mask()
+    rho = fr.sum(0)
+    jx = (G.CX[:, None, None] * fr).sum(0)
+    jy = (G.CY[:, None, None] * fr).sum(0)
+    cnt = np.maximum(fl.sum(1), 1)
+    srho = np.where(fl, rho, 0).sum(1)
+    rr = np.where(srho > 0, srho / cnt, 1.0)
+    ru = np.where(srho > 0, np.where(fl, jx, 0).sum(1) / np.where(srho > 0, srho, 1), 0.0)
+    rv = np.where(srho > 0, np.where(fl, jy, 0).sum(1) / np.where(srho > 0, srho, 1), 0.0)
+    R = lambda a: np.repeat(a[:, None], ch.nx_full, 1).ravel()  # noqa: E731
+    e = fluid_pops(ch, f.reshape(9, -1) - G.feq(R(rr), R(ru), R(rv)))
+    # e rounded to FP16 (half an ulp: 2^-11 of |e|), plus the FP32 equilibrium
+    assert np.all(np.abs(a - b) <= 2.0 ** -11 * np.abs(e) + 2e-8)
+    cfg = make_cfg(nx, ny, 1.25, 1e-5, 0.1)
+    sim = OracleSim(oracle, cfg, ch.ntype, ch.dX, ch.wallD, f)
+    sim.step(1)
+    err = np.abs(fluid_pops(ch, g1) - fluid_pops(ch, sim.FA))
+    assert err.max() < 2.0 ** -9 * np.abs(e).max() + 1e-7, (err.max(), np.abs(e).max())

@@ -86,7 +86,7 @@ def _lattice(ch, rate, g, mu, komega, storage=_abi.STORE_FP32, **desc):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage,tol", [(_abi.STORE_FP32, 1e-5), (_abi.STORE_FP16_NEQ, 1e-4),
-                                         (_abi.STORE_FP16_NEQ32, 1e-4)])
+                                         (_abi.STORE_FP16_NEQ32, 1e-4), (_abi.STORE_FP16_ROW, 1e-4)])
 def test_wavy_laminar_matches_oracle(kofm_lib, oracle, storage, tol):
     """Interpolated bounce-back with q from 0.03 to 0.97; the FP16 f - feq
     form decodes every gathered, bounced and interpolated population with the
