@@ -85,7 +85,8 @@ extern "C" {
                                  at kofm_set_state, re-centred on the row means
                                  of the moments every 32 collides that save
                                  them (the stored values re-encoded).  FP32
-                                 collide arithmetic.  Suited to flows close to
+                                 collide arithmetic, u from FP64 sums of the
+                                 deviations.  Suited to flows close to
                                  their row profile (straight channels); not in
                                  kofm_batch.  No counterpart in the reference. */
 

@@ -319,6 +319,21 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
         const AT rho = AT(1) + drho;
         const AT jx = d[1][j] - d[2][j] + d[5][j] - d[6][j] + d[7][j] - d[8][j];
         const AT jy = d[3][j] - d[4][j] + d[5][j] - d[6][j] - d[7][j] + d[8][j];
+        // ROW with FP32 arithmetic: u from FP64 sums of the deviations (an FP32
+        // quotient of FP32 sums rounds u the same way at every node of a row
+        // of equal values, step after step)
+        double m64x = 0.0, m64y = 0.0;
+        if (ROW && sizeof(AT) == 4) {
+            double dr = 0.0;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) dr += (double)d[q][j];
+            const double ax = (double)d[1][j] - (double)d[2][j] + (double)d[5][j] - (double)d[6][j] +
+                              (double)d[7][j] - (double)d[8][j];
+            const double ay = (double)d[3][j] - (double)d[4][j] + (double)d[5][j] - (double)d[6][j] -
+                              (double)d[7][j] + (double)d[8][j];
+            m64x = ax / (1.0 + dr);
+            m64y = ay / (1.0 + dr);
+        }
         AT w = tau0;
         AT inv;  // 1 / rho
         if (KOMEGA) {
@@ -351,7 +366,8 @@ __device__ __forceinline__ void lb_block(const LbParams& p, int bx, int by, int 
         } else {
             inv = AT(1) / rho;
         }
-        const AT ux = inv * jx, uy = inv * jy;
+        const AT ux = (ROW && sizeof(AT) == 4) ? AT(m64x) : inv * jx;
+        const AT uy = (ROW && sizeof(AT) == 4) ? AT(m64y) : inv * jy;
         AT sxx_n = AT(0), sxy_n = AT(0), syy_n = AT(0);
         // NEQ32: the mass and momentum that the FP32 moments leave out -- rho
         // = 1 + drho rounded on the FP32 grid near 1 (up to 6e-8), u = j / rho
